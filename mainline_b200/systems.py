@@ -1,0 +1,218 @@
+"""Seeded synthetic QWalk input decks for the walker-engine workloads.
+
+Every deck is a plain QWalk input file (SYSTEM / PSEUDO / TRIALFUNC / METHOD
+sections, same grammar as the reference's ``qmc_io.cpp`` parser) plus the
+``.orb`` file its ORBITALS section names.  The same files drive the reference
+CPU build and this engine, so both sides read byte-identical inputs.
+
+Workloads (sizes are fixed; only the seed varies):
+
+* ``n2_allelectron``  two Z=7 atoms at z=+-1.0375 bohr, 14 electrons (7 up,
+  7 down); 40 contracted Cartesian Gaussians per atom (10 S + 6 P + 2 6D
+  shells, 3 primitives each, exponents log-uniform in [0.1, 1e4]); a random
+  orthonormal 80x7 MO block per spin; Jastrow = CUTOFF_CUSP e-e (GAMMA 24,
+  like 0.25 / unlike 0.5 cusp) + POLYPADE e-n (BETA0 1.2, 4 functions,
+  coefficients ~N(0, 0.1)).
+* ``n2_pseudo``  the same molecule and electrons with each nucleus replaced by
+  a Z_eff=5 semilocal RGAUSSIAN pseudopotential: l=0 and l=1 nonlocal
+  channels plus a local channel, 3 Gaussians each (exponents U[1,10],
+  coefficients U(-5,5)), 12-point quadrature (AIP 12).
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+SHELL_NFUNC = {"S": 1, "P": 3, "5D": 5, "6D": 6, "7F": 7, "10F": 10}
+
+
+@dataclass
+class Deck:
+    """Paths and sizes of one generated system."""
+    path: str               # QWalk input file
+    orb_path: str
+    nup: int
+    ndown: int
+    natoms: int
+    nbasis: int             # basis functions (all centers)
+    kind: str
+    seed: int
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def nelec(self) -> int:
+        return self.nup + self.ndown
+
+
+def _fmt(x: float) -> str:
+    return repr(float(x))
+
+
+def _basis_shells(rng, nshell: dict, nprim=3, lo=0.1, hi=1e4):
+    shells = []
+    for sym in ("S", "P", "6D"):
+        for _ in range(nshell.get(sym, 0)):
+            ex = np.exp(rng.uniform(np.log(lo), np.log(hi), size=nprim))
+            co = rng.uniform(0.1, 1.0, size=nprim)
+            shells.append((sym, ex, co))
+    return shells
+
+
+def _basis_text(label: str, shells, cutoff=None) -> str:
+    lines = [f"BASIS {{ {label}", "AOSPLINE"]
+    if cutoff is not None:
+        lines.append(f"CUTOFF {_fmt(cutoff)}")
+    lines.append("GAMESS {")
+    for sym, ex, co in shells:
+        lines.append(f"{sym} {len(ex)}")
+        for i, (e, c) in enumerate(zip(ex, co)):
+            lines.append(f"  {i + 1} {_fmt(e)} {_fmt(c)}")
+    lines.append("}")
+    lines.append("}")
+    return "\n".join(lines)
+
+
+def _random_orthonormal(rng, nb: int, nmo: int) -> np.ndarray:
+    q, r = np.linalg.qr(rng.standard_normal((nb, nmo)))
+    return q * np.sign(np.diag(r))[None, :]
+
+
+def _write_orb(path: str, coeff: np.ndarray, nfunc_per_center: list[int]) -> None:
+    """ORB file: ``mo basis center label`` lines (1-based), COEFFICIENTS, then
+    the coefficient list (format read by readorb_noexpand, MO_matrix.h:264-332).
+    ``coeff`` is [totbasis, nmo] with basis functions ordered center by center."""
+    nb, nmo = coeff.shape
+    lines = []
+    vals = []
+    label = 0
+    for mo in range(nmo):
+        row = 0
+        for c, nf in enumerate(nfunc_per_center):
+            for f in range(nf):
+                label += 1
+                lines.append(f"{mo + 1} {f + 1} {c + 1} {label}")
+                vals.append(coeff[row, mo])
+                row += 1
+    with open(path, "w") as fh:
+        fh.write("\n".join(lines))
+        fh.write("\nCOEFFICIENTS\n")
+        for i in range(0, len(vals), 4):
+            fh.write(" ".join(repr(float(v)) for v in vals[i:i + 4]) + "\n")
+
+
+def _jastrow_text(label: str, onebody: np.ndarray, threebody=None, twobody_pp=None) -> str:
+    g2 = [
+        "GROUP {",
+        f"  EIBASIS {{ {label} POLYPADE BETA0 1.2 NFUNC 4 RCUT 7.5 }}",
+        "  ONEBODY {",
+        f"    COEFFICIENTS {{ {label} " + " ".join(_fmt(c) for c in onebody) + " }",
+        "  }",
+    ]
+    if threebody is not None:
+        g2.insert(1, "  EEBASIS { EE POLYPADE BETA0 0.5 NFUNC 3 RCUT 7.5 }")
+        g2 += ["  THREEBODY {",
+               f"    COEFFICIENTS {{ {label} " + " ".join(_fmt(c) for c in threebody) + " }",
+               "  }"]
+        if twobody_pp is not None:
+            g2 += ["  TWOBODY {",
+                   "    COEFFICIENTS { " + " ".join(_fmt(c) for c in twobody_pp) + " }",
+                   "  }"]
+    g2.append("}")
+    return "\n".join([
+        "JASTROW2",
+        "GROUP {",
+        "  EEBASIS { EE CUTOFF_CUSP GAMMA 24.0 CUSP 1.0 CUTOFF 7.5 }",
+        "  EEBASIS { EE CUTOFF_CUSP GAMMA 24.0 CUSP 1.0 CUTOFF 7.5 }",
+        "  TWOBODY_SPIN { FREEZE",
+        "    LIKE_COEFFICIENTS { 0.25 0.0 }",
+        "    UNLIKE_COEFFICIENTS { 0.0 0.5 }",
+        "  }",
+        "}",
+    ] + g2)
+
+
+def _pseudo_text(rng, label: str, aip: int = 12) -> str:
+    """RGAUSSIAN OLDQMC block: channels l=0, l=1 and the local channel (the
+    reference treats the LAST listed channel as local, Pseudopotential.cpp:790)."""
+    lines = [f"PSEUDO {{ {label}", f"  AIP {aip}", f"  BASIS {{ {label}", "  RGAUSSIAN", "  OLDQMC {",
+             "  0.0 3", "  3 3 3"]
+    for _l in range(3):
+        for _ in range(3):
+            lines.append(f"    2 {_fmt(rng.uniform(1.0, 10.0))} {_fmt(rng.uniform(-5.0, 5.0))}")
+    lines += ["  }", "  }", "}"]
+    return "\n".join(lines)
+
+
+def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | None = None,
+             name: str | None = None) -> Deck:
+    """Two-atom molecule of the all-electron (``pseudo=False``) or Z_eff=5
+    pseudopotential (``pseudo=True``) workload.  ``method`` is an optional
+    METHOD section body written into the deck (e.g. ``"VMC NBLOCK 50 ..."``)."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    label = "N"
+    charge = 5 if pseudo else 7
+    nup = ndown = 7
+    shells = _basis_shells(rng, {"S": 10, "P": 6, "6D": 2})
+    nper = sum(SHELL_NFUNC[s] for s, _, _ in shells)
+    nb = 2 * nper
+    cup = _random_orthonormal(rng, nb, nup)
+    cdn = _random_orthonormal(rng, nb, ndown)
+    onebody = rng.normal(0.0, 0.1, size=4)
+    pp = _pseudo_text(rng, label) if pseudo else ""
+    name = name or ("n2_pseudo" if pseudo else "n2_allelectron")
+    orb = os.path.join(outdir, f"{name}.orb")
+    _write_orb(orb, np.concatenate([cup, cdn], axis=1), [nper, nper])
+    states_up = " ".join(str(i + 1) for i in range(nup))
+    states_dn = " ".join(str(nup + i + 1) for i in range(ndown))
+    deck = "\n".join([
+        f"# seeded synthetic workload {name} (seed {seed})",
+        f"RANDOMSEED {{ {1 + seed % 100000} {7 + seed % 7919} }}",
+        "SYSTEM { MOLECULE",
+        f"  NSPIN {{ {nup} {ndown} }}",
+        f"  ATOM {{ {label} {charge} COOR 0.0 0.0 -1.0375 }}",
+        f"  ATOM {{ {label} {charge} COOR 0.0 0.0 1.0375 }}",
+        "}",
+        pp,
+        "TRIALFUNC { SLATER-JASTROW",
+        "  WF1 { SLATER",
+        "    ORBITALS { BLAS_MO",
+        f"      NMO {nup + ndown}",
+        f"      ORBFILE {os.path.basename(orb)}",
+        _basis_text(label, shells),
+        "      CENTERS { USEATOMS }",
+        "    }",
+        "    DETWT { 1.0 }",
+        f"    STATES {{ {states_up} {states_dn} }}",
+        "  }",
+        "  WF2 {",
+        _jastrow_text(label, onebody),
+        "  }",
+        "}",
+        f"METHOD {{ {method} }}" if method else "",
+    ]) + "\n"
+    path = os.path.join(outdir, f"{name}.qw")
+    with open(path, "w") as fh:
+        fh.write(deck)
+    return Deck(path=path, orb_path=orb, nup=nup, ndown=ndown, natoms=2, nbasis=nb,
+                kind=name, seed=seed)
+
+
+def random_configs(deck: Deck, nconf: int, seed: int, spread: float = 1.2) -> np.ndarray:
+    """Seeded electron configurations [nconf, nelec, 3]: each electron sits
+    near a random atom with a Gaussian spread (bohr)."""
+    rng = np.random.default_rng(seed)
+    atoms = np.array([[0.0, 0.0, -1.0375], [0.0, 0.0, 1.0375]])
+    which = rng.integers(0, len(atoms), size=(nconf, deck.nelec))
+    return atoms[which] + rng.normal(0.0, spread, size=(nconf, deck.nelec, 3))
+
+
+def random_rotation(rng) -> np.ndarray:
+    """Uniform random rotation (rows are the rotated x, y, z axes)."""
+    q, r = np.linalg.qr(rng.standard_normal((3, 3)))
+    q = q * np.sign(np.diag(r))[None, :]
+    if np.linalg.det(q) < 0:
+        q[:, 0] *= -1
+    return q.T.copy()

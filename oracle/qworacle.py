@@ -1,0 +1,735 @@
+"""CPU restatement (numpy) of QWalk's per-configuration Slater-Jastrow
+evaluation for molecular systems.
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline leg import this module, and only as the checker.
+The product path (mainline_b200 + its CUDA library) never imports it.
+
+Parity is pinned: tests/test_oracle_golden.py checks every quantity below
+against golden vectors written by the reference itself (oracle/_ref harness,
+tests/golden/make_golden.py).
+
+Reference files cited as path:line inside QWalk/mainline ``src/``.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+# ----------------------------------------------------------------------------
+# input grammar (program_utils/qmc_io.cpp:280-345 parsefile, :168-230 readsection)
+
+
+def tokenize(path: str) -> list[str]:
+    words: list[str] = []
+    base = os.path.dirname(os.path.abspath(path))
+    with open(path) as fh:
+        for line in fh:
+            line = line.split("#", 1)[0]
+            for tok in line.split():
+                # '{' and '}' become words of their own
+                buf = ""
+                for ch in tok:
+                    if ch in "{}":
+                        if buf:
+                            words.append(buf)
+                        words.append(ch)
+                        buf = ""
+                    else:
+                        buf += ch
+                if buf:
+                    words.append(buf)
+    out: list[str] = []
+    i = 0
+    while i < len(words):
+        if words[i].upper() == "INCLUDE":
+            inc = words[i + 1]
+            if not os.path.isabs(inc):
+                inc = os.path.join(base, inc)
+            out.extend(tokenize(inc))
+            i += 2
+        else:
+            out.append(words[i])
+            i += 1
+    return out
+
+
+def sections(words: list[str], name: str) -> list[list[str]]:
+    """All level-0 sections ``name { ... }`` (contents without the braces)."""
+    res, level, i = [], 0, 0
+    while i < len(words):
+        w = words[i]
+        if w == "{":
+            level += 1
+        elif w == "}":
+            level -= 1
+        elif level == 0 and w.upper() == name.upper() and i + 1 < len(words) and words[i + 1] == "{":
+            depth, j = 0, i + 2
+            while j < len(words):
+                if words[j] == "{":
+                    depth += 1
+                elif words[j] == "}":
+                    if depth == 0:
+                        break
+                    depth -= 1
+                j += 1
+            res.append(words[i + 2:j])
+            i = j
+        i += 1
+    return res
+
+
+def section(words, name):
+    s = sections(words, name)
+    return s[0] if s else None
+
+
+def value(words, name, default=None, conv=float):
+    level = 0
+    for i, w in enumerate(words):
+        if w == "{":
+            level += 1
+        elif w == "}":
+            level -= 1
+        elif level == 0 and w.upper() == name.upper():
+            return conv(words[i + 1])
+    return default
+
+
+def haskey(words, name):
+    level = 0
+    for w in words:
+        if w == "{":
+            level += 1
+        elif w == "}":
+            level -= 1
+        elif level == 0 and w.upper() == name.upper():
+            return True
+    return False
+
+
+# ----------------------------------------------------------------------------
+# cubic spline radial functions (basis_function/Cubic_spline_build.cpp:396-660,
+# Spline_fitter.cpp:153-293)
+
+LVAL = {"S": 0, "P": 1, "5D": 2, "6D": 2, "D": 2, "7F": 3, "10F": 3, "F": 3}
+NFUNC = {"S": 1, "P": 3, "5D": 5, "6D": 6, "D": 6, "10F": 10, "F": 10}
+
+
+def spline_fit(x, y, yp1, ypn):
+    """Natural/clamped cubic spline (Spline_fitter.cpp:208-293)."""
+    n = len(x)
+    y2 = np.zeros(n)
+    u = np.zeros(n)
+    if yp1 > 0.99e30:
+        y2[0] = 0.0
+        u[0] = 0.0
+    else:
+        y2[0] = -0.5
+        u[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1)
+    for i in range(1, n - 1):
+        sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1])
+        p = sig * y2[i - 1] + 2.0
+        y2[i] = (sig - 1.0) / p
+        u[i] = (6.0 * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]))
+                / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p
+    if ypn > 0.99e30:
+        qn = un = 0.0
+    else:
+        qn = 0.5
+        un = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]))
+    y2[n - 1] = (un - qn * u[n - 2]) / (qn * y2[n - 2] + 1.0)
+    for k in range(n - 2, -1, -1):
+        y2[k] = y2[k] * y2[k + 1] + u[k]
+    c = np.zeros((n, 4))
+    h = x[1:] - x[:-1]
+    c[:-1, 0] = y[:-1]
+    c[:-1, 1] = (y[1:] - y[:-1]) / h - h * (2.0 * y2[:-1] + y2[1:]) / 6.0
+    c[:-1, 2] = y2[:-1] / 2.0
+    c[:-1, 3] = (y2[1:] - y2[:-1]) / (6.0 * h)
+    c[-1, 0] = y[-1]
+    return c
+
+
+def spline_findcutoff(c, spacing, threshold):
+    """Spline_fitter::findCutoff (Spline_fitter.cpp:153-184)."""
+    mx = min(float(np.max(np.abs(c[:, 0]))), 1.0)
+    thr = 1e-10 * mx
+    x = threshold - 0.5
+    inv = 1.0 / spacing
+    while x >= 0:
+        i = int(x * inv)
+        h = x - i * spacing
+        t = c[i, 0] + h * (c[i, 1] + h * (c[i, 2] + h * c[i, 3]))
+        if abs(t) > thr:
+            return x + 0.5
+        x -= 0.5
+    return 0.0
+
+
+class SplineBasis:
+    """One AOSPLINE basis object (Cubic_spline)."""
+
+    def __init__(self, words):
+        self.label = words[0]
+        assert words[1].upper() == "AOSPLINE", words[1]
+        spacing, n = 0.02, 2500
+        self.norm_type = value(words, "NORMTYPE", "GAMESSNORM", str)
+        self.renorm = not haskey(words, "NORENORMALIZE")
+        req_cut = value(words, "CUTOFF", -1.0)
+        sp = value(words, "SPACING", None)
+        if sp is not None:
+            spacing, n = sp, int(50.0 / sp)
+        g = section(words, "GAMESS")
+        shells = []
+        p = 0
+        while p < len(g):
+            sym = g[p].upper()
+            ng = int(g[p + 1])
+            ex, co = [], []
+            for i in range(ng):
+                ex.append(float(g[p + 3 + 3 * i]))
+                co.append(float(g[p + 4 + 3 * i]))
+            p += 2 + 3 * ng
+            shells.append((sym, ex, co))
+        x = np.arange(n) * spacing
+        self.spacing = spacing
+        self.syms = []
+        coeffs = []
+        for sym, ex, co in shells:
+            y = np.zeros(n)
+            for e, cc in zip(ex, co):
+                fac = math.sqrt(2.0 * e / math.pi)
+                feg = 4.0 * e
+                feg2 = feg * feg
+                L = LVAL[sym]
+                norm = [math.sqrt(2.0 * feg * fac), math.sqrt(2.0 * feg2 * fac / 3.0),
+                        math.sqrt(2.0 * feg * feg2 * fac / 15.0),
+                        math.sqrt(2.0 * feg2 * feg2 * fac / 105.0)][L]
+                y += norm * cc * np.exp(-e * x * x)
+            if self.renorm:
+                pw = LVAL[sym] + 1
+                s = float(np.sum(spacing * x ** (2 * pw) * y * y))
+                if abs(s - 1.0) > 1e-5:
+                    y = y / math.sqrt(s)
+            if req_cut > 0:
+                cutmax = req_cut - 1e-6
+                cutmin = cutmax - 1.2
+                zz = (x - cutmin) / 1.2
+                y = np.where(x > cutmax, 0.0, np.where(x > cutmin, y * (1 - zz ** 3 * (6 * zz * zz - 15 * zz + 10)), y))
+            yp1 = (y[1] - y[0]) / spacing
+            ypn = (y[n - 1] - y[n - 2]) / spacing
+            coeffs.append(spline_fit(x, y, yp1, ypn))
+            self.syms.append(sym)
+        thr0 = x[n - 1]
+        cuts = [spline_findcutoff(c, spacing, thr0) for c in coeffs]
+        self.threshold = max(cuts)
+        # pad each table out to the common threshold (Spline_fitter::pad)
+        self.coeffs = []
+        for c in coeffs:
+            if thr0 < self.threshold:
+                extra = int((self.threshold - thr0) / spacing) + 1
+                c = np.vstack([c, np.zeros((extra, 4))])
+            self.coeffs.append(c)
+        self.nfunc = sum(NFUNC[s] for s in self.syms)
+
+    def eval_lap(self, d):
+        """Values [..., nfunc, 5] = (f, df/dx, df/dy, df/dz, lap) at
+        displacement d [..., 3] from the center (Cubic_spline_calc.cpp:353-)."""
+        d = np.asarray(d, dtype=float)
+        r2 = np.sum(d * d, axis=-1)
+        r = np.sqrt(r2)
+        inside = r < self.threshold
+        rr = np.where(inside, r, 0.0)
+        out = np.zeros(d.shape[:-1] + (self.nfunc, 5))
+        x, y, z = d[..., 0], d[..., 1], d[..., 2]
+        inv = 1.0 / self.spacing
+        k = 0
+        with np.errstate(divide="ignore", invalid="ignore"):
+            for sym, c in zip(self.syms, self.coeffs):
+                i = (rr * inv).astype(np.int64)
+                h = rr - i * self.spacing
+                c0, c1, c2, c3 = c[i, 0], c[i, 1], c[i, 2], c[i, 3]
+                f = c0 + h * (c1 + h * (c2 + h * c3))
+                fd = (c1 + h * (2 * c2 + h * (3 * c3))) / rr
+                f2 = 2 * c2 + 6 * h * c3
+                for (ang, ax, ay, az, lapA, L) in _angular(sym, x, y, z):
+                    val = ang * f
+                    h1 = ang * fd
+                    out[..., k, 0] = val
+                    out[..., k, 1] = h1 * x + ax * f
+                    out[..., k, 2] = h1 * y + ay * f
+                    out[..., k, 3] = h1 * z + az * f
+                    out[..., k, 4] = ang * f2 + (2 * L + 2) * h1 + lapA * f
+                    k += 1
+        out[~inside] = 0.0
+        return out
+
+
+def _angular(sym, x, y, z):
+    """Cartesian angular factors A, dA/dx, dA/dy, dA/dz, lap A, l (the
+    GAMESS orderings of Cubic_spline_build.cpp:660-760)."""
+    o, zr = np.ones_like(x), np.zeros_like(x)
+    if sym == "S":
+        return [(o, zr, zr, zr, zr, 0)]
+    if sym == "P":
+        return [(x, o, zr, zr, zr, 1), (y, zr, o, zr, zr, 1), (z, zr, zr, o, zr, 1)]
+    if sym in ("6D", "D"):
+        return [(x * x, 2 * x, zr, zr, 2 * o, 2), (y * y, zr, 2 * y, zr, 2 * o, 2),
+                (z * z, zr, zr, 2 * z, 2 * o, 2), (x * y, y, x, zr, zr, 2),
+                (x * z, z, zr, x, zr, 2), (y * z, zr, z, y, zr, 2)]
+    if sym == "5D":
+        return [(2 * z * z - x * x - y * y, -2 * x, -2 * y, 4 * z, zr, 2), (x * z, z, zr, x, zr, 2),
+                (y * z, zr, z, y, zr, 2), (x * x - y * y, 2 * x, -2 * y, zr, zr, 2), (x * y, y, x, zr, zr, 2)]
+    raise NotImplementedError(sym)
+
+
+# ----------------------------------------------------------------------------
+# Jastrow radial functions
+
+
+def cutoff_cusp(r, cusp, gamma, rcut):
+    """Cutoff_cusp::calcLap (Cutoff_cusp.cpp:122-154): returns (f, f'/r, lap)."""
+    inside = r < rcut
+    with np.errstate(divide="ignore", invalid="ignore"):
+        zz = r / rcut
+        zz2 = zz * zz
+        pp = zz - zz2 + zz * zz2 / 3
+        pade = 1.0 / (1 + gamma * pp)
+        pade0 = 1.0 / (3.0 + gamma)
+        f = cusp * rcut * (pp * pade - pade0)
+        pade2 = pade * pade
+        ppd = 1.0 - 2.0 * zz + zz2
+        ppdd = -2.0 + 2.0 * zz
+        dadr = ppd * pade2 / r
+        lap = ppdd * pade2 / rcut - 2.0 * gamma * ppd * ppd * pade2 * pade / rcut + 2.0 * dadr
+    return (np.where(inside, f, 0.0), np.where(inside, cusp * dadr, 0.0), np.where(inside, cusp * lap, 0.0))
+
+
+def poly_pade(r, beta, rcut):
+    """Poly_pade_function::calcLap (Poly_pade_function.cpp:183-237) for one
+    beta: returns (f, f'/r, lap)."""
+    inside = r < rcut
+    with np.errstate(divide="ignore", invalid="ignore"):
+        zz = r / rcut
+        zz2 = zz * zz
+        zpp = zz2 * (6.0 - 8.0 * zz + 3.0 * zz2)
+        zpp1 = 1 - zpp
+        zppd = 12.0 * zz * (1.0 - 2.0 * zz + zz2)
+        zppdd2 = 6.0 - 24.0 * zz + 18 * zz2
+        zpade = 1.0 / (1 + beta * zpp)
+        zpade2 = zpade * zpade
+        crs = zpp1 * zpade
+        crsd = -zppd * zpade2 * (beta + 1) / (r * rcut)
+        crsdd2 = -zpade2 * (zppdd2 - beta * zppd * zppd * zpade) * (beta + 1) / (rcut * rcut)
+        lap = 2 * (crsdd2 + crsd)
+    return (np.where(inside, crs, 0.0), np.where(inside, crsd, 0.0), np.where(inside, lap, 0.0))
+
+
+class RadialSet:
+    """A Jastrow EIBASIS/EEBASIS object: list of scalar radial functions."""
+
+    def __init__(self, words):
+        self.label = words[0]
+        t = words[1].upper()
+        self.kind = t
+        if t == "CUTOFF_CUSP":
+            self.cusp = value(words, "CUSP")
+            self.gamma = value(words, "GAMMA")
+            self.rcut = value(words, "CUTOFF")
+            self.n = 1
+        elif t == "POLYPADE":
+            self.rcut = value(words, "RCUT")
+            b0 = value(words, "BETA0")
+            self.n = int(value(words, "NFUNC", conv=int))
+            b1 = math.log(b0 + 1.00001)
+            self.beta = [b0] + [math.exp(b1 + 1.6 * i) - 1 for i in range(1, self.n)]
+        else:
+            raise NotImplementedError(t)
+
+    def eval(self, r):
+        """[..., n, 3] = (f, f'/r, lap)."""
+        if self.kind == "CUTOFF_CUSP":
+            return np.stack(cutoff_cusp(r, self.cusp, self.gamma, self.rcut), axis=-1)[..., None, :]
+        return np.stack([np.stack(poly_pade(r, b, self.rcut), axis=-1) for b in self.beta], axis=-2)
+
+
+# ----------------------------------------------------------------------------
+# the system
+
+
+class System:
+    """Molecule + Slater-Jastrow wave function + pseudopotential, built from a
+    QWalk deck with the reference's rules."""
+
+    def __init__(self, deck_path: str):
+        self.deck_path = deck_path
+        words = tokenize(deck_path)
+        sysw = section(words, "SYSTEM")
+        assert sysw[0].upper() in ("MOLECULE", "MOLECULAR"), sysw[0]
+        ns = section(sysw, "NSPIN")
+        self.nup, self.ndn = int(ns[0]), int(ns[1])
+        self.nelec = self.nup + self.ndn
+        self.labels, self.charges, pos = [], [], []
+        for a in sections(sysw, "ATOM"):
+            self.labels.append(a[0])
+            self.charges.append(float(a[1]))
+            i = [k for k, w in enumerate(a) if w.upper() == "COOR"][0]
+            pos.append([float(a[i + 1]), float(a[i + 2]), float(a[i + 3])])
+        self.atoms = np.array(pos)
+        self.charges = np.array(self.charges)
+        tf = section(words, "TRIALFUNC")
+        wf1 = section(tf, "WF1")
+        wf2 = section(tf, "WF2")
+        self._read_slater(wf1, os.path.dirname(os.path.abspath(deck_path)))
+        self._read_jastrow(wf2)
+        self._read_pseudo(sections(words, "PSEUDO"))
+
+    # Slater determinant (wavefunction/Slat_wf_data.cpp:34-303, MO_matrix.h:383-462,
+    # MO_matrix_blas.h:101-190)
+    def _read_slater(self, w, base):
+        orbw = section(w, "ORBITALS")
+        self.mo_kind = orbw[0].upper()
+        self.nmo = int(value(orbw, "NMO", conv=int))
+        self.basis = [SplineBasis(b) for b in sections(orbw, "BASIS")]
+        # centers = atoms (USEATOMS / USEGLOBAL for molecules)
+        self.center_basis = []
+        for lab in self.labels:
+            self.center_basis.append([b for b in self.basis if b.label == lab])
+        self.nfunc_center = [sum(b.nfunc for b in bl) for bl in self.center_basis]
+        self.totbasis = sum(self.nfunc_center)
+        orbfile = value(orbw, "ORBFILE", conv=str)
+        if not os.path.isabs(orbfile) and not os.path.exists(orbfile):
+            orbfile = os.path.join(base, orbfile)
+        self.moc = self._read_orb(orbfile)
+        states = [int(s) - 1 for s in section(w, "STATES")]
+        self.occ = [states[:self.nup], states[self.nup:]]
+
+    def _read_orb(self, path):
+        toks = open(path).read().split()
+        k = toks.index("COEFFICIENTS")
+        ent = np.array(toks[:k], dtype=np.int64).reshape(-1, 4) - 1
+        coef = np.array(toks[k + 1:], dtype=float)
+        maxbasis = max(self.nfunc_center)
+        cm = -np.ones((self.nmo, len(self.labels), maxbasis), dtype=np.int64)
+        for mo, b, c, lab in ent:
+            if mo <= self.nmo:
+                if mo < self.nmo:
+                    cm[mo, c, b] = lab
+        moc = np.zeros((self.totbasis, self.nmo))
+        row = 0
+        for c, nf in enumerate(self.nfunc_center):
+            for f in range(nf):
+                for mo in range(self.nmo):
+                    moc[row, mo] = coef[cm[mo, c, f]] if cm[mo, c, f] >= 0 else 0.0
+                row += 1
+        return moc
+
+    def _read_jastrow(self, w):
+        assert w[0].upper() == "JASTROW2", w[0]
+        self.groups = []
+        for g in sections(w, "GROUP"):
+            grp = {"ee": [RadialSet(b) for b in sections(g, "EEBASIS")],
+                   "ei": [RadialSet(b) for b in sections(g, "EIBASIS")]}
+            ob = section(g, "ONEBODY")
+            if ob is not None:
+                grp["onebody"] = {c[0]: [float(x) for x in c[1:]] for c in sections(ob, "COEFFICIENTS")}
+            tb = section(g, "TWOBODY_SPIN")
+            if tb is not None:
+                grp["twobody_spin"] = ([float(x) for x in section(tb, "LIKE_COEFFICIENTS")],
+                                       [float(x) for x in section(tb, "UNLIKE_COEFFICIENTS")])
+            tb = section(g, "TWOBODY")
+            if tb is not None:
+                grp["twobody"] = [float(x) for x in section(tb, "COEFFICIENTS")]
+            th = section(g, "THREEBODY")
+            if th is not None:
+                grp["threebody"] = {c[0]: [float(x) for x in c[1:]] for c in sections(th, "COEFFICIENTS")}
+            self.groups.append(grp)
+
+    # Pseudopotential (system/Pseudopotential.cpp:874-1033, Rgaussian_function.cpp)
+    def _read_pseudo(self, pstexts):
+        self.pp = {}
+        for t in pstexts:
+            lab = t[0]
+            aip = int(value(t, "AIP", 6, int))
+            bw = section(t, "BASIS")
+            oq = section(bw, "OLDQMC")
+            it = 0
+            it += 1  # zeff
+            nl = int(oq[it]); it += 1
+            nper = [int(oq[it + l]) for l in range(nl)]
+            it += nl
+            chans = []
+            for l in range(nl):
+                terms = []
+                for _ in range(nper[l]):
+                    terms.append((float(oq[it]) - 2.0, float(oq[it + 1]), float(oq[it + 2])))
+                    it += 3
+                chans.append(terms)
+            self.pp[lab] = {"aip": aip, "chans": chans}
+        for lab, p in self.pp.items():
+            p["quad"], p["w"] = gesqua(p["aip"])
+            p["cutoff"] = self._pp_cutoff(p["chans"])
+
+    @staticmethod
+    def _vl(chans, r):
+        r = np.asarray(r, dtype=float)
+        out = []
+        for terms in chans:
+            v = np.zeros_like(r)
+            for n, a, c in terms:
+                v = v + c * r ** n * np.exp(-np.minimum(a * r * r, 60.0))
+            out.append(v)
+        return out
+
+    def _pp_cutoff(self, chans):
+        """Cutoff scan from 20 bohr down in 0.05 steps (Pseudopotential.cpp:985-1026)."""
+        nl = len(chans)
+        cutL = [20.0] * (nl - 1)
+        found = [False] * (nl - 1)
+        r = 20.0
+        while r > 0:
+            vl = self._vl(chans, r)
+            for l in range(nl - 1):
+                if abs(float(vl[l])) > 1e-5 and not found[l]:
+                    cutL[l] = r - 0.05
+                    found[l] = True
+            r -= 0.05
+        return max(cutL) if cutL else 0.0
+
+    # ------------------------------------------------------------------
+    # evaluation
+
+    def mo_lap(self, P):
+        """MO values for positions P [..., 3]: [..., nmo, 5] (MO_matrix_blas::updateLap,
+        MO_matrix_blas.h:411-491, including its |value| > 1e-8 basis skip)."""
+        P = np.asarray(P, dtype=float)
+        vals = []
+        for c, bl in enumerate(self.center_basis):
+            d = P - self.atoms[c]
+            for b in bl:
+                v = b.eval_lap(d)
+                keep = np.abs(v[..., 0]) > 1e-8
+                vals.append(np.where(keep[..., None], v, 0.0))
+        B = np.concatenate(vals, axis=-2)          # [..., totbasis, 5]
+        return np.einsum("...bk,bm->...mk", B, self.moc)
+
+    def slater(self, R):
+        """log|D|, sign, grad ratios [nc,N,3], lap ratios [nc,N] from the
+        transpose-inverse convention of Slat_wf::calcLap/getDetLap."""
+        nc = R.shape[0]
+        mo = self.mo_lap(R)                           # [nc, N, nmo, 5]
+        logd = np.zeros(nc)
+        sign = np.ones(nc)
+        g = np.zeros((nc, self.nelec, 3))
+        l = np.zeros((nc, self.nelec))
+        inv_all = []
+        for s, (e0, ns) in enumerate([(0, self.nup), (self.nup, self.ndn)]):
+            if ns == 0:
+                inv_all.append(None)
+                continue
+            occ = self.occ[s]
+            M = mo[:, e0:e0 + ns][:, :, occ, :]      # [nc, e, i, 5]
+            A = M[..., 0]
+            sgn, ld = np.linalg.slogdet(A)
+            logd += ld
+            sign *= sgn
+            Ainv = np.linalg.inv(A)                  # Ainv[i, e]
+            # ratio_k(e) = sum_i dphi_i(r_e) Ainv[i, e]
+            r = np.einsum("ceik,cie->cek", M[..., 1:], Ainv)
+            g[:, e0:e0 + ns] = r[..., :3]
+            l[:, e0:e0 + ns] = r[..., 3]
+            inv_all.append(Ainv)
+        return logd, sign, g, l, inv_all, mo
+
+    def jastrow(self, R):
+        """U, per-electron grad U [nc,N,3], lap U [nc,N] (Jastrow2_wf.cpp:988-1221)."""
+        nc, N, _ = R.shape
+        U = np.zeros(nc)
+        G = np.zeros((nc, N, 3))
+        L = np.zeros((nc, N))
+        spin = np.array([0] * self.nup + [1] * self.ndn)
+        for grp in self.groups:
+            # e-n one-body
+            if "onebody" in grp or "threebody" in grp:
+                ei = {}
+                for a, lab in enumerate(self.labels):
+                    d = R - self.atoms[a]                         # [nc,N,3]
+                    r = np.sqrt(np.sum(d * d, axis=-1))
+                    fs = [b.eval(r) for b in grp["ei"] if b.label == lab]
+                    F = np.concatenate(fs, axis=-2) if fs else np.zeros((nc, N, 0, 3))
+                    ei[a] = (F, d)
+            if "onebody" in grp:
+                for a, lab in enumerate(self.labels):
+                    cf = np.array(grp["onebody"][lab])
+                    F, d = ei[a]
+                    k = len(cf)
+                    U += np.einsum("cnk,k->c", F[..., :k, 0], cf)
+                    fd = np.einsum("cnk,k->cn", F[..., :k, 1], cf)
+                    G += fd[..., None] * d
+                    L += np.einsum("cnk,k->cn", F[..., :k, 2], cf)
+            # e-e
+            if "twobody_spin" in grp or "twobody" in grp or "threebody" in grp:
+                eef = []
+                iu, ju = np.triu_indices(N, 1)
+                d = R[:, iu] - R[:, ju]                            # r_i - r_j
+                r = np.sqrt(np.sum(d * d, axis=-1))
+                E = np.concatenate([b.eval(r) for b in grp["ee"]], axis=-2)   # [nc,P,k,3]
+                if "twobody_spin" in grp or "twobody" in grp:
+                    if "twobody_spin" in grp:
+                        like, unlike = grp["twobody_spin"]
+                        same = (spin[iu] == spin[ju])
+                        cf = np.where(same[:, None], np.array(like)[None, :], np.array(unlike)[None, :])
+                    else:
+                        cf = np.broadcast_to(np.array(grp["twobody"])[None, :], (len(iu), len(grp["twobody"])))
+                    k = cf.shape[1]
+                    u = np.einsum("cpk,pk->cp", E[..., :k, 0], cf)
+                    fd = np.einsum("cpk,pk->cp", E[..., :k, 1], cf)
+                    lp = np.einsum("cpk,pk->cp", E[..., :k, 2], cf)
+                    U += u.sum(axis=1)
+                    gi = fd[..., None] * d
+                    np.add.at(G, (slice(None), iu), gi)
+                    np.add.at(G, (slice(None), ju), -gi)
+                    np.add.at(L, (slice(None), iu), lp)
+                    np.add.at(L, (slice(None), ju), lp)
+                if "threebody" in grp:
+                    self._threebody(grp, R, ei, E, d, iu, ju, U, G, L)
+        return U, G, L
+
+    def _threebody(self, grp, R, ei, E, dij, iu, ju, U, G, L):
+        """e-e-n term sum_at sum_{i<j} sum_p c_p (a_k(i)a_l(j)+a_l(i)a_k(j)) b_m(ij)
+        (Jastrow2_three.cpp:138-404, default klm table :30-46)."""
+        klm = [(1, 1, 0), (1, 0, 1), (1, 1, 1), (2, 2, 0), (2, 0, 1), (2, 0, 2), (2, 2, 2), (3, 3, 0),
+               (3, 0, 2), (3, 3, 2), (1, 2, 2), (2, 3, 2)]
+        for a, lab in enumerate(self.labels):
+            cfs = grp["threebody"][lab]
+            F, dia = ei[a]                         # F [nc,N,k,3], dia [nc,N,3]
+            for p, c in enumerate(cfs):
+                k, l, m = klm[p]
+                ak = F[..., k, :]                  # [nc,N,3] (f, f'/r, lap)
+                al = F[..., l, :]
+                b = E[..., m, :]                   # [nc,P,3]
+                # values
+                aki, akj = ak[:, iu, 0], ak[:, ju, 0]
+                ali, alj = al[:, iu, 0], al[:, ju, 0]
+                s = aki * alj + ali * akj          # [nc,P]
+                U += c * np.sum(s * b[..., 0], axis=1)
+                # gradients of a at i and j (vectors)
+                gki = ak[:, iu, 1:2] * dia[:, iu]
+                gkj = ak[:, ju, 1:2] * dia[:, ju]
+                gli = al[:, iu, 1:2] * dia[:, iu]
+                glj = al[:, ju, 1:2] * dia[:, ju]
+                gs_i = gki * alj[..., None] + gli * akj[..., None]     # d s / d r_i
+                gs_j = aki[..., None] * glj + ali[..., None] * gkj     # d s / d r_j
+                gb = b[..., 1:2] * dij                                  # d b / d r_i (= -d b/ d r_j)
+                gi = c * (gs_i * b[..., 0:1] + s[..., None] * gb)
+                gj = c * (gs_j * b[..., 0:1] - s[..., None] * gb)
+                lsi = ak[:, iu, 2] * alj + al[:, iu, 2] * akj
+                lsj = aki * al[:, ju, 2] + ali * ak[:, ju, 2]
+                li = c * (lsi * b[..., 0] + s * b[..., 2] + 2 * np.sum(gs_i * gb, axis=-1))
+                lj = c * (lsj * b[..., 0] + s * b[..., 2] - 2 * np.sum(gs_j * gb, axis=-1))
+                np.add.at(G, (slice(None), iu), gi)
+                np.add.at(G, (slice(None), ju), gj)
+                np.add.at(L, (slice(None), iu), li)
+                np.add.at(L, (slice(None), ju), lj)
+
+    def evaluate(self, R):
+        """Full evaluation of configurations R [nc, N, 3]."""
+        R = np.asarray(R, dtype=float)
+        logd, sign, gD, lD, inv, mo = self.slater(R)
+        U, gU, lU = self.jastrow(R)
+        grad = gD + gU
+        lap = lD + lU + np.sum(gU * gU, axis=-1) + 2 * np.sum(gD * gU, axis=-1)
+        out = {"logpsi": logd + U, "sign": sign, "grad": grad, "lap": lap,
+               "kinetic": -0.5 * lap.sum(axis=1), "potential": self.coulomb(R)}
+        return out
+
+    def logpsi(self, R):
+        logd, sign, *_ = self.slater(R)
+        U, _, _ = self.jastrow(R)
+        return logd + U, sign
+
+    def coulomb(self, R):
+        """Molecular_system::calcLoc (Molecular_system.cpp:209-287), no field."""
+        nc, N, _ = R.shape
+        pot = np.zeros(nc)
+        for a in range(len(self.atoms)):
+            r = np.sqrt(np.sum((R - self.atoms[a]) ** 2, axis=-1))
+            pot -= self.charges[a] * np.sum(1.0 / r, axis=1)
+        for i in range(len(self.atoms)):
+            for j in range(i):
+                pot += self.charges[i] * self.charges[j] / np.linalg.norm(self.atoms[i] - self.atoms[j])
+        iu, ju = np.triu_indices(N, 1)
+        pot += np.sum(1.0 / np.sqrt(np.sum((R[:, iu] - R[:, ju]) ** 2, axis=-1)), axis=1)
+        return pot
+
+    def nonlocal_pp(self, R, rot):
+        """Deterministic semilocal PP (Pseudopotential.cpp:596-815): local
+        channel plus Q-point quadrature of the nonlocal channels for every
+        (electron, atom) pair with |r| < cutoff.  rot [nc,3,3] rows x,y,z."""
+        R = np.asarray(R, dtype=float)
+        nc, N, _ = R.shape
+        tot = np.zeros(nc)
+        lp0, sg0 = self.logpsi(R)
+        for a, lab in enumerate(self.labels):
+            p = self.pp.get(lab)
+            if p is None:
+                continue
+            d = R - self.atoms[a]
+            r = np.sqrt(np.sum(d * d, axis=-1))
+            vl = self._vl(p["chans"], r)
+            nl = len(p["chans"])
+            tot += np.sum(vl[nl - 1], axis=1)
+            q = np.einsum("qk,ckj->cqj", p["quad"], rot)     # rotated points [nc,Q,3]
+            for e in range(N):
+                acc = r[:, e] < p["cutoff"]
+                if not np.any(acc):
+                    continue
+                for iq in range(len(p["w"])):
+                    Rn = R.copy()
+                    Rn[:, e] = self.atoms[a] + q[:, iq] * r[:, e:e + 1]
+                    lp, sg = self.logpsi(Rn)
+                    ratio = np.exp(lp - lp0) * sg * sg0 * p["w"][iq]
+                    cosq = np.sum(q[:, iq] * d[:, e], axis=-1) / r[:, e]
+                    ts = np.zeros(nc)
+                    for l in range(nl - 1):
+                        ts += (2 * l + 1) * vl[l][:, e] * legendre(cosq, l)
+                    tot += np.where(acc, ts * ratio, 0.0)
+        return tot
+
+    def move_ratio(self, R, e, rnew):
+        """ln|psi(R')| - ln|psi(R)|, sign ratio, grad and lap of electron e at R'."""
+        R = np.asarray(R, dtype=float)
+        lp0, s0 = self.logpsi(R)
+        Rn = R.copy()
+        Rn[np.arange(len(R)), e] = rnew
+        ev = self.evaluate(Rn)
+        idx = np.arange(len(R))
+        return ev["logpsi"] - lp0, ev["sign"] * s0, ev["grad"][idx, e], ev["lap"][idx, e]
+
+
+def legendre(x, l):
+    """Pseudopotential.cpp:35-55."""
+    return [np.ones_like(x), x, 0.5 * (3 * x * x - 1), 0.5 * (5 * x ** 3 - 3 * x)][l]
+
+
+def gesqua(aip):
+    """Quadrature points/weights (system/gesqua.cpp:32-120) for AIP 4, 6, 12."""
+    if aip < 6:
+        q = 1.0 / math.sqrt(3.0)
+        pts = np.array([[q, q, q], [q, -q, -q], [-q, q, -q], [-q, -q, q]])
+        return pts, np.full(4, 0.25)
+    if aip < 12:
+        pts = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], dtype=float)
+        return pts, np.full(6, 1.0 / 6.0)
+    fi0 = math.pi / 5.0
+    c, s = 1.0 / math.sqrt(5.0), 2.0 / math.sqrt(5.0)
+    pts = np.zeros((12, 3))
+    pts[0, 2], pts[1, 2] = 1.0, -1.0
+    for i in range(5):
+        rk2 = 2 * i
+        pts[i + 2] = [s * math.cos(rk2 * fi0), s * math.sin(rk2 * fi0), c]
+        pts[i + 7] = [s * math.cos((rk2 + 1) * fi0), s * math.sin((rk2 + 1) * fi0), -c]
+    return pts, np.full(12, 1.0 / 12.0)

@@ -1,0 +1,48 @@
+"""Regenerate the golden vectors in tests/golden/ from the reference itself.
+
+Run in a container that has the reference sources:
+    make -C oracle REF=<reference checkout> -j8
+    python tests/golden/make_golden.py
+
+For each workload deck it draws seeded electron configurations, quadrature
+rotations and single-electron moves, runs the reference harness
+(oracle/_ref/qwref_harness, linked against the reference's own objects) and
+stores inputs + outputs as <name>.npz next to the deck and .orb file.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from mainline_b200 import systems  # noqa: E402
+import refrun  # noqa: E402
+
+NCONF = 256
+NMOVE = 2
+WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseudo=True), 12)]
+
+
+def make(name, kw, seed):
+    deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
+    R = systems.random_configs(deck, NCONF, seed=seed + 1000)
+    rng = np.random.default_rng(seed + 2000)
+    rot = np.stack([systems.random_rotation(rng) for _ in range(NCONF)])
+    me = rng.integers(0, deck.nelec, size=(NCONF, NMOVE)).astype(np.int32)
+    mp = R[np.arange(NCONF)[:, None], me] + rng.normal(0.0, 0.4, size=(NCONF, NMOVE, 3))
+    out = refrun.run_harness(deck.path, R, rot, me, mp)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), R=R, rot=rot, move_e=me, move_pos=mp, **out)
+    print(name, "logpsi[:3]", out["logpsi"][:3])
+
+
+if __name__ == "__main__":
+    if not refrun.harness_available():
+        sys.exit("build the reference harness first: make -C oracle REF=<reference> -j8")
+    for name, kw, seed in WORKLOADS:
+        make(name, kw, seed)

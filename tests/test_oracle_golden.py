@@ -1,0 +1,53 @@
+"""Pin the numpy oracle against golden vectors written by the reference
+itself (tests/golden/make_golden.py ran the reference harness)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+import qworacle
+
+NAMES = ["n2_allelectron", "n2_pseudo"]
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b))))
+
+
+@pytest.fixture(scope="module", params=NAMES)
+def case(request):
+    g = dict(np.load(os.path.join(GOLDEN, request.param + ".npz")))
+    return request.param, qworacle.System(os.path.join(GOLDEN, request.param + ".qw")), g
+
+
+def test_evaluate_matches_reference(case):
+    name, S, g = case
+    ev = S.evaluate(g["R"])
+    assert np.array_equal(ev["sign"], g["sign"])
+    assert _rel(ev["logpsi"], g["logpsi"]) < 1e-12
+    assert _rel(ev["grad"], g["grad"]) < 1e-10
+    # Laplacians near the nuclei are large (|lap| up to ~1e4): relative bound
+    assert np.max(np.abs(ev["lap"] - g["lap"]) / np.maximum(1.0, np.abs(g["lap"]))) < 1e-9
+    assert _rel(ev["kinetic"], g["kinetic"]) < 1e-9
+    assert _rel(ev["potential"], g["potential"]) < 1e-12
+
+
+def test_moves_match_reference(case):
+    name, S, g = case
+    for m in range(g["move_e"].shape[1]):
+        dl, sg, gr, lp = S.move_ratio(g["R"], g["move_e"][:, m], g["move_pos"][:, m])
+        assert _rel(dl, g["move_dlogpsi"][:, m]) < 1e-11
+        assert np.array_equal(sg, g["move_sign"][:, m])
+        assert _rel(gr, g["move_grad"][:, m]) < 1e-10
+        assert _rel(lp, g["move_lap"][:, m]) < 1e-9
+
+
+def test_nonlocal_matches_reference(case):
+    name, S, g = case
+    if not S.pp:
+        pytest.skip("all-electron deck")
+    n = 32
+    nl = S.nonlocal_pp(g["R"][:n], g["rot"][:n])
+    assert _rel(nl, g["nonlocal"][:n]) < 1e-11
