@@ -1,0 +1,307 @@
+"""Benchmark: DMC walker-steps/s of the B200 walker engine (mixed precision vs
+FP64) with p50/p99 block latency, on the seeded Z_eff=5 pseudopotential
+two-atom molecule (14 electrons, 80 basis functions, 4096 walkers, tau=0.01).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+A step is one DMC step of the whole population: every walker moves each of
+its 14 electrons (drift-diffusion Metropolis, node restriction), evaluates its
+local energy (kinetic + Coulomb + nonlocal pseudopotential) and updates its
+weight; branching runs every 5 steps (feedback interval).  walker-steps/s =
+walkers x steps / device time.  One process per GPU; the population does not
+shard (independent replicas, scaling "weak"); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NWALK = 4096
+TAU = 0.01
+FEEDBACK_INTERVAL = 5
+SEED = 20261203
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
+                          s[3 + i].lower() in ("active", "1")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def make_workload(tmpdir):
+    from mainline_b200 import systems
+    deck = systems.write_n2(tmpdir, seed=12, pseudo=True, name="n2_pseudo_bench")
+    R0 = systems.random_configs(deck, NWALK, seed=SEED)
+    return deck, R0
+
+
+def algorithmic_bytes_per_walker_step(N, M, nb, precision_bytes):
+    """Resident walker state read + written once per step (positions, both
+    inverse matrices, MO gradient/Laplacian rows, Jastrow sums, scalars)."""
+    state = 8 * 3 * N + precision_bytes * (2 * M * M + N * M * 4) + 8 * 4 * N + 64
+    return 2 * state
+
+
+def run_engine(args, rank, world):
+    import torch
+    from mainline_b200 import engine
+    torch.cuda.set_device(rank % max(torch.cuda.device_count(), 1))
+    dev = torch.device("cuda", rank % max(torch.cuda.device_count(), 1))
+    tmp = tempfile.mkdtemp(prefix="qwg_bench_")
+    deck, R0 = make_workload(tmp)
+    stream = torch.cuda.Stream(device=dev)
+    results = {}
+    for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
+        E = engine.Engine(deck.path, prec, max_walkers=NWALK, stream=stream.cuda_stream)
+        E.set_walkers(R0)
+        for b in range(3):  # VMC equilibration from the seeded start
+            E.vmc_block(20, 0.3, seed=SEED + 17 * rank + b)
+        steps = max(FEEDBACK_INTERVAL, (args.steps // FEEDBACK_INTERVAL) * FEEDBACK_INTERVAL)
+        E.dmc_init(timestep=TAU, nstep=steps, seed=SEED + rank)
+        for _ in range(max(args.warmup, 3) // 1):
+            E.dmc_block()  # warm-up blocks (untimed)
+        # timed: one block of `steps` steps, CUDA events on the engine's stream
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        lat = []
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            torch.distributed.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        E.reset_launch_count()
+        with ClockSampler(rank % max(torch.cuda.device_count(), 1)) as cs:
+            e0.record(stream)
+            st = E.dmc_block()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        launches = E.launch_count()
+        # block latency: several shorter blocks (20 steps), host wall time from
+        # block start to block statistics on the host
+        E.dmc_init(timestep=TAU, nstep=20, seed=SEED + 99 + rank)
+        energies = []
+        for b in range(args.latency_blocks):
+            t0 = time.perf_counter()
+            s2 = E.dmc_block()
+            lat.append((time.perf_counter() - t0) * 1e3)
+            energies.append(s2["energy"])
+        results[label] = {"ms": ms, "steps": steps, "stats": st, "launches": launches, "clocks": cs.summary(),
+                          "lat": lat, "energies": energies, "kernel_ms": st["block_ms"]}
+        E.close()
+    # end-to-end through the C-ABI with host buffers: upload walkers, run the
+    # block, download walkers + statistics, every step amortised
+    E = engine.Engine(deck.path, engine.MIXED, max_walkers=NWALK, stream=stream.cuda_stream)
+    E.set_walkers(R0)
+    E.vmc_block(20, 0.3, seed=SEED)
+    steps = results["mixed"]["steps"]
+    E.dmc_init(timestep=TAU, nstep=steps, seed=SEED + 5)
+    E.dmc_block()
+    Rh = E.get_walkers()
+    Rpinned = torch.from_numpy(Rh).pin_memory().numpy()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    E.set_walkers(Rpinned)
+    E.dmc_init(timestep=TAU, nstep=steps, seed=SEED + 6)
+    st = E.dmc_block()
+    Rout = E.get_walkers()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1)
+    E.close()
+    return results, e2e_ms, steps, deck
+
+
+def cpu_reference(deck_path, seconds_target=20.0, cores=None):
+    """Reference qwalk (oracle/_ref/qwalk-Linux, shipped -O3 -ffast-math flags)
+    on the host cores: one process per core, DMC on the same deck.  Per-block
+    cost from the difference of a 1-block and a 3-block run (removes start-up
+    and the reference's own VMC warm-up)."""
+    qw = os.path.join(ROOT, "oracle", "_ref", "qwalk-Linux")
+    if not os.path.exists(qw):
+        return None
+    cores = cores or os.cpu_count() or 1
+    nconf, nstep = 64, 50
+    base = open(deck_path).read()
+    d = os.path.dirname(deck_path)
+
+    def run(nblock):
+        procs = []
+        t0 = time.perf_counter()
+        for p in range(cores):
+            path = os.path.join(d, f"cpu_{nblock}_{p}.qw")
+            txt = re.sub(r"RANDOMSEED\s*\{[^}]*\}", f"RANDOMSEED {{ {101 + p} {203 + p} }}", base)
+            txt += (f"\nMETHOD {{ DMC NCONFIG {nconf} NBLOCK {nblock} NSTEP {nstep} TIMESTEP {TAU} }}\n")
+            open(path, "w").write(txt)
+            procs.append(subprocess.Popen([qw, os.path.basename(path)], cwd=d, stdout=subprocess.DEVNULL,
+                                          stderr=subprocess.DEVNULL))
+        for p in procs:
+            p.wait()
+        return time.perf_counter() - t0
+
+    t1 = run(1)
+    t3 = run(3)
+    per_block = max((t3 - t1) / 2.0, 1e-6)
+    ws = cores * nconf * nstep / per_block
+    return {"value": ws, "unit": "walker-steps/s", "cores": cores, "kind": "reference",
+            "sample": f"{cores} qwalk processes x {nconf} walkers x {nstep} DMC steps/block; "
+                      f"per-block time from 3-block minus 1-block wall ({t3:.1f}s - {t1:.1f}s)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--latency-blocks", type=int, default=12)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        tmp = tempfile.mkdtemp(prefix="qwg_ref_")
+        deck, _ = make_workload(tmp)
+        ref = cpu_reference(deck.path)
+        if ref is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/qwalk-Linux was not built"}))
+            return
+        line = {"impl": "reference", "metric": "DMC walker-steps/s", "value": ref["value"],
+                "unit": "walker-steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded deck)",
+                "config": {"workload": "n2_pseudo: 2 Z_eff=5 atoms, 14 e, 80 basis fns, tau=0.01"},
+                "cpu_baseline": ref,
+                "e2e": {"value": ref["value"], "unit": "walker-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    results, e2e_ms, steps, deck = run_engine(args, rank, world)
+    mx = results["mixed"]
+    fp = results["fp64"]
+    # max over ranks of the device time
+    ms = mx["ms"]
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([ms, e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    ws = NWALK * steps * world / (ms / 1e3)
+    ws64 = NWALK * fp["steps"] * world / (fp["ms"] / 1e3)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    N, M, nb = 14, 7, 80
+    hbm, src = _peaks()
+    # dominant kernel: the walker-step kernel; algorithmic bytes per launch =
+    # walkers x steps-per-launch x resident-state read+write per walker-step
+    bytes_launch = NWALK * FEEDBACK_INTERVAL * algorithmic_bytes_per_walker_step(N, M, nb, 4)
+    kern_ms_per_launch = mx["kernel_ms"] / (steps / FEEDBACK_INTERVAL)
+    achieved = bytes_launch / (kern_ms_per_launch / 1e3) / 1e9
+    lat = np.array(mx["lat"])
+    line = {
+        "metric": "DMC walker-steps/s (mixed precision engine; FP64 beside it)",
+        "value": ws, "unit": "walker-steps/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32/f64 mixed (FP64 refresh, energies, weights)", "data": "synthetic (seeded QWalk deck)",
+        "config": {"workload": "n2_pseudo DMC: 2 Z_eff=5 atoms, 14 electrons, 80 basis fns, 12-pt quadrature",
+                   "walkers_per_gpu": NWALK, "tau": TAU, "feedback_interval": FEEDBACK_INTERVAL,
+                   "parallelism": f"replicas x{world}", "l2": "walker state resident (working set < L2); "
+                   "256 MiB buffer written before the timed block"},
+        "fp64": {"value": ws64, "unit": "walker-steps/s", "ms_per_step": fp["ms"] / fp["steps"],
+                 "block_energy_mean": float(np.mean(fp["energies"])),
+                 "block_energy_sem": float(np.std(fp["energies"]) / np.sqrt(len(fp["energies"])))},
+        "mixed_vs_fp64": ws / ws64,
+        "mixed_block_energy": {"mean": float(np.mean(mx["energies"])),
+                               "sem": float(np.std(mx["energies"]) / np.sqrt(len(mx["energies"])))},
+        "block_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                             "steps_per_block": 20, "walkers": NWALK},
+        "e2e": {"value": NWALK * steps / (e2e_ms / 1e3), "unit": "walker-steps/s",
+                "h2d_bytes_per_step": NWALK * N * 3 * 8 / steps, "d2h_bytes_per_step": (NWALK * N * 3 * 8 + 96) / steps},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": src, "traffic": None,
+                     "note": "walker-step kernel; algorithmic bytes = resident state read+write per walker-step"},
+        "gpu_launches": mx["launches"],
+        "clocks": mx["clocks"],
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference(os.path.abspath(deck.path))
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

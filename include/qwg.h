@@ -1,0 +1,161 @@
+/*
+ * qwg.h -- C-ABI of the B200 walker engine for QWalk VMC/DMC.
+ *
+ * One opaque context = one system (deck) + one resident walker population on
+ * one GPU, bound to one CUDA stream.  All entry points return an int status
+ * (QWG_OK or a negative error class); qwg_last_error() gives the text.  No C++
+ * exceptions cross this boundary.  Host buffers are caller-owned; device
+ * memory is owned by the context.
+ *
+ * Reference interfaces each entry point replaces (QWalk/mainline src/):
+ *   qwg_create          System / Pseudopotential / Wavefunction_data factories
+ *                       driven by the input file: allocate(System)
+ *                       system/System.cpp:29-49, System::generatePseudo
+ *                       system/System.cpp:145-149, allocate(Wavefunction_data)
+ *                       wavefunction/Wavefunction_data.cpp:32-59 (module chosen
+ *                       by the first word of each section, same grammar as
+ *                       program_utils/qmc_io.cpp:280-345).
+ *   qwg_set_walkers /   Config_save_point::restorePos / savePos
+ *   qwg_get_walkers     system/Sample_point.cpp:61-85 (walker positions, 3N
+ *                       doubles each).
+ *   qwg_eval            Slat_Jastrow::updateLap + getVal + getLap for every
+ *                       electron (wavefunction/Slat_Jastrow.cpp:101-123,
+ *                       235-381), System::calcKinetic (system/System.cpp:105-140),
+ *                       System::calcLoc (system/Molecular_system.cpp:209-287)
+ *                       and Pseudopotential::calcNonlocWithTest in its
+ *                       deterministic mode (system/Pseudopotential.cpp:412-424,
+ *                       596-815), batched over walkers.
+ *   qwg_ratio           Sample_point::setElectronPos + Wavefunction::updateLap +
+ *                       getVal/getLap for one electron per walker
+ *                       (wavefunction/Slat_wf.h:1145-1172, Jastrow2_wf.cpp:988-1157).
+ *   qwg_vmc_block       Vmc_method::runWithVariables, one block
+ *                       (method/Vmc_method.cpp:389-536) with the Split_sampler
+ *                       depth-1 move (method/Split_sample.cpp:380-540).
+ *   qwg_dmc_block       Dmc_method::runWithVariables, one block
+ *                       (method/Dmc_method.cpp:373-552): moves, gatherData,
+ *                       getWeight (:801-824), updateEtrial (:780-797),
+ *                       calcBranch/match_walkers (:961-1156).
+ *   qwg_dmc_init        Dmc_method::restorecheckpoint tail: gatherData for every
+ *                       walker, find_cutoffs (:262-300), updateEtrial.
+ */
+#ifndef QWG_H
+#define QWG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QWG_OK 0
+#define QWG_ERR_ARG -1      /* bad argument / size beyond a limit */
+#define QWG_ERR_INPUT -2    /* deck or orbital file could not be read/understood */
+#define QWG_ERR_CUDA -3     /* CUDA runtime error */
+#define QWG_ERR_STATE -4    /* call made in the wrong state (e.g. no walkers) */
+#define QWG_ERR_NUMERIC -5  /* non-finite walker or singular determinant */
+
+#define QWG_FP64 0          /* all arithmetic in double precision */
+#define QWG_MIXED 1         /* FP32 basis/MO/ratios/inverse; FP64 LU refresh,
+                               log|det|, energies and weights */
+
+typedef struct qwg_ctx qwg_ctx;
+
+typedef struct {
+  int nelec, nup, ndown, natoms, nbasis, nshell, nmo_up, nmo_down;
+  int has_pseudo;      /* 1 if any atom carries a PSEUDO section */
+  int max_walkers;
+  int precision;
+  int walkers_per_cta; /* launch shape picked at create time */
+  double ion_ion;      /* constant ion-ion energy */
+} qwg_info;
+
+/* Per-walker outputs of qwg_eval (host arrays, caller-owned, sized by nw). */
+typedef struct {
+  double* logpsi;      /* [nw]          ln|psi|                        */
+  double* sign;        /* [nw]          sign of psi                    */
+  double* grad;        /* [nw][nelec][3] grad ln|psi| per electron     */
+  double* lap;         /* [nw][nelec]   (lap psi)/psi per electron     */
+  double* kinetic;     /* [nw]  -1/2 sum_e lap                         */
+  double* potential;   /* [nw]  Coulomb e-e, e-i, i-i                  */
+  double* nonlocal;    /* [nw]  pseudopotential (local + nonlocal)     */
+} qwg_eval_out;
+
+/* Block statistics (weighted averages over steps x walkers in the block,
+ * Properties_manager::endBlock, properties/Properties.cpp:578-652). */
+typedef struct {
+  double energy, kinetic, potential, nonlocal;
+  double weight;          /* average walker weight                      */
+  double energy_var;      /* weighted variance of E_L over the block    */
+  double acceptance;      /* accepted / attempted single-electron moves */
+  double etrial;          /* E_T after the block                        */
+  double block_ms;        /* device time of the block (CUDA events)     */
+  int nsteps, nwalkers;
+  int nonfinite;          /* walkers whose E_L or weight went non-finite */
+} qwg_block_stats;
+
+/* DMC parameters (Dmc_method::read defaults, method/Dmc_method.cpp:33-160). */
+typedef struct {
+  double timestep;        /* TIMESTEP                                   */
+  int nstep;              /* steps per block (default 1/tau)            */
+  int feedback_interval;  /* FEEDBACK_INTERVAL (5)                      */
+  double feedback;        /* FEEDBACK (1.0)                             */
+  double max_poss_weight; /* MAX_POSS_WEIGHT (7.0)                      */
+  double branch_start_cutoff; /* BRANCH_START_CUTOFF (10); stop = 1.5x  */
+  int refresh_interval;   /* steps between full recomputes (MIXED: LU refresh) */
+  int deterministic_pp;   /* 1: evaluate every pair inside the cutoff   */
+  uint64_t seed;
+} qwg_dmc_params;
+
+const char* qwg_version(void);
+const char* qwg_last_error(const qwg_ctx* ctx);
+
+/* Build a context from a QWalk input file.  stream may be NULL (the context
+ * then creates its own) or a cudaStream_t the caller owns.  On failure *out is
+ * NULL and qwg_last_error(NULL) returns the reason (per calling thread). */
+int qwg_create(const char* deck_path, int precision, int max_walkers, void* stream, qwg_ctx** out);
+int qwg_destroy(qwg_ctx* ctx);
+int qwg_get_info(const qwg_ctx* ctx, qwg_info* info);
+
+/* Host-side table check without a GPU: parse the deck and build the device
+ * tables on the host only; returns sizes through info.  Used by CPU tests. */
+int qwg_inspect_deck(const char* deck_path, qwg_info* info, char* err, int errlen);
+/* Radial spline table of basis shell s (host copy, [npts][4]); npts returned. */
+int qwg_inspect_spline(const char* deck_path, int shell, double* coef, int maxpts, int* npts,
+                       double* spacing, double* cutoff);
+
+/* Walker positions: R is [nw][nelec][3] doubles.  Host buffers. */
+int qwg_set_walkers(qwg_ctx* ctx, const double* R, int nw);
+int qwg_get_walkers(qwg_ctx* ctx, double* R, int nw);
+/* Device-buffer variants (pointers in device memory, stream-ordered). */
+int qwg_set_walkers_device(qwg_ctx* ctx, const double* dR, int nw);
+
+/* Full evaluation of every resident walker.  rot: [nw][3][3] quadrature
+ * rotations (rows x,y,z; Pseudopotential::rotateQuadrature) or NULL for the
+ * unrotated points.  The pseudopotential is evaluated deterministically. */
+int qwg_eval(qwg_ctx* ctx, const double* rot, qwg_eval_out* out);
+
+/* Single-electron move per walker: electron e[w] to Rnew[w][3].  Returns
+ * ln|psi'|-ln|psi|, sign ratio, grad ln psi' [nw][3] and lap psi'/psi' of
+ * the moved electron. */
+int qwg_ratio(qwg_ctx* ctx, const int* e, const double* Rnew, double* dlogpsi, double* sign,
+              double* grad, double* lap);
+
+/* VMC block on the resident walkers: nstep sweeps (each = one drift-diffusion
+ * Metropolis move per electron + one local energy).  stochastic PP unless
+ * deterministic_pp. */
+int qwg_vmc_block(qwg_ctx* ctx, int nstep, double timestep, uint64_t seed, int deterministic_pp,
+                  qwg_block_stats* stats);
+
+/* DMC: initialise (energies of the resident walkers, E_ref, branch cut-offs,
+ * E_T), then run blocks on the device-resident population. */
+int qwg_dmc_init(qwg_ctx* ctx, const qwg_dmc_params* p);
+int qwg_dmc_block(qwg_ctx* ctx, qwg_block_stats* stats);
+
+/* Number of kernel launches the context issued since the last reset. */
+long long qwg_launch_count(const qwg_ctx* ctx);
+void qwg_reset_launch_count(qwg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,723 @@
+// QWalk input grammar + table builder for the walker engine.
+//
+// Module semantics follow the reference (QWalk/mainline src/):
+//   grammar            program_utils/qmc_io.cpp:168-345
+//   AOSPLINE basis     basis_function/Cubic_spline_build.cpp:139-660 (GAMESS
+//                      shells, GAMESSNORM, numerical renormalisation, optional
+//                      smooth CUTOFF, clamped cubic spline on a 0.02 grid)
+//   spline fit/cutoff  basis_function/Spline_fitter.cpp:153-293
+//   MO coefficients    orbitals/MO_matrix.h:264-332 (ORB file), MO_matrix_blas.h:101-190
+//   occupations        wavefunction/Slat_wf_data.cpp:34-303 (STATES, one determinant)
+//   Jastrow groups     wavefunction/Jastrow2_wf.cpp:29-160, Jastrow2_one.cpp:25-100,
+//                      Jastrow2_two.cpp:28-45/220-245, Jastrow2_three.cpp:29-100
+//   radial functions   basis_function/Cutoff_cusp.cpp:26-60,
+//                      Poly_pade_function.cpp:26-85
+//   pseudopotential    system/Pseudopotential.cpp:874-1033, Rgaussian_function.cpp:24-100
+//   quadrature         system/gesqua.cpp:32-120
+#include "qwg_deck.hpp"
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <sstream>
+
+namespace qwg {
+
+static bool ieq(const std::string& a, const std::string& b) {
+  if (a.size() != b.size()) return false;
+  for (size_t i = 0; i < a.size(); i++)
+    if (std::toupper((unsigned char)a[i]) != std::toupper((unsigned char)b[i])) return false;
+  return true;
+}
+
+static std::string dirname_of(const std::string& p) {
+  size_t k = p.find_last_of('/');
+  return k == std::string::npos ? std::string(".") : p.substr(0, k);
+}
+
+static bool file_exists(const std::string& p) {
+  std::ifstream f(p);
+  return bool(f);
+}
+
+std::vector<std::string> tokenize_file(const std::string& path) {
+  std::ifstream in(path);
+  if (!in) throw InputError("cannot open " + path);
+  std::vector<std::string> raw;
+  std::string line;
+  while (std::getline(in, line)) {
+    size_t hash = line.find('#');
+    if (hash != std::string::npos) line.erase(hash);
+    std::istringstream ss(line);
+    std::string tok;
+    while (ss >> tok) {
+      std::string buf;
+      for (char ch : tok) {
+        if (ch == '{' || ch == '}') {
+          if (!buf.empty()) raw.push_back(buf);
+          raw.push_back(std::string(1, ch));
+          buf.clear();
+        } else {
+          buf.push_back(ch);
+        }
+      }
+      if (!buf.empty()) raw.push_back(buf);
+    }
+  }
+  std::vector<std::string> out;
+  for (size_t i = 0; i < raw.size(); i++) {
+    if (ieq(raw[i], "INCLUDE")) {
+      if (i + 1 >= raw.size()) throw InputError("INCLUDE without a file name in " + path);
+      std::string inc = raw[i + 1];
+      if (inc[0] != '/' && !file_exists(inc)) inc = dirname_of(path) + "/" + inc;
+      std::vector<std::string> sub = tokenize_file(inc);
+      out.insert(out.end(), sub.begin(), sub.end());
+      i++;
+    } else {
+      out.push_back(raw[i]);
+    }
+  }
+  return out;
+}
+
+bool find_section(const std::vector<std::string>& w, const std::string& name, size_t& pos,
+                  std::vector<std::string>& out) {
+  out.clear();
+  int level = 0;
+  for (; pos < w.size(); pos++) {
+    if (w[pos] == "{") level++;
+    else if (w[pos] == "}") level--;
+    if (level < 0) { pos++; return false; }
+    if (level == 0 && ieq(w[pos], name)) {
+      if (pos + 1 >= w.size() || w[pos + 1] != "{")
+        throw InputError("section " + name + " must be followed by {");
+      pos += 2;
+      int depth = 0;
+      for (; pos < w.size(); pos++) {
+        if (w[pos] == "{") depth++;
+        if (w[pos] == "}") { if (depth == 0) break; depth--; }
+        out.push_back(w[pos]);
+      }
+      if (pos >= w.size()) throw InputError("unterminated section " + name);
+      pos++;
+      return true;
+    }
+  }
+  return false;
+}
+
+std::vector<std::vector<std::string>> all_sections(const std::vector<std::string>& w, const std::string& name) {
+  std::vector<std::vector<std::string>> res;
+  size_t pos = 0;
+  std::vector<std::string> s;
+  while (find_section(w, name, pos, s)) res.push_back(s);
+  return res;
+}
+
+bool has_section(const std::vector<std::string>& w, const std::string& name) {
+  size_t pos = 0;
+  std::vector<std::string> s;
+  return find_section(w, name, pos, s);
+}
+
+static std::vector<std::string> get_section(const std::vector<std::string>& w, const std::string& name) {
+  size_t pos = 0;
+  std::vector<std::string> s;
+  if (!find_section(w, name, pos, s)) throw InputError("missing section " + name);
+  return s;
+}
+
+bool find_value(const std::vector<std::string>& w, const std::string& name, std::string& out) {
+  int level = 0;
+  for (size_t i = 0; i < w.size(); i++) {
+    if (w[i] == "{") level++;
+    else if (w[i] == "}") level--;
+    if (level < 0) return false;
+    if (level == 0 && ieq(w[i], name)) {
+      if (i + 1 >= w.size()) throw InputError("keyword " + name + " without a value");
+      out = w[i + 1];
+      return true;
+    }
+  }
+  return false;
+}
+
+bool has_keyword(const std::vector<std::string>& w, const std::string& name) {
+  int level = 0;
+  for (auto& t : w) {
+    if (t == "{") level++;
+    else if (t == "}") level--;
+    if (level == 0 && ieq(t, name)) return true;
+  }
+  return false;
+}
+
+static double to_d(const std::string& s) {
+  char* end = nullptr;
+  double v = std::strtod(s.c_str(), &end);
+  if (end == s.c_str()) throw InputError("expected a number, got '" + s + "'");
+  return v;
+}
+static int to_i(const std::string& s) {
+  char* end = nullptr;
+  long v = std::strtol(s.c_str(), &end, 10);
+  if (end == s.c_str()) throw InputError("expected an integer, got '" + s + "'");
+  return (int)v;
+}
+static double value_d(const std::vector<std::string>& w, const std::string& k, double def, bool required = false) {
+  std::string s;
+  if (find_value(w, k, s)) return to_d(s);
+  if (required) throw InputError("missing keyword " + k);
+  return def;
+}
+
+// ---------------------------------------------------------------------------
+// cubic spline (clamped, uniform grid)
+
+static void spline_fit(const std::vector<double>& x, const std::vector<double>& y, double yp1, double ypn,
+                       double* coef /* [n][4] */) {
+  const int n = (int)x.size();
+  std::vector<double> y2(n), u(n);
+  if (yp1 > 0.99e30) {
+    y2[0] = 0; u[0] = 0;
+  } else {
+    y2[0] = -0.5;
+    u[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1);
+  }
+  for (int i = 1; i < n - 1; i++) {
+    double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]);
+    double p = sig * y2[i - 1] + 2.0;
+    y2[i] = (sig - 1.0) / p;
+    u[i] = (6.0 * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1])) /
+                (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p;
+  }
+  double qn, un;
+  if (ypn > 0.99e30) { qn = 0; un = 0; }
+  else {
+    qn = 0.5;
+    un = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]));
+  }
+  y2[n - 1] = (un - qn * u[n - 2]) / (qn * y2[n - 2] + 1.0);
+  for (int k = n - 2; k >= 0; k--) y2[k] = y2[k] * y2[k + 1] + u[k];
+  for (int i = 0; i < n - 1; i++) {
+    double h = x[i + 1] - x[i];
+    coef[4 * i + 0] = y[i];
+    coef[4 * i + 1] = (y[i + 1] - y[i]) / h - h * (2.0 * y2[i] + y2[i + 1]) / 6.0;
+    coef[4 * i + 2] = y2[i] / 2.0;
+    coef[4 * i + 3] = (y2[i + 1] - y2[i]) / (6.0 * h);
+  }
+  coef[4 * (n - 1) + 0] = y[n - 1];
+  coef[4 * (n - 1) + 1] = coef[4 * (n - 1) + 2] = coef[4 * (n - 1) + 3] = 0.0;
+}
+
+// Largest r (0.5 bohr steps down from the grid end) where |f| exceeds
+// 1e-10 * min(max|f|, 1).
+static double spline_cutoff(const double* c, int n, double spacing, double threshold) {
+  double mx = 0;
+  for (int i = 0; i < n; i++) mx = std::max(mx, std::fabs(c[4 * i]));
+  mx = std::min(mx, 1.0);
+  const double thr = 1e-10 * mx;
+  const double inv = 1.0 / spacing;
+  for (double x = threshold - 0.5; x >= 0; x -= 0.5) {
+    int i = int(x * inv);
+    double h = x - i * spacing;
+    double t = c[4 * i] + h * (c[4 * i + 1] + h * (c[4 * i + 2] + h * c[4 * i + 3]));
+    if (std::fabs(t) > thr) return x + 0.5;
+  }
+  return 0.0;
+}
+
+static int sym_of(const std::string& s) {
+  if (ieq(s, "S")) return SYM_S;
+  if (ieq(s, "P")) return SYM_P;
+  if (ieq(s, "D") || ieq(s, "6D")) return SYM_6D;
+  if (ieq(s, "5D")) return SYM_5D;
+  throw InputError("unsupported AOSPLINE shell symmetry " + s + " (supported: S P 5D 6D)");
+}
+static int sym_nfunc(int s) { return s == SYM_S ? 1 : s == SYM_P ? 3 : s == SYM_6D ? 6 : 5; }
+static int sym_l(int s) { return s == SYM_S ? 0 : s == SYM_P ? 1 : 2; }
+
+struct BasisObj {
+  std::string label;
+  std::vector<int> syms;
+  std::vector<int> spline_ids;  // into HostSystem::spline table
+  double threshold = 0;
+  int nfunc = 0;
+};
+
+static BasisObj read_aospline(const std::vector<std::string>& w, HostSystem& S,
+                              std::vector<std::vector<double>>& tables) {
+  BasisObj B;
+  if (w.size() < 2) throw InputError("empty BASIS section");
+  B.label = w[0];
+  if (!ieq(w[1], "AOSPLINE")) throw InputError("BASIS type " + w[1] + " not supported (AOSPLINE only)");
+  double spacing = 0.02;
+  int n = 2500;
+  std::string ntype = "GAMESSNORM", tmp;
+  if (find_value(w, "NORMTYPE", tmp)) ntype = tmp;
+  bool renorm = !has_keyword(w, "NORENORMALIZE");
+  double reqcut = value_d(w, "CUTOFF", -1.0);
+  if (find_value(w, "SPACING", tmp)) { spacing = to_d(tmp); n = int(50.0 / spacing); }
+  if (has_keyword(w, "CUSP") || has_keyword(w, "ZERO_DERIVATIVE"))
+    throw InputError("AOSPLINE CUSP/ZERO_DERIVATIVE options are not supported");
+  if (S.nspline > 0 && std::fabs(spacing - S.spline_spacing) > 1e-12)
+    throw InputError("all AOSPLINE bases must share one SPACING");
+  S.spline_spacing = spacing;
+  auto g = get_section(w, "GAMESS");
+  std::vector<double> x(n), y(n);
+  for (int j = 0; j < n; j++) x[j] = j * spacing;
+  size_t p = 0;
+  std::vector<std::vector<double>> coefs;
+  while (p < g.size()) {
+    int sym = sym_of(g[p]);
+    if (p + 1 >= g.size()) throw InputError("truncated GAMESS section");
+    int ng = to_i(g[p + 1]);
+    if (ng <= 0 || p + 2 + 3 * (size_t)ng > g.size()) throw InputError("unexpected end of GAMESS section");
+    std::fill(y.begin(), y.end(), 0.0);
+    for (int i = 0; i < ng; i++) {
+      double ex = to_d(g[p + 3 + 3 * i]);
+      double cc = to_d(g[p + 4 + 3 * i]);
+      double norm;
+      if (ieq(ntype, "GAMESSNORM")) {
+        double fac = std::sqrt(2.0 * ex / M_PI), feg = 4.0 * ex, feg2 = feg * feg;
+        const double nl[3] = {std::sqrt(2.0 * feg * fac), std::sqrt(2.0 * feg2 * fac / 3.0),
+                              std::sqrt(2.0 * feg * feg2 * fac / 15.0)};
+        norm = nl[sym_l(sym)];
+      } else if (ieq(ntype, "CRYSTAL")) {
+        const double nl[3] = {1.0, 1.0 / std::sqrt(3.0), 1.0 / std::sqrt(5.0)};
+        norm = nl[sym_l(sym)];
+      } else if (ieq(ntype, "NONE")) {
+        norm = 1.0;
+      } else {
+        throw InputError("NORMTYPE " + ntype + " not understood");
+      }
+      for (int j = 0; j < n; j++) y[j] += norm * cc * std::exp(-ex * x[j] * x[j]);
+    }
+    if (renorm) {
+      int pw = sym_l(sym) + 1;
+      double sum = 0;
+      for (int j = 0; j < n; j++) sum += spacing * std::pow(x[j], 2 * pw) * y[j] * y[j];
+      if (std::fabs(sum - 1) > 1e-5)
+        for (int j = 0; j < n; j++) y[j] /= std::sqrt(sum);
+    }
+    if (reqcut > 0) {
+      const double cutmax = reqcut - 1e-6, cutmin = cutmax - 1.2;
+      for (int j = 0; j < n; j++) {
+        if (x[j] > cutmin) {
+          if (x[j] > cutmax) y[j] = 0;
+          else {
+            double zz = (x[j] - cutmin) / 1.2;
+            y[j] *= (1 - zz * zz * zz * (6 * zz * zz - 15 * zz + 10));
+          }
+        }
+      }
+    }
+    double yp1 = (y[1] - y[0]) / spacing, ypn = (y[n - 1] - y[n - 2]) / spacing;
+    std::vector<double> c(4 * (size_t)n);
+    spline_fit(x, y, yp1, ypn, c.data());
+    coefs.push_back(std::move(c));
+    B.syms.push_back(sym);
+    p += 2 + 3 * ng;
+  }
+  double thr0 = x[n - 1];
+  double thr = 0;
+  for (auto& c : coefs) thr = std::max(thr, spline_cutoff(c.data(), n, spacing, thr0));
+  B.threshold = thr;
+  for (auto& c : coefs) {
+    if (thr0 < thr) {  // pad with zeros out to the common threshold
+      int extra = int((thr - thr0) / spacing) + 1;
+      c.resize(c.size() + 4 * (size_t)extra, 0.0);
+    }
+    B.spline_ids.push_back((int)tables.size());
+    tables.push_back(std::move(c));
+  }
+  S.nspline = (int)tables.size();
+  for (int s : B.syms) B.nfunc += sym_nfunc(s);
+  return B;
+}
+
+// ORB file: "mo basis center label" records until COEFFICIENTS, then the
+// coefficient list; each (mo, center, basis) entry points at a label.
+static void read_orb(const std::string& path, int nmo, const std::vector<int>& nfunc_center,
+                     std::vector<double>& moc /* [nbasis][nmo] */) {
+  std::ifstream in(path);
+  if (!in) throw InputError("cannot open ORBFILE " + path);
+  int ncent = (int)nfunc_center.size();
+  int maxb = 0;
+  for (int v : nfunc_center) maxb = std::max(maxb, v);
+  std::vector<long> cm((size_t)nmo * ncent * maxb, -1);
+  std::string t;
+  long maxlabel = 0;
+  while (true) {
+    if (!(in >> t)) throw InputError("ORBFILE " + path + ": no COEFFICIENTS");
+    if (t == "COEFFICIENTS") break;
+    int mo = to_i(t) - 1;
+    std::string sb, sc, sl;
+    in >> sb >> sc >> sl;
+    int b = to_i(sb) - 1, c = to_i(sc) - 1;
+    long l = to_i(sl) - 1;
+    if (mo < nmo) {
+      if (b < 0 || b >= maxb || c < 0 || c >= ncent) throw InputError("ORBFILE entry out of range");
+      cm[((size_t)mo * ncent + c) * maxb + b] = l;
+    }
+    maxlabel = std::max(maxlabel, l + 1);
+  }
+  std::vector<double> coef(maxlabel);
+  for (long i = 0; i < maxlabel; i++) {
+    if (!(in >> t)) throw InputError("ORBFILE " + path + ": too few coefficients");
+    coef[i] = to_d(t);
+  }
+  int nbasis = 0;
+  for (int v : nfunc_center) nbasis += v;
+  moc.assign((size_t)nbasis * nmo, 0.0);
+  int row = 0;
+  for (int c = 0; c < ncent; c++)
+    for (int f = 0; f < nfunc_center[c]; f++, row++)
+      for (int mo = 0; mo < nmo; mo++) {
+        long l = cm[((size_t)mo * ncent + c) * maxb + f];
+        moc[(size_t)row * nmo + mo] = l >= 0 ? coef[l] : 0.0;
+      }
+}
+
+static std::vector<Radial> read_radial(const std::vector<std::string>& w) {
+  if (w.size() < 2) throw InputError("empty Jastrow basis section");
+  std::vector<Radial> out;
+  if (ieq(w[1], "CUTOFF_CUSP")) {
+    Radial r;
+    r.kind = RAD_CUTOFF_CUSP;
+    r.a = value_d(w, "CUSP", 0, true);
+    r.b = value_d(w, "GAMMA", 0, true);
+    r.rcut = value_d(w, "CUTOFF", 0, true);
+    if (r.rcut < 0) throw InputError("CUTOFF_CUSP cutoff must be positive");
+    out.push_back(r);
+  } else if (ieq(w[1], "POLYPADE")) {
+    double rcut = value_d(w, "RCUT", 0, true);
+    double b0 = value_d(w, "BETA0", 0, true);
+    int nf = (int)value_d(w, "NFUNC", 0, true);
+    double b1 = std::log(b0 + 1.00001);
+    for (int i = 0; i < nf; i++) {
+      Radial r;
+      r.kind = RAD_POLYPADE;
+      r.rcut = rcut;
+      r.a = i == 0 ? b0 : std::exp(b1 + 1.6 * i) - 1;
+      r.b = 0;
+      out.push_back(r);
+    }
+  } else {
+    throw InputError("Jastrow basis type " + w[1] + " not supported (CUTOFF_CUSP, POLYPADE)");
+  }
+  return out;
+}
+
+static void gesqua(int& aip, std::vector<double>& q, std::vector<double>& wq) {
+  if (aip < 4) throw InputError("AIP must be at least 4");
+  q.clear(); wq.clear();
+  if (aip < 6) {
+    aip = 4;
+    double s = 1.0 / std::sqrt(3.0);
+    double p[4][3] = {{s, s, s}, {s, -s, -s}, {-s, s, -s}, {-s, -s, s}};
+    for (auto& r : p) { q.insert(q.end(), r, r + 3); wq.push_back(0.25); }
+  } else if (aip < 12) {
+    aip = 6;
+    double p[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    for (auto& r : p) { q.insert(q.end(), r, r + 3); wq.push_back(1.0 / 6.0); }
+  } else if (aip < 18) {
+    // icosahedron vertices: the poles and two staggered rings of five
+    aip = 12;
+    q.assign(36, 0.0);
+    q[2] = 1.0; q[5] = -1.0;
+    const double fi0 = M_PI / 5.0, c = 1.0 / std::sqrt(5.0), s = 2.0 / std::sqrt(5.0);
+    for (int i = 0; i < 5; i++) {
+      double rk2 = 2 * i;
+      q[3 * (i + 2) + 0] = s * std::cos(rk2 * fi0);
+      q[3 * (i + 2) + 1] = s * std::sin(rk2 * fi0);
+      q[3 * (i + 2) + 2] = c;
+      q[3 * (i + 7) + 0] = s * std::cos((rk2 + 1) * fi0);
+      q[3 * (i + 7) + 1] = s * std::sin((rk2 + 1) * fi0);
+      q[3 * (i + 7) + 2] = -c;
+    }
+    wq.assign(12, 1.0 / 12.0);
+  } else {
+    throw InputError("AIP >= 18 quadratures are not supported (use 4, 6 or 12)");
+  }
+}
+
+static double pp_radial(const PPAtom& P, int l, double r) {
+  double v = 0;
+  for (int t = P.term_first[l]; t < P.term_first[l + 1]; t++) {
+    double ex = std::min(P.term_a[t] * r * r, 60.0);
+    v += P.term_c[t] * std::pow(r, P.term_n[t]) * std::exp(-ex);
+  }
+  return v;
+}
+
+HostSystem build_system(const std::string& deck_path) {
+  HostSystem S;
+  S.deck_path = deck_path;
+  auto words = tokenize_file(deck_path);
+  std::string base = dirname_of(deck_path);
+
+  // ---- SYSTEM
+  auto sysw = get_section(words, "SYSTEM");
+  if (sysw.empty() || !(ieq(sysw[0], "MOLECULE") || ieq(sysw[0], "MOLECULAR")))
+    throw InputError("only SYSTEM { MOLECULE } is supported by this engine build");
+  auto ns = get_section(sysw, "NSPIN");
+  if (ns.size() != 2) throw InputError("NSPIN needs two numbers");
+  S.nup = to_i(ns[0]);
+  S.ndn = to_i(ns[1]);
+  S.nelec = S.nup + S.ndn;
+  for (auto& a : all_sections(sysw, "ATOM")) {
+    if (a.size() < 2) throw InputError("bad ATOM section");
+    S.labels.push_back(a[0]);
+    S.atom_charge.push_back(to_d(a[1]));
+    size_t k = 0;
+    while (k < a.size() && !ieq(a[k], "COOR")) k++;
+    if (k + 3 >= a.size()) throw InputError("ATOM needs COOR x y z");
+    for (int d = 0; d < 3; d++) S.atom_pos.push_back(to_d(a[k + 1 + d]));
+  }
+  S.natoms = (int)S.labels.size();
+  if (S.natoms == 0) throw InputError("no ATOM in SYSTEM");
+  if (S.nelec <= 0 || S.nup < 0 || S.ndn < 0) throw InputError("bad NSPIN");
+  for (int i = 0; i < S.natoms; i++)
+    for (int j = 0; j < i; j++) {
+      double d2 = 0;
+      for (int d = 0; d < 3; d++) {
+        double t = S.atom_pos[3 * i + d] - S.atom_pos[3 * j + d];
+        d2 += t * t;
+      }
+      S.ion_ion += S.atom_charge[i] * S.atom_charge[j] / std::sqrt(d2);
+    }
+
+  // ---- TRIALFUNC
+  auto tf = get_section(words, "TRIALFUNC");
+  if (tf.empty() || !ieq(tf[0], "SLATER-JASTROW"))
+    throw InputError("TRIALFUNC must be SLATER-JASTROW");
+  auto wf1 = get_section(tf, "WF1");
+  auto wf2 = get_section(tf, "WF2");
+  if (wf1.empty() || !ieq(wf1[0], "SLATER")) throw InputError("WF1 must be SLATER");
+  if (wf2.empty() || !ieq(wf2[0], "JASTROW2")) throw InputError("WF2 must be JASTROW2");
+
+  // Slater: single determinant
+  auto detwt = get_section(wf1, "DETWT");
+  if (detwt.size() != 1) throw InputError("only single-determinant SLATER is supported");
+  if (has_section(wf1, "CSF")) throw InputError("CSF expansions are not supported");
+  auto orbw = get_section(wf1, "ORBITALS");
+  if (!orbw.empty() && (ieq(orbw[0], "CUTOFF_MO") || ieq(orbw[0], "EINSPLINE_MO") || ieq(orbw[0], "BASFUNC_MO")))
+    throw InputError("ORBITALS type " + orbw[0] + " not supported (the dense BLAS_MO evaluator is used)");
+  std::string tmp;
+  if (!find_value(orbw, "NMO", tmp)) throw InputError("Need NMO in molecular orbital section");
+  int nmo = to_i(tmp);
+  std::vector<std::vector<double>> tables;
+  std::vector<BasisObj> bases;
+  for (auto& b : all_sections(orbw, "BASIS")) bases.push_back(read_aospline(b, S, tables));
+  if (bases.empty()) throw InputError("Didn't find a BASIS section");
+  size_t cpos = 0;
+  std::vector<std::string> cent;
+  if (find_section(orbw, "CENTERS", cpos, cent) && !has_keyword(cent, "USEATOMS") && !has_keyword(cent, "USEGLOBAL"))
+    throw InputError("CENTERS must be USEATOMS or USEGLOBAL");
+  std::vector<int> nfunc_center(S.natoms, 0);
+  int first = 0;
+  for (int c = 0; c < S.natoms; c++) {
+    for (auto& B : bases) {
+      if (B.label != S.labels[c]) continue;
+      for (size_t k = 0; k < B.syms.size(); k++) {
+        Shell sh;
+        sh.center = c;
+        sh.spline = B.spline_ids[k];
+        sh.sym = B.syms[k];
+        sh.first = first;
+        sh.nfunc = sym_nfunc(B.syms[k]);
+        sh.cutoff = B.threshold;
+        first += sh.nfunc;
+        S.shells.push_back(sh);
+      }
+      nfunc_center[c] += B.nfunc;
+    }
+  }
+  S.nbasis = first;
+  // flatten spline tables (all share npts after padding to the longest)
+  size_t maxlen = 0;
+  for (auto& t : tables) maxlen = std::max(maxlen, t.size());
+  S.spline_npts = (int)(maxlen / 4);
+  S.spline_coef.assign(tables.size() * maxlen, 0.0);
+  for (size_t i = 0; i < tables.size(); i++) std::copy(tables[i].begin(), tables[i].end(), S.spline_coef.begin() + i * maxlen);
+
+  std::string orbfile;
+  if (!find_value(orbw, "ORBFILE", orbfile)) throw InputError("Must specify ORBFILE for MO matrix");
+  if (orbfile[0] != '/' && !file_exists(orbfile)) orbfile = base + "/" + orbfile;
+  std::vector<double> moc_all;
+  read_orb(orbfile, nmo, nfunc_center, moc_all);
+  auto states = get_section(wf1, "STATES");
+  if ((int)states.size() != S.nelec) throw InputError("STATES must list nup+ndown orbitals");
+  for (int s = 0; s < 2; s++) {
+    int ne = s == 0 ? S.nup : S.ndn, off = s == 0 ? 0 : S.nup;
+    S.nmo[s] = ne;
+    S.moc[s].assign((size_t)S.nbasis * std::max(ne, 1), 0.0);
+    for (int i = 0; i < ne; i++) {
+      int mo = to_i(states[off + i]) - 1;
+      if (mo < 0 || mo >= nmo) throw InputError("STATES entry beyond NMO");
+      for (int f = 0; f < S.nbasis; f++) S.moc[s][(size_t)f * ne + i] = moc_all[(size_t)f * nmo + mo];
+    }
+  }
+
+  // ---- Jastrow groups
+  S.ei_first.assign(S.natoms, 0);
+  S.ei_count.assign(S.natoms, 0);
+  std::vector<std::vector<Radial>> ei_at(S.natoms);
+  std::vector<std::vector<double>> ob_at(S.natoms);
+  std::vector<std::vector<ThreeBodyTerm>> tb_at(S.natoms);
+  static const int klm_default[12][3] = {{1, 1, 0}, {1, 0, 1}, {1, 1, 1}, {2, 2, 0}, {2, 0, 1}, {2, 0, 2},
+                                         {2, 2, 2}, {3, 3, 0}, {3, 0, 2}, {3, 3, 2}, {1, 2, 2}, {2, 3, 2}};
+  for (auto& g : all_sections(wf2, "GROUP")) {
+    int ee0 = (int)S.ee.size();
+    for (auto& b : all_sections(g, "EEBASIS")) {
+      auto r = read_radial(b);
+      S.ee.insert(S.ee.end(), r.begin(), r.end());
+    }
+    int nee_g = (int)S.ee.size() - ee0;
+    S.ee_like.resize(S.ee.size(), 0.0);
+    S.ee_unlike.resize(S.ee.size(), 0.0);
+    // e-n functions of this group, per atom, in EIBASIS order
+    std::vector<int> ei0(S.natoms);
+    for (int a = 0; a < S.natoms; a++) ei0[a] = (int)ei_at[a].size();
+    for (auto& b : all_sections(g, "EIBASIS")) {
+      auto r = read_radial(b);
+      bool found = false;
+      for (int a = 0; a < S.natoms; a++)
+        if (S.labels[a] == b[0]) { ei_at[a].insert(ei_at[a].end(), r.begin(), r.end()); found = true; }
+      if (!found) throw InputError("Couldn't find center for basis label " + b[0]);
+    }
+    for (int a = 0; a < S.natoms; a++) ob_at[a].resize(ei_at[a].size(), 0.0);
+    size_t pos = 0;
+    std::vector<std::string> sec;
+    if (find_section(g, "ONEBODY", pos, sec)) {
+      for (auto& c : all_sections(sec, "COEFFICIENTS")) {
+        bool found = false;
+        for (int a = 0; a < S.natoms; a++) {
+          if (S.labels[a] != c[0]) continue;
+          found = true;
+          int np = (int)c.size() - 1;
+          if (np > (int)ei_at[a].size() - ei0[a]) throw InputError("ONEBODY has more coefficients than EIBASIS functions");
+          for (int i = 0; i < np; i++) ob_at[a][ei0[a] + i] += to_d(c[i + 1]);
+        }
+        if (!found) throw InputError("Couldn't find a matching center for " + c[0]);
+      }
+    }
+    bool has2 = false;
+    pos = 0;
+    if (find_section(g, "TWOBODY_SPIN", pos, sec)) {
+      auto like = get_section(sec, "LIKE_COEFFICIENTS");
+      auto unlike = get_section(sec, "UNLIKE_COEFFICIENTS");
+      if (like.size() != unlike.size()) throw InputError("TWOBODY_SPIN like/unlike sizes differ");
+      if ((int)like.size() > nee_g) throw InputError("Not enough EE basis functions for TWOBODY_SPIN");
+      for (size_t p = 0; p < like.size(); p++) {
+        S.ee_like[ee0 + p] += to_d(like[p]);
+        S.ee_unlike[ee0 + p] += to_d(unlike[p]);
+      }
+      has2 = true;
+    }
+    pos = 0;
+    if (find_section(g, "TWOBODY", pos, sec)) {
+      if (has2) throw InputError("Can only have one of TWOBODY_SPIN or TWOBODY");
+      auto c = get_section(sec, "COEFFICIENTS");
+      if ((int)c.size() > nee_g) throw InputError("Not enough EE basis functions for TWOBODY");
+      for (size_t p = 0; p < c.size(); p++) {
+        S.ee_like[ee0 + p] += to_d(c[p]);
+        S.ee_unlike[ee0 + p] += to_d(c[p]);
+      }
+    }
+    pos = 0;
+    if (find_section(g, "THREEBODY", pos, sec)) {
+      if (has_section(sec, "SM_TERMS")) throw InputError("custom SM_TERMS are not supported");
+      double scale = value_d(sec, "SCALE", 1.0);
+      for (auto& c : all_sections(sec, "COEFFICIENTS")) {
+        int np = (int)c.size() - 1;
+        if (np > 12) throw InputError("too many three-body parameters");
+        for (int a = 0; a < S.natoms; a++) {
+          if (S.labels[a] != c[0]) continue;
+          for (int i = 0; i < np; i++) {
+            ThreeBodyTerm t;
+            t.k = ei0[a] + klm_default[i][0];
+            t.l = ei0[a] + klm_default[i][1];
+            t.m = ee0 + klm_default[i][2];
+            t.c = to_d(c[i + 1]) * scale;
+            if (klm_default[i][0] >= (int)ei_at[a].size() - ei0[a] || klm_default[i][1] >= (int)ei_at[a].size() - ei0[a] ||
+                klm_default[i][2] >= nee_g)
+              throw InputError("Threebody needs more basis functions");
+            tb_at[a].push_back(t);
+          }
+        }
+      }
+    }
+    if (has_section(g, "THREEBODY_SPIN")) throw InputError("THREEBODY_SPIN is not supported");
+  }
+  for (int a = 0; a < S.natoms; a++) {
+    S.ei_first[a] = (int)S.ei.size();
+    S.ei_count[a] = (int)ei_at[a].size();
+    // three-body indices were per atom slice: rebase to the global list
+    for (auto& t : tb_at[a]) { t.k += S.ei_first[a]; t.l += S.ei_first[a]; }
+    S.ei.insert(S.ei.end(), ei_at[a].begin(), ei_at[a].end());
+    S.onebody.insert(S.onebody.end(), ob_at[a].begin(), ob_at[a].end());
+  }
+  S.tb_first.assign(S.natoms, 0);
+  S.tb_count.assign(S.natoms, 0);
+  for (int a = 0; a < S.natoms; a++) {
+    S.tb_first[a] = (int)S.tb.size();
+    S.tb_count[a] = (int)tb_at[a].size();
+    S.tb.insert(S.tb.end(), tb_at[a].begin(), tb_at[a].end());
+  }
+
+  // ---- PSEUDO
+  S.pp.assign(S.natoms, PPAtom());
+  for (auto& t : all_sections(words, "PSEUDO")) {
+    if (has_keyword(t, "SPIN_DEP")) throw InputError("SPIN_DEP pseudopotentials are not supported");
+    if (has_keyword(t, "ADD_ZEFF")) throw InputError("ADD_ZEFF is not supported");
+    PPAtom P;
+    P.aip = (int)value_d(t, "AIP", 6);
+    auto bw = get_section(t, "BASIS");
+    if (bw.size() < 2 || !ieq(bw[1], "RGAUSSIAN")) throw InputError("PSEUDO BASIS must be RGAUSSIAN");
+    auto oq = get_section(bw, "OLDQMC");
+    if (oq.size() < 2) throw InputError("badly formed OLDQMC section");
+    size_t it = 1;
+    P.nchan = to_i(oq[it++]);
+    std::vector<int> nper(P.nchan);
+    for (int l = 0; l < P.nchan; l++) nper[l] = to_i(oq[it++]);
+    P.term_first.push_back(0);
+    for (int l = 0; l < P.nchan; l++) {
+      for (int j = 0; j < nper[l]; j++) {
+        if (it + 2 >= oq.size()) throw InputError("truncated OLDQMC section");
+        P.term_n.push_back(to_d(oq[it]) - 2.0);
+        P.term_a.push_back(to_d(oq[it + 1]));
+        P.term_c.push_back(to_d(oq[it + 2]));
+        it += 3;
+      }
+      P.term_first.push_back((int)P.term_n.size());
+    }
+    gesqua(P.aip, P.quad, P.weight);
+    // evaluation radius: scan from 20 bohr down in 0.05 steps for the first
+    // |v_l| > 1e-5 of each nonlocal channel (a channel never above it keeps 20)
+    std::vector<double> cutL(std::max(P.nchan - 1, 0), 20.0);
+    std::vector<int> found(cutL.size(), 0);
+    for (double r = 20.0; r > 0; r -= 0.05)
+      for (int l = 0; l + 1 < P.nchan; l++)
+        if (std::fabs(pp_radial(P, l, r)) > 1e-5 && !found[l]) { cutL[l] = r - 0.05; found[l] = 1; }
+    P.cutoff = 0;
+    for (double c : cutL) P.cutoff = std::max(P.cutoff, c);
+    bool any = false;
+    for (int a = 0; a < S.natoms; a++)
+      if (S.labels[a] == t[0]) {
+        if (S.pp[a].nchan) throw InputError("There are two PSEUDO sections for " + t[0]);
+        S.pp[a] = P;
+        any = true;
+      }
+    (void)any;
+    S.has_pp = true;
+    S.max_aip = std::max(S.max_aip, P.aip);
+  }
+  return S;
+}
+
+}  // namespace qwg

@@ -1,0 +1,98 @@
+// Host side of the walker engine: QWalk input grammar and the flat tables the
+// kernels consume.  Built once per context on the host, then uploaded.
+#pragma once
+#include <string>
+#include <vector>
+#include <stdexcept>
+
+namespace qwg {
+
+struct InputError : std::runtime_error {
+  explicit InputError(const std::string& m) : std::runtime_error(m) {}
+};
+
+// Token list of a QWalk input file: '{' and '}' are words of their own, '#'
+// starts a comment, INCLUDE <file> splices another file in place
+// (program_utils/qmc_io.cpp:280-345).
+std::vector<std::string> tokenize_file(const std::string& path);
+
+// Level-0 section / value lookups (program_utils/qmc_io.cpp:168-230,
+// qmc_io.h:62-124).  Keys compare case-insensitively.
+bool find_section(const std::vector<std::string>& w, const std::string& name, size_t& pos,
+                  std::vector<std::string>& out);
+std::vector<std::vector<std::string>> all_sections(const std::vector<std::string>& w, const std::string& name);
+bool has_section(const std::vector<std::string>& w, const std::string& name);
+bool find_value(const std::vector<std::string>& w, const std::string& name, std::string& out);
+bool has_keyword(const std::vector<std::string>& w, const std::string& name);
+
+enum ShellSym { SYM_S = 0, SYM_P = 1, SYM_6D = 2, SYM_5D = 3 };
+enum RadialKind { RAD_CUTOFF_CUSP = 0, RAD_POLYPADE = 1 };
+
+// One radial spline x Cartesian angular set attached to one center.
+struct Shell {
+  int center;      // atom index
+  int spline;      // radial table index
+  int sym;         // ShellSym
+  int first;       // first basis function (global index)
+  int nfunc;
+  double cutoff;   // basis-object threshold: r >= cutoff gives zero
+};
+
+// A scalar Jastrow radial function (f, f'/r, lap).
+struct Radial {
+  int kind;        // RadialKind
+  double rcut;
+  double a, b;     // CUTOFF_CUSP: cusp, gamma ; POLYPADE: beta, unused
+};
+
+struct ThreeBodyTerm {
+  int k, l, m;     // global e-n (per atom) function indices k,l and e-e index m
+  double c;
+};
+
+struct PPAtom {
+  int nchan = 0;                 // channels incl. the local one (last)
+  int aip = 0;                   // quadrature points
+  double cutoff = 0.0;           // nonlocal evaluation radius
+  std::vector<int> term_first;   // [nchan+1]
+  std::vector<double> term_n;    // r power (already n-2)
+  std::vector<double> term_a;    // Gaussian exponent
+  std::vector<double> term_c;    // coefficient
+  std::vector<double> quad;      // [aip][3]
+  std::vector<double> weight;    // [aip]
+};
+
+struct HostSystem {
+  std::string deck_path;
+  int nup = 0, ndn = 0, nelec = 0, natoms = 0;
+  std::vector<std::string> labels;
+  std::vector<double> atom_pos;      // [A][3]
+  std::vector<double> atom_charge;   // [A]
+  double ion_ion = 0.0;
+  // basis
+  std::vector<Shell> shells;
+  int nbasis = 0;
+  int nspline = 0, spline_npts = 0;
+  double spline_spacing = 0.02;
+  std::vector<double> spline_coef;   // [nspline][npts][4]
+  // molecular orbitals per spin: [nbasis][m_s]
+  int nmo[2] = {0, 0};
+  std::vector<double> moc[2];
+  // Jastrow
+  std::vector<Radial> ee;            // global e-e function list
+  std::vector<double> ee_like, ee_unlike;  // two-body coefficients per ee function
+  std::vector<Radial> ei;            // global e-n function list
+  std::vector<int> ei_first, ei_count;     // per atom slice into ei
+  std::vector<double> onebody;       // per ei function (already per atom slice)
+  std::vector<int> tb_first, tb_count;     // per atom slice into tb
+  std::vector<ThreeBodyTerm> tb;
+  // pseudopotential (per atom; nchan == 0 if none)
+  std::vector<PPAtom> pp;
+  bool has_pp = false;
+  int max_aip = 0;
+};
+
+// Parse the deck and build every table (throws InputError).
+HostSystem build_system(const std::string& deck_path);
+
+}  // namespace qwg

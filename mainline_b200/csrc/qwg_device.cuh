@@ -1,0 +1,562 @@
+// Device code of the B200 walker engine.
+//
+// Execution model: one warp owns one walker for a whole kernel (a DMC
+// feedback interval or a VMC block).  The walker's state -- positions, the
+// transposed inverse Slater matrices of both spins, the MO gradient/Laplacian
+// rows of every electron, the Jastrow gradient/Laplacian sums -- lives in
+// shared memory while the warp works on it and is written back to its HBM
+// slot once at the end.  Read-only tables (radial spline coefficients, MO
+// coefficients, Jastrow and pseudopotential parameters) are shared by all
+// walkers: MO coefficients are staged into shared memory per CTA, splines are
+// read through L1/L2 (they fit in L2 many times over).
+//
+// Within a walker, lanes split the independent pieces of each phase: basis
+// shells for one position, (MO, component) outputs of the MO contraction,
+// electrons or pairs for the Jastrow, quadrature points for the pseudopotential
+// (one lane evaluates a whole point: basis, MOs, determinant ratio and
+// Jastrow).  Phases communicate through shared memory with __syncwarp().
+//
+// Real = double: everything in FP64.  Real = float (mixed precision): basis,
+// MO values, determinant ratios, inverse and its Sherman-Morrison updates in
+// FP32; the periodic full re-inversion (Gauss-Jordan), log|det|, Jastrow sums,
+// local energies and weights in FP64.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace qwg {
+
+// ---------------------------------------------------------------------------
+// tables
+
+struct DRadial {
+  int kind;         // 0 CUTOFF_CUSP, 1 POLYPADE
+  double rcut, a, b;
+};
+struct DTB {
+  int k, l, m;
+  double c;
+};
+
+template <typename Real>
+struct DevSys {
+  int nelec, nup, ndn, natoms, nbasis, nshell;
+  int m[2];                      // MOs per spin (= electrons per spin)
+  int mstride;                   // padded MO stride of moc rows (= MMAX)
+  const double* atom_pos;        // [A][3]
+  const double* atom_charge;     // [A]
+  double ion_ion;
+  const int4* shell_i;           // (center, spline, sym, first)
+  const double* shell_cut;       // [nshell]
+  const Real* spline;            // [nspline][npts][4] (Real: used by value-only points)
+  const double* spline64;        // [nspline][npts][4] FP64 copy (value/gradient/Laplacian)
+  int npts;
+  double spacing, inv_spacing;
+  const Real* moc;               // [2][nbasis][mstride]
+  // Jastrow
+  int nee;
+  const DRadial* ee;             // [nee]
+  const double* ee_like;         // [nee]
+  const double* ee_unlike;       // [nee]
+  const DRadial* ei;             // [nei]
+  const int* ei_first;           // [A]
+  const int* ei_count;           // [A]
+  const double* onebody;         // [nei]
+  const int* tb_first;           // [A]
+  const int* tb_count;           // [A]
+  const DTB* tb;
+  int max_ei;                    // max functions on one atom
+  // pseudopotential
+  int has_pp;
+  const int* pp_nchan;           // [A] (0: none)
+  const int* pp_aip;             // [A]
+  const double* pp_cutoff;       // [A]
+  const int* pp_term_first;      // [A][8] offsets (nchan+1 used)
+  const double* pp_term;         // [nterm][3] = (n, a, c)
+  const double* pp_quad;         // [A][maxaip][3]
+  const double* pp_w;            // [A][maxaip]
+  int max_aip;
+};
+
+// Per-walker shared-memory layout (byte offsets, host computed).
+struct WLayout {
+  int R, inv, mov, gU, lU, scal, bas, newcol, dG, Ue, lu, items, rot, bytes;
+  int state_bytes;  // prefix [0, state_bytes) is the persistent walker state
+};
+
+// Persistent scalars of a walker (inside the state prefix).
+struct WScal {
+  double logdet[2];
+  double sign[2];
+  double U;
+  double eold;      // previous local energy (DMC weight)
+  double weight;
+  double pad;
+};
+
+struct BlockAcc {   // per-launch reduction target (double atomics)
+  double sum_w, sum_we, sum_wk, sum_wv, sum_wnl, sum_we2, accepted, attempted;
+  double nonfinite, npts;
+};
+
+// Launch parameters shared by the step kernels.
+struct StepParams {
+  int nwalk;
+  int nsteps;
+  int refresh;          // 1: full recompute at start (else load state)
+  int dmc;              // 1: DMC weights + node restriction
+  int deterministic_pp;
+  double tau;           // move time step
+  double teff;          // DMC effective time step (weights)
+  const double* etrial; // device scalar
+  double branch_start, branch_stop, max_weight;
+  uint64_t seed;
+  uint64_t step0;       // global step counter of the first step
+  double* R;            // [W][N][3]
+  unsigned char* state; // [W][state_bytes]
+  BlockAcc* acc;
+};
+
+// ---------------------------------------------------------------------------
+// counter-based RNG: Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) and
+// Box-Muller normals.
+
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox4x32(U4 c, uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+    uint32_t hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+    U4 n;
+    n.x = hi1 ^ c.y ^ k0;
+    n.y = lo1;
+    n.z = hi0 ^ c.w ^ k1;
+    n.w = lo0;
+    c = n;
+    k0 += W0;
+    k1 += W1;
+  }
+  return c;
+}
+
+// uniform in (0, 1]
+__device__ __forceinline__ double u01(uint32_t a) { return (double(a) + 1.0) * (1.0 / 4294967296.0); }
+
+struct Rand4 { double u[4]; };
+
+__device__ __forceinline__ Rand4 rand4(uint64_t seed, uint32_t walker, uint64_t step, uint32_t e, uint32_t purpose) {
+  U4 c;
+  c.x = walker;
+  c.y = (uint32_t)step;
+  c.z = (uint32_t)(step >> 32) ^ (e << 8) ^ purpose;
+  c.w = purpose * 0x9E3779B9u + e;
+  U4 r = philox4x32(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  Rand4 o;
+  o.u[0] = u01(r.x); o.u[1] = u01(r.y); o.u[2] = u01(r.z); o.u[3] = u01(r.w);
+  return o;
+}
+
+__device__ __forceinline__ void box_muller(double u1, double u2, double& g1, double& g2) {
+  double rad = sqrt(-2.0 * log(u1));
+  double s, c;
+  sincospi(2.0 * u2, &s, &c);
+  g1 = rad * c;
+  g2 = rad * s;
+}
+
+// ---------------------------------------------------------------------------
+// warp helpers
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// radial functions
+
+// Cubic spline: f, f'/r, f'' at r (r < table threshold); s = spline index.
+template <typename Real>
+__device__ __forceinline__ void spline_lap(const DevSys<Real>& S, int s, Real r, Real& f, Real& fd, Real& f2) {
+  int i = int(r * Real(S.inv_spacing));
+  Real h = r - Real(i) * Real(S.spacing);
+  const Real* c = S.spline + ((size_t)s * S.npts + i) * 4;
+  Real c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2), c3 = __ldg(c + 3);
+  f = c0 + h * (c1 + h * (c2 + h * c3));
+  fd = (c1 + h * (Real(2) * c2 + h * (Real(3) * c3))) / r;
+  f2 = Real(2) * c2 + Real(6) * h * c3;
+}
+template <typename Real>
+__device__ __forceinline__ Real spline_val(const DevSys<Real>& S, int s, Real r) {
+  int i = int(r * Real(S.inv_spacing));
+  Real h = r - Real(i) * Real(S.spacing);
+  const Real* c = S.spline + ((size_t)s * S.npts + i) * 4;
+  return __ldg(c) + h * (__ldg(c + 1) + h * (__ldg(c + 2) + h * __ldg(c + 3)));
+}
+
+// Jastrow radial function (value, f'/r, 3D Laplacian).  Zero at r >= rcut.
+template <typename T>
+__device__ __forceinline__ void radial_lap(const DRadial& q, T r, T& f, T& fd, T& lap) {
+  if (!(r < T(q.rcut))) { f = fd = lap = T(0); return; }
+  const T rcut = T(q.rcut);
+  if (q.kind == 0) {  // CUTOFF_CUSP (cusp a, gamma b)
+    const T cusp = T(q.a), gamma = T(q.b);
+    T zz = r / rcut, zz2 = zz * zz;
+    T pp = zz - zz2 + zz * zz2 / T(3);
+    T pade = T(1) / (T(1) + gamma * pp);
+    T pade0 = T(1) / (T(3) + gamma);
+    f = cusp * rcut * (pp * pade - pade0);
+    T pade2 = pade * pade;
+    T ppd = T(1) - T(2) * zz + zz2;
+    T ppdd = T(-2) + T(2) * zz;
+    T dadr = ppd * pade2 / r;
+    fd = cusp * dadr;
+    lap = cusp * (ppdd * pade2 / rcut - T(2) * gamma * ppd * ppd * pade2 * pade / rcut + T(2) * dadr);
+  } else {            // POLYPADE (beta a)
+    const T beta = T(q.a);
+    T zz = r / rcut, zz2 = zz * zz;
+    T zpp = zz2 * (T(6) - T(8) * zz + T(3) * zz2);
+    T zppd = T(12) * zz * (T(1) - T(2) * zz + zz2);
+    T zppdd2 = T(6) - T(24) * zz + T(18) * zz2;
+    T zpade = T(1) / (T(1) + beta * zpp), zpade2 = zpade * zpade;
+    f = (T(1) - zpp) * zpade;
+    fd = -zppd * zpade2 * (beta + T(1)) / (r * rcut);
+    T crsdd2 = -zpade2 * (zppdd2 - beta * zppd * zppd * zpade) * (beta + T(1)) / (rcut * rcut);
+    lap = T(2) * (crsdd2 + fd);
+  }
+}
+template <typename T>
+__device__ __forceinline__ T radial_val(const DRadial& q, T r) {
+  T f, fd, l;
+  if (!(r < T(q.rcut))) return T(0);
+  radial_lap(q, r, f, fd, l);
+  return f;
+}
+
+// ---------------------------------------------------------------------------
+// angular parts of a shell: fills v[k][5] = (value, d/dx, d/dy, d/dz, lap) of
+// the Cartesian Gaussian-type function A(x,y,z) f(r) from f, f'/r, f''.
+// lap = A f'' + (2l+2) A f'/r + f lap(A) for a homogeneous A of degree l.
+template <typename Real>
+__device__ __forceinline__ int shell_lap(int sym, Real x, Real y, Real z, Real f, Real fd, Real f2, Real v[6][5]) {
+  auto put = [&](int k, Real A, Real ax, Real ay, Real az, Real lapA, int l) {
+    Real h = A * fd;
+    v[k][0] = A * f;
+    v[k][1] = h * x + ax * f;
+    v[k][2] = h * y + ay * f;
+    v[k][3] = h * z + az * f;
+    v[k][4] = A * f2 + Real(2 * l + 2) * h + lapA * f;
+  };
+  const Real o = Real(1), zr = Real(0);
+  switch (sym) {
+    case 0: put(0, o, zr, zr, zr, zr, 0); return 1;
+    case 1:
+      put(0, x, o, zr, zr, zr, 1); put(1, y, zr, o, zr, zr, 1); put(2, z, zr, zr, o, zr, 1);
+      return 3;
+    case 2:
+      put(0, x * x, Real(2) * x, zr, zr, Real(2), 2);
+      put(1, y * y, zr, Real(2) * y, zr, Real(2), 2);
+      put(2, z * z, zr, zr, Real(2) * z, Real(2), 2);
+      put(3, x * y, y, x, zr, zr, 2);
+      put(4, x * z, z, zr, x, zr, 2);
+      put(5, y * z, zr, z, y, zr, 2);
+      return 6;
+    default:
+      put(0, Real(2) * z * z - x * x - y * y, Real(-2) * x, Real(-2) * y, Real(4) * z, zr, 2);
+      put(1, x * z, z, zr, x, zr, 2);
+      put(2, y * z, zr, z, y, zr, 2);
+      put(3, x * x - y * y, Real(2) * x, Real(-2) * y, zr, zr, 2);
+      put(4, x * y, y, x, zr, zr, 2);
+      return 5;
+  }
+}
+template <typename Real>
+__device__ __forceinline__ int shell_val(int sym, Real x, Real y, Real z, Real f, Real v[6]) {
+  switch (sym) {
+    case 0: v[0] = f; return 1;
+    case 1: v[0] = x * f; v[1] = y * f; v[2] = z * f; return 3;
+    case 2:
+      v[0] = x * x * f; v[1] = y * y * f; v[2] = z * z * f;
+      v[3] = x * y * f; v[4] = x * z * f; v[5] = y * z * f;
+      return 6;
+    default:
+      v[0] = (Real(2) * z * z - x * x - y * y) * f; v[1] = x * z * f; v[2] = y * z * f;
+      v[3] = (x * x - y * y) * f; v[4] = x * y * f;
+      return 5;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MO evaluation (value, gradient, Laplacian) of one position, warp-cooperative.
+// bas: [nbasis][5] scratch; out: [M][5]; moc_s: [nbasis][mstride] (shared).
+// A basis function whose value is within 1e-8 of zero contributes nothing
+// (the dense MO evaluator's skip, MO_matrix_blas.h:468-470).
+template <typename Real>
+__device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz, int M,
+                            Real* bas, Real* out, int lane) {
+  // radial spline and angular factors in FP64 (the Laplacian of the tight
+  // shells cancels strongly); the basis values are then stored as Real
+  for (int s = lane; s < S.nshell; s += 32) {
+    int4 si = S.shell_i[s];
+    const double* ap = S.atom_pos + 3 * si.x;
+    double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    double v[6][5];
+    int nf;
+    if (r < S.shell_cut[s]) {
+      int i = int(r * S.inv_spacing);
+      double h = r - double(i) * S.spacing;
+      const double2* c2p = reinterpret_cast<const double2*>(S.spline64 + ((size_t)si.y * S.npts + i) * 4);
+      double2 ca = __ldg(c2p), cb = __ldg(c2p + 1);
+      double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
+      double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
+      double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
+      nf = shell_lap(si.z, dx, dy, dz, f, fd, f2, v);
+      for (int k = 0; k < nf; k++)
+        if (!(fabs(v[k][0]) > 1e-8))
+          for (int c = 0; c < 5; c++) v[k][c] = 0.0;
+    } else {
+      nf = si.z == 0 ? 1 : si.z == 1 ? 3 : si.z == 2 ? 6 : 5;
+      for (int k = 0; k < nf; k++)
+        for (int c = 0; c < 5; c++) v[k][c] = 0.0;
+    }
+    for (int k = 0; k < nf; k++)
+      for (int c = 0; c < 5; c++) bas[(si.w + k) * 5 + c] = Real(v[k][c]);
+  }
+  __syncwarp();
+  const int nout = M * 5;
+  for (int o = lane; o < nout; o += 32) {
+    int mo = o / 5, c = o - mo * 5;
+    Real acc = Real(0);
+    const Real* b = bas + c;
+    const Real* w = moc_s + mo;
+    for (int f = 0; f < S.nbasis; f++) acc += b[f * 5] * w[f * S.mstride];
+    out[mo * 5 + c] = acc;
+  }
+  __syncwarp();
+}
+
+// MO values of one position evaluated entirely by the calling lane.
+template <typename Real, int MMAX>
+__device__ __forceinline__ void mo_val_lane(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz,
+                                            Real phi[MMAX]) {
+#pragma unroll
+  for (int m = 0; m < MMAX; m++) phi[m] = Real(0);
+  for (int s = 0; s < S.nshell; s++) {
+    int4 si = S.shell_i[s];
+    const double* ap = S.atom_pos + 3 * si.x;
+    double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(r < S.shell_cut[s])) continue;
+    Real f = spline_val(S, si.y, Real(r));
+    Real v[6];
+    int nf = shell_val(si.z, Real(dx), Real(dy), Real(dz), f, v);
+    for (int k = 0; k < nf; k++) {
+      if (!(fabs(double(v[k])) > 1e-8)) continue;
+      const Real* w = moc_s + (size_t)(si.w + k) * MMAX;
+#pragma unroll
+      for (int m = 0; m < MMAX; m++) phi[m] += v[k] * w[m];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Jastrow pieces (all in double: a few hundred flops per electron)
+
+// Two-body u(r_ij) for a pair of given spins: value, f'/r, lap.
+template <typename Real>
+__device__ __forceinline__ void jas_pair(const DevSys<Real>& S, bool same, double r, double& u, double& fd, double& lap) {
+  u = fd = lap = 0.0;
+  for (int k = 0; k < S.nee; k++) {
+    double c = same ? S.ee_like[k] : S.ee_unlike[k];
+    if (c == 0.0) continue;
+    double f, d, l;
+    radial_lap(S.ee[k], r, f, d, l);
+    u += c * f; fd += c * d; lap += c * l;
+  }
+}
+
+// One-body sum over atoms for an electron at p: value, gradient, lap.
+template <typename Real>
+__device__ __forceinline__ void jas_onebody(const DevSys<Real>& S, double px, double py, double pz, double& u,
+                                            double g[3], double& lap) {
+  u = 0; g[0] = g[1] = g[2] = 0; lap = 0;
+  for (int a = 0; a < S.natoms; a++) {
+    const double* ap = S.atom_pos + 3 * a;
+    double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    int f0 = S.ei_first[a], nf = S.ei_count[a];
+    for (int k = 0; k < nf; k++) {
+      double c = S.onebody[f0 + k];
+      if (c == 0.0) continue;
+      double f, d, l;
+      radial_lap(S.ei[f0 + k], r, f, d, l);
+      u += c * f; g[0] += c * d * dx; g[1] += c * d * dy; g[2] += c * d * dz; lap += c * l;
+    }
+  }
+}
+
+// Three-body (e-e-n) contribution of the pair (i, j) at all atoms, with
+// gradients/laps for both electrons.  di: r_i - atom, dj: r_j - atom.
+template <typename Real>
+__device__ void jas_threebody_pair(const DevSys<Real>& S, const double pi[3], const double pj[3], double& u,
+                                   double gi[3], double& li, double gj[3], double& lj, bool need_derivs) {
+  u = 0; li = lj = 0;
+  for (int d = 0; d < 3; d++) gi[d] = gj[d] = 0;
+  double dij[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
+  double rij = sqrt(dij[0] * dij[0] + dij[1] * dij[1] + dij[2] * dij[2]);
+  for (int a = 0; a < S.natoms; a++) {
+    int nt = S.tb_count[a];
+    if (!nt) continue;
+    const double* ap = S.atom_pos + 3 * a;
+    double di[3] = {pi[0] - ap[0], pi[1] - ap[1], pi[2] - ap[2]};
+    double dj[3] = {pj[0] - ap[0], pj[1] - ap[1], pj[2] - ap[2]};
+    double ri = sqrt(di[0] * di[0] + di[1] * di[1] + di[2] * di[2]);
+    double rj = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
+    for (int t = 0; t < nt; t++) {
+      DTB q = S.tb[S.tb_first[a] + t];
+      double aki, akdi, akli, akj, akdj, aklj, ali, aldi, alli, alj, aldj, allj, b, bd, bl;
+      radial_lap(S.ei[q.k], ri, aki, akdi, akli);
+      radial_lap(S.ei[q.k], rj, akj, akdj, aklj);
+      radial_lap(S.ei[q.l], ri, ali, aldi, alli);
+      radial_lap(S.ei[q.l], rj, alj, aldj, allj);
+      radial_lap(S.ee[q.m], rij, b, bd, bl);
+      double s = aki * alj + ali * akj;
+      u += q.c * s * b;
+      if (!need_derivs) continue;
+      double gsi[3], gsj[3], gb[3];
+      double dsi = 0, dsj = 0;
+      for (int d = 0; d < 3; d++) {
+        gsi[d] = akdi * di[d] * alj + aldi * di[d] * akj;
+        gsj[d] = aki * aldj * dj[d] + ali * akdj * dj[d];
+        gb[d] = bd * dij[d];
+        dsi += gsi[d] * gb[d];
+        dsj += gsj[d] * gb[d];
+      }
+      for (int d = 0; d < 3; d++) {
+        gi[d] += q.c * (gsi[d] * b + s * gb[d]);
+        gj[d] += q.c * (gsj[d] * b - s * gb[d]);
+      }
+      li += q.c * ((akli * alj + alli * akj) * b + s * bl + 2 * dsi);
+      lj += q.c * ((aki * allj + ali * aklj) * b + s * bl - 2 * dsj);
+    }
+  }
+}
+
+// Everything of the Jastrow exponent that depends on electron i placed at p
+// (others at R): value U_i (one-body + all pairs with i), gradient, lap.
+template <typename Real>
+__device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, double px, double py, double pz,
+                             double& u, double g[3], double& lap, bool need_derivs) {
+  double ob, og[3], ol;
+  jas_onebody(S, px, py, pz, ob, og, ol);
+  u = ob; lap = ol;
+  for (int d = 0; d < 3; d++) g[d] = og[d];
+  const bool si = i < S.nup;
+  const bool has3 = S.tb != nullptr;
+  const double pi[3] = {px, py, pz};
+  for (int j = 0; j < S.nelec; j++) {
+    if (j == i) continue;
+    double dx = px - R[3 * j], dy = py - R[3 * j + 1], dz = pz - R[3 * j + 2];
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    double pu, pfd, pl;
+    jas_pair(S, si == (j < S.nup), r, pu, pfd, pl);
+    u += pu; lap += pl;
+    g[0] += pfd * dx; g[1] += pfd * dy; g[2] += pfd * dz;
+    if (has3) {
+      double tu, tgi[3], tli, tgj[3], tlj;
+      jas_threebody_pair(S, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, need_derivs);
+      u += tu; lap += tli;
+      for (int d = 0; d < 3; d++) g[d] += tgi[d];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dense linear algebra in the warp
+
+// Gauss-Jordan inversion with partial pivoting of A (M x M, M <= 32, row-major,
+// A[e][i] = phi_i(r_e)) held in aug[M][2M] (double).  Writes the transposed
+// inverse invT[e][i] = (A^-1)[i][e] and returns log|det A| and its sign.
+// Singular: logdet = -1e201 (the log of an exact zero determinant).
+template <typename Real>
+__device__ void gj_inverse_warp(double* aug, int M, Real* invT, int invstride, double& logdet, double& sign, int lane) {
+  const int W = 2 * M;
+  for (int idx = lane; idx < M * M; idx += 32) {
+    int i = idx / M, k = idx - i * M;
+    aug[i * W + M + k] = (i == k) ? 1.0 : 0.0;
+  }
+  __syncwarp();
+  double ld = 0.0, sg = 1.0;
+  bool singular = false;
+  for (int k = 0; k < M; k++) {
+    // pivot search over rows k..M-1 (lane i looks at row i)
+    double best = -1.0;
+    int bi = k;
+    for (int i = k + lane; i < M; i += 32) {
+      double v = fabs(aug[i * W + k]);
+      if (v > best) { best = v; bi = i; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (!(best > 0.0)) { singular = true; break; }
+    if (bi != k) {
+      for (int c = lane; c < W; c += 32) {
+        double t = aug[k * W + c];
+        aug[k * W + c] = aug[bi * W + c];
+        aug[bi * W + c] = t;
+      }
+      sg = -sg;
+    }
+    __syncwarp();
+    double piv = aug[k * W + k];
+    ld += log(fabs(piv));
+    if (piv < 0) sg = -sg;
+    double inv = 1.0 / piv;
+    __syncwarp();
+    for (int c = lane; c < W; c += 32) aug[k * W + c] *= inv;
+    __syncwarp();
+    // factors of every row in column k (lane i holds row i), captured
+    // before the update; lane c owns columns c and c + 32 (W <= 64)
+    double fac = (lane < M) ? aug[lane * W + k] : 0.0;
+    double pk0 = (lane < W) ? aug[k * W + lane] : 0.0;
+    double pk1 = (lane + 32 < W) ? aug[k * W + lane + 32] : 0.0;
+    __syncwarp();
+    for (int i = 0; i < M; i++) {
+      double f = __shfl_sync(0xffffffffu, fac, i);
+      if (i == k) continue;
+      if (lane < W) aug[i * W + lane] -= f * pk0;
+      if (lane + 32 < W) aug[i * W + lane + 32] -= f * pk1;
+    }
+    __syncwarp();
+  }
+  if (singular) {
+    ld = -1e201;
+    for (int idx = lane; idx < M * M; idx += 32) {
+      int e = idx / M, i = idx - e * M;
+      invT[e * invstride + i] = Real(0);
+    }
+  } else {
+    for (int idx = lane; idx < M * M; idx += 32) {
+      int e = idx / M, i = idx - e * M;
+      invT[e * invstride + i] = Real(aug[i * W + M + e]);
+    }
+  }
+  __syncwarp();
+  logdet = ld;
+  sign = sg;
+}
+
+}  // namespace qwg

@@ -1,0 +1,761 @@
+// Context, device tables, launch shapes and the C-ABI of the walker engine.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/qwg.h"
+#include "qwg_deck.hpp"
+#include "qwg_kernels.cuh"
+
+using namespace qwg;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& m) : std::runtime_error(m) {}
+};
+
+#define CK(x)                                                                                  \
+  do {                                                                                         \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { if (p) cudaFree(p); }
+  void alloc(size_t bytes) {
+    if (p) { cudaFree(p); p = nullptr; }
+    n = bytes;
+    if (bytes) CK(cudaMalloc(&p, bytes));
+  }
+  template <class T> T* as() const { return (T*)p; }
+};
+
+template <class T>
+static void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+  b.alloc(std::max<size_t>(v.size() * sizeof(T), 16));
+  if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+static int mmax_for(int m) {
+  if (m <= 8) return 8;
+  if (m <= 16) return 16;
+  if (m <= 32) return 32;
+  return -1;
+}
+
+}  // namespace
+
+struct qwg_ctx {
+  std::string err;
+  HostSystem H;
+  int precision = QWG_FP64;
+  int max_walkers = 0;
+  int nwalk = 0;
+  int mmax = 8;
+  int wpc = 4;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  long long launches = 0;
+  // tables
+  DevBuf d_atom_pos, d_atom_charge, d_shell_i, d_shell_cut, d_spline, d_spline64, d_moc, d_ee, d_ee_like, d_ee_unlike, d_ei,
+      d_ei_first, d_ei_count, d_onebody, d_tb_first, d_tb_count, d_tb, d_pp_nchan, d_pp_aip, d_pp_cutoff,
+      d_pp_term_first, d_pp_term, d_pp_quad, d_pp_w;
+  DevSys<double> sys_d{};
+  DevSys<float> sys_f{};
+  WLayout L{};
+  size_t smem_bytes = 0;
+  // walkers
+  DevBuf d_R, d_R2, d_state, d_state2;
+  bool state_valid = false;
+  // io scratch
+  DevBuf d_io, d_acc, d_dyn, d_src, d_neww, d_energy;
+  size_t io_bytes = 0;
+  // dynamics
+  uint64_t step_counter = 0;
+  uint64_t last_refresh = 0;
+  uint64_t branch_counter = 0;
+  qwg_dmc_params dmc{};
+  bool dmc_ready = false;
+  double eref = 0, branch_start = 0, branch_stop = 0;
+  std::vector<double> block_energies, block_weights;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+template <typename Real>
+static void fill_sys(qwg_ctx* c, DevSys<Real>& S) {
+  const HostSystem& H = c->H;
+  S.nelec = H.nelec; S.nup = H.nup; S.ndn = H.ndn; S.natoms = H.natoms;
+  S.nbasis = H.nbasis; S.nshell = (int)H.shells.size();
+  S.m[0] = H.nmo[0]; S.m[1] = H.nmo[1];
+  S.mstride = c->mmax;
+  S.atom_pos = c->d_atom_pos.as<double>();
+  S.atom_charge = c->d_atom_charge.as<double>();
+  S.ion_ion = H.ion_ion;
+  S.shell_i = c->d_shell_i.as<int4>();
+  S.shell_cut = c->d_shell_cut.as<double>();
+  S.spline = c->d_spline.as<Real>();
+  S.spline64 = c->d_spline64.as<double>();
+  S.moc = c->d_moc.as<Real>();
+  S.npts = H.spline_npts;
+  S.spacing = H.spline_spacing;
+  S.inv_spacing = 1.0 / H.spline_spacing;
+  S.nee = (int)H.ee.size();
+  S.ee = c->d_ee.as<DRadial>();
+  S.ee_like = c->d_ee_like.as<double>();
+  S.ee_unlike = c->d_ee_unlike.as<double>();
+  S.ei = c->d_ei.as<DRadial>();
+  S.ei_first = c->d_ei_first.as<int>();
+  S.ei_count = c->d_ei_count.as<int>();
+  S.onebody = c->d_onebody.as<double>();
+  S.tb_first = c->d_tb_first.as<int>();
+  S.tb_count = c->d_tb_count.as<int>();
+  S.tb = H.tb.empty() ? nullptr : c->d_tb.as<DTB>();
+  int mx = 0;
+  for (int a = 0; a < H.natoms; a++) mx = std::max(mx, H.ei_count[a]);
+  S.max_ei = mx;
+  S.has_pp = H.has_pp ? 1 : 0;
+  S.pp_nchan = c->d_pp_nchan.as<int>();
+  S.pp_aip = c->d_pp_aip.as<int>();
+  S.pp_cutoff = c->d_pp_cutoff.as<double>();
+  S.pp_term_first = c->d_pp_term_first.as<int>();
+  S.pp_term = c->d_pp_term.as<double>();
+  S.pp_quad = c->d_pp_quad.as<double>();
+  S.pp_w = c->d_pp_w.as<double>();
+  S.max_aip = std::max(H.max_aip, 1);
+}
+
+static void build_tables(qwg_ctx* c) {
+  const HostSystem& H = c->H;
+  cudaStream_t st = c->stream;
+  const int A = H.natoms;
+  upload(c->d_atom_pos, H.atom_pos, st);
+  upload(c->d_atom_charge, H.atom_charge, st);
+  std::vector<int4> si;
+  std::vector<double> sc;
+  for (auto& s : H.shells) {
+    si.push_back(make_int4(s.center, s.spline, s.sym, s.first));
+    sc.push_back(s.cutoff);
+  }
+  upload(c->d_shell_i, si, st);
+  upload(c->d_shell_cut, sc, st);
+  // MO coefficients padded to MMAX columns, both spins
+  const int mm = c->mmax;
+  std::vector<double> moc((size_t)2 * H.nbasis * mm, 0.0);
+  for (int s = 0; s < 2; s++)
+    for (int f = 0; f < H.nbasis; f++)
+      for (int i = 0; i < H.nmo[s]; i++) moc[((size_t)s * H.nbasis + f) * mm + i] = H.moc[s][(size_t)f * H.nmo[s] + i];
+  upload(c->d_spline64, H.spline_coef, st);
+  if (c->precision == QWG_FP64) {
+    upload(c->d_spline, H.spline_coef, st);
+    upload(c->d_moc, moc, st);
+  } else {
+    std::vector<float> sf(H.spline_coef.begin(), H.spline_coef.end());
+    std::vector<float> mf(moc.begin(), moc.end());
+    upload(c->d_spline, sf, st);
+    upload(c->d_moc, mf, st);
+  }
+  std::vector<DRadial> ee, ei;
+  for (auto& r : H.ee) ee.push_back(DRadial{r.kind, r.rcut, r.a, r.b});
+  for (auto& r : H.ei) ei.push_back(DRadial{r.kind, r.rcut, r.a, r.b});
+  upload(c->d_ee, ee, st);
+  upload(c->d_ee_like, H.ee_like, st);
+  upload(c->d_ee_unlike, H.ee_unlike, st);
+  upload(c->d_ei, ei, st);
+  upload(c->d_ei_first, H.ei_first, st);
+  upload(c->d_ei_count, H.ei_count, st);
+  upload(c->d_onebody, H.onebody, st);
+  upload(c->d_tb_first, H.tb_first, st);
+  upload(c->d_tb_count, H.tb_count, st);
+  std::vector<DTB> tb;
+  for (auto& t : H.tb) tb.push_back(DTB{t.k, t.l, t.m, t.c});
+  upload(c->d_tb, tb, st);
+  // pseudopotential
+  const int maq = std::max(H.max_aip, 1);
+  std::vector<int> nch(A), aip(A), tf((size_t)A * 8, 0);
+  std::vector<double> cut(A), term, quad((size_t)A * maq * 3, 0.0), w((size_t)A * maq, 0.0);
+  for (int a = 0; a < A; a++) {
+    const PPAtom& P = H.pp[a];
+    nch[a] = P.nchan;
+    aip[a] = P.aip;
+    cut[a] = P.cutoff;
+    if (P.nchan > 7) throw InputError("too many pseudopotential channels");
+    if (P.nchan > 5) throw InputError("pseudopotential channels beyond l=3 are not supported");
+    int t0 = (int)term.size() / 3;
+    for (int l = 0; l <= P.nchan; l++) tf[(size_t)a * 8 + l] = t0 + (P.nchan ? P.term_first[l] : 0);
+    for (size_t t = 0; t < P.term_n.size(); t++) {
+      term.push_back(P.term_n[t]); term.push_back(P.term_a[t]); term.push_back(P.term_c[t]);
+    }
+    for (int q = 0; q < P.aip; q++) {
+      for (int d = 0; d < 3; d++) quad[((size_t)a * maq + q) * 3 + d] = P.quad[3 * q + d];
+      w[(size_t)a * maq + q] = P.weight[q];
+    }
+  }
+  upload(c->d_pp_nchan, nch, st);
+  upload(c->d_pp_aip, aip, st);
+  upload(c->d_pp_cutoff, cut, st);
+  upload(c->d_pp_term_first, tf, st);
+  upload(c->d_pp_term, term, st);
+  upload(c->d_pp_quad, quad, st);
+  upload(c->d_pp_w, w, st);
+  fill_sys<double>(c, c->sys_d);
+  fill_sys<float>(c, c->sys_f);
+  const void* req[] = {c->sys_d.atom_pos, c->sys_d.atom_charge, c->sys_d.shell_i, c->sys_d.shell_cut,
+                       c->sys_d.spline, c->sys_d.spline64, c->sys_d.moc, c->sys_d.ee, c->sys_d.ee_like, c->sys_d.ee_unlike,
+                       c->sys_d.ei, c->sys_d.ei_first, c->sys_d.ei_count, c->sys_d.onebody, c->sys_d.tb_first,
+                       c->sys_d.tb_count, c->sys_d.pp_nchan, c->sys_d.pp_aip, c->sys_d.pp_cutoff,
+                       c->sys_d.pp_term_first, c->sys_d.pp_term, c->sys_d.pp_quad, c->sys_d.pp_w};
+  for (const void* p : req)
+    if (!p) throw std::runtime_error("internal: device table pointer left unset");
+}
+
+static int align16(int x) { return (x + 15) / 16 * 16; }
+
+static void make_layout(qwg_ctx* c) {
+  const HostSystem& H = c->H;
+  const int N = H.nelec, mm = c->mmax, A = H.natoms;
+  const int rs = c->precision == QWG_FP64 ? 8 : 4;
+  WLayout& L = c->L;
+  int o = 0;
+  L.scal = o; o = align16(o + (int)sizeof(WScal));
+  L.R = o; o = align16(o + 8 * 3 * N);
+  L.inv = o; o = align16(o + rs * 2 * mm * mm);
+  L.mov = o; o = align16(o + rs * N * mm * 4);
+  L.gU = o; o = align16(o + 8 * 3 * N);
+  L.lU = o; o = align16(o + 8 * N);
+  L.state_bytes = o;
+  L.bas = o; o = align16(o + rs * H.nbasis * 5);
+  L.newcol = o; o = align16(o + rs * mm * 5);
+  L.dG = o; o = align16(o + 8 * 4 * N);
+  L.Ue = o; o = align16(o + 8 * N);
+  L.lu = o; o = align16(o + 8 * mm * 2 * mm);
+  L.items = o; o = align16(o + (int)sizeof(PPItem) * N * A);
+  L.rot = o; o = align16(o + 8 * 9);
+  L.bytes = o;
+  const size_t moc_bytes = ((size_t)2 * H.nbasis * mm * rs + 15) / 16 * 16;
+  // walkers per CTA: up to 4 while the CTA stays under ~110 KB (2 CTAs/SM)
+  int wpc = 4;
+  while (wpc > 1 && moc_bytes + (size_t)wpc * L.bytes > 110 * 1024) wpc--;
+  c->wpc = wpc;
+  c->smem_bytes = moc_bytes + (size_t)wpc * L.bytes;
+  if (c->smem_bytes > 227 * 1024) throw InputError("system too large for the shared-memory walker kernel");
+}
+
+template <typename Real, int MM>
+static void launch_walkers_t(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int mode,
+                             int nwalk) {
+  auto kern = k_walkers<Real, MM>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
+  int grid = (nwalk + c->wpc - 1) / c->wpc;
+  kern<<<grid, 32 * c->wpc, c->smem_bytes, c->stream>>>(S, c->L, P, io, mode);
+  CK(cudaGetLastError());
+  c->launches++;
+}
+
+static void launch_walkers(qwg_ctx* c, const StepParams& P, const EvalIO& io, int mode, int nwalk) {
+  if (c->precision == QWG_FP64) {
+    switch (c->mmax) {
+      case 8: launch_walkers_t<double, 8>(c, c->sys_d, P, io, mode, nwalk); break;
+      case 16: launch_walkers_t<double, 16>(c, c->sys_d, P, io, mode, nwalk); break;
+      default: launch_walkers_t<double, 32>(c, c->sys_d, P, io, mode, nwalk); break;
+    }
+  } else {
+    switch (c->mmax) {
+      case 8: launch_walkers_t<float, 8>(c, c->sys_f, P, io, mode, nwalk); break;
+      case 16: launch_walkers_t<float, 16>(c, c->sys_f, P, io, mode, nwalk); break;
+      default: launch_walkers_t<float, 32>(c, c->sys_f, P, io, mode, nwalk); break;
+    }
+  }
+}
+
+static StepParams base_params(qwg_ctx* c) {
+  StepParams P{};
+  P.nwalk = c->nwalk;
+  P.R = c->d_R.as<double>();
+  P.state = c->d_state.as<unsigned char>();
+  P.acc = c->d_acc.as<BlockAcc>();
+  P.etrial = c->d_dyn.as<double>();
+  P.refresh = 1;
+  return P;
+}
+
+static int fail(qwg_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
+
+template <class F>
+static int guarded(qwg_ctx* c, F&& f) {
+  try {
+    return f();
+  } catch (const InputError& e) {
+    return fail(c, QWG_ERR_INPUT, e.what());
+  } catch (const CudaError& e) {
+    return fail(c, QWG_ERR_CUDA, e.what());
+  } catch (const std::exception& e) {
+    return fail(c, QWG_ERR_ARG, e.what());
+  }
+}
+
+static void ensure_io(qwg_ctx* c, size_t bytes) {
+  if (c->io_bytes < bytes) {
+    c->d_io.alloc(bytes);
+    c->io_bytes = bytes;
+  }
+}
+
+// One chunk of steps on the resident population (plus DMC branching).
+static void run_chunk(qwg_ctx* c, int nsteps, double tau, uint64_t seed, int det_pp, bool dmc, BlockAcc* acc,
+                      double* energy_out) {
+  StepParams P = base_params(c);
+  P.nsteps = nsteps;
+  P.tau = tau;
+  P.dmc = dmc ? 1 : 0;
+  P.deterministic_pp = det_pp;
+  P.seed = seed;
+  P.step0 = c->step_counter;
+  P.acc = acc;
+  P.branch_start = c->branch_start;
+  P.branch_stop = c->branch_stop;
+  P.max_weight = dmc ? c->dmc.max_poss_weight : 1.0;
+  // full recompute (FP64 re-inversion) when the resident state is stale or
+  // refresh_interval steps have passed since the last one
+  int refresh_every = std::max(1, dmc ? c->dmc.refresh_interval : nsteps);
+  P.refresh = (!c->state_valid || c->step_counter - c->last_refresh >= (uint64_t)refresh_every) ? 1 : 0;
+  if (P.refresh) c->last_refresh = c->step_counter;
+  EvalIO io{};
+  io.energy = energy_out;
+  launch_walkers(c, P, io, KM_STEPS, c->nwalk);
+  c->state_valid = true;
+  c->step_counter += nsteps;
+}
+
+static void run_branch(qwg_ctx* c, const BlockAcc* acc) {
+  BranchParams B{};
+  B.nwalk = c->nwalk;
+  int p2 = 1;
+  while (p2 < c->nwalk) p2 <<= 1;
+  B.npow2 = p2;
+  B.eref = c->eref;
+  B.feedback = c->dmc.feedback;
+  B.timestep = c->dmc.timestep;
+  B.seed = c->dmc.seed ^ 0x5bd1e995ull;
+  B.counter = c->branch_counter++;
+  B.state = c->d_state.as<unsigned char>();
+  B.state_bytes = c->L.state_bytes;
+  B.scal_off = c->L.scal;
+  B.acc = acc;
+  B.dyn = c->d_dyn.as<double>();
+  B.src_of = c->d_src.as<int>();
+  B.new_w = c->d_neww.as<double>();
+  size_t sm = (size_t)p2 * (8 + 4) + (size_t)c->nwalk * 4 + 16 + (size_t)c->nwalk * 8;
+  CK(cudaFuncSetAttribute(k_branch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_branch<<<1, 1024, sm, c->stream>>>(B);
+  CK(cudaGetLastError());
+  const int n3 = 3 * c->H.nelec;
+  k_gather<<<c->nwalk, 128, 0, c->stream>>>(c->nwalk, n3, c->L.state_bytes, c->L.scal, c->d_src.as<int>(),
+                                            c->d_neww.as<double>(), c->d_R.as<double>(),
+                                            c->d_state.as<unsigned char>(), c->d_R2.as<double>(),
+                                            c->d_state2.as<unsigned char>());
+  CK(cudaGetLastError());
+  c->launches += 2;
+  std::swap(c->d_R.p, c->d_R2.p);
+  std::swap(c->d_state.p, c->d_state2.p);
+}
+
+static void acc_to_stats(const std::vector<BlockAcc>& v, qwg_block_stats* s) {
+  BlockAcc t{};
+  for (auto& a : v) {
+    t.sum_w += a.sum_w; t.sum_we += a.sum_we; t.sum_wk += a.sum_wk; t.sum_wv += a.sum_wv; t.sum_wnl += a.sum_wnl;
+    t.sum_we2 += a.sum_we2; t.accepted += a.accepted; t.attempted += a.attempted; t.nonfinite += a.nonfinite;
+    t.npts += a.npts;
+  }
+  double W = t.sum_w > 0 ? t.sum_w : 1.0;
+  s->energy = t.sum_we / W;
+  s->kinetic = t.sum_wk / W;
+  s->potential = t.sum_wv / W;
+  s->nonlocal = t.sum_wnl / W;
+  s->energy_var = t.sum_we2 / W - s->energy * s->energy;
+  s->weight = t.npts > 0 ? t.sum_w / t.npts : 0.0;
+  s->acceptance = t.attempted > 0 ? t.accepted / t.attempted : 0.0;
+  s->nonfinite = (int)t.nonfinite;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C-ABI
+
+extern "C" {
+
+const char* qwg_version(void) { return "mainline_b200 qwg 0.1 (sm_100a)"; }
+
+// Error text of the last failed qwg_create on this thread (context is NULL then).
+static thread_local std::string g_create_error;
+
+const char* qwg_last_error(const qwg_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int qwg_inspect_deck(const char* deck_path, qwg_info* info, char* err, int errlen) {
+  try {
+    HostSystem H = build_system(deck_path);
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->nelec = H.nelec; info->nup = H.nup; info->ndown = H.ndn; info->natoms = H.natoms;
+      info->nbasis = H.nbasis; info->nshell = (int)H.shells.size(); info->nmo_up = H.nmo[0];
+      info->nmo_down = H.nmo[1]; info->has_pseudo = H.has_pp; info->ion_ion = H.ion_ion;
+    }
+    return QWG_OK;
+  } catch (const std::exception& e) {
+    if (err && errlen > 0) { strncpy(err, e.what(), errlen - 1); err[errlen - 1] = 0; }
+    return QWG_ERR_INPUT;
+  }
+}
+
+int qwg_inspect_spline(const char* deck_path, int shell, double* coef, int maxpts, int* npts, double* spacing,
+                       double* cutoff) {
+  try {
+    HostSystem H = build_system(deck_path);
+    if (shell < 0 || shell >= (int)H.shells.size()) return QWG_ERR_ARG;
+    const Shell& s = H.shells[shell];
+    int n = std::min(maxpts, H.spline_npts);
+    if (coef) memcpy(coef, H.spline_coef.data() + (size_t)s.spline * H.spline_npts * 4, sizeof(double) * 4 * n);
+    if (npts) *npts = H.spline_npts;
+    if (spacing) *spacing = H.spline_spacing;
+    if (cutoff) *cutoff = s.cutoff;
+    return QWG_OK;
+  } catch (const std::exception&) {
+    return QWG_ERR_INPUT;
+  }
+}
+
+int qwg_create(const char* deck_path, int precision, int max_walkers, void* stream, qwg_ctx** out) {
+  if (!out || !deck_path) return QWG_ERR_ARG;
+  *out = nullptr;
+  if (precision != QWG_FP64 && precision != QWG_MIXED) return QWG_ERR_ARG;
+  if (max_walkers <= 0 || max_walkers > (1 << 22)) return QWG_ERR_ARG;
+  std::unique_ptr<qwg_ctx> c(new qwg_ctx());
+  c->precision = precision;
+  c->max_walkers = max_walkers;
+  int rc = guarded(c.get(), [&]() -> int {
+    c->H = build_system(deck_path);
+    int mm = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
+    if (mm < 0) throw InputError("more than 32 electrons of one spin: beyond this engine build");
+    c->mmax = mm;
+    if (stream) {
+      c->stream = (cudaStream_t)stream;
+    } else {
+      CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      c->own_stream = true;
+    }
+    build_tables(c.get());
+    make_layout(c.get());
+    const int N = c->H.nelec;
+    c->d_R.alloc((size_t)max_walkers * 3 * N * 8);
+    c->d_R2.alloc((size_t)max_walkers * 3 * N * 8);
+    c->d_state.alloc((size_t)max_walkers * c->L.state_bytes);
+    c->d_state2.alloc((size_t)max_walkers * c->L.state_bytes);
+    c->d_acc.alloc(sizeof(BlockAcc) * 1024);
+    c->d_dyn.alloc(8 * 8);
+    CK(cudaMemsetAsync(c->d_dyn.p, 0, 64, c->stream));
+    c->d_src.alloc((size_t)max_walkers * 4);
+    c->d_neww.alloc((size_t)max_walkers * 8);
+    c->d_energy.alloc((size_t)max_walkers * 8);
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+    CK(cudaStreamSynchronize(c->stream));
+    return QWG_OK;
+  });
+  if (rc != QWG_OK) {
+    g_create_error = c->err;
+    return rc;
+  }
+  *out = c.release();
+  return QWG_OK;
+}
+
+int qwg_destroy(qwg_ctx* ctx) {
+  if (!ctx) return QWG_OK;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  cudaStream_t st = ctx->own_stream ? ctx->stream : nullptr;
+  delete ctx;
+  if (st) cudaStreamDestroy(st);
+  return QWG_OK;
+}
+
+int qwg_get_info(const qwg_ctx* c, qwg_info* info) {
+  if (!c || !info) return QWG_ERR_ARG;
+  memset(info, 0, sizeof(*info));
+  const HostSystem& H = c->H;
+  info->nelec = H.nelec; info->nup = H.nup; info->ndown = H.ndn; info->natoms = H.natoms;
+  info->nbasis = H.nbasis; info->nshell = (int)H.shells.size(); info->nmo_up = H.nmo[0]; info->nmo_down = H.nmo[1];
+  info->has_pseudo = H.has_pp; info->max_walkers = c->max_walkers; info->precision = c->precision;
+  info->walkers_per_cta = c->wpc; info->ion_ion = H.ion_ion;
+  return QWG_OK;
+}
+
+int qwg_set_walkers(qwg_ctx* c, const double* R, int nw) {
+  if (!c || !R || nw <= 0 || nw > c->max_walkers) return fail(c, QWG_ERR_ARG, "qwg_set_walkers: bad walker count");
+  return guarded(c, [&]() -> int {
+    const size_t bytes = (size_t)nw * 3 * c->H.nelec * 8;
+    CK(cudaMemcpyAsync(c->d_R.p, R, bytes, cudaMemcpyHostToDevice, c->stream));
+    c->nwalk = nw;
+    c->state_valid = false;
+    c->dmc_ready = false;
+    return QWG_OK;
+  });
+}
+
+int qwg_set_walkers_device(qwg_ctx* c, const double* dR, int nw) {
+  if (!c || !dR || nw <= 0 || nw > c->max_walkers) return fail(c, QWG_ERR_ARG, "qwg_set_walkers_device: bad walker count");
+  return guarded(c, [&]() -> int {
+    CK(cudaMemcpyAsync(c->d_R.p, dR, (size_t)nw * 3 * c->H.nelec * 8, cudaMemcpyDeviceToDevice, c->stream));
+    c->nwalk = nw;
+    c->state_valid = false;
+    c->dmc_ready = false;
+    return QWG_OK;
+  });
+}
+
+int qwg_get_walkers(qwg_ctx* c, double* R, int nw) {
+  if (!c || !R || nw <= 0 || nw > c->nwalk) return fail(c, QWG_ERR_ARG, "qwg_get_walkers: bad walker count");
+  return guarded(c, [&]() -> int {
+    CK(cudaMemcpyAsync(R, c->d_R.p, (size_t)nw * 3 * c->H.nelec * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return QWG_OK;
+  });
+}
+
+int qwg_eval(qwg_ctx* c, const double* rot, qwg_eval_out* out) {
+  if (!c || !out) return QWG_ERR_ARG;
+  if (c->nwalk <= 0) return fail(c, QWG_ERR_STATE, "qwg_eval: no walkers");
+  return guarded(c, [&]() -> int {
+    const int W = c->nwalk, N = c->H.nelec;
+    size_t n_rot = (size_t)W * 9, n_g = (size_t)W * N * 3, n_l = (size_t)W * N;
+    size_t total = 8 * (n_rot + 5 * (size_t)W + n_g + n_l);
+    ensure_io(c, total);
+    double* base = c->d_io.as<double>();
+    double* d_rot = base;
+    double* d_lp = d_rot + n_rot;
+    double* d_sg = d_lp + W;
+    double* d_k = d_sg + W;
+    double* d_v = d_k + W;
+    double* d_nl = d_v + W;
+    double* d_g = d_nl + W;
+    double* d_l = d_g + n_g;
+    if (rot) CK(cudaMemcpyAsync(d_rot, rot, 8 * n_rot, cudaMemcpyHostToDevice, c->stream));
+    EvalIO io{};
+    io.rot = rot ? d_rot : nullptr;
+    io.logpsi = d_lp; io.sign = d_sg; io.kinetic = d_k; io.potential = d_v; io.nonlocal = d_nl;
+    io.grad = d_g; io.lap = d_l;
+    StepParams P = base_params(c);
+    launch_walkers(c, P, io, KM_EVAL, W);
+    auto dl = [&](double* h, const double* d, size_t n) {
+      if (h) CK(cudaMemcpyAsync(h, d, 8 * n, cudaMemcpyDeviceToHost, c->stream));
+    };
+    dl(out->logpsi, d_lp, W); dl(out->sign, d_sg, W); dl(out->kinetic, d_k, W); dl(out->potential, d_v, W);
+    dl(out->nonlocal, d_nl, W); dl(out->grad, d_g, n_g); dl(out->lap, d_l, n_l);
+    CK(cudaStreamSynchronize(c->stream));
+    c->state_valid = false;  // eval leaves scratch state unsaved
+    return QWG_OK;
+  });
+}
+
+int qwg_ratio(qwg_ctx* c, const int* e, const double* Rnew, double* dlogpsi, double* sign, double* grad,
+              double* lap) {
+  if (!c || !e || !Rnew) return QWG_ERR_ARG;
+  if (c->nwalk <= 0) return fail(c, QWG_ERR_STATE, "qwg_ratio: no walkers");
+  for (int w = 0; w < c->nwalk; w++)
+    if (e[w] < 0 || e[w] >= c->H.nelec) return fail(c, QWG_ERR_ARG, "qwg_ratio: electron index out of range");
+  return guarded(c, [&]() -> int {
+    const int W = c->nwalk;
+    size_t total = 8 * ((size_t)W * 3 + (size_t)W * 3 + 3 * (size_t)W) + 4 * (size_t)W + 64;
+    ensure_io(c, total);
+    double* d_r = c->d_io.as<double>();
+    double* d_lp = d_r + 3 * W;
+    double* d_sg = d_lp + W;
+    double* d_g = d_sg + W;
+    double* d_l = d_g + 3 * W;
+    int* d_e = (int*)(d_l + W);
+    CK(cudaMemcpyAsync(d_r, Rnew, 8 * 3 * (size_t)W, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_e, e, 4 * (size_t)W, cudaMemcpyHostToDevice, c->stream));
+    EvalIO io{};
+    io.move_e = d_e; io.move_r = d_r; io.logpsi = d_lp; io.sign = d_sg; io.grad = d_g; io.lap = d_l;
+    StepParams P = base_params(c);
+    launch_walkers(c, P, io, KM_RATIO, W);
+    if (dlogpsi) CK(cudaMemcpyAsync(dlogpsi, d_lp, 8 * (size_t)W, cudaMemcpyDeviceToHost, c->stream));
+    if (sign) CK(cudaMemcpyAsync(sign, d_sg, 8 * (size_t)W, cudaMemcpyDeviceToHost, c->stream));
+    if (grad) CK(cudaMemcpyAsync(grad, d_g, 8 * 3 * (size_t)W, cudaMemcpyDeviceToHost, c->stream));
+    if (lap) CK(cudaMemcpyAsync(lap, d_l, 8 * (size_t)W, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->state_valid = false;
+    return QWG_OK;
+  });
+}
+
+int qwg_vmc_block(qwg_ctx* c, int nstep, double timestep, uint64_t seed, int deterministic_pp,
+                  qwg_block_stats* stats) {
+  if (!c || nstep <= 0 || !(timestep > 0)) return fail(c, QWG_ERR_ARG, "qwg_vmc_block: bad arguments");
+  if (c->nwalk <= 0) return fail(c, QWG_ERR_STATE, "qwg_vmc_block: no walkers");
+  return guarded(c, [&]() -> int {
+    BlockAcc* acc = c->d_acc.as<BlockAcc>();
+    CK(cudaMemsetAsync(acc, 0, sizeof(BlockAcc), c->stream));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    c->state_valid = false;  // VMC: full recompute at the start of each block
+    run_chunk(c, nstep, timestep, seed, deterministic_pp, false, acc, nullptr);
+    CK(cudaEventRecord(c->ev1, c->stream));
+    std::vector<BlockAcc> h(1);
+    CK(cudaMemcpyAsync(h.data(), acc, sizeof(BlockAcc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (stats) {
+      memset(stats, 0, sizeof(*stats));
+      acc_to_stats(h, stats);
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+      stats->block_ms = ms;
+      stats->nsteps = nstep;
+      stats->nwalkers = c->nwalk;
+    }
+    c->dmc_ready = false;
+    return QWG_OK;
+  });
+}
+
+int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
+  if (!c || !p || !(p->timestep > 0)) return fail(c, QWG_ERR_ARG, "qwg_dmc_init: bad parameters");
+  if (c->nwalk <= 0) return fail(c, QWG_ERR_STATE, "qwg_dmc_init: no walkers");
+  return guarded(c, [&]() -> int {
+    c->dmc = *p;
+    if (c->dmc.nstep <= 0) c->dmc.nstep = std::max(int(1.0 / p->timestep + 0.5), 1);
+    if (c->dmc.feedback_interval <= 0) c->dmc.feedback_interval = 5;
+    if (c->dmc.max_poss_weight <= 0) c->dmc.max_poss_weight = 7.0;
+    if (c->dmc.branch_start_cutoff <= 0) c->dmc.branch_start_cutoff = 10.0;
+    if (c->dmc.refresh_interval <= 0)
+      c->dmc.refresh_interval = c->precision == QWG_FP64 ? c->dmc.feedback_interval : 32;
+    const int W = c->nwalk;
+    // energies of the starting walkers: one gather step without moves is a
+    // zero-step launch, so run the local energy through KM_STEPS with
+    // nsteps = 0 ... simpler: evaluate with the stochastic PP like gatherData.
+    BlockAcc* acc = c->d_acc.as<BlockAcc>();
+    CK(cudaMemsetAsync(acc, 0, sizeof(BlockAcc), c->stream));
+    CK(cudaMemsetAsync(c->d_dyn.p, 0, 64, c->stream));
+    // evaluate E_L of each walker (deterministic PP for a clean start)
+    size_t n_g = (size_t)W * c->H.nelec * 3, n_l = (size_t)W * c->H.nelec;
+    ensure_io(c, 8 * (5 * (size_t)W + n_g + n_l));
+    double* base = c->d_io.as<double>();
+    EvalIO io{};
+    io.logpsi = base; io.sign = base + W; io.kinetic = base + 2 * W; io.potential = base + 3 * W;
+    io.nonlocal = base + 4 * W; io.grad = base + 5 * W; io.lap = io.grad + n_g;
+    StepParams P = base_params(c);
+    launch_walkers(c, P, io, KM_EVAL, W);
+    std::vector<double> k(W), v(W), nl(W), el(W);
+    CK(cudaMemcpyAsync(k.data(), io.kinetic, 8 * W, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(v.data(), io.potential, 8 * W, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(nl.data(), io.nonlocal, 8 * W, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double sum = 0;
+    int good = 0;
+    for (int w = 0; w < W; w++) {
+      el[w] = k[w] + v[w] + nl[w];
+      if (std::isfinite(el[w])) { sum += el[w]; good++; }
+    }
+    if (!good) return fail(c, QWG_ERR_NUMERIC, "qwg_dmc_init: no walker has a finite local energy");
+    // find_cutoffs (Dmc_method.cpp:262-300)
+    double eavg = sum / good, var = 0;
+    for (int w = 0; w < W; w++)
+      if (std::isfinite(el[w])) var += (el[w] - eavg) * (el[w] - eavg);
+      else el[w] = eavg;
+    var /= W;
+    double sigma = std::sqrt(var);
+    c->eref = eavg;
+    c->branch_start = c->dmc.branch_start_cutoff * sigma;
+    c->branch_stop = c->branch_start * 1.5;
+    CK(cudaMemcpyAsync(c->d_energy.p, el.data(), 8 * W, cudaMemcpyHostToDevice, c->stream));
+    // state: weights 1, E_old = E_L; E_T = E_ref (start_feedback * log(1) = 0)
+    c->state_valid = false;
+    StepParams P2 = base_params(c);
+    P2.nsteps = 0;
+    P2.refresh = 1;
+    P2.acc = acc;
+    EvalIO io2{};
+    launch_walkers(c, P2, io2, KM_STEPS, W);  // builds and stores the resident state
+    k_init_weights<<<(W + 255) / 256, 256, 0, c->stream>>>(c->d_state.as<unsigned char>(), W, c->L.state_bytes,
+                                                           c->L.scal, c->d_energy.as<double>());
+    CK(cudaGetLastError());
+    c->launches++;
+    double dyn0[4] = {c->eref, c->dmc.timestep, double(W), 0.0};
+    CK(cudaMemcpyAsync(c->d_dyn.p, dyn0, sizeof(dyn0), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->state_valid = true;
+    c->dmc_ready = true;
+    c->block_energies.clear();
+    c->block_weights.clear();
+    return QWG_OK;
+  });
+}
+
+int qwg_dmc_block(qwg_ctx* c, qwg_block_stats* stats) {
+  if (!c) return QWG_ERR_ARG;
+  if (!c->dmc_ready) return fail(c, QWG_ERR_STATE, "qwg_dmc_block: call qwg_dmc_init first");
+  return guarded(c, [&]() -> int {
+    const int nstep = c->dmc.nstep, fi = c->dmc.feedback_interval;
+    const int nchunk = (nstep + fi - 1) / fi;
+    if (nchunk > 1024) throw std::runtime_error("too many feedback intervals per block");
+    BlockAcc* acc = c->d_acc.as<BlockAcc>();
+    CK(cudaMemsetAsync(acc, 0, sizeof(BlockAcc) * nchunk, c->stream));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int ch = 0, step = 0; ch < nchunk; ch++) {
+      int np = std::min(fi, nstep - step);
+      run_chunk(c, np, c->dmc.timestep, c->dmc.seed, c->dmc.deterministic_pp, true, acc + ch, nullptr);
+      run_branch(c, acc + ch);
+      step += np;
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    std::vector<BlockAcc> h(nchunk);
+    CK(cudaMemcpyAsync(h.data(), acc, sizeof(BlockAcc) * nchunk, cudaMemcpyDeviceToHost, c->stream));
+    double dyn[4];
+    CK(cudaMemcpyAsync(dyn, c->d_dyn.p, sizeof(dyn), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    qwg_block_stats s{};
+    acc_to_stats(h, &s);
+    // E_ref = average of the block energies so far (the first fifth of the
+    // blocks is treated as equilibration once there are more than five)
+    c->block_energies.push_back(s.energy);
+    size_t nb = c->block_energies.size(), b0 = nb > 5 ? nb / 5 : 0;
+    double se = 0;
+    for (size_t b = b0; b < nb; b++) se += c->block_energies[b];
+    c->eref = se / double(nb - b0);
+    k_set_etrial<<<1, 32, 0, c->stream>>>(c->d_dyn.as<double>(), c->eref, c->dmc.feedback, c->nwalk);
+    CK(cudaGetLastError());
+    c->launches++;
+    if (stats) {
+      *stats = s;
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+      stats->block_ms = ms;
+      stats->nsteps = nstep;
+      stats->nwalkers = c->nwalk;
+      stats->etrial = c->eref - c->dmc.feedback * std::log(dyn[2] / double(c->nwalk));
+    }
+    return QWG_OK;
+  });
+}
+
+long long qwg_launch_count(const qwg_ctx* c) { return c ? c->launches : 0; }
+void qwg_reset_launch_count(qwg_ctx* c) { if (c) c->launches = 0; }
+
+}  // extern "C"

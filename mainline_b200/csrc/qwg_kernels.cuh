@@ -1,0 +1,707 @@
+// Walker kernels: full evaluation, single-electron ratio, VMC/DMC steps,
+// branching and population gather.  See qwg_device.cuh for the execution
+// model.  Reference semantics cited per routine (QWalk/mainline src/).
+#pragma once
+#include "qwg_device.cuh"
+
+namespace qwg {
+
+enum KMode { KM_EVAL = 0, KM_RATIO = 1, KM_STEPS = 2 };
+
+struct EvalIO {
+  const double* rot;     // [W][9] quadrature rotations (KM_EVAL) or nullptr
+  const int* move_e;     // [W] (KM_RATIO)
+  const double* move_r;  // [W][3]
+  double* logpsi;        // [W]
+  double* sign;          // [W]
+  double* grad;          // [W][N][3] (KM_EVAL) or [W][3] (KM_RATIO)
+  double* lap;           // [W][N] or [W]
+  double* kinetic;       // [W]
+  double* potential;     // [W]
+  double* nonlocal;      // [W]
+  double* energy;        // [W] local energy after the last step (KM_STEPS)
+};
+
+struct PPItem {
+  int e, a;
+  double r;
+  double dx, dy, dz;     // electron - atom
+  double vl[4];          // nonlocal channel radials (already scaled)
+};
+
+template <typename Real, int MMAX>
+struct Walker {
+  const DevSys<Real>& S;
+  const WLayout& L;
+  unsigned char* base;
+  const Real* moc_s;     // [2][nbasis][MMAX] in shared memory
+  int lane;
+
+  __device__ double* R() const { return (double*)(base + L.R); }
+  __device__ Real* inv(int s) const { return (Real*)(base + L.inv) + s * MMAX * MMAX; }
+  __device__ Real* mov() const { return (Real*)(base + L.mov); }
+  __device__ double* gU() const { return (double*)(base + L.gU); }
+  __device__ double* lU() const { return (double*)(base + L.lU); }
+  __device__ WScal* sc() const { return (WScal*)(base + L.scal); }
+  __device__ Real* bas() const { return (Real*)(base + L.bas); }
+  __device__ Real* newcol() const { return (Real*)(base + L.newcol); }
+  __device__ double* dG() const { return (double*)(base + L.dG); }
+  __device__ double* Ue() const { return (double*)(base + L.Ue); }
+  __device__ double* lu() const { return (double*)(base + L.lu); }
+  __device__ PPItem* items() const { return (PPItem*)(base + L.items); }
+  __device__ double* rot() const { return (double*)(base + L.rot); }
+
+  __device__ int spin(int e) const { return e < S.nup ? 0 : 1; }
+  __device__ int eloc(int e) const { return e < S.nup ? e : e - S.nup; }
+  __device__ const Real* mocs(int s) const { return moc_s + (size_t)s * S.nbasis * MMAX; }
+
+  // ---- full recompute: Slat_wf::calcLap (Slat_wf.h:948-1016) + the Jastrow
+  // recomputation of every electron (Jastrow2_wf.cpp:988-1157).
+  __device__ void recompute() {
+    double* Rp = R();
+    Real* nc = newcol();
+    double* aug = lu();
+    WScal* w = sc();
+    for (int s = 0; s < 2; s++) {
+      const int M = S.m[s];
+      const int e0 = s == 0 ? 0 : S.nup;
+      for (int el = 0; el < M; el++) {
+        const int e = e0 + el;
+        mo_lap_warp(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], M, bas(), nc, lane);
+        for (int i = lane; i < M; i += 32) {
+          aug[el * 2 * M + i] = double(nc[i * 5]);
+          Real* mv = mov() + ((size_t)e * MMAX + i) * 4;
+          mv[0] = nc[i * 5 + 1]; mv[1] = nc[i * 5 + 2]; mv[2] = nc[i * 5 + 3]; mv[3] = nc[i * 5 + 4];
+        }
+        __syncwarp();
+      }
+      if (M > 0) {
+        double ld, sg;
+        gj_inverse_warp(aug, M, inv(s), MMAX, ld, sg, lane);
+        if (lane == 0) { w->logdet[s] = ld; w->sign[s] = sg; }
+      } else if (lane == 0) {
+        w->logdet[s] = 0.0; w->sign[s] = 1.0;
+      }
+      __syncwarp();
+    }
+    // Jastrow: every electron's gradient and Laplacian; U from the
+    // one-body values and half the pair values.
+    double usum = 0.0;
+    for (int i = lane; i < S.nelec; i += 32) {
+      double u, g[3], l, ob, og[3], ol;
+      jas_electron(S, Rp, i, Rp[3 * i], Rp[3 * i + 1], Rp[3 * i + 2], u, g, l, true);
+      jas_onebody(S, Rp[3 * i], Rp[3 * i + 1], Rp[3 * i + 2], ob, og, ol);
+      gU()[3 * i] = g[0]; gU()[3 * i + 1] = g[1]; gU()[3 * i + 2] = g[2];
+      lU()[i] = l;
+      usum += 0.5 * (u + ob);
+    }
+    usum = warp_sum(usum);
+    if (lane == 0) w->U = usum;
+    __syncwarp();
+  }
+
+  // Slater gradient and Laplacian ratios of electron e at its position.
+  __device__ void slater_gl(int e, double g[3], double& l) const {
+    const int s = spin(e), el = eloc(e), M = S.m[s];
+    const Real* iv = inv(s) + el * MMAX;
+    const Real* mv = mov() + (size_t)e * MMAX * 4;
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;  // FP64 accumulation of the short dots
+    for (int i = 0; i < M; i++) {
+      double c = iv[i];
+      a0 += c * double(mv[4 * i]); a1 += c * double(mv[4 * i + 1]); a2 += c * double(mv[4 * i + 2]);
+      a3 += c * double(mv[4 * i + 3]);
+    }
+    g[0] = a0; g[1] = a1; g[2] = a2; l = a3;
+  }
+
+  // ---- proposal of electron e at p: everything except the decision.
+  // Fills the new MO column (newcol), the Jastrow deltas of the other
+  // electrons (dG), and returns the determinant ratio, ln-ratio of the
+  // Jastrow, new drift and lap of e.  (Slat_wf::updateLap + Jastrow2_wf::
+  // updateLap + Slat_Jastrow::getLap for one electron.)
+  __device__ void propose(int e, double px, double py, double pz, double& ratioD, double& dU, double gnew[3],
+                          double& lapnew) {
+    const int s = spin(e), el = eloc(e), M = S.m[s];
+    const double* Rp = R();
+    Real* nc = newcol();
+    mo_lap_warp(S, mocs(s), px, py, pz, M, bas(), nc, lane);
+    const Real* iv = inv(s) + el * MMAX;
+    double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
+    for (int i = 0; i < M; i++) {
+      double c = iv[i];
+      r0 += c * double(nc[i * 5]); r1 += c * double(nc[i * 5 + 1]); r2 += c * double(nc[i * 5 + 2]);
+      r3 += c * double(nc[i * 5 + 3]); r4 += c * double(nc[i * 5 + 4]);
+    }
+    ratioD = double(r0);
+    double gD[3] = {double(r1) / ratioD, double(r2) / ratioD, double(r3) / ratioD};
+    double lD = double(r4) / ratioD;
+    // Jastrow: lanes over the other electrons
+    const double ox = Rp[3 * e], oy = Rp[3 * e + 1], oz = Rp[3 * e + 2];
+    const bool se = s == 0;
+    const bool has3 = S.tb != nullptr;
+    double du = 0.0, ge[3] = {0, 0, 0}, le = 0.0;
+    for (int j = lane; j < S.nelec; j += 32) {
+      double* dg = dG() + 4 * j;
+      if (j == e) continue;
+      const double* pj = Rp + 3 * j;
+      const bool same = se == (j < S.nup);
+      double nx = px - pj[0], ny = py - pj[1], nz = pz - pj[2];
+      double qx = ox - pj[0], qy = oy - pj[1], qz = oz - pj[2];
+      double rn = sqrt(nx * nx + ny * ny + nz * nz), ro = sqrt(qx * qx + qy * qy + qz * qz);
+      double un, fn, ln, uo, fo, lo;
+      jas_pair(S, same, rn, un, fn, ln);
+      jas_pair(S, same, ro, uo, fo, lo);
+      du += un - uo;
+      ge[0] += fn * nx; ge[1] += fn * ny; ge[2] += fn * nz;
+      le += ln;
+      // gradient w.r.t. r_j of u(r_e - r_j) = -f'/r (r_e - r_j)
+      double g0 = -fn * nx + fo * qx, g1 = -fn * ny + fo * qy, g2 = -fn * nz + fo * qz, l0 = ln - lo;
+      if (has3) {
+        double pn[3] = {px, py, pz}, po[3] = {ox, oy, oz};
+        double tu, tgi[3], tli, tgj[3], tlj, su, sgi[3], sli, sgj[3], slj;
+        jas_threebody_pair(S, pn, pj, tu, tgi, tli, tgj, tlj, true);
+        jas_threebody_pair(S, po, pj, su, sgi, sli, sgj, slj, true);
+        du += tu - su;
+        ge[0] += tgi[0]; ge[1] += tgi[1]; ge[2] += tgi[2];
+        le += tli;
+        g0 += tgj[0] - sgj[0]; g1 += tgj[1] - sgj[1]; g2 += tgj[2] - sgj[2];
+        l0 += tlj - slj;
+      }
+      dg[0] = g0; dg[1] = g1; dg[2] = g2; dg[3] = l0;
+    }
+    du = warp_sum(du);
+    ge[0] = warp_sum(ge[0]); ge[1] = warp_sum(ge[1]); ge[2] = warp_sum(ge[2]);
+    le = warp_sum(le);
+    double obn, ogn[3], oln, obo, ogo[3], olo;
+    jas_onebody(S, px, py, pz, obn, ogn, oln);
+    jas_onebody(S, ox, oy, oz, obo, ogo, olo);
+    dU = du + obn - obo;
+    double gu[3] = {ge[0] + ogn[0], ge[1] + ogn[1], ge[2] + ogn[2]};
+    double lu_ = le + oln;
+    double dot = 0, gg = 0;
+    for (int d = 0; d < 3; d++) {
+      gnew[d] = gD[d] + gu[d];
+      dot += gD[d] * gu[d];
+      gg += gu[d] * gu[d];
+    }
+    lapnew = lD + lu_ + gg + 2 * dot;
+    // stash the new Jastrow gradient/lap of e for an accept
+    __syncwarp();
+    if (lane == 0) { dG()[4 * e] = gu[0]; dG()[4 * e + 1] = gu[1]; dG()[4 * e + 2] = gu[2]; dG()[4 * e + 3] = lu_; }
+    __syncwarp();
+  }
+
+  // ---- accept the proposal of electron e: Sherman-Morrison update of the
+  // transposed inverse (InverseUpdateColumn, MatrixAlgebrac.cpp:766-838),
+  // the stored MO row, position and Jastrow sums.
+  __device__ void accept(int e, double px, double py, double pz, double ratioD, double dU) {
+    const int s = spin(e), el = eloc(e), M = S.m[s];
+    Real* iv = inv(s);
+    Real* nc = newcol();
+    // scratch: wk[k] = sum_i phi'_i invT[k][i], rowe[i] = invT[el][i]
+    Real* wk = (Real*)lu();
+    Real* rowe = wk + MMAX;
+    for (int k = lane; k < M; k += 32) {
+      Real acc = 0;
+      for (int i = 0; i < M; i++) acc += nc[i * 5] * iv[k * MMAX + i];
+      wk[k] = acc;
+      rowe[k] = iv[el * MMAX + k];
+    }
+    __syncwarp();
+    const Real invr = Real(1.0 / ratioD);
+    for (int idx = lane; idx < M * M; idx += 32) {
+      int k = idx / M, i = idx - k * M;
+      if (k == el) iv[k * MMAX + i] = rowe[i] * invr;
+      else iv[k * MMAX + i] -= rowe[i] * wk[k] * invr;
+    }
+    for (int i = lane; i < M; i += 32) {
+      Real* mv = mov() + ((size_t)e * MMAX + i) * 4;
+      mv[0] = nc[i * 5 + 1]; mv[1] = nc[i * 5 + 2]; mv[2] = nc[i * 5 + 3]; mv[3] = nc[i * 5 + 4];
+    }
+    for (int j = lane; j < S.nelec; j += 32) {
+      const double* dg = dG() + 4 * j;
+      if (j == e) {
+        gU()[3 * j] = dg[0]; gU()[3 * j + 1] = dg[1]; gU()[3 * j + 2] = dg[2]; lU()[j] = dg[3];
+      } else {
+        gU()[3 * j] += dg[0]; gU()[3 * j + 1] += dg[1]; gU()[3 * j + 2] += dg[2]; lU()[j] += dg[3];
+      }
+    }
+    if (lane == 0) {
+      double* Rp = R();
+      Rp[3 * e] = px; Rp[3 * e + 1] = py; Rp[3 * e + 2] = pz;
+      WScal* w = sc();
+      w->logdet[s] += log(fabs(ratioD));
+      if (ratioD < 0) w->sign[s] = -w->sign[s];
+      w->U += dU;
+    }
+    __syncwarp();
+  }
+
+  __device__ void electron_grad(int e, double g[3], double& lap) const {
+    double gD[3], lD;
+    slater_gl(e, gD, lD);
+    const double* gu = gU() + 3 * e;
+    double dot = 0, gg = 0;
+    for (int d = 0; d < 3; d++) {
+      g[d] = gD[d] + gu[d];
+      dot += gD[d] * gu[d];
+      gg += gu[d] * gu[d];
+    }
+    lap = lD + lU()[e] + gg + 2 * dot;
+  }
+
+  // ---- local energy pieces
+  __device__ double kinetic() const {
+    double k = 0;
+    for (int e = lane; e < S.nelec; e += 32) {
+      double g[3], l;
+      electron_grad(e, g, l);
+      k += l;
+    }
+    return -0.5 * warp_sum(k);
+  }
+
+  // Molecular_system::calcLoc (Molecular_system.cpp:209-287), no field.
+  __device__ double coulomb() const {
+    const double* Rp = R();
+    const int N = S.nelec, A = S.natoms;
+    double v = 0;
+    for (int idx = lane; idx < N * A; idx += 32) {
+      int e = idx / A, a = idx - e * A;
+      const double* ap = S.atom_pos + 3 * a;
+      double dx = Rp[3 * e] - ap[0], dy = Rp[3 * e + 1] - ap[1], dz = Rp[3 * e + 2] - ap[2];
+      v -= S.atom_charge[a] / sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    for (int idx = lane; idx < N * N; idx += 32) {
+      int i = idx / N, j = idx - i * N;
+      if (i >= j) continue;
+      double dx = Rp[3 * i] - Rp[3 * j], dy = Rp[3 * i + 1] - Rp[3 * j + 1], dz = Rp[3 * i + 2] - Rp[3 * j + 2];
+      v += 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    return warp_sum(v) + S.ion_ion;
+  }
+
+  __device__ double pp_radial(int a, int l, double r) const {
+    double v = 0;
+    const int* tf = S.pp_term_first + 8 * a;
+    for (int t = tf[l]; t < tf[l + 1]; t++) {
+      const double* q = S.pp_term + 3 * t;
+      double ex = fmin(q[1] * r * r, 60.0);
+      v += q[2] * pow(r, q[0]) * exp(-ex);
+    }
+    return v;
+  }
+
+  // Semilocal pseudopotential (Pseudopotential::calcNonlocWithAllvariables,
+  // Pseudopotential.cpp:596-815): local channel for every (e, atom) and the
+  // Q-point quadrature of the nonlocal channels for the pairs selected
+  // deterministically (r < cutoff) or stochastically (rand < strength, with
+  // the nonlocal radials divided by the strength).  rot: 3x3 rows x,y,z.
+  __device__ double pseudo(const double* rotm, bool deterministic, uint64_t seed, uint32_t wid, uint64_t step) {
+    const double* Rp = R();
+    const int N = S.nelec, A = S.natoms;
+    double vloc = 0;
+    // per-electron Jastrow value at the current position
+    for (int e = lane; e < N; e += 32) {
+      double u, g[3], l;
+      jas_electron(S, Rp, e, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], u, g, l, false);
+      Ue()[e] = u;
+    }
+    // item list
+    int nitems = 0;
+    PPItem* it = items();
+    for (int base0 = 0; base0 < N * A; base0 += 32) {
+      int idx = base0 + lane;
+      bool take = false;
+      PPItem item;
+      if (idx < N * A) {
+        int e = idx / A, a = idx - e * A;
+        int nch = S.pp_nchan[a];
+        if (nch > 0) {
+          const double* ap = S.atom_pos + 3 * a;
+          item.e = e; item.a = a;
+          item.dx = Rp[3 * e] - ap[0]; item.dy = Rp[3 * e + 1] - ap[1]; item.dz = Rp[3 * e + 2] - ap[2];
+          item.r = sqrt(item.dx * item.dx + item.dy * item.dy + item.dz * item.dz);
+          vloc += pp_radial(a, nch - 1, item.r);
+          for (int l = 0; l < 4; l++) item.vl[l] = (l < nch - 1) ? pp_radial(a, l, item.r) : 0.0;
+          if (deterministic) {
+            take = item.r < S.pp_cutoff[a];
+          } else {
+            double strength = 0;
+            for (int l = 0; l < nch - 1; l++) strength += 10.0 * (2 * l + 1) * fabs(item.vl[l]);
+            strength = fmin(1.0, strength);
+            Rand4 rr = rand4(seed, wid, step, (uint32_t)idx, 7u);
+            if (fabs(strength) > 0)
+              for (int l = 0; l < nch - 1; l++) item.vl[l] /= strength;
+            take = strength > rr.u[0];
+          }
+        }
+      }
+      unsigned m = __ballot_sync(0xffffffffu, take);
+      int pos = nitems + __popc(m & ((1u << lane) - 1u));
+      if (take) it[pos] = item;
+      nitems += __popc(m);
+    }
+    __syncwarp();
+    double vnl = 0;
+    int total = 0;
+    for (int k = 0; k < nitems; k++) total += S.pp_aip[it[k].a];
+    // lanes over (item, quadrature point)
+    int k = 0, qoff = 0;  // running item cursor for this lane's points
+    for (int p = lane; p < total; p += 32) {
+      while (p >= qoff + S.pp_aip[it[k].a]) { qoff += S.pp_aip[it[k].a]; k++; }
+      const PPItem& I = it[k];
+      const int q = p - qoff;
+      const double* q0 = S.pp_quad + ((size_t)I.a * S.max_aip + q) * 3;
+      double qx = q0[0] * rotm[0] + q0[1] * rotm[3] + q0[2] * rotm[6];
+      double qy = q0[0] * rotm[1] + q0[1] * rotm[4] + q0[2] * rotm[7];
+      double qz = q0[0] * rotm[2] + q0[1] * rotm[5] + q0[2] * rotm[8];
+      const double* ap = S.atom_pos + 3 * I.a;
+      double nx = ap[0] + qx * I.r, ny = ap[1] + qy * I.r, nz = ap[2] + qz * I.r;
+      const int s = spin(I.e), el = eloc(I.e), M = S.m[s];
+      Real phi[MMAX];
+      mo_val_lane<Real, MMAX>(S, mocs(s), nx, ny, nz, phi);
+      const Real* iv = inv(s) + el * MMAX;
+      Real rd = 0;
+#pragma unroll
+      for (int i = 0; i < MMAX; i++)
+        if (i < M) rd += iv[i] * phi[i];
+      double u, g[3], l;
+      jas_electron(S, Rp, I.e, nx, ny, nz, u, g, l, false);
+      double ratio = double(rd) * exp(u - Ue()[I.e]) * S.pp_w[(size_t)I.a * S.max_aip + q];
+      // cos of the angle between the original and the quadrature direction
+      double ndx = nx - ap[0], ndy = ny - ap[1], ndz = nz - ap[2];
+      double nr = sqrt(ndx * ndx + ndy * ndy + ndz * ndz);
+      double c = (ndx * I.dx + ndy * I.dy + ndz * I.dz) / (nr * I.r);
+      double P[4] = {1.0, c, 0.5 * (3 * c * c - 1), 0.5 * (5 * c * c * c - 3 * c)};
+      double ts = 0;
+      for (int ll = 0; ll < 4; ll++) ts += (2 * ll + 1) * I.vl[ll] * P[ll];
+      vnl += ts * ratio;
+    }
+    return warp_sum(vloc) + warp_sum(vnl);
+  }
+};
+
+// Limited drift of Split_sampler (limDrift, drift_cyrus, Split_sample.cpp:40-88).
+__device__ __forceinline__ void lim_drift(const double d[3], double tau, double out[3]) {
+  double d2 = (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) * 0.25;
+  double a = d2 > 1e-8 ? (sqrt(1.0 + 2.0 * tau * d2) - 1.0) / d2 : tau;
+  out[0] = d[0] * a; out[1] = d[1] * a; out[2] = d[2] * a;
+}
+
+// Uniform random rotation from a random unit quaternion (Shoemake 1992).
+__device__ __forceinline__ void random_rotation(const Rand4& r, double m[9]) {
+  double s1 = sqrt(1.0 - r.u[0]), s2 = sqrt(r.u[0]);
+  double a1, b1, a2, b2;
+  sincospi(2.0 * r.u[1], &a1, &b1);
+  sincospi(2.0 * r.u[2], &a2, &b2);
+  double x = s1 * a1, y = s1 * b1, z = s2 * a2, w = s2 * b2;
+  m[0] = 1 - 2 * (y * y + z * z); m[1] = 2 * (x * y + z * w);     m[2] = 2 * (x * z - y * w);
+  m[3] = 2 * (x * y - z * w);     m[4] = 1 - 2 * (x * x + z * z); m[5] = 2 * (y * z + x * w);
+  m[6] = 2 * (x * z + y * w);     m[7] = 2 * (y * z - x * w);     m[8] = 1 - 2 * (x * x + y * y);
+}
+
+template <typename Real, int MMAX>
+__global__ void __launch_bounds__(128) k_walkers(DevSys<Real> S, WLayout L, StepParams P, EvalIO io, int mode) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int wpc = blockDim.x / 32;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+  Real* moc_s = (Real*)smem;
+  const size_t moc_elems = (size_t)2 * S.nbasis * MMAX;
+  for (size_t i = threadIdx.x; i < moc_elems; i += blockDim.x) moc_s[i] = S.moc[i];
+  const size_t moc_bytes = (moc_elems * sizeof(Real) + 15) / 16 * 16;
+  __syncthreads();
+  __shared__ double cta_acc[10];
+  if (threadIdx.x < 10) cta_acc[threadIdx.x] = 0.0;
+  __syncthreads();
+
+  const int wid = blockIdx.x * wpc + warp;
+  if (wid < P.nwalk) {
+    unsigned char* wb = smem + moc_bytes + (size_t)warp * L.bytes;
+    Walker<Real, MMAX> W{S, L, wb, moc_s, lane};
+    const int N = S.nelec;
+    double* Rp = W.R();
+    unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
+    if (mode != KM_STEPS || P.refresh) {
+      for (int i = lane; i < 3 * N; i += 32) Rp[i] = P.R[(size_t)wid * 3 * N + i];
+      double keep_e = 0, keep_w = 1;
+      if (mode == KM_STEPS) { keep_e = ((WScal*)(gstate + L.scal))->eold; keep_w = ((WScal*)(gstate + L.scal))->weight; }
+      __syncwarp();
+      W.recompute();
+      if (lane == 0 && mode == KM_STEPS) { W.sc()->eold = keep_e; W.sc()->weight = keep_w; }
+      __syncwarp();
+    } else {
+      // resident state: one coalesced copy HBM -> shared memory
+      const int4* src = (const int4*)gstate;
+      int4* dst = (int4*)wb;
+      for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
+      __syncwarp();
+    }
+
+    if (mode == KM_EVAL) {
+      double rm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+      if (io.rot)
+        for (int k = 0; k < 9; k++) rm[k] = io.rot[(size_t)wid * 9 + k];
+      for (int e = lane; e < N; e += 32) {
+        double g[3], l;
+        W.electron_grad(e, g, l);
+        double* go = io.grad + ((size_t)wid * N + e) * 3;
+        go[0] = g[0]; go[1] = g[1]; go[2] = g[2];
+        io.lap[(size_t)wid * N + e] = l;
+      }
+      double kin = W.kinetic();
+      double pot = W.coulomb();
+      double nl = S.has_pp ? W.pseudo(rm, true, 0, wid, 0) : 0.0;
+      if (lane == 0) {
+        WScal* w = W.sc();
+        io.logpsi[wid] = w->logdet[0] + w->logdet[1] + w->U;
+        io.sign[wid] = w->sign[0] * w->sign[1];
+        io.kinetic[wid] = kin;
+        io.potential[wid] = pot;
+        io.nonlocal[wid] = nl;
+      }
+    } else if (mode == KM_RATIO) {
+      const int e = io.move_e[wid];
+      const double* rn = io.move_r + 3 * (size_t)wid;
+      double ratioD, dU, g[3], l;
+      W.propose(e, rn[0], rn[1], rn[2], ratioD, dU, g, l);
+      if (lane == 0) {
+        io.logpsi[wid] = log(fabs(ratioD)) + dU;
+        io.sign[wid] = ratioD < 0 ? -1.0 : 1.0;
+        io.grad[3 * (size_t)wid] = g[0]; io.grad[3 * (size_t)wid + 1] = g[1]; io.grad[3 * (size_t)wid + 2] = g[2];
+        io.lap[wid] = l;
+      }
+    } else {
+      // ---- VMC / DMC steps
+      const double sqt = sqrt(P.tau);
+      double nacc = 0, natt = 0;
+      double sw = 0, swe = 0, swk = 0, swv = 0, swnl = 0, swe2 = 0, nbad = 0;
+      const double etr = P.dmc ? *P.etrial : 0.0;
+      const double teff = P.dmc ? P.etrial[1] : 0.0;
+      for (int st = 0; st < P.nsteps; st++) {
+        const uint64_t step = P.step0 + st;
+        for (int e = 0; e < N; e++) {
+          // Split_sampler::split_driver depth 1 (Split_sample.cpp:380-478)
+          double g0[3], l0;
+          W.electron_grad(e, g0, l0);
+          double dv[3];
+          lim_drift(g0, P.tau, dv);
+          Rand4 ra = rand4(P.seed, wid, step, e, 1u);
+          Rand4 rb = rand4(P.seed, wid, step, e, 2u);
+          double ga[4];
+          box_muller(ra.u[0], ra.u[1], ga[0], ga[1]);
+          box_muller(ra.u[2], ra.u[3], ga[2], ga[3]);
+          const double ox = Rp[3 * e], oy = Rp[3 * e + 1], oz = Rp[3 * e + 2];
+          double nx = ox + ga[0] * sqt + dv[0];
+          double ny = oy + ga[1] * sqt + dv[1];
+          double nz = oz + ga[2] * sqt + dv[2];
+          double ratioD, dU, g1[3], l1;
+          W.propose(e, nx, ny, nz, ratioD, dU, g1, l1);
+          // get_acceptance (Split_sample.cpp:302-373): psi ratio squared
+          // times the ratio of drift-diffusion Green's functions
+          double ratio = ratioD * exp(dU);
+          double acc;
+          if (P.dmc && ratio < 0) acc = 0;  // node restriction
+          else {
+            double bd[3];
+            lim_drift(g1, P.tau, bd);
+            double fw = 0, bw = 0;
+            fw -= (nx - ox - dv[0]) * (nx - ox - dv[0]) + (ny - oy - dv[1]) * (ny - oy - dv[1]) +
+                  (nz - oz - dv[2]) * (nz - oz - dv[2]);
+            bw -= (ox - nx - bd[0]) * (ox - nx - bd[0]) + (oy - ny - bd[1]) * (oy - ny - bd[1]) +
+                  (oz - nz - bd[2]) * (oz - nz - bd[2]);
+            acc = fmin(1.0, ratio * ratio * exp((bw - fw) / (2.0 * P.tau)));
+          }
+          natt += 1;
+          if (acc + rb.u[0] > 1.0) {
+            W.accept(e, nx, ny, nz, ratioD, dU);
+            nacc += 1;
+          }
+        }
+        // gatherData (Properties_gather.cpp:40-74)
+        Rand4 rr = rand4(P.seed, wid, step, 0xffffu, 3u);
+        double rm[9];
+        random_rotation(rr, rm);
+        double kin = W.kinetic();
+        double pot = W.coulomb();
+        double nl = S.has_pp ? W.pseudo(rm, P.deterministic_pp != 0, P.seed, wid, step) : 0.0;
+        double el = kin + pot + nl;
+        WScal* w = W.sc();
+        double wt = 1.0;
+        if (P.dmc) {
+          // Dmc_method::getWeight (Dmc_method.cpp:801-824) + weight clamp
+          double eold = w->eold;
+          double teffac = teff / 2.0;
+          double fbet = fmax(etr - el, etr - eold);
+          if (fbet > P.branch_stop) teffac = 0;
+          else if (fbet > P.branch_start)
+            teffac = teffac * (1. - (fbet - P.branch_start) / (P.branch_stop - P.branch_start));
+          wt = w->weight * exp(teffac * (etr * 2 - el - eold));
+          if (wt > P.max_weight) wt = P.max_weight;
+          if (!isfinite(el) || !isfinite(wt)) { nbad += 1; wt = 0.0; el = etr; }
+          __syncwarp();
+          if (lane == 0) { w->weight = wt; w->eold = el; }
+          __syncwarp();
+        } else {
+          if (!isfinite(el)) { nbad += 1; el = 0.0; wt = 0.0; }
+          if (lane == 0) w->eold = el;
+        }
+        sw += wt; swe += wt * el; swk += wt * kin; swv += wt * pot; swnl += wt * nl; swe2 += wt * el * el;
+      }
+      if (lane == 0) {
+        atomicAdd(&cta_acc[0], sw); atomicAdd(&cta_acc[1], swe); atomicAdd(&cta_acc[2], swk);
+        atomicAdd(&cta_acc[3], swv); atomicAdd(&cta_acc[4], swnl); atomicAdd(&cta_acc[5], swe2);
+        atomicAdd(&cta_acc[6], nacc); atomicAdd(&cta_acc[7], natt); atomicAdd(&cta_acc[8], nbad);
+        atomicAdd(&cta_acc[9], double(P.nsteps));
+        if (io.energy) io.energy[wid] = W.sc()->eold;
+      }
+      // write back positions and the resident state
+      __syncwarp();
+      for (int i = lane; i < 3 * N; i += 32) P.R[(size_t)wid * 3 * N + i] = Rp[i];
+      int4* dst = (int4*)gstate;
+      const int4* src = (const int4*)wb;
+      for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
+    }
+  }
+  if (mode == KM_STEPS) {
+    __syncthreads();
+    if (threadIdx.x < 10) atomicAdd(&((double*)P.acc)[threadIdx.x], cta_acc[threadIdx.x]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// DMC population control on one CTA: E_T feedback (Dmc_method::updateEtrial,
+// :780-797), constant-population split/kill pairing (match_walkers,
+// :961-995), and the copy order of calcBranch (:1099-1107): survivors in
+// walker order, each repeated by its branch count.
+//
+// dyn[0] = E_T, dyn[1] = teff, dyn[2] = sum of weights, dyn[3] = branched pairs
+struct BranchParams {
+  int nwalk, npow2;
+  double eref, feedback, timestep;
+  uint64_t seed, counter;
+  const unsigned char* state;
+  int state_bytes, scal_off;
+  const BlockAcc* acc;    // running acceptance of this chunk
+  double* dyn;
+  int* src_of;            // [W] output mapping
+  double* new_w;          // [W] weight of the slot after branching
+};
+
+__global__ void __launch_bounds__(1024) k_branch(BranchParams B) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  double* key = (double*)sm;                 // [npow2]
+  int* idx = (int*)(key + B.npow2);          // [npow2]
+  int* cnt = idx + B.npow2;                  // [nwalk]
+  double* nw = (double*)(((uintptr_t)(cnt + B.nwalk) + 15) & ~(uintptr_t)15);  // [nwalk]
+  __shared__ double red[32];
+  const int t = threadIdx.x, nt = blockDim.x;
+  double local = 0;
+  for (int i = t; i < B.npow2; i += nt) {
+    double w = 1e300;
+    if (i < B.nwalk) {
+      w = ((const WScal*)(B.state + (size_t)i * B.state_bytes + B.scal_off))->weight;
+      local += w;
+      cnt[i] = 1;
+      nw[i] = w;
+    }
+    key[i] = w;
+    idx[i] = i;
+  }
+  local = warp_sum(local);
+  if ((t & 31) == 0) red[t >> 5] = local;
+  __syncthreads();
+  if (t < 32) {
+    double v = (t < nt / 32) ? red[t] : 0.0;
+    v = warp_sum(v);
+    if (t == 0) {
+      double acc_ratio = B.acc->attempted > 0 ? B.acc->accepted / B.acc->attempted : 1.0;
+      B.dyn[1] = B.timestep * acc_ratio;
+      B.dyn[0] = B.eref - B.feedback * log(v / double(B.nwalk));
+      B.dyn[2] = v;
+    }
+  }
+  // bitonic sort ascending by weight (ties by index)
+  for (int k = 2; k <= B.npow2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      __syncthreads();
+      for (int i = t; i < B.npow2; i += nt) {
+        int ixj = i ^ j;
+        if (ixj > i) {
+          bool up = (i & k) == 0;
+          double a = key[i], b = key[ixj];
+          int ia = idx[i], ib = idx[ixj];
+          bool gt = a > b || (a == b && ia > ib);
+          if (gt == up) { key[i] = b; key[ixj] = a; idx[i] = ib; idx[ixj] = ia; }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // pairs k: the k-th largest (while >= 1.8) with the k-th smallest
+  const int W = B.nwalk;
+  int npair = 0;
+  for (int k = t; k < W / 2; k += nt) {
+    int big = W - 1 - k;
+    if (big > 1 && key[big] >= 1.8 && k < big) {
+      // all larger slots also qualify (sorted), so pair k is taken
+      int wb = idx[big], ws = idx[k];
+      double w1 = key[big], w2 = key[k];
+      double weight1 = w1 / (w1 + w2);
+      Rand4 r = rand4(B.seed, (uint32_t)k, B.counter, 0u, 5u);
+      double merged = (w1 + w2) / 2.0;
+      if (weight1 + r.u[0] >= 1.0) { cnt[wb] = 2; cnt[ws] = 0; nw[wb] = merged; }
+      else { cnt[wb] = 0; cnt[ws] = 2; nw[ws] = merged; }
+      npair++;
+    }
+  }
+  __syncthreads();
+  // exclusive prefix sum of counts in walker order (single pass per thread chunk)
+  __shared__ int chunk_sum[1024];
+  const int per = (W + nt - 1) / nt;
+  int s0 = t * per, s1 = min(W, s0 + per), cs = 0;
+  for (int i = s0; i < s1; i++) cs += cnt[i];
+  chunk_sum[t] = cs;
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+    for (int i = 0; i < nt; i++) { int v = chunk_sum[i]; chunk_sum[i] = run; run += v; }
+  }
+  __syncthreads();
+  int off = chunk_sum[t];
+  for (int i = s0; i < s1; i++) {
+    for (int c = 0; c < cnt[i]; c++) {
+      if (off < W) { B.src_of[off] = i; B.new_w[off] = nw[i]; }
+      off++;
+    }
+  }
+  if (npair) atomicAdd(&B.dyn[3], double(npair));
+}
+
+// Gather walkers into their new slots (positions + resident state).
+__global__ void k_gather(int nwalk, int n3, int state_bytes, int scal_off, const int* src_of, const double* new_w,
+                         const double* R, const unsigned char* state, double* R2, unsigned char* state2) {
+  const int w = blockIdx.x;
+  if (w >= nwalk) return;
+  const int s = src_of[w];
+  for (int i = threadIdx.x; i < n3; i += blockDim.x) R2[(size_t)w * n3 + i] = R[(size_t)s * n3 + i];
+  const int4* src = (const int4*)(state + (size_t)s * state_bytes);
+  int4* dst = (int4*)(state2 + (size_t)w * state_bytes);
+  for (int i = threadIdx.x; i < state_bytes / 16; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+  if (threadIdx.x == 0) ((WScal*)(state2 + (size_t)w * state_bytes + scal_off))->weight = new_w[w];
+}
+
+__global__ void k_set_etrial(double* dyn, double eref, double feedback, int nwalk) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) dyn[0] = eref - feedback * log(dyn[2] / double(nwalk));
+}
+
+__global__ void k_init_weights(unsigned char* state, int nwalk, int state_bytes, int scal_off, const double* eloc) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= nwalk) return;
+  WScal* s = (WScal*)(state + (size_t)w * state_bytes + scal_off);
+  s->weight = 1.0;
+  s->eold = eloc[w];
+}
+
+}  // namespace qwg

@@ -1,0 +1,240 @@
+"""Python binding (ctypes) of the walker engine's C-ABI (include/qwg.h).
+
+This mirrors the reference's module surface for the walker path: a context is
+built from a QWalk input file (SYSTEM / PSEUDO / TRIALFUNC sections), walkers
+are QWalk configurations (N x 3 positions), and the calls map onto the
+reference's per-walker operations (Slat_Jastrow::updateLap/getLap/getVal,
+System::calcKinetic/calcLoc, Pseudopotential::calcNonlocWithTest,
+Vmc_method / Dmc_method blocks).  Errors raise QwgError with the library's
+message; there is no CPU fallback: without the built library or a GPU the
+calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqwg.so")
+
+FP64 = 0
+MIXED = 1
+
+EXPORTS = [
+    "qwg_version", "qwg_last_error", "qwg_create", "qwg_destroy", "qwg_get_info", "qwg_inspect_deck",
+    "qwg_inspect_spline", "qwg_set_walkers", "qwg_get_walkers", "qwg_set_walkers_device", "qwg_eval",
+    "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_launch_count",
+    "qwg_reset_launch_count",
+]
+
+
+class QwgError(RuntimeError):
+    pass
+
+
+class Info(C.Structure):
+    _fields_ = [("nelec", C.c_int), ("nup", C.c_int), ("ndown", C.c_int), ("natoms", C.c_int),
+                ("nbasis", C.c_int), ("nshell", C.c_int), ("nmo_up", C.c_int), ("nmo_down", C.c_int),
+                ("has_pseudo", C.c_int), ("max_walkers", C.c_int), ("precision", C.c_int),
+                ("walkers_per_cta", C.c_int), ("ion_ion", C.c_double)]
+
+
+class EvalOut(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in
+                ("logpsi", "sign", "grad", "lap", "kinetic", "potential", "nonlocal")]
+
+
+class BlockStats(C.Structure):
+    _fields_ = [("energy", C.c_double), ("kinetic", C.c_double), ("potential", C.c_double),
+                ("nonlocal", C.c_double), ("weight", C.c_double), ("energy_var", C.c_double),
+                ("acceptance", C.c_double), ("etrial", C.c_double), ("block_ms", C.c_double),
+                ("nsteps", C.c_int), ("nwalkers", C.c_int), ("nonfinite", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class DmcParams(C.Structure):
+    _fields_ = [("timestep", C.c_double), ("nstep", C.c_int), ("feedback_interval", C.c_int),
+                ("feedback", C.c_double), ("max_poss_weight", C.c_double),
+                ("branch_start_cutoff", C.c_double), ("refresh_interval", C.c_int),
+                ("deterministic_pp", C.c_int), ("seed", C.c_uint64)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libqwg.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise QwgError(f"engine library not built: {path} (run python -m mainline_b200.build)")
+    lib = C.CDLL(path)
+    P = C.POINTER
+    dp = P(C.c_double)
+    sig = {
+        "qwg_version": (C.c_char_p, []),
+        "qwg_last_error": (C.c_char_p, [C.c_void_p]),
+        "qwg_create": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_void_p, P(C.c_void_p)]),
+        "qwg_destroy": (C.c_int, [C.c_void_p]),
+        "qwg_get_info": (C.c_int, [C.c_void_p, P(Info)]),
+        "qwg_inspect_deck": (C.c_int, [C.c_char_p, P(Info), C.c_char_p, C.c_int]),
+        "qwg_inspect_spline": (C.c_int, [C.c_char_p, C.c_int, dp, C.c_int, P(C.c_int), dp, dp]),
+        "qwg_set_walkers": (C.c_int, [C.c_void_p, dp, C.c_int]),
+        "qwg_get_walkers": (C.c_int, [C.c_void_p, dp, C.c_int]),
+        "qwg_set_walkers_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+        "qwg_eval": (C.c_int, [C.c_void_p, dp, P(EvalOut)]),
+        "qwg_ratio": (C.c_int, [C.c_void_p, P(C.c_int), dp, dp, dp, dp, dp]),
+        "qwg_vmc_block": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_int, P(BlockStats)]),
+        "qwg_dmc_init": (C.c_int, [C.c_void_p, P(DmcParams)]),
+        "qwg_dmc_block": (C.c_int, [C.c_void_p, P(BlockStats)]),
+        "qwg_launch_count": (C.c_longlong, [C.c_void_p]),
+        "qwg_reset_launch_count": (None, [C.c_void_p]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def inspect_deck(deck_path: str) -> Info:
+    lib = load_library()
+    info = Info()
+    err = C.create_string_buffer(512)
+    rc = lib.qwg_inspect_deck(deck_path.encode(), C.byref(info), err, 512)
+    if rc != 0:
+        raise QwgError(err.value.decode())
+    return info
+
+
+def inspect_spline(deck_path: str, shell: int):
+    lib = load_library()
+    n = C.c_int(0)
+    sp = C.c_double(0)
+    cut = C.c_double(0)
+    rc = lib.qwg_inspect_spline(deck_path.encode(), shell, None, 0, C.byref(n), C.byref(sp), C.byref(cut))
+    if rc != 0:
+        raise QwgError(f"qwg_inspect_spline failed ({rc})")
+    coef = np.zeros((n.value, 4))
+    lib.qwg_inspect_spline(deck_path.encode(), shell, _ptr(coef), n.value, C.byref(n), C.byref(sp), C.byref(cut))
+    return coef, sp.value, cut.value
+
+
+@dataclass
+class EvalResult:
+    logpsi: np.ndarray
+    sign: np.ndarray
+    grad: np.ndarray
+    lap: np.ndarray
+    kinetic: np.ndarray
+    potential: np.ndarray
+    nonlocal_: np.ndarray
+
+    @property
+    def energy(self):
+        return self.kinetic + self.potential + self.nonlocal_
+
+
+class Engine:
+    """One GPU walker engine context built from a QWalk deck."""
+
+    def __init__(self, deck_path: str, precision: int = FP64, max_walkers: int = 4096, stream=None):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.qwg_create(os.path.abspath(deck_path).encode(), precision, max_walkers,
+                                 C.c_void_p(stream) if stream else None, C.byref(h))
+        if rc != 0:
+            raise QwgError(f"qwg_create failed ({rc}): {self.lib.qwg_last_error(None).decode()}")
+        self.h = h
+        self.info = Info()
+        self.lib.qwg_get_info(self.h, C.byref(self.info))
+        self.nelec = self.info.nelec
+        self.nwalk = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.qwg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise QwgError(f"{what} failed ({rc}): {self.lib.qwg_last_error(self.h).decode()}")
+
+    def set_walkers(self, R: np.ndarray):
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        assert R.ndim == 3 and R.shape[1] == self.nelec and R.shape[2] == 3
+        self._check(self.lib.qwg_set_walkers(self.h, _ptr(R), R.shape[0]), "qwg_set_walkers")
+        self.nwalk = R.shape[0]
+
+    def set_walkers_device(self, ptr: int, nw: int):
+        self._check(self.lib.qwg_set_walkers_device(self.h, C.c_void_p(ptr), nw), "qwg_set_walkers_device")
+        self.nwalk = nw
+
+    def get_walkers(self) -> np.ndarray:
+        R = np.zeros((self.nwalk, self.nelec, 3))
+        self._check(self.lib.qwg_get_walkers(self.h, _ptr(R), self.nwalk), "qwg_get_walkers")
+        return R
+
+    def eval(self, rot: np.ndarray | None = None) -> EvalResult:
+        W, N = self.nwalk, self.nelec
+        o = {k: np.zeros(W) for k in ("logpsi", "sign", "kinetic", "potential", "nonlocal")}
+        o["grad"] = np.zeros((W, N, 3))
+        o["lap"] = np.zeros((W, N))
+        out = EvalOut(*[_ptr(o[k]) for k in ("logpsi", "sign", "grad", "lap", "kinetic", "potential", "nonlocal")])
+        rp = None
+        if rot is not None:
+            rot = np.ascontiguousarray(rot, dtype=np.float64).reshape(W, 9)
+            rp = _ptr(rot)
+        self._check(self.lib.qwg_eval(self.h, rp, C.byref(out)), "qwg_eval")
+        return EvalResult(o["logpsi"], o["sign"], o["grad"], o["lap"], o["kinetic"], o["potential"], o["nonlocal"])
+
+    def ratio(self, e: np.ndarray, rnew: np.ndarray):
+        W = self.nwalk
+        e = np.ascontiguousarray(e, dtype=np.int32)
+        rnew = np.ascontiguousarray(rnew, dtype=np.float64)
+        dl, sg, lp = np.zeros(W), np.zeros(W), np.zeros(W)
+        g = np.zeros((W, 3))
+        self._check(self.lib.qwg_ratio(self.h, e.ctypes.data_as(C.POINTER(C.c_int)), _ptr(rnew), _ptr(dl),
+                                       _ptr(sg), _ptr(g), _ptr(lp)), "qwg_ratio")
+        return dl, sg, g, lp
+
+    def vmc_block(self, nstep: int, timestep: float, seed: int = 1, deterministic_pp: bool = False) -> dict:
+        st = BlockStats()
+        self._check(self.lib.qwg_vmc_block(self.h, nstep, timestep, seed, int(deterministic_pp), C.byref(st)),
+                    "qwg_vmc_block")
+        return st.as_dict()
+
+    def dmc_init(self, timestep: float, nstep: int = 0, seed: int = 1, feedback_interval: int = 5,
+                 feedback: float = 1.0, max_poss_weight: float = 7.0, branch_start_cutoff: float = 10.0,
+                 refresh_interval: int = 0, deterministic_pp: bool = False):
+        p = DmcParams(timestep, nstep, feedback_interval, feedback, max_poss_weight, branch_start_cutoff,
+                      refresh_interval, int(deterministic_pp), seed)
+        self._check(self.lib.qwg_dmc_init(self.h, C.byref(p)), "qwg_dmc_init")
+
+    def dmc_block(self) -> dict:
+        st = BlockStats()
+        self._check(self.lib.qwg_dmc_block(self.h, C.byref(st)), "qwg_dmc_block")
+        return st.as_dict()
+
+    def launch_count(self) -> int:
+        return int(self.lib.qwg_launch_count(self.h))
+
+    def reset_launch_count(self):
+        self.lib.qwg_reset_launch_count(self.h)

@@ -15,8 +15,10 @@ Workloads (sizes are fixed; only the seed varies):
   coefficients ~N(0, 0.1)).
 * ``n2_pseudo``  the same molecule and electrons with each nucleus replaced by
   a Z_eff=5 semilocal RGAUSSIAN pseudopotential: l=0 and l=1 nonlocal
-  channels plus a local channel, 3 Gaussians each (exponents U[1,10],
-  coefficients U(-5,5)), 12-point quadrature (AIP 12).
+  channels (3 Gaussians each, exponents U[1,10], coefficients U(-5,5)) plus a
+  local channel whose Z_eff/r Gaussian cancels the ion's -Z_eff/r at the
+  nucleus; 12-point quadrature (AIP 12).  Same shell structure (40 functions
+  per atom) with valence exponents log-uniform in [0.1, 10].
 """
 from __future__ import annotations
 
@@ -133,14 +135,21 @@ def _jastrow_text(label: str, onebody: np.ndarray, threebody=None, twobody_pp=No
     ] + g2)
 
 
-def _pseudo_text(rng, label: str, aip: int = 12) -> str:
+def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
     """RGAUSSIAN OLDQMC block: channels l=0, l=1 and the local channel (the
-    reference treats the LAST listed channel as local, Pseudopotential.cpp:790)."""
+    reference treats the LAST listed channel as local, Pseudopotential.cpp:790).
+    Nonlocal channels: 3 Gaussians each, exponents U[1,10], coefficients
+    U(-5,5).  Local channel: Z_eff/r exp(-a r^2) (cancels the bare -Z_eff/r of
+    the ion at the nucleus, as semilocal pseudopotentials do) plus two
+    Gaussians of the same distribution."""
     lines = [f"PSEUDO {{ {label}", f"  AIP {aip}", f"  BASIS {{ {label}", "  RGAUSSIAN", "  OLDQMC {",
              "  0.0 3", "  3 3 3"]
-    for _l in range(3):
+    for _l in range(2):
         for _ in range(3):
             lines.append(f"    2 {_fmt(rng.uniform(1.0, 10.0))} {_fmt(rng.uniform(-5.0, 5.0))}")
+    lines.append(f"    1 {_fmt(rng.uniform(1.0, 10.0))} {_fmt(zeff)}")
+    for _ in range(2):
+        lines.append(f"    2 {_fmt(rng.uniform(1.0, 10.0))} {_fmt(rng.uniform(-5.0, 5.0))}")
     lines += ["  }", "  }", "}"]
     return "\n".join(lines)
 
@@ -155,13 +164,16 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
     label = "N"
     charge = 5 if pseudo else 7
     nup = ndown = 7
-    shells = _basis_shells(rng, {"S": 10, "P": 6, "6D": 2})
+    # all-electron cores need the tight exponents; pseudopotential atoms use the
+    # valence range (with [0.1, 1e4] the random-MO trial function sends the
+    # reference's own DMC to E_T < -3e4 Ha within 10 blocks)
+    shells = _basis_shells(rng, {"S": 10, "P": 6, "6D": 2}, hi=10.0 if pseudo else 1e4)
     nper = sum(SHELL_NFUNC[s] for s, _, _ in shells)
     nb = 2 * nper
     cup = _random_orthonormal(rng, nb, nup)
     cdn = _random_orthonormal(rng, nb, ndown)
     onebody = rng.normal(0.0, 0.1, size=4)
-    pp = _pseudo_text(rng, label) if pseudo else ""
+    pp = _pseudo_text(rng, label, charge) if pseudo else ""
     name = name or ("n2_pseudo" if pseudo else "n2_allelectron")
     orb = os.path.join(outdir, f"{name}.orb")
     _write_orb(orb, np.concatenate([cup, cdn], axis=1), [nper, nper])

@@ -1,0 +1,66 @@
+"""CPU-side checks of the C-ABI library: it loads without a GPU, exports every
+symbol include/qwg.h declares, and its host table builder (deck parser +
+spline fit) reproduces the oracle's tables."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+import qworacle
+from mainline_b200 import engine
+
+HEADER = os.path.join(ROOT, "include", "qwg.h")
+
+
+def _declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(qwg_[a-z_]+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(engine.LIB_PATH):
+        from mainline_b200 import build
+        build.build()
+    return engine.load_library()
+
+
+def test_exports_every_declared_symbol(lib):
+    names = _declared()
+    assert set(names) == set(engine.EXPORTS)
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_version(lib):
+    assert b"sm_100a" in lib.qwg_version()
+
+
+@pytest.mark.parametrize("name", ["n2_allelectron", "n2_pseudo"])
+def test_inspect_deck(lib, name):
+    info = engine.inspect_deck(os.path.join(GOLDEN, name + ".qw"))
+    assert (info.nelec, info.nup, info.ndown, info.natoms, info.nbasis) == (14, 7, 7, 2, 80)
+    assert info.nshell == 36
+    assert info.has_pseudo == (name == "n2_pseudo")
+
+
+def test_spline_tables_match_oracle(lib):
+    deck = os.path.join(GOLDEN, "n2_pseudo.qw")
+    S = qworacle.System(deck)
+    shells = [(b, k) for b in S.center_basis[0] for k in range(len(b.syms))]
+    for sh, (b, k) in enumerate(shells):
+        coef, spacing, cut = engine.inspect_spline(deck, sh)
+        ref = b.coeffs[k]
+        assert spacing == b.spacing
+        assert cut == b.threshold
+        # rounding-level differences (tridiagonal solve order)
+        np.testing.assert_allclose(coef[:len(ref)], ref, rtol=1e-7, atol=1e-12 * np.abs(ref).max())
+
+
+def test_bad_deck_reports_error(lib, tmp_path):
+    p = tmp_path / "bad.qw"
+    p.write_text("SYSTEM { MOLECULE NSPIN { 1 0 } ATOM { H 1 COOR 0 0 0 } }\nTRIALFUNC { SLATER }\n")
+    with pytest.raises(engine.QwgError, match="SLATER-JASTROW"):
+        engine.inspect_deck(str(p))
