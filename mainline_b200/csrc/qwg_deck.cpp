@@ -520,8 +520,13 @@ HostSystem build_system(const std::string& deck_path) {
     throw InputError("CENTERS must be USEATOMS or USEGLOBAL");
   std::vector<int> nfunc_center(S.natoms, 0);
   int first = 0;
+  for (auto& B : bases) {
+    S.obj_first.push_back(B.spline_ids.empty() ? 0 : B.spline_ids[0]);
+    S.obj_count.push_back((int)B.spline_ids.size());
+  }
   for (int c = 0; c < S.natoms; c++) {
-    for (auto& B : bases) {
+    for (size_t bi = 0; bi < bases.size(); bi++) {
+      auto& B = bases[bi];
       if (B.label != S.labels[c]) continue;
       for (size_t k = 0; k < B.syms.size(); k++) {
         Shell sh;
@@ -531,6 +536,8 @@ HostSystem build_system(const std::string& deck_path) {
         sh.first = first;
         sh.nfunc = sym_nfunc(B.syms[k]);
         sh.cutoff = B.threshold;
+        sh.obj = (int)bi;
+        sh.k = (int)k;
         first += sh.nfunc;
         S.shells.push_back(sh);
       }

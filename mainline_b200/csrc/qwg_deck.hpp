@@ -36,6 +36,8 @@ struct Shell {
   int first;       // first basis function (global index)
   int nfunc;
   double cutoff;   // basis-object threshold: r >= cutoff gives zero
+  int obj;         // basis object (BASIS section) the spline belongs to
+  int k;           // spline index inside its basis object
 };
 
 // A scalar Jastrow radial function (f, f'/r, lap).
@@ -75,6 +77,7 @@ struct HostSystem {
   int nspline = 0, spline_npts = 0;
   double spline_spacing = 0.02;
   std::vector<double> spline_coef;   // [nspline][npts][4]
+  std::vector<int> obj_first, obj_count;   // per basis object: its splines
   // molecular orbitals per spin: [nbasis][m_s]
   int nmo[2] = {0, 0};
   std::vector<double> moc[2];

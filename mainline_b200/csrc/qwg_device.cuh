@@ -46,10 +46,15 @@ struct DevSys {
   const double* atom_pos;        // [A][3]
   const double* atom_charge;     // [A]
   double ion_ion;
-  const int4* shell_i;           // (center, spline, sym, first)
+  const int4* shell_i;           // (center, sym, first, k) per shell, sorted by center
+  const int2* shell_obj;         // (table base in 4-tuples, splines in the object)
   const double* shell_cut;       // [nshell]
-  const Real* spline;            // [nspline][npts][4] (Real: used by value-only points)
-  const double* spline64;        // [nspline][npts][4] FP64 copy (value/gradient/Laplacian)
+  const int2* center_shells;     // per atom: (first shell, count)
+  // radial spline tables, interval-major per basis object: the 4 cubic
+  // coefficients of every spline of an object for interval i are contiguous
+  // (one row of nk x 4 values), so all shells of a center read one row.
+  const Real* spline;            // Real copy (value-only quadrature points)
+  const double* spline64;        // FP64 copy (value/gradient/Laplacian)
   int npts;
   double spacing, inv_spacing;
   const Real* moc;               // [2][nbasis][mstride]
@@ -183,25 +188,6 @@ __device__ __forceinline__ float warp_sum(float v) {
 // ---------------------------------------------------------------------------
 // radial functions
 
-// Cubic spline: f, f'/r, f'' at r (r < table threshold); s = spline index.
-template <typename Real>
-__device__ __forceinline__ void spline_lap(const DevSys<Real>& S, int s, Real r, Real& f, Real& fd, Real& f2) {
-  int i = int(r * Real(S.inv_spacing));
-  Real h = r - Real(i) * Real(S.spacing);
-  const Real* c = S.spline + ((size_t)s * S.npts + i) * 4;
-  Real c0 = __ldg(c), c1 = __ldg(c + 1), c2 = __ldg(c + 2), c3 = __ldg(c + 3);
-  f = c0 + h * (c1 + h * (c2 + h * c3));
-  fd = (c1 + h * (Real(2) * c2 + h * (Real(3) * c3))) / r;
-  f2 = Real(2) * c2 + Real(6) * h * c3;
-}
-template <typename Real>
-__device__ __forceinline__ Real spline_val(const DevSys<Real>& S, int s, Real r) {
-  int i = int(r * Real(S.inv_spacing));
-  Real h = r - Real(i) * Real(S.spacing);
-  const Real* c = S.spline + ((size_t)s * S.npts + i) * 4;
-  return __ldg(c) + h * (__ldg(c + 1) + h * (__ldg(c + 2) + h * __ldg(c + 3)));
-}
-
 // Jastrow radial function (value, f'/r, 3D Laplacian).  Zero at r >= rcut.
 template <typename T>
 __device__ __forceinline__ void radial_lap(const DRadial& q, T r, T& f, T& fd, T& lap) {
@@ -235,135 +221,169 @@ __device__ __forceinline__ void radial_lap(const DRadial& q, T r, T& f, T& fd, T
 }
 template <typename T>
 __device__ __forceinline__ T radial_val(const DRadial& q, T r) {
-  T f, fd, l;
   if (!(r < T(q.rcut))) return T(0);
-  radial_lap(q, r, f, fd, l);
-  return f;
+  const T rcut = T(q.rcut);
+  T zz = r / rcut, zz2 = zz * zz;
+  if (q.kind == 0) {
+    T pp = zz - zz2 + zz * zz2 / T(3);
+    return T(q.a) * rcut * (pp / (T(1) + T(q.b) * pp) - T(1) / (T(3) + T(q.b)));
+  }
+  T zpp = zz2 * (T(6) - T(8) * zz + T(3) * zz2);
+  return (T(1) - zpp) / (T(1) + T(q.a) * zpp);
 }
 
 // ---------------------------------------------------------------------------
-// angular parts of a shell: fills v[k][5] = (value, d/dx, d/dy, d/dz, lap) of
-// the Cartesian Gaussian-type function A(x,y,z) f(r) from f, f'/r, f''.
+// Basis functions: Cartesian Gaussian-type A(x,y,z) f(r) from the spline's
+// f, f'/r, f''.  Value, gradient (dA f + A f'/r r_vec) and Laplacian
 // lap = A f'' + (2l+2) A f'/r + f lap(A) for a homogeneous A of degree l.
+// Orderings follow the GAMESS conventions of Cubic_spline_build.cpp:660-760.
+
+// Writes the 5 components of one function to out[0..4] (a basis row).
 template <typename Real>
-__device__ __forceinline__ int shell_lap(int sym, Real x, Real y, Real z, Real f, Real fd, Real f2, Real v[6][5]) {
-  auto put = [&](int k, Real A, Real ax, Real ay, Real az, Real lapA, int l) {
-    Real h = A * fd;
-    v[k][0] = A * f;
-    v[k][1] = h * x + ax * f;
-    v[k][2] = h * y + ay * f;
-    v[k][3] = h * z + az * f;
-    v[k][4] = A * f2 + Real(2 * l + 2) * h + lapA * f;
-  };
-  const Real o = Real(1), zr = Real(0);
-  switch (sym) {
-    case 0: put(0, o, zr, zr, zr, zr, 0); return 1;
-    case 1:
-      put(0, x, o, zr, zr, zr, 1); put(1, y, zr, o, zr, zr, 1); put(2, z, zr, zr, o, zr, 1);
-      return 3;
-    case 2:
-      put(0, x * x, Real(2) * x, zr, zr, Real(2), 2);
-      put(1, y * y, zr, Real(2) * y, zr, Real(2), 2);
-      put(2, z * z, zr, zr, Real(2) * z, Real(2), 2);
-      put(3, x * y, y, x, zr, zr, 2);
-      put(4, x * z, z, zr, x, zr, 2);
-      put(5, y * z, zr, z, y, zr, 2);
-      return 6;
-    default:
-      put(0, Real(2) * z * z - x * x - y * y, Real(-2) * x, Real(-2) * y, Real(4) * z, zr, 2);
-      put(1, x * z, z, zr, x, zr, 2);
-      put(2, y * z, zr, z, y, zr, 2);
-      put(3, x * x - y * y, Real(2) * x, Real(-2) * y, zr, zr, 2);
-      put(4, x * y, y, x, zr, zr, 2);
-      return 5;
-  }
+__device__ __forceinline__ void put_lap(Real* out, double A, double ax, double ay, double az, double lapA, int l,
+                                        double x, double y, double z, double f, double fd, double f2) {
+  double v = A * f;
+  double h = A * fd;
+  bool keep = fabs(v) > 1e-8;   // the dense evaluator drops |value| <= 1e-8
+  out[0] = Real(keep ? v : 0.0);
+  out[1] = Real(keep ? h * x + ax * f : 0.0);
+  out[2] = Real(keep ? h * y + ay * f : 0.0);
+  out[3] = Real(keep ? h * z + az * f : 0.0);
+  out[4] = Real(keep ? A * f2 + double(2 * l + 2) * h + lapA * f : 0.0);
 }
+
 template <typename Real>
-__device__ __forceinline__ int shell_val(int sym, Real x, Real y, Real z, Real f, Real v[6]) {
+__device__ __forceinline__ void shell_lap_store(int sym, double x, double y, double z, double f, double fd, double f2,
+                                                Real* b /* [nf][5] */) {
   switch (sym) {
-    case 0: v[0] = f; return 1;
-    case 1: v[0] = x * f; v[1] = y * f; v[2] = z * f; return 3;
+    case 0: put_lap(b, 1.0, 0.0, 0.0, 0.0, 0.0, 0, x, y, z, f, fd, f2); break;
+    case 1:
+      put_lap(b, x, 1.0, 0.0, 0.0, 0.0, 1, x, y, z, f, fd, f2);
+      put_lap(b + 5, y, 0.0, 1.0, 0.0, 0.0, 1, x, y, z, f, fd, f2);
+      put_lap(b + 10, z, 0.0, 0.0, 1.0, 0.0, 1, x, y, z, f, fd, f2);
+      break;
     case 2:
-      v[0] = x * x * f; v[1] = y * y * f; v[2] = z * z * f;
-      v[3] = x * y * f; v[4] = x * z * f; v[5] = y * z * f;
-      return 6;
+      put_lap(b, x * x, 2 * x, 0.0, 0.0, 2.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 5, y * y, 0.0, 2 * y, 0.0, 2.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 10, z * z, 0.0, 0.0, 2 * z, 2.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 15, x * y, y, x, 0.0, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 20, x * z, z, 0.0, x, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 25, y * z, 0.0, z, y, 0.0, 2, x, y, z, f, fd, f2);
+      break;
     default:
-      v[0] = (Real(2) * z * z - x * x - y * y) * f; v[1] = x * z * f; v[2] = y * z * f;
-      v[3] = (x * x - y * y) * f; v[4] = x * y * f;
-      return 5;
+      put_lap(b, 2 * z * z - x * x - y * y, -2 * x, -2 * y, 4 * z, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 5, x * z, z, 0.0, x, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 10, y * z, 0.0, z, y, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 15, x * x - y * y, 2 * x, -2 * y, 0.0, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap(b + 20, x * y, y, x, 0.0, 0.0, 2, x, y, z, f, fd, f2);
+      break;
   }
 }
 
-// ---------------------------------------------------------------------------
-// MO evaluation (value, gradient, Laplacian) of one position, warp-cooperative.
-// bas: [nbasis][5] scratch; out: [M][5]; moc_s: [nbasis][mstride] (shared).
-// A basis function whose value is within 1e-8 of zero contributes nothing
-// (the dense MO evaluator's skip, MO_matrix_blas.h:468-470).
+__device__ __forceinline__ int sym_nfunc(int sym) { return sym == 0 ? 1 : sym == 1 ? 3 : sym == 2 ? 6 : 5; }
+
+// MO value, gradient and Laplacian of one position, warp-cooperative.
+// Lanes split the shells (radial spline and angular factors in FP64: the
+// Laplacian of the tight shells cancels strongly), basis rows go to bas
+// [nbasis][5] as Real, then lanes split the (MO, component) outputs of the
+// contraction with the MO coefficients moc_s [nbasis][mstride].
 template <typename Real>
 __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz, int M,
                             Real* bas, Real* out, int lane) {
-  // radial spline and angular factors in FP64 (the Laplacian of the tight
-  // shells cancels strongly); the basis values are then stored as Real
   for (int s = lane; s < S.nshell; s += 32) {
     int4 si = S.shell_i[s];
+    int2 so = S.shell_obj[s];
     const double* ap = S.atom_pos + 3 * si.x;
     double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
     double r = sqrt(dx * dx + dy * dy + dz * dz);
-    double v[6][5];
-    int nf;
+    Real* b = bas + si.z * 5;
     if (r < S.shell_cut[s]) {
       int i = int(r * S.inv_spacing);
       double h = r - double(i) * S.spacing;
-      const double2* c2p = reinterpret_cast<const double2*>(S.spline64 + ((size_t)si.y * S.npts + i) * 4);
+      const double2* c2p = reinterpret_cast<const double2*>(S.spline64 + ((size_t)so.x + (size_t)i * so.y + si.w) * 4);
       double2 ca = __ldg(c2p), cb = __ldg(c2p + 1);
       double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
       double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
       double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
-      nf = shell_lap(si.z, dx, dy, dz, f, fd, f2, v);
-      for (int k = 0; k < nf; k++)
-        if (!(fabs(v[k][0]) > 1e-8))
-          for (int c = 0; c < 5; c++) v[k][c] = 0.0;
+      shell_lap_store(si.y, dx, dy, dz, f, fd, f2, b);
     } else {
-      nf = si.z == 0 ? 1 : si.z == 1 ? 3 : si.z == 2 ? 6 : 5;
-      for (int k = 0; k < nf; k++)
-        for (int c = 0; c < 5; c++) v[k][c] = 0.0;
+      const int nf = sym_nfunc(si.y);
+      for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
     }
-    for (int k = 0; k < nf; k++)
-      for (int c = 0; c < 5; c++) bas[(si.w + k) * 5 + c] = Real(v[k][c]);
   }
   __syncwarp();
   const int nout = M * 5;
   for (int o = lane; o < nout; o += 32) {
     int mo = o / 5, c = o - mo * 5;
-    Real acc = Real(0);
-    const Real* b = bas + c;
+    Real a0 = Real(0), a1 = Real(0);
+    const Real* bb = bas + c;
     const Real* w = moc_s + mo;
-    for (int f = 0; f < S.nbasis; f++) acc += b[f * 5] * w[f * S.mstride];
-    out[mo * 5 + c] = acc;
+    int f = 0;
+    for (; f + 1 < S.nbasis; f += 2) {
+      a0 += bb[f * 5] * w[f * S.mstride];
+      a1 += bb[(f + 1) * 5] * w[(f + 1) * S.mstride];
+    }
+    if (f < S.nbasis) a0 += bb[f * 5] * w[f * S.mstride];
+    out[mo * 5 + c] = a0 + a1;
   }
   __syncwarp();
 }
 
-// MO values of one position evaluated entirely by the calling lane.
+// MO values of one position evaluated entirely by the calling lane (the
+// quadrature points of the pseudopotential).  Centers in turn: one distance
+// and one spline row per center, all shells of the center from that row.
+template <typename Real, int MMAX>
+__device__ __forceinline__ void acc_fn(Real phi[MMAX], const Real* moc_s, int f, Real v) {
+  v = fabs(v) > Real(1e-8) ? v : Real(0);
+  const Real* w = moc_s + (size_t)f * MMAX;
+#pragma unroll
+  for (int m = 0; m < MMAX; m++) phi[m] += v * w[m];
+}
+
 template <typename Real, int MMAX>
 __device__ __forceinline__ void mo_val_lane(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz,
                                             Real phi[MMAX]) {
 #pragma unroll
   for (int m = 0; m < MMAX; m++) phi[m] = Real(0);
-  for (int s = 0; s < S.nshell; s++) {
-    int4 si = S.shell_i[s];
-    const double* ap = S.atom_pos + 3 * si.x;
-    double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
-    double r = sqrt(dx * dx + dy * dy + dz * dz);
-    if (!(r < S.shell_cut[s])) continue;
-    Real f = spline_val(S, si.y, Real(r));
-    Real v[6];
-    int nf = shell_val(si.z, Real(dx), Real(dy), Real(dz), f, v);
-    for (int k = 0; k < nf; k++) {
-      if (!(fabs(double(v[k])) > 1e-8)) continue;
-      const Real* w = moc_s + (size_t)(si.w + k) * MMAX;
-#pragma unroll
-      for (int m = 0; m < MMAX; m++) phi[m] += v[k] * w[m];
+  for (int c = 0; c < S.natoms; c++) {
+    int2 cs = S.center_shells[c];
+    if (cs.y == 0) continue;
+    const double* ap = S.atom_pos + 3 * c;
+    double dxd = px - ap[0], dyd = py - ap[1], dzd = pz - ap[2];
+    double rd = sqrt(dxd * dxd + dyd * dyd + dzd * dzd);
+    const Real x = Real(dxd), y = Real(dyd), z = Real(dzd);
+    const int i = int(rd * S.inv_spacing);
+    const Real h = Real(rd - double(i) * S.spacing);
+    for (int s = cs.x; s < cs.x + cs.y; s++) {
+      if (!(rd < S.shell_cut[s])) continue;
+      int4 si = S.shell_i[s];
+      int2 so = S.shell_obj[s];
+      const Real* cp = S.spline + ((size_t)so.x + (size_t)i * so.y + si.w) * 4;
+      Real f = __ldg(cp) + h * (__ldg(cp + 1) + h * (__ldg(cp + 2) + h * __ldg(cp + 3)));
+      const int fb = si.z;
+      switch (si.y) {
+        case 0: acc_fn<Real, MMAX>(phi, moc_s, fb, f); break;
+        case 1: {
+          acc_fn<Real, MMAX>(phi, moc_s, fb, x * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 1, y * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 2, z * f);
+        } break;
+        case 2: {
+          acc_fn<Real, MMAX>(phi, moc_s, fb, x * x * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 1, y * y * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 2, z * z * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 3, x * y * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 4, x * z * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 5, y * z * f);
+        } break;
+        default: {
+          acc_fn<Real, MMAX>(phi, moc_s, fb, (Real(2) * z * z - x * x - y * y) * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 1, x * z * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 2, y * z * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 3, (x * x - y * y) * f);
+          acc_fn<Real, MMAX>(phi, moc_s, fb + 4, x * y * f);
+        } break;
+      }
     }
   }
 }
@@ -478,6 +498,41 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
       for (int d = 0; d < 3; d++) g[d] += tgi[d];
     }
   }
+}
+
+// Value-only version of jas_electron (the pseudopotential quadrature points).
+template <typename Real>
+__device__ double jas_electron_val(const DevSys<Real>& S, const double* R, int i, double px, double py, double pz) {
+  double u = 0.0;
+  for (int a = 0; a < S.natoms; a++) {
+    const double* ap = S.atom_pos + 3 * a;
+    double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    int f0 = S.ei_first[a], nf = S.ei_count[a];
+    for (int k = 0; k < nf; k++) {
+      double c = S.onebody[f0 + k];
+      if (c != 0.0) u += c * radial_val(S.ei[f0 + k], r);
+    }
+  }
+  const bool si = i < S.nup;
+  const bool has3 = S.tb != nullptr;
+  const double pi[3] = {px, py, pz};
+  for (int j = 0; j < S.nelec; j++) {
+    if (j == i) continue;
+    double dx = px - R[3 * j], dy = py - R[3 * j + 1], dz = pz - R[3 * j + 2];
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const bool same = si == (j < S.nup);
+    for (int k = 0; k < S.nee; k++) {
+      double c = same ? S.ee_like[k] : S.ee_unlike[k];
+      if (c != 0.0) u += c * radial_val(S.ee[k], r);
+    }
+    if (has3) {
+      double tu, tgi[3], tli, tgj[3], tlj;
+      jas_threebody_pair(S, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false);
+      u += tu;
+    }
+  }
+  return u;
 }
 
 // ---------------------------------------------------------------------------

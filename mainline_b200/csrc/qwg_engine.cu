@@ -69,7 +69,7 @@ struct qwg_ctx {
   bool own_stream = false;
   long long launches = 0;
   // tables
-  DevBuf d_atom_pos, d_atom_charge, d_shell_i, d_shell_cut, d_spline, d_spline64, d_moc, d_ee, d_ee_like, d_ee_unlike, d_ei,
+  DevBuf d_atom_pos, d_atom_charge, d_shell_i, d_shell_obj, d_center_shells, d_shell_cut, d_spline, d_spline64, d_moc, d_ee, d_ee_like, d_ee_unlike, d_ei,
       d_ei_first, d_ei_count, d_onebody, d_tb_first, d_tb_count, d_tb, d_pp_nchan, d_pp_aip, d_pp_cutoff,
       d_pp_term_first, d_pp_term, d_pp_quad, d_pp_w;
   DevSys<double> sys_d{};
@@ -106,6 +106,8 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S) {
   S.atom_charge = c->d_atom_charge.as<double>();
   S.ion_ion = H.ion_ion;
   S.shell_i = c->d_shell_i.as<int4>();
+  S.shell_obj = c->d_shell_obj.as<int2>();
+  S.center_shells = c->d_center_shells.as<int2>();
   S.shell_cut = c->d_shell_cut.as<double>();
   S.spline = c->d_spline.as<Real>();
   S.spline64 = c->d_spline64.as<double>();
@@ -144,13 +146,35 @@ static void build_tables(qwg_ctx* c) {
   const int A = H.natoms;
   upload(c->d_atom_pos, H.atom_pos, st);
   upload(c->d_atom_charge, H.atom_charge, st);
+  // interval-major spline tables: object o occupies npts x count_o x 4 values
+  const int npts = H.spline_npts;
+  std::vector<int> obj_base(H.obj_first.size());
+  size_t total4 = 0;
+  for (size_t o = 0; o < H.obj_first.size(); o++) {
+    obj_base[o] = (int)total4;
+    total4 += (size_t)npts * H.obj_count[o];
+  }
+  std::vector<double> il(total4 * 4, 0.0);
+  for (size_t o = 0; o < H.obj_first.size(); o++)
+    for (int i = 0; i < npts; i++)
+      for (int k = 0; k < H.obj_count[o]; k++)
+        for (int q = 0; q < 4; q++)
+          il[((size_t)obj_base[o] + (size_t)i * H.obj_count[o] + k) * 4 + q] =
+              H.spline_coef[((size_t)(H.obj_first[o] + k) * npts + i) * 4 + q];
   std::vector<int4> si;
+  std::vector<int2> so, cs(A, make_int2(0, 0));
   std::vector<double> sc;
-  for (auto& s : H.shells) {
-    si.push_back(make_int4(s.center, s.spline, s.sym, s.first));
+  for (size_t k = 0; k < H.shells.size(); k++) {
+    const Shell& s = H.shells[k];
+    si.push_back(make_int4(s.center, s.sym, s.first, s.k));
+    so.push_back(make_int2(obj_base[s.obj], H.obj_count[s.obj]));
     sc.push_back(s.cutoff);
+    if (cs[s.center].y == 0) cs[s.center].x = (int)k;
+    cs[s.center].y++;
   }
   upload(c->d_shell_i, si, st);
+  upload(c->d_shell_obj, so, st);
+  upload(c->d_center_shells, cs, st);
   upload(c->d_shell_cut, sc, st);
   // MO coefficients padded to MMAX columns, both spins
   const int mm = c->mmax;
@@ -158,12 +182,12 @@ static void build_tables(qwg_ctx* c) {
   for (int s = 0; s < 2; s++)
     for (int f = 0; f < H.nbasis; f++)
       for (int i = 0; i < H.nmo[s]; i++) moc[((size_t)s * H.nbasis + f) * mm + i] = H.moc[s][(size_t)f * H.nmo[s] + i];
-  upload(c->d_spline64, H.spline_coef, st);
+  upload(c->d_spline64, il, st);
   if (c->precision == QWG_FP64) {
-    upload(c->d_spline, H.spline_coef, st);
+    upload(c->d_spline, il, st);
     upload(c->d_moc, moc, st);
   } else {
-    std::vector<float> sf(H.spline_coef.begin(), H.spline_coef.end());
+    std::vector<float> sf(il.begin(), il.end());
     std::vector<float> mf(moc.begin(), moc.end());
     upload(c->d_spline, sf, st);
     upload(c->d_moc, mf, st);
@@ -213,7 +237,8 @@ static void build_tables(qwg_ctx* c) {
   upload(c->d_pp_w, w, st);
   fill_sys<double>(c, c->sys_d);
   fill_sys<float>(c, c->sys_f);
-  const void* req[] = {c->sys_d.atom_pos, c->sys_d.atom_charge, c->sys_d.shell_i, c->sys_d.shell_cut,
+  const void* req[] = {c->sys_d.atom_pos, c->sys_d.atom_charge, c->sys_d.shell_i, c->sys_d.shell_obj,
+                       c->sys_d.center_shells, c->sys_d.shell_cut,
                        c->sys_d.spline, c->sys_d.spline64, c->sys_d.moc, c->sys_d.ee, c->sys_d.ee_like, c->sys_d.ee_unlike,
                        c->sys_d.ei, c->sys_d.ei_first, c->sys_d.ei_count, c->sys_d.onebody, c->sys_d.tb_first,
                        c->sys_d.tb_count, c->sys_d.pp_nchan, c->sys_d.pp_aip, c->sys_d.pp_cutoff,
@@ -239,10 +264,14 @@ static void make_layout(qwg_ctx* c) {
   L.state_bytes = o;
   L.bas = o; o = align16(o + rs * H.nbasis * 5);
   L.newcol = o; o = align16(o + rs * mm * 5);
-  L.dG = o; o = align16(o + 8 * 4 * N);
-  L.Ue = o; o = align16(o + 8 * N);
-  L.lu = o; o = align16(o + 8 * mm * 2 * mm);
-  L.items = o; o = align16(o + (int)sizeof(PPItem) * N * A);
+  // dG (move proposals) and Ue (pseudopotential) are never live together;
+  // nor are lu (re-inversion, Sherman-Morrison scratch) and the PP items
+  L.dG = o;
+  L.Ue = o;
+  o = align16(o + std::max(8 * 4 * N, 8 * N));
+  L.lu = o;
+  L.items = o;
+  o = align16(o + std::max(8 * mm * 2 * mm, (int)sizeof(PPItem) * N * A));
   L.rot = o; o = align16(o + 8 * 9);
   L.bytes = o;
   const size_t moc_bytes = ((size_t)2 * H.nbasis * mm * rs + 15) / 16 * 16;
@@ -254,15 +283,22 @@ static void make_layout(qwg_ctx* c) {
   if (c->smem_bytes > 227 * 1024) throw InputError("system too large for the shared-memory walker kernel");
 }
 
+template <typename Real, int MM, int MODE>
+static void launch_mode(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int nwalk) {
+  auto kern = k_walkers<Real, MM, MODE>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
+  int grid = (nwalk + c->wpc - 1) / c->wpc;
+  kern<<<grid, 32 * c->wpc, c->smem_bytes, c->stream>>>(S, c->L, P, io);
+  CK(cudaGetLastError());
+  c->launches++;
+}
+
 template <typename Real, int MM>
 static void launch_walkers_t(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int mode,
                              int nwalk) {
-  auto kern = k_walkers<Real, MM>;
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
-  int grid = (nwalk + c->wpc - 1) / c->wpc;
-  kern<<<grid, 32 * c->wpc, c->smem_bytes, c->stream>>>(S, c->L, P, io, mode);
-  CK(cudaGetLastError());
-  c->launches++;
+  if (mode == KM_EVAL) launch_mode<Real, MM, KM_EVAL>(c, S, P, io, nwalk);
+  else if (mode == KM_RATIO) launch_mode<Real, MM, KM_RATIO>(c, S, P, io, nwalk);
+  else launch_mode<Real, MM, KM_STEPS>(c, S, P, io, nwalk);
 }
 
 static void launch_walkers(qwg_ctx* c, const StepParams& P, const EvalIO& io, int mode, int nwalk) {

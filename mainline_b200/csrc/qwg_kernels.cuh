@@ -169,15 +169,27 @@ struct Walker {
       }
       dg[0] = g0; dg[1] = g1; dg[2] = g2; dg[3] = l0;
     }
-    du = warp_sum(du);
-    ge[0] = warp_sum(ge[0]); ge[1] = warp_sum(ge[1]); ge[2] = warp_sum(ge[2]);
-    le = warp_sum(le);
-    double obn, ogn[3], oln, obo, ogo[3], olo;
-    jas_onebody(S, px, py, pz, obn, ogn, oln);
-    jas_onebody(S, ox, oy, oz, obo, ogo, olo);
-    dU = du + obn - obo;
-    double gu[3] = {ge[0] + ogn[0], ge[1] + ogn[1], ge[2] + ogn[2]};
-    double lu_ = le + oln;
+    // one-body terms: lanes over (atom, function) pairs
+    for (int a = 0; a < S.natoms; a++) {
+      const int f0 = S.ei_first[a], nf = S.ei_count[a];
+      if (lane >= nf) continue;
+      for (int k = lane; k < nf; k += 32) {
+        const double c = S.onebody[f0 + k];
+        if (c == 0.0) continue;
+        const double* ap = S.atom_pos + 3 * a;
+        double nx = px - ap[0], ny = py - ap[1], nz = pz - ap[2];
+        double qx = ox - ap[0], qy = oy - ap[1], qz = oz - ap[2];
+        double rn = sqrt(nx * nx + ny * ny + nz * nz), ro = sqrt(qx * qx + qy * qy + qz * qz);
+        double fnv, fnd, fnl;
+        radial_lap(S.ei[f0 + k], rn, fnv, fnd, fnl);
+        du += c * (fnv - radial_val(S.ei[f0 + k], ro));
+        ge[0] += c * fnd * nx; ge[1] += c * fnd * ny; ge[2] += c * fnd * nz;
+        le += c * fnl;
+      }
+    }
+    dU = warp_sum(du);
+    double gu[3] = {warp_sum(ge[0]), warp_sum(ge[1]), warp_sum(ge[2])};
+    double lu_ = warp_sum(le);
     double dot = 0, gg = 0;
     for (int d = 0; d < 3; d++) {
       gnew[d] = gD[d] + gu[d];
@@ -302,11 +314,7 @@ struct Walker {
     const int N = S.nelec, A = S.natoms;
     double vloc = 0;
     // per-electron Jastrow value at the current position
-    for (int e = lane; e < N; e += 32) {
-      double u, g[3], l;
-      jas_electron(S, Rp, e, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], u, g, l, false);
-      Ue()[e] = u;
-    }
+    for (int e = lane; e < N; e += 32) Ue()[e] = jas_electron_val(S, Rp, e, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2]);
     // item list
     int nitems = 0;
     PPItem* it = items();
@@ -366,8 +374,7 @@ struct Walker {
 #pragma unroll
       for (int i = 0; i < MMAX; i++)
         if (i < M) rd += iv[i] * phi[i];
-      double u, g[3], l;
-      jas_electron(S, Rp, I.e, nx, ny, nz, u, g, l, false);
+      const double u = jas_electron_val(S, Rp, I.e, nx, ny, nz);
       double ratio = double(rd) * exp(u - Ue()[I.e]) * S.pp_w[(size_t)I.a * S.max_aip + q];
       // cos of the angle between the original and the quadrature direction
       double ndx = nx - ap[0], ndy = ny - ap[1], ndz = nz - ap[2];
@@ -401,8 +408,11 @@ __device__ __forceinline__ void random_rotation(const Rand4& r, double m[9]) {
   m[6] = 2 * (x * z + y * w);     m[7] = 2 * (y * z - x * w);     m[8] = 1 - 2 * (x * x + y * y);
 }
 
-template <typename Real, int MMAX>
-__global__ void __launch_bounds__(128) k_walkers(DevSys<Real> S, WLayout L, StepParams P, EvalIO io, int mode) {
+#ifndef QWG_MIN_BLOCKS
+#define QWG_MIN_BLOCKS 4  // resident 128-thread CTAs per SM the register budget is sized for
+#endif
+template <typename Real, int MMAX, int mode>
+__global__ void __launch_bounds__(128, QWG_MIN_BLOCKS) k_walkers(DevSys<Real> S, WLayout L, StepParams P, EvalIO io) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int wpc = blockDim.x / 32;
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
@@ -438,7 +448,7 @@ __global__ void __launch_bounds__(128) k_walkers(DevSys<Real> S, WLayout L, Step
       __syncwarp();
     }
 
-    if (mode == KM_EVAL) {
+    if constexpr (mode == KM_EVAL) {
       double rm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
       if (io.rot)
         for (int k = 0; k < 9; k++) rm[k] = io.rot[(size_t)wid * 9 + k];
@@ -460,7 +470,7 @@ __global__ void __launch_bounds__(128) k_walkers(DevSys<Real> S, WLayout L, Step
         io.potential[wid] = pot;
         io.nonlocal[wid] = nl;
       }
-    } else if (mode == KM_RATIO) {
+    } else if constexpr (mode == KM_RATIO) {
       const int e = io.move_e[wid];
       const double* rn = io.move_r + 3 * (size_t)wid;
       double ratioD, dU, g[3], l;
@@ -563,7 +573,7 @@ __global__ void __launch_bounds__(128) k_walkers(DevSys<Real> S, WLayout L, Step
       for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
     }
   }
-  if (mode == KM_STEPS) {
+  if constexpr (mode == KM_STEPS) {
     __syncthreads();
     if (threadIdx.x < 10) atomicAdd(&((double*)P.acc)[threadIdx.x], cta_acc[threadIdx.x]);
   }
