@@ -151,6 +151,36 @@ int qwg_vmc_block(qwg_ctx* ctx, int nstep, double timestep, uint64_t seed, int d
 int qwg_dmc_init(qwg_ctx* ctx, const qwg_dmc_params* p);
 int qwg_dmc_block(qwg_ctx* ctx, qwg_block_stats* stats);
 
+/* VMC block that allocates no device memory.
+ *
+ * No counterpart in the reference: QWalk's walker loop runs on the CPU.
+ *
+ * For callers that must not allocate device memory while they run: a serving
+ * loop that has already divided HBM among the jobs it admitted, a host that
+ * works inside a fixed device-memory budget owned by another allocator, or
+ * code with kernels of other jobs in flight that must not wait on the
+ * device-wide synchronisation cudaMalloc/cudaFree can cause.  The context
+ * (tables) is built beforehand with qwg_create; this call then only launches.
+ *
+ * It runs the same kernel as qwg_vmc_block, but the walkers' resident state
+ * and the block accumulators live in one file-scope device array of
+ * QWG_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library holds
+ * until the process exits.  nw * (per-walker state bytes) + 256 must fit in
+ * it, else QWG_ERR_ARG (qwg_last_error names the largest nw that fits).
+ * Buffers are the caller's device memory, ordered on the context's stream:
+ *   d_R       [nw][nelec][3] walker positions, read and overwritten
+ *   d_energy  [nw] local energy of each walker after the last step (or NULL)
+ *   d_sums    [10] block sums: sum w, sum wE, sum wT, sum wV, sum wV_NL,
+ *             sum wE^2, accepted moves, attempted moves, non-finite, points
+ * The first call on a device looks up that device's address of the array
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture.  All calls share the one array and it keeps the
+ * last call's contents: the accumulators are cleared on every call, and calls
+ * whose work overlaps on the GPU (other streams, other contexts) race on it. */
+#define QWG_NOALLOC_SCRATCH_BYTES (16u << 20)
+int qwg_vmc_block_noalloc(qwg_ctx* ctx, double* d_R, int nw, int nstep, double timestep, uint64_t seed,
+                          int deterministic_pp, double* d_energy, double* d_sums);
+
 /* Number of kernel launches the context issued since the last reset. */
 long long qwg_launch_count(const qwg_ctx* ctx);
 void qwg_reset_launch_count(qwg_ctx* ctx);

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -787,6 +788,86 @@ int qwg_dmc_block(qwg_ctx* c, qwg_block_stats* stats) {
       stats->nwalkers = c->nwalk;
       stats->etrial = c->eref - c->dmc.feedback * std::log(dyn[2] / double(c->nwalk));
     }
+    return QWG_OK;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free VMC block: the walker state and the accumulators live in one
+// file-scope device array instead of the context's buffers.  In host code
+// g_noalloc_scratch names a host-side stand-in, not a device address; the
+// device address is looked up once per device and passed to the kernel.
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[QWG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on the current device (first call per
+// device does the lookup).
+void* noalloc_scratch_device_ptr(std::string& err) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) {
+    err = std::string("qwg_vmc_block_noalloc: no usable current device: ") + cudaGetErrorString(e);
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      err = std::string("qwg_vmc_block_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+      return nullptr;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double timestep, uint64_t seed,
+                          int deterministic_pp, double* d_energy, double* d_sums) {
+  if (!c) return QWG_ERR_ARG;
+  if (!d_R || !d_sums || nw <= 0 || nstep <= 0 || !(timestep > 0))
+    return fail(c, QWG_ERR_ARG, "qwg_vmc_block_noalloc: bad arguments");
+  const size_t acc_bytes = 256;  // BlockAcc at the start, walker state after it
+  static_assert(sizeof(BlockAcc) <= 256, "accumulator block exceeds its scratch slot");
+  const size_t need = acc_bytes + (size_t)nw * c->L.state_bytes;
+  if (need > QWG_NOALLOC_SCRATCH_BYTES) {
+    const size_t maxw = (QWG_NOALLOC_SCRATCH_BYTES - acc_bytes) / c->L.state_bytes;
+    return fail(c, QWG_ERR_ARG, "qwg_vmc_block_noalloc: " + std::to_string(nw) + " walkers need " +
+                                    std::to_string(need) + " bytes of scratch; the fixed scratch holds " +
+                                    std::to_string(QWG_NOALLOC_SCRATCH_BYTES) + " bytes (at most " +
+                                    std::to_string(maxw) + " walkers of this system)");
+  }
+  std::string err;
+  unsigned char* base = (unsigned char*)noalloc_scratch_device_ptr(err);
+  if (!base) return fail(c, QWG_ERR_CUDA, err);
+  return guarded(c, [&]() -> int {
+    BlockAcc* acc = (BlockAcc*)base;
+    CK(cudaMemsetAsync(acc, 0, sizeof(BlockAcc), c->stream));
+    StepParams P{};
+    P.nwalk = nw;
+    P.nsteps = nstep;
+    P.refresh = 1;
+    P.dmc = 0;
+    P.deterministic_pp = deterministic_pp;
+    P.tau = timestep;
+    P.seed = seed;
+    P.step0 = c->step_counter;
+    P.max_weight = 1.0;
+    P.R = d_R;
+    P.state = base + acc_bytes;
+    P.acc = acc;
+    P.etrial = c->d_dyn.as<double>();
+    EvalIO io{};
+    io.energy = d_energy;
+    launch_walkers(c, P, io, KM_STEPS, nw);
+    CK(cudaMemcpyAsync(d_sums, acc, 10 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    c->step_counter += nstep;
     return QWG_OK;
   });
 }
