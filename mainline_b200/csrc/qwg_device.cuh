@@ -349,13 +349,12 @@ __device__ __forceinline__ void mo_val_lane(const DevSys<Real>& S, const Real* m
     int2 cs = S.center_shells[c];
     if (cs.y == 0) continue;
     const double* ap = S.atom_pos + 3 * c;
-    double dxd = px - ap[0], dyd = py - ap[1], dzd = pz - ap[2];
-    double rd = sqrt(dxd * dxd + dyd * dyd + dzd * dzd);
-    const Real x = Real(dxd), y = Real(dyd), z = Real(dzd);
-    const int i = int(rd * S.inv_spacing);
-    const Real h = Real(rd - double(i) * S.spacing);
+    const Real x = Real(px - ap[0]), y = Real(py - ap[1]), z = Real(pz - ap[2]);
+    const Real rd = sqrt(x * x + y * y + z * z);
+    const int i = int(rd * Real(S.inv_spacing));
+    const Real h = rd - Real(i) * Real(S.spacing);
     for (int s = cs.x; s < cs.x + cs.y; s++) {
-      if (!(rd < S.shell_cut[s])) continue;
+      if (!(rd < Real(S.shell_cut[s]))) continue;
       int4 si = S.shell_i[s];
       int2 so = S.shell_obj[s];
       const Real* cp = S.spline + ((size_t)so.x + (size_t)i * so.y + si.w) * 4;
@@ -402,6 +401,20 @@ __device__ __forceinline__ void jas_pair(const DevSys<Real>& S, bool same, doubl
     radial_lap(S.ee[k], r, f, d, l);
     u += c * f; fd += c * d; lap += c * l;
   }
+}
+
+// Two-body u(r) evaluated in precision T, returned as doubles.
+template <typename T, typename Real>
+__device__ __forceinline__ void jas_pair_t(const DevSys<Real>& S, bool same, T r, double& u, double& fd, double& lap) {
+  T uu = T(0), ff = T(0), ll = T(0);
+  for (int k = 0; k < S.nee; k++) {
+    const double c = same ? S.ee_like[k] : S.ee_unlike[k];
+    if (c == 0.0) continue;
+    T f, d, l;
+    radial_lap<T>(S.ee[k], r, f, d, l);
+    uu += T(c) * f; ff += T(c) * d; ll += T(c) * l;
+  }
+  u = double(uu); fd = double(ff); lap = double(ll);
 }
 
 // One-body sum over atoms for an electron at p: value, gradient, lap.
@@ -473,7 +486,7 @@ __device__ void jas_threebody_pair(const DevSys<Real>& S, const double pi[3], co
 
 // Everything of the Jastrow exponent that depends on electron i placed at p
 // (others at R): value U_i (one-body + all pairs with i), gradient, lap.
-template <typename Real>
+template <bool TB, typename Real>
 __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, double px, double py, double pz,
                              double& u, double g[3], double& lap, bool need_derivs) {
   double ob, og[3], ol;
@@ -481,7 +494,7 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
   u = ob; lap = ol;
   for (int d = 0; d < 3; d++) g[d] = og[d];
   const bool si = i < S.nup;
-  const bool has3 = S.tb != nullptr;
+  constexpr bool has3 = TB;  // e-e-n terms compiled in only when the deck has them
   const double pi[3] = {px, py, pz};
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
@@ -491,7 +504,7 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
     jas_pair(S, si == (j < S.nup), r, pu, pfd, pl);
     u += pu; lap += pl;
     g[0] += pfd * dx; g[1] += pfd * dy; g[2] += pfd * dz;
-    if (has3) {
+    if constexpr (has3) {
       double tu, tgi[3], tli, tgj[3], tlj;
       jas_threebody_pair(S, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, need_derivs);
       u += tu; lap += tli;
@@ -500,36 +513,38 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
   }
 }
 
-// Value-only version of jas_electron (the pseudopotential quadrature points).
-template <typename Real>
-__device__ double jas_electron_val(const DevSys<Real>& S, const double* R, int i, double px, double py, double pz) {
-  double u = 0.0;
+// Value-only version of jas_electron (the pseudopotential quadrature points),
+// in the working precision T (float on the mixed path): differences of the
+// FP64 positions are taken first, then everything runs in T.
+template <typename T, bool TB, typename Real>
+__device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, double px, double py, double pz) {
+  T u = T(0);
   for (int a = 0; a < S.natoms; a++) {
     const double* ap = S.atom_pos + 3 * a;
-    double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
-    double r = sqrt(dx * dx + dy * dy + dz * dz);
-    int f0 = S.ei_first[a], nf = S.ei_count[a];
+    const T dx = T(px - ap[0]), dy = T(py - ap[1]), dz = T(pz - ap[2]);
+    const T r = sqrt(dx * dx + dy * dy + dz * dz);
+    const int f0 = S.ei_first[a], nf = S.ei_count[a];
     for (int k = 0; k < nf; k++) {
-      double c = S.onebody[f0 + k];
-      if (c != 0.0) u += c * radial_val(S.ei[f0 + k], r);
+      const double c = S.onebody[f0 + k];
+      if (c != 0.0) u += T(c) * radial_val<T>(S.ei[f0 + k], r);
     }
   }
   const bool si = i < S.nup;
-  const bool has3 = S.tb != nullptr;
+  constexpr bool has3 = TB;  // e-e-n terms compiled in only when the deck has them
   const double pi[3] = {px, py, pz};
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
-    double dx = px - R[3 * j], dy = py - R[3 * j + 1], dz = pz - R[3 * j + 2];
-    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const T dx = T(px - R[3 * j]), dy = T(py - R[3 * j + 1]), dz = T(pz - R[3 * j + 2]);
+    const T r = sqrt(dx * dx + dy * dy + dz * dz);
     const bool same = si == (j < S.nup);
     for (int k = 0; k < S.nee; k++) {
-      double c = same ? S.ee_like[k] : S.ee_unlike[k];
-      if (c != 0.0) u += c * radial_val(S.ee[k], r);
+      const double c = same ? S.ee_like[k] : S.ee_unlike[k];
+      if (c != 0.0) u += T(c) * radial_val<T>(S.ee[k], r);
     }
-    if (has3) {
+    if constexpr (has3) {
       double tu, tgi[3], tli, tgj[3], tlj;
       jas_threebody_pair(S, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false);
-      u += tu;
+      u += T(tu);
     }
   }
   return u;

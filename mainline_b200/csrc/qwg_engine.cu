@@ -286,7 +286,7 @@ static void make_layout(qwg_ctx* c) {
 
 template <typename Real, int MM, int MODE>
 static void launch_mode(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int nwalk) {
-  auto kern = k_walkers<Real, MM, MODE>;
+  auto kern = S.tb ? k_walkers<Real, MM, MODE, true> : k_walkers<Real, MM, MODE, false>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
   int grid = (nwalk + c->wpc - 1) / c->wpc;
   kern<<<grid, 32 * c->wpc, c->smem_bytes, c->stream>>>(S, c->L, P, io);

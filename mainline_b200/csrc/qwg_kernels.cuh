@@ -29,7 +29,7 @@ struct PPItem {
   double vl[4];          // nonlocal channel radials (already scaled)
 };
 
-template <typename Real, int MMAX>
+template <typename Real, int MMAX, bool TB>
 struct Walker {
   const DevSys<Real>& S;
   const WLayout& L;
@@ -89,7 +89,7 @@ struct Walker {
     double usum = 0.0;
     for (int i = lane; i < S.nelec; i += 32) {
       double u, g[3], l, ob, og[3], ol;
-      jas_electron(S, Rp, i, Rp[3 * i], Rp[3 * i + 1], Rp[3 * i + 2], u, g, l, true);
+      jas_electron<TB>(S, Rp, i, Rp[3 * i], Rp[3 * i + 1], Rp[3 * i + 2], u, g, l, true);
       jas_onebody(S, Rp[3 * i], Rp[3 * i + 1], Rp[3 * i + 2], ob, og, ol);
       gU()[3 * i] = g[0]; gU()[3 * i + 1] = g[1]; gU()[3 * i + 2] = g[2];
       lU()[i] = l;
@@ -138,25 +138,26 @@ struct Walker {
     // Jastrow: lanes over the other electrons
     const double ox = Rp[3 * e], oy = Rp[3 * e + 1], oz = Rp[3 * e + 2];
     const bool se = s == 0;
-    const bool has3 = S.tb != nullptr;
+    constexpr bool has3 = TB;
     double du = 0.0, ge[3] = {0, 0, 0}, le = 0.0;
     for (int j = lane; j < S.nelec; j += 32) {
       double* dg = dG() + 4 * j;
       if (j == e) continue;
       const double* pj = Rp + 3 * j;
       const bool same = se == (j < S.nup);
-      double nx = px - pj[0], ny = py - pj[1], nz = pz - pj[2];
-      double qx = ox - pj[0], qy = oy - pj[1], qz = oz - pj[2];
-      double rn = sqrt(nx * nx + ny * ny + nz * nz), ro = sqrt(qx * qx + qy * qy + qz * qz);
+      const double nx = px - pj[0], ny = py - pj[1], nz = pz - pj[2];
+      const double qx = ox - pj[0], qy = oy - pj[1], qz = oz - pj[2];
+      // pair functions in the working precision, sums in FP64
+      const Real rn = sqrt(Real(nx * nx + ny * ny + nz * nz)), ro = sqrt(Real(qx * qx + qy * qy + qz * qz));
       double un, fn, ln, uo, fo, lo;
-      jas_pair(S, same, rn, un, fn, ln);
-      jas_pair(S, same, ro, uo, fo, lo);
+      jas_pair_t<Real>(S, same, rn, un, fn, ln);
+      jas_pair_t<Real>(S, same, ro, uo, fo, lo);
       du += un - uo;
       ge[0] += fn * nx; ge[1] += fn * ny; ge[2] += fn * nz;
       le += ln;
       // gradient w.r.t. r_j of u(r_e - r_j) = -f'/r (r_e - r_j)
       double g0 = -fn * nx + fo * qx, g1 = -fn * ny + fo * qy, g2 = -fn * nz + fo * qz, l0 = ln - lo;
-      if (has3) {
+      if constexpr (has3) {
         double pn[3] = {px, py, pz}, po[3] = {ox, oy, oz};
         double tu, tgi[3], tli, tgj[3], tlj, su, sgi[3], sli, sgj[3], slj;
         jas_threebody_pair(S, pn, pj, tu, tgi, tli, tgj, tlj, true);
@@ -299,7 +300,10 @@ struct Walker {
     for (int t = tf[l]; t < tf[l + 1]; t++) {
       const double* q = S.pp_term + 3 * t;
       double ex = fmin(q[1] * r * r, 60.0);
-      v += q[2] * pow(r, q[0]) * exp(-ex);
+      const double n = q[0];
+      const double rn = n == 0.0 ? 1.0 : n == -1.0 ? 1.0 / r : n == 1.0 ? r : n == -2.0 ? 1.0 / (r * r)
+                      : n == 2.0 ? r * r : pow(r, n);
+      v += q[2] * rn * exp(-ex);
     }
     return v;
   }
@@ -314,7 +318,8 @@ struct Walker {
     const int N = S.nelec, A = S.natoms;
     double vloc = 0;
     // per-electron Jastrow value at the current position
-    for (int e = lane; e < N; e += 32) Ue()[e] = jas_electron_val(S, Rp, e, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2]);
+    for (int e = lane; e < N; e += 32)
+      Ue()[e] = double(jas_electron_val<Real, TB>(S, Rp, e, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2]));
     // item list
     int nitems = 0;
     PPItem* it = items();
@@ -374,8 +379,8 @@ struct Walker {
 #pragma unroll
       for (int i = 0; i < MMAX; i++)
         if (i < M) rd += iv[i] * phi[i];
-      const double u = jas_electron_val(S, Rp, I.e, nx, ny, nz);
-      double ratio = double(rd) * exp(u - Ue()[I.e]) * S.pp_w[(size_t)I.a * S.max_aip + q];
+      const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);
+      double ratio = double(rd * exp(u - Real(Ue()[I.e]))) * S.pp_w[(size_t)I.a * S.max_aip + q];
       // cos of the angle between the original and the quadrature direction
       double ndx = nx - ap[0], ndy = ny - ap[1], ndz = nz - ap[2];
       double nr = sqrt(ndx * ndx + ndy * ndy + ndz * ndz);
@@ -411,7 +416,7 @@ __device__ __forceinline__ void random_rotation(const Rand4& r, double m[9]) {
 #ifndef QWG_MIN_BLOCKS
 #define QWG_MIN_BLOCKS 4  // resident 128-thread CTAs per SM the register budget is sized for
 #endif
-template <typename Real, int MMAX, int mode>
+template <typename Real, int MMAX, int mode, bool TB>
 __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS) k_walkers(DevSys<Real> S, WLayout L, StepParams P, EvalIO io) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int wpc = blockDim.x / 32;
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS) k_walkers(DevSys<Real> S,
   const int wid = blockIdx.x * wpc + warp;
   if (wid < P.nwalk) {
     unsigned char* wb = smem + moc_bytes + (size_t)warp * L.bytes;
-    Walker<Real, MMAX> W{S, L, wb, moc_s, lane};
+    Walker<Real, MMAX, TB> W{S, L, wb, moc_s, lane};
     const int N = S.nelec;
     double* Rp = W.R();
     unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
