@@ -13,8 +13,9 @@
 // Within a walker, lanes split the independent pieces of each phase: basis
 // shells for one position, (MO, component) outputs of the MO contraction,
 // electrons or pairs for the Jastrow, quadrature points for the pseudopotential
-// (one lane evaluates a whole point: basis, MOs, determinant ratio and
-// Jastrow).  Phases communicate through shared memory with __syncwarp().
+// (one lane evaluates a whole point: basis values dotted with the electron's
+// projected coefficients, and the Jastrow).  Phases communicate through
+// shared memory with __syncwarp().
 //
 // Real = double: everything in FP64.  Real = float (mixed precision): basis,
 // MO values, determinant ratios, inverse and its Sherman-Morrison updates in
@@ -31,25 +32,38 @@ namespace qwg {
 
 struct DRadial {
   int kind;         // 0 CUTOFF_CUSP, 1 POLYPADE
-  double rcut, a, b;
+  double rcut, inv_rcut;
+  double a, b, c;   // CUTOFF_CUSP: cusp, gamma, 1/(3+gamma) ; POLYPADE: beta
 };
 struct DTB {
-  int k, l, m;
+  int k, l, m;      // e-n functions k, l of the atom's type, e-e function m
   double c;
 };
 
+// Capacities of the tables carried in the kernel parameter bank.
+constexpr int QWG_MAXA = 64;       // atoms
+constexpr int QWG_MAXT = 8;        // atom types (labels)
+constexpr int QWG_MAXEE = 8;       // e-e radial functions
+constexpr int QWG_MAXEI = 8;       // e-n radial functions per type
+constexpr int QWG_MAXTB = 12;      // e-e-n terms per type
+constexpr int QWG_MAXPPT = 16;     // pseudopotential Gaussian terms per type
+constexpr int QWG_MAXQ = 12;       // quadrature points
+constexpr int QWG_MAXSHELL = 1024; // basis shells
+
+// System tables.  Large tables (splines, MO coefficients, the per-shell
+// arrays read by lanes that each take a different shell) live in HBM; the
+// small ones are carried by value in the kernel's __grid_constant__
+// parameter, so the uniform reads of the Jastrow, pseudopotential and
+// per-center loops come from the constant cache instead of L1/L2.
 template <typename Real>
 struct DevSys {
   int nelec, nup, ndn, natoms, nbasis, nshell;
   int m[2];                      // MOs per spin (= electrons per spin)
   int mstride;                   // padded MO stride of moc rows (= MMAX)
-  const double* atom_pos;        // [A][3]
-  const double* atom_charge;     // [A]
   double ion_ion;
   const int4* shell_i;           // (center, sym, first, k) per shell, sorted by center
   const int2* shell_obj;         // (table base in 4-tuples, splines in the object)
   const double* shell_cut;       // [nshell]
-  const int2* center_shells;     // per atom: (first shell, count)
   // radial spline tables, interval-major per basis object: the 4 cubic
   // coefficients of every spline of an object for interval i are contiguous
   // (one row of nk x 4 values), so all shells of a center read one row.
@@ -58,34 +72,36 @@ struct DevSys {
   int npts;
   double spacing, inv_spacing;
   const Real* moc;               // [2][nbasis][mstride]
+  // ---- parameter-bank tables
+  double atom_pos[QWG_MAXA][3];
+  double atom_charge[QWG_MAXA];
+  int atom_type[QWG_MAXA];
+  int4 center_seg[QWG_MAXA];     // (first shell, shells, spline-object base, splines in the object)
+  double center_cut[QWG_MAXA];   // basis-object threshold of the center
+  int shell_pack[QWG_MAXSHELL];  // sym | first << 4 | k << 20
   // Jastrow
   int nee;
-  const DRadial* ee;             // [nee]
-  const double* ee_like;         // [nee]
-  const double* ee_unlike;       // [nee]
-  const DRadial* ei;             // [nei]
-  const int* ei_first;           // [A]
-  const int* ei_count;           // [A]
-  const double* onebody;         // [nei]
-  const int* tb_first;           // [A]
-  const int* tb_count;           // [A]
-  const DTB* tb;
-  int max_ei;                    // max functions on one atom
-  // pseudopotential
+  DRadial ee[QWG_MAXEE];
+  double ee_like[QWG_MAXEE], ee_unlike[QWG_MAXEE];
+  int ei_n[QWG_MAXT];
+  DRadial ei[QWG_MAXT][QWG_MAXEI];
+  double onebody[QWG_MAXT][QWG_MAXEI];
+  int tb_n[QWG_MAXT];
+  DTB tb[QWG_MAXT][QWG_MAXTB];
+  int has_tb;
+  // pseudopotential per type (nchan 0: none)
   int has_pp;
-  const int* pp_nchan;           // [A] (0: none)
-  const int* pp_aip;             // [A]
-  const double* pp_cutoff;       // [A]
-  const int* pp_term_first;      // [A][8] offsets (nchan+1 used)
-  const double* pp_term;         // [nterm][3] = (n, a, c)
-  const double* pp_quad;         // [A][maxaip][3]
-  const double* pp_w;            // [A][maxaip]
-  int max_aip;
+  int pp_nchan[QWG_MAXT], pp_aip[QWG_MAXT];
+  double pp_cutoff[QWG_MAXT];
+  int pp_term_first[QWG_MAXT][8];
+  double pp_term[QWG_MAXT][QWG_MAXPPT][3];  // (n, a, c)
+  double pp_quad[QWG_MAXT][QWG_MAXQ][3];
+  double pp_w[QWG_MAXT][QWG_MAXQ];
 };
 
 // Per-walker shared-memory layout (byte offsets, host computed).
 struct WLayout {
-  int R, inv, mov, gU, lU, scal, bas, newcol, dG, Ue, lu, items, rot, bytes;
+  int R, inv, mov, gU, lU, scal, bas, newcol, dG, Ue, lu, items, rot, wproj, wchunk, bytes;
   int state_bytes;  // prefix [0, state_bytes) is the persistent walker state
 };
 
@@ -192,41 +208,39 @@ __device__ __forceinline__ float warp_sum(float v) {
 template <typename T>
 __device__ __forceinline__ void radial_lap(const DRadial& q, T r, T& f, T& fd, T& lap) {
   if (!(r < T(q.rcut))) { f = fd = lap = T(0); return; }
-  const T rcut = T(q.rcut);
-  if (q.kind == 0) {  // CUTOFF_CUSP (cusp a, gamma b)
+  const T ircut = T(q.inv_rcut);
+  const T zz = r * ircut, zz2 = zz * zz;
+  const T ir = T(1) / r;
+  if (q.kind == 0) {  // CUTOFF_CUSP (cusp a, gamma b, 1/(3+gamma) c)
     const T cusp = T(q.a), gamma = T(q.b);
-    T zz = r / rcut, zz2 = zz * zz;
-    T pp = zz - zz2 + zz * zz2 / T(3);
+    T pp = zz - zz2 + zz * zz2 * T(1.0 / 3.0);
     T pade = T(1) / (T(1) + gamma * pp);
-    T pade0 = T(1) / (T(3) + gamma);
-    f = cusp * rcut * (pp * pade - pade0);
+    f = cusp * T(q.rcut) * (pp * pade - T(q.c));
     T pade2 = pade * pade;
     T ppd = T(1) - T(2) * zz + zz2;
     T ppdd = T(-2) + T(2) * zz;
-    T dadr = ppd * pade2 / r;
+    T dadr = ppd * pade2 * ir;
     fd = cusp * dadr;
-    lap = cusp * (ppdd * pade2 / rcut - T(2) * gamma * ppd * ppd * pade2 * pade / rcut + T(2) * dadr);
+    lap = cusp * ((ppdd * pade2 - T(2) * gamma * ppd * ppd * pade2 * pade) * ircut + T(2) * dadr);
   } else {            // POLYPADE (beta a)
     const T beta = T(q.a);
-    T zz = r / rcut, zz2 = zz * zz;
     T zpp = zz2 * (T(6) - T(8) * zz + T(3) * zz2);
     T zppd = T(12) * zz * (T(1) - T(2) * zz + zz2);
     T zppdd2 = T(6) - T(24) * zz + T(18) * zz2;
     T zpade = T(1) / (T(1) + beta * zpp), zpade2 = zpade * zpade;
     f = (T(1) - zpp) * zpade;
-    fd = -zppd * zpade2 * (beta + T(1)) / (r * rcut);
-    T crsdd2 = -zpade2 * (zppdd2 - beta * zppd * zppd * zpade) * (beta + T(1)) / (rcut * rcut);
+    fd = -zppd * zpade2 * (beta + T(1)) * ir * ircut;
+    T crsdd2 = -zpade2 * (zppdd2 - beta * zppd * zppd * zpade) * (beta + T(1)) * ircut * ircut;
     lap = T(2) * (crsdd2 + fd);
   }
 }
 template <typename T>
 __device__ __forceinline__ T radial_val(const DRadial& q, T r) {
   if (!(r < T(q.rcut))) return T(0);
-  const T rcut = T(q.rcut);
-  T zz = r / rcut, zz2 = zz * zz;
+  const T zz = r * T(q.inv_rcut), zz2 = zz * zz;
   if (q.kind == 0) {
-    T pp = zz - zz2 + zz * zz2 / T(3);
-    return T(q.a) * rcut * (pp / (T(1) + T(q.b) * pp) - T(1) / (T(3) + T(q.b)));
+    T pp = zz - zz2 + zz * zz2 * T(1.0 / 3.0);
+    return T(q.a) * T(q.rcut) * (pp / (T(1) + T(q.b) * pp) - T(q.c));
   }
   T zpp = zz2 * (T(6) - T(8) * zz + T(3) * zz2);
   return (T(1) - zpp) / (T(1) + T(q.a) * zpp);
@@ -293,7 +307,7 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
   for (int s = lane; s < S.nshell; s += 32) {
     int4 si = S.shell_i[s];
     int2 so = S.shell_obj[s];
-    const double* ap = S.atom_pos + 3 * si.x;
+    const double* ap = S.atom_pos[si.x];
     double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
     double r = sqrt(dx * dx + dy * dy + dz * dz);
     Real* b = bas + si.z * 5;
@@ -312,98 +326,93 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
     }
   }
   __syncwarp();
-  const int nout = M * 5;
-  for (int o = lane; o < nout; o += 32) {
-    int mo = o / 5, c = o - mo * 5;
-    Real a0 = Real(0), a1 = Real(0);
-    const Real* bb = bas + c;
+  // contraction: lane (mo, chunk) sums the 5 components of one MO over a
+  // slice of the basis (5 independent accumulators), then the slices of an
+  // MO are added with shuffles
+  const int nch = M > 16 ? 1 : M > 8 ? 2 : M > 4 ? 4 : 8;  // lanes per MO (M * nch <= 32)
+  const int mo = lane / nch, ch = lane - mo * nch;
+  const int fper = (S.nbasis + nch - 1) / nch;
+  Real a0 = Real(0), a1 = Real(0), a2 = Real(0), a3 = Real(0), a4 = Real(0);
+  if (mo < M) {
+    const int f0 = ch * fper, f1 = min(S.nbasis, f0 + fper);
     const Real* w = moc_s + mo;
-    int f = 0;
-    for (; f + 1 < S.nbasis; f += 2) {
-      a0 += bb[f * 5] * w[f * S.mstride];
-      a1 += bb[(f + 1) * 5] * w[(f + 1) * S.mstride];
+    for (int f = f0; f < f1; f++) {
+      const Real c = w[f * S.mstride];
+      const Real* bb = bas + f * 5;
+      a0 += bb[0] * c; a1 += bb[1] * c; a2 += bb[2] * c; a3 += bb[3] * c; a4 += bb[4] * c;
     }
-    if (f < S.nbasis) a0 += bb[f * 5] * w[f * S.mstride];
-    out[mo * 5 + c] = a0 + a1;
+  }
+  for (int o = 1; o < nch; o <<= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+    a4 += __shfl_xor_sync(0xffffffffu, a4, o);
+  }
+  if (mo < M && ch == 0) {
+    out[mo * 5] = a0; out[mo * 5 + 1] = a1; out[mo * 5 + 2] = a2; out[mo * 5 + 3] = a3; out[mo * 5 + 4] = a4;
   }
   __syncwarp();
 }
 
-// MO values of one position evaluated entirely by the calling lane (the
-// quadrature points of the pseudopotential).  Centers in turn: one distance
-// and one spline row per center, all shells of the center from that row.
-template <typename Real, int MMAX>
-__device__ __forceinline__ void acc_fn(Real phi[MMAX], const Real* moc_s, int f, Real v) {
-  v = fabs(v) > Real(1e-8) ? v : Real(0);
-  const Real* w = moc_s + (size_t)f * MMAX;
-#pragma unroll
-  for (int m = 0; m < MMAX; m++) phi[m] += v * w[m];
-}
-
-template <typename Real, int MMAX>
-__device__ __forceinline__ void mo_val_lane(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz,
-                                            Real phi[MMAX]) {
-#pragma unroll
-  for (int m = 0; m < MMAX; m++) phi[m] = Real(0);
+// Determinant ratio of one electron moved to p, evaluated entirely by the
+// calling lane (pseudopotential quadrature points): with the projected
+// coefficients w_f = sum_m C[f][m] (A^-1)[m][e] of that electron,
+//   psi_D(p)/psi_D = sum_m phi_m(p) (A^-1)[m][e] = sum_f b_f(p) w_f,
+// an nbasis-term dot product instead of the nbasis x M MO contraction.
+template <typename Real>
+__device__ __forceinline__ Real basis_dot_lane(const DevSys<Real>& S, double px, double py, double pz,
+                                               const Real* w) {
+  Real acc = Real(0);
+  auto add = [&](int f, Real v) { acc += (fabs(v) > Real(1e-8) ? v : Real(0)) * w[f]; };
+  constexpr int B = sizeof(Real) == 4 ? 6 : 4;  // spline rows loaded per batch
   for (int c = 0; c < S.natoms; c++) {
-    int2 cs = S.center_shells[c];
+    const int4 cs = S.center_seg[c];  // first shell, shells, object base, splines per row
     if (cs.y == 0) continue;
-    const double* ap = S.atom_pos + 3 * c;
+    const double* ap = S.atom_pos[c];
     const Real x = Real(px - ap[0]), y = Real(py - ap[1]), z = Real(pz - ap[2]);
     const Real rd = sqrt(x * x + y * y + z * z);
+    if (!(rd < Real(S.center_cut[c]))) continue;
     const int i = int(rd * Real(S.inv_spacing));
     const Real h = rd - Real(i) * Real(S.spacing);
-    for (int s = cs.x; s < cs.x + cs.y; s++) {
-      if (!(rd < Real(S.shell_cut[s]))) continue;
-      int4 si = S.shell_i[s];
-      int2 so = S.shell_obj[s];
-      const Real* cp = S.spline + ((size_t)so.x + (size_t)i * so.y + si.w) * 4;
-      Real f = __ldg(cp) + h * (__ldg(cp + 1) + h * (__ldg(cp + 2) + h * __ldg(cp + 3)));
-      const int fb = si.z;
-      switch (si.y) {
-        case 0: acc_fn<Real, MMAX>(phi, moc_s, fb, f); break;
-        case 1: {
-          acc_fn<Real, MMAX>(phi, moc_s, fb, x * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 1, y * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 2, z * f);
-        } break;
-        case 2: {
-          acc_fn<Real, MMAX>(phi, moc_s, fb, x * x * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 1, y * y * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 2, z * z * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 3, x * y * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 4, x * z * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 5, y * z * f);
-        } break;
-        default: {
-          acc_fn<Real, MMAX>(phi, moc_s, fb, (Real(2) * z * z - x * x - y * y) * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 1, x * z * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 2, y * z * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 3, (x * x - y * y) * f);
-          acc_fn<Real, MMAX>(phi, moc_s, fb + 4, x * y * f);
-        } break;
+    const Real* row = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4;
+    for (int k0 = 0; k0 < cs.y; k0 += B) {
+      Real cf[B][4];
+#pragma unroll
+      for (int j = 0; j < B; j++)
+        if (k0 + j < cs.y) {
+          const int k = (S.shell_pack[cs.x + k0 + j] >> 20) & 0xff;
+#pragma unroll
+          for (int q = 0; q < 4; q++) cf[j][q] = __ldg(row + 4 * k + q);
+        }
+#pragma unroll
+      for (int j = 0; j < B; j++) {
+        if (k0 + j >= cs.y) break;
+        const int pk = S.shell_pack[cs.x + k0 + j];
+        const int sym = pk & 0xf, fb = (pk >> 4) & 0xffff;
+        const Real f = cf[j][0] + h * (cf[j][1] + h * (cf[j][2] + h * cf[j][3]));
+        switch (sym) {
+          case 0: add(fb, f); break;
+          case 1: add(fb, x * f); add(fb + 1, y * f); add(fb + 2, z * f); break;
+          case 2:
+            add(fb, x * x * f); add(fb + 1, y * y * f); add(fb + 2, z * z * f);
+            add(fb + 3, x * y * f); add(fb + 4, x * z * f); add(fb + 5, y * z * f);
+            break;
+          default:
+            add(fb, (Real(2) * z * z - x * x - y * y) * f); add(fb + 1, x * z * f); add(fb + 2, y * z * f);
+            add(fb + 3, (x * x - y * y) * f); add(fb + 4, x * y * f);
+            break;
+        }
       }
     }
   }
+  return acc;
 }
 
 // ---------------------------------------------------------------------------
-// Jastrow pieces (all in double: a few hundred flops per electron)
+// Jastrow pieces (tables from the parameter bank; sums in double)
 
-// Two-body u(r_ij) for a pair of given spins: value, f'/r, lap.
-template <typename Real>
-__device__ __forceinline__ void jas_pair(const DevSys<Real>& S, bool same, double r, double& u, double& fd, double& lap) {
-  u = fd = lap = 0.0;
-  for (int k = 0; k < S.nee; k++) {
-    double c = same ? S.ee_like[k] : S.ee_unlike[k];
-    if (c == 0.0) continue;
-    double f, d, l;
-    radial_lap(S.ee[k], r, f, d, l);
-    u += c * f; fd += c * d; lap += c * l;
-  }
-}
-
-// Two-body u(r) evaluated in precision T, returned as doubles.
+// Two-body u(r) for a pair of given spins: value, f'/r, lap (precision T).
 template <typename T, typename Real>
 __device__ __forceinline__ void jas_pair_t(const DevSys<Real>& S, bool same, T r, double& u, double& fd, double& lap) {
   T uu = T(0), ff = T(0), ll = T(0);
@@ -423,22 +432,23 @@ __device__ __forceinline__ void jas_onebody(const DevSys<Real>& S, double px, do
                                             double g[3], double& lap) {
   u = 0; g[0] = g[1] = g[2] = 0; lap = 0;
   for (int a = 0; a < S.natoms; a++) {
-    const double* ap = S.atom_pos + 3 * a;
+    const int t = S.atom_type[a];
+    const double* ap = S.atom_pos[a];
     double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
     double r = sqrt(dx * dx + dy * dy + dz * dz);
-    int f0 = S.ei_first[a], nf = S.ei_count[a];
-    for (int k = 0; k < nf; k++) {
-      double c = S.onebody[f0 + k];
+    for (int k = 0; k < S.ei_n[t]; k++) {
+      double c = S.onebody[t][k];
       if (c == 0.0) continue;
       double f, d, l;
-      radial_lap(S.ei[f0 + k], r, f, d, l);
+      radial_lap(S.ei[t][k], r, f, d, l);
       u += c * f; g[0] += c * d * dx; g[1] += c * d * dy; g[2] += c * d * dz; lap += c * l;
     }
   }
 }
 
 // Three-body (e-e-n) contribution of the pair (i, j) at all atoms, with
-// gradients/laps for both electrons.  di: r_i - atom, dj: r_j - atom.
+// gradients/laps for both electrons: sum_atom sum_terms c (a_k(i) a_l(j) +
+// a_l(i) a_k(j)) b_m(r_ij) (Jastrow2_three.cpp:138-404).
 template <typename Real>
 __device__ void jas_threebody_pair(const DevSys<Real>& S, const double pi[3], const double pj[3], double& u,
                                    double gi[3], double& li, double gj[3], double& lj, bool need_derivs) {
@@ -447,20 +457,21 @@ __device__ void jas_threebody_pair(const DevSys<Real>& S, const double pi[3], co
   double dij[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
   double rij = sqrt(dij[0] * dij[0] + dij[1] * dij[1] + dij[2] * dij[2]);
   for (int a = 0; a < S.natoms; a++) {
-    int nt = S.tb_count[a];
+    const int t = S.atom_type[a];
+    const int nt = S.tb_n[t];
     if (!nt) continue;
-    const double* ap = S.atom_pos + 3 * a;
+    const double* ap = S.atom_pos[a];
     double di[3] = {pi[0] - ap[0], pi[1] - ap[1], pi[2] - ap[2]};
     double dj[3] = {pj[0] - ap[0], pj[1] - ap[1], pj[2] - ap[2]};
     double ri = sqrt(di[0] * di[0] + di[1] * di[1] + di[2] * di[2]);
     double rj = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
-    for (int t = 0; t < nt; t++) {
-      DTB q = S.tb[S.tb_first[a] + t];
+    for (int n = 0; n < nt; n++) {
+      const DTB& q = S.tb[t][n];
       double aki, akdi, akli, akj, akdj, aklj, ali, aldi, alli, alj, aldj, allj, b, bd, bl;
-      radial_lap(S.ei[q.k], ri, aki, akdi, akli);
-      radial_lap(S.ei[q.k], rj, akj, akdj, aklj);
-      radial_lap(S.ei[q.l], ri, ali, aldi, alli);
-      radial_lap(S.ei[q.l], rj, alj, aldj, allj);
+      radial_lap(S.ei[t][q.k], ri, aki, akdi, akli);
+      radial_lap(S.ei[t][q.k], rj, akj, akdj, aklj);
+      radial_lap(S.ei[t][q.l], ri, ali, aldi, alli);
+      radial_lap(S.ei[t][q.l], rj, alj, aldj, allj);
       radial_lap(S.ee[q.m], rij, b, bd, bl);
       double s = aki * alj + ali * akj;
       u += q.c * s * b;
@@ -494,17 +505,16 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
   u = ob; lap = ol;
   for (int d = 0; d < 3; d++) g[d] = og[d];
   const bool si = i < S.nup;
-  constexpr bool has3 = TB;  // e-e-n terms compiled in only when the deck has them
   const double pi[3] = {px, py, pz};
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
     double dx = px - R[3 * j], dy = py - R[3 * j + 1], dz = pz - R[3 * j + 2];
     double r = sqrt(dx * dx + dy * dy + dz * dz);
     double pu, pfd, pl;
-    jas_pair(S, si == (j < S.nup), r, pu, pfd, pl);
+    jas_pair_t<double>(S, si == (j < S.nup), r, pu, pfd, pl);
     u += pu; lap += pl;
     g[0] += pfd * dx; g[1] += pfd * dy; g[2] += pfd * dz;
-    if constexpr (has3) {
+    if constexpr (TB) {  // e-e-n terms compiled in only when the deck has them
       double tu, tgi[3], tli, tgj[3], tlj;
       jas_threebody_pair(S, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, need_derivs);
       u += tu; lap += tli;
@@ -520,17 +530,16 @@ template <typename T, bool TB, typename Real>
 __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, double px, double py, double pz) {
   T u = T(0);
   for (int a = 0; a < S.natoms; a++) {
-    const double* ap = S.atom_pos + 3 * a;
+    const int t = S.atom_type[a];
+    const double* ap = S.atom_pos[a];
     const T dx = T(px - ap[0]), dy = T(py - ap[1]), dz = T(pz - ap[2]);
     const T r = sqrt(dx * dx + dy * dy + dz * dz);
-    const int f0 = S.ei_first[a], nf = S.ei_count[a];
-    for (int k = 0; k < nf; k++) {
-      const double c = S.onebody[f0 + k];
-      if (c != 0.0) u += T(c) * radial_val<T>(S.ei[f0 + k], r);
+    for (int k = 0; k < S.ei_n[t]; k++) {
+      const double c = S.onebody[t][k];
+      if (c != 0.0) u += T(c) * radial_val<T>(S.ei[t][k], r);
     }
   }
   const bool si = i < S.nup;
-  constexpr bool has3 = TB;  // e-e-n terms compiled in only when the deck has them
   const double pi[3] = {px, py, pz};
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
@@ -541,7 +550,7 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
       const double c = same ? S.ee_like[k] : S.ee_unlike[k];
       if (c != 0.0) u += T(c) * radial_val<T>(S.ee[k], r);
     }
-    if constexpr (has3) {
+    if constexpr (TB) {
       double tu, tgi[3], tli, tgj[3], tlj;
       jas_threebody_pair(S, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false);
       u += T(tu);

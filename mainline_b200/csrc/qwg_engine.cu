@@ -70,9 +70,7 @@ struct qwg_ctx {
   bool own_stream = false;
   long long launches = 0;
   // tables
-  DevBuf d_atom_pos, d_atom_charge, d_shell_i, d_shell_obj, d_center_shells, d_shell_cut, d_spline, d_spline64, d_moc, d_ee, d_ee_like, d_ee_unlike, d_ei,
-      d_ei_first, d_ei_count, d_onebody, d_tb_first, d_tb_count, d_tb, d_pp_nchan, d_pp_aip, d_pp_cutoff,
-      d_pp_term_first, d_pp_term, d_pp_quad, d_pp_w;
+  DevBuf d_shell_i, d_shell_obj, d_shell_cut, d_spline, d_spline64, d_moc;
   DevSys<double> sys_d{};
   DevSys<float> sys_f{};
   WLayout L{};
@@ -96,19 +94,36 @@ struct qwg_ctx {
 
 namespace {
 
+// Host-side copy of the parameter-bank tables, filled once from HostSystem.
+struct ParamTables {
+  std::vector<int> atom_type;
+  std::vector<int4> center_seg;
+  std::vector<double> center_cut;
+  std::vector<int> shell_pack;
+};
+
+static DRadial to_dradial(const Radial& r) {
+  DRadial d{};
+  d.kind = r.kind;
+  d.rcut = r.rcut;
+  d.inv_rcut = 1.0 / r.rcut;
+  d.a = r.a;
+  d.b = r.b;
+  d.c = r.kind == RAD_CUTOFF_CUSP ? 1.0 / (3.0 + r.b) : 0.0;
+  return d;
+}
+
 template <typename Real>
-static void fill_sys(qwg_ctx* c, DevSys<Real>& S) {
+static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_base) {
   const HostSystem& H = c->H;
+  memset(&S, 0, sizeof(S));
   S.nelec = H.nelec; S.nup = H.nup; S.ndn = H.ndn; S.natoms = H.natoms;
   S.nbasis = H.nbasis; S.nshell = (int)H.shells.size();
   S.m[0] = H.nmo[0]; S.m[1] = H.nmo[1];
   S.mstride = c->mmax;
-  S.atom_pos = c->d_atom_pos.as<double>();
-  S.atom_charge = c->d_atom_charge.as<double>();
   S.ion_ion = H.ion_ion;
   S.shell_i = c->d_shell_i.as<int4>();
   S.shell_obj = c->d_shell_obj.as<int2>();
-  S.center_shells = c->d_center_shells.as<int2>();
   S.shell_cut = c->d_shell_cut.as<double>();
   S.spline = c->d_spline.as<Real>();
   S.spline64 = c->d_spline64.as<double>();
@@ -116,37 +131,86 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S) {
   S.npts = H.spline_npts;
   S.spacing = H.spline_spacing;
   S.inv_spacing = 1.0 / H.spline_spacing;
+  // ---- limits of the parameter bank
+  if (H.natoms > QWG_MAXA) throw InputError("more than 64 atoms: beyond this engine build");
+  if ((int)H.shells.size() > QWG_MAXSHELL) throw InputError("more than 1024 basis shells: beyond this engine build");
+  if ((int)H.ee.size() > QWG_MAXEE) throw InputError("more than 8 e-e Jastrow functions");
+  // atom types = distinct labels
+  std::vector<std::string> types;
+  for (int a = 0; a < H.natoms; a++) {
+    int t = (int)(std::find(types.begin(), types.end(), H.labels[a]) - types.begin());
+    if (t == (int)types.size()) types.push_back(H.labels[a]);
+    if (t >= QWG_MAXT) throw InputError("more than 8 atom labels: beyond this engine build");
+    S.atom_type[a] = t;
+    for (int d = 0; d < 3; d++) S.atom_pos[a][d] = H.atom_pos[3 * a + d];
+    S.atom_charge[a] = H.atom_charge[a];
+  }
+  // centers: one basis object per center, shells contiguous and in object order
+  std::vector<int> seen(H.natoms, 0);
+  for (size_t k = 0; k < H.shells.size(); k++) {
+    const Shell& sh = H.shells[k];
+    int4& cs = S.center_seg[sh.center];
+    if (!seen[sh.center]) {
+      seen[sh.center] = 1;
+      cs = make_int4((int)k, 0, obj_base[sh.obj], H.obj_count[sh.obj]);
+      S.center_cut[sh.center] = sh.cutoff;
+    } else if (obj_base[sh.obj] != cs.z) {
+      throw InputError("one BASIS section per atom label is supported");
+    }
+    cs.y++;
+    if (sh.first >= (1 << 16) || sh.k >= 256) throw InputError("basis too large for the shell table");
+    S.shell_pack[k] = sh.sym | (sh.first << 4) | (sh.k << 20);
+  }
+  // Jastrow
   S.nee = (int)H.ee.size();
-  S.ee = c->d_ee.as<DRadial>();
-  S.ee_like = c->d_ee_like.as<double>();
-  S.ee_unlike = c->d_ee_unlike.as<double>();
-  S.ei = c->d_ei.as<DRadial>();
-  S.ei_first = c->d_ei_first.as<int>();
-  S.ei_count = c->d_ei_count.as<int>();
-  S.onebody = c->d_onebody.as<double>();
-  S.tb_first = c->d_tb_first.as<int>();
-  S.tb_count = c->d_tb_count.as<int>();
-  S.tb = H.tb.empty() ? nullptr : c->d_tb.as<DTB>();
-  int mx = 0;
-  for (int a = 0; a < H.natoms; a++) mx = std::max(mx, H.ei_count[a]);
-  S.max_ei = mx;
+  for (int k = 0; k < S.nee; k++) {
+    S.ee[k] = to_dradial(H.ee[k]);
+    S.ee_like[k] = H.ee_like[k];
+    S.ee_unlike[k] = H.ee_unlike[k];
+  }
+  S.has_tb = H.tb.empty() ? 0 : 1;
   S.has_pp = H.has_pp ? 1 : 0;
-  S.pp_nchan = c->d_pp_nchan.as<int>();
-  S.pp_aip = c->d_pp_aip.as<int>();
-  S.pp_cutoff = c->d_pp_cutoff.as<double>();
-  S.pp_term_first = c->d_pp_term_first.as<int>();
-  S.pp_term = c->d_pp_term.as<double>();
-  S.pp_quad = c->d_pp_quad.as<double>();
-  S.pp_w = c->d_pp_w.as<double>();
-  S.max_aip = std::max(H.max_aip, 1);
+  std::vector<int> type_done(types.size(), 0);
+  for (int a = 0; a < H.natoms; a++) {
+    const int t = S.atom_type[a];
+    if (type_done[t]) continue;
+    type_done[t] = 1;
+    if (H.ei_count[a] > QWG_MAXEI) throw InputError("more than 8 e-n Jastrow functions on one atom");
+    S.ei_n[t] = H.ei_count[a];
+    for (int k = 0; k < H.ei_count[a]; k++) {
+      S.ei[t][k] = to_dradial(H.ei[H.ei_first[a] + k]);
+      S.onebody[t][k] = H.onebody[H.ei_first[a] + k];
+    }
+    if (H.tb_count[a] > QWG_MAXTB) throw InputError("more than 12 e-e-n terms on one atom");
+    S.tb_n[t] = H.tb_count[a];
+    for (int n = 0; n < H.tb_count[a]; n++) {
+      const ThreeBodyTerm& q = H.tb[H.tb_first[a] + n];
+      S.tb[t][n] = DTB{q.k - H.ei_first[a], q.l - H.ei_first[a], q.m, q.c};
+    }
+    const PPAtom& P = H.pp[a];
+    S.pp_nchan[t] = P.nchan;
+    S.pp_aip[t] = P.aip;
+    S.pp_cutoff[t] = P.cutoff;
+    if (P.nchan > 5) throw InputError("pseudopotential channels beyond l=3 are not supported");
+    if ((int)P.term_n.size() > QWG_MAXPPT) throw InputError("more than 16 pseudopotential terms on one atom");
+    if (P.aip > QWG_MAXQ) throw InputError("quadratures above 12 points are not supported");
+    for (int l = 0; l <= P.nchan && P.nchan; l++) S.pp_term_first[t][l] = P.term_first[l];
+    for (size_t n = 0; n < P.term_n.size(); n++) {
+      S.pp_term[t][n][0] = P.term_n[n];
+      S.pp_term[t][n][1] = P.term_a[n];
+      S.pp_term[t][n][2] = P.term_c[n];
+    }
+    for (int q = 0; q < P.aip; q++) {
+      for (int d = 0; d < 3; d++) S.pp_quad[t][q][d] = P.quad[3 * q + d];
+      S.pp_w[t][q] = P.weight[q];
+    }
+  }
 }
 
 static void build_tables(qwg_ctx* c) {
   const HostSystem& H = c->H;
   cudaStream_t st = c->stream;
   const int A = H.natoms;
-  upload(c->d_atom_pos, H.atom_pos, st);
-  upload(c->d_atom_charge, H.atom_charge, st);
   // interval-major spline tables: object o occupies npts x count_o x 4 values
   const int npts = H.spline_npts;
   std::vector<int> obj_base(H.obj_first.size());
@@ -163,19 +227,17 @@ static void build_tables(qwg_ctx* c) {
           il[((size_t)obj_base[o] + (size_t)i * H.obj_count[o] + k) * 4 + q] =
               H.spline_coef[((size_t)(H.obj_first[o] + k) * npts + i) * 4 + q];
   std::vector<int4> si;
-  std::vector<int2> so, cs(A, make_int2(0, 0));
+  std::vector<int2> so;
   std::vector<double> sc;
   for (size_t k = 0; k < H.shells.size(); k++) {
     const Shell& s = H.shells[k];
     si.push_back(make_int4(s.center, s.sym, s.first, s.k));
     so.push_back(make_int2(obj_base[s.obj], H.obj_count[s.obj]));
     sc.push_back(s.cutoff);
-    if (cs[s.center].y == 0) cs[s.center].x = (int)k;
-    cs[s.center].y++;
   }
+  (void)A;
   upload(c->d_shell_i, si, st);
   upload(c->d_shell_obj, so, st);
-  upload(c->d_center_shells, cs, st);
   upload(c->d_shell_cut, sc, st);
   // MO coefficients padded to MMAX columns, both spins
   const int mm = c->mmax;
@@ -193,57 +255,10 @@ static void build_tables(qwg_ctx* c) {
     upload(c->d_spline, sf, st);
     upload(c->d_moc, mf, st);
   }
-  std::vector<DRadial> ee, ei;
-  for (auto& r : H.ee) ee.push_back(DRadial{r.kind, r.rcut, r.a, r.b});
-  for (auto& r : H.ei) ei.push_back(DRadial{r.kind, r.rcut, r.a, r.b});
-  upload(c->d_ee, ee, st);
-  upload(c->d_ee_like, H.ee_like, st);
-  upload(c->d_ee_unlike, H.ee_unlike, st);
-  upload(c->d_ei, ei, st);
-  upload(c->d_ei_first, H.ei_first, st);
-  upload(c->d_ei_count, H.ei_count, st);
-  upload(c->d_onebody, H.onebody, st);
-  upload(c->d_tb_first, H.tb_first, st);
-  upload(c->d_tb_count, H.tb_count, st);
-  std::vector<DTB> tb;
-  for (auto& t : H.tb) tb.push_back(DTB{t.k, t.l, t.m, t.c});
-  upload(c->d_tb, tb, st);
-  // pseudopotential
-  const int maq = std::max(H.max_aip, 1);
-  std::vector<int> nch(A), aip(A), tf((size_t)A * 8, 0);
-  std::vector<double> cut(A), term, quad((size_t)A * maq * 3, 0.0), w((size_t)A * maq, 0.0);
-  for (int a = 0; a < A; a++) {
-    const PPAtom& P = H.pp[a];
-    nch[a] = P.nchan;
-    aip[a] = P.aip;
-    cut[a] = P.cutoff;
-    if (P.nchan > 7) throw InputError("too many pseudopotential channels");
-    if (P.nchan > 5) throw InputError("pseudopotential channels beyond l=3 are not supported");
-    int t0 = (int)term.size() / 3;
-    for (int l = 0; l <= P.nchan; l++) tf[(size_t)a * 8 + l] = t0 + (P.nchan ? P.term_first[l] : 0);
-    for (size_t t = 0; t < P.term_n.size(); t++) {
-      term.push_back(P.term_n[t]); term.push_back(P.term_a[t]); term.push_back(P.term_c[t]);
-    }
-    for (int q = 0; q < P.aip; q++) {
-      for (int d = 0; d < 3; d++) quad[((size_t)a * maq + q) * 3 + d] = P.quad[3 * q + d];
-      w[(size_t)a * maq + q] = P.weight[q];
-    }
-  }
-  upload(c->d_pp_nchan, nch, st);
-  upload(c->d_pp_aip, aip, st);
-  upload(c->d_pp_cutoff, cut, st);
-  upload(c->d_pp_term_first, tf, st);
-  upload(c->d_pp_term, term, st);
-  upload(c->d_pp_quad, quad, st);
-  upload(c->d_pp_w, w, st);
-  fill_sys<double>(c, c->sys_d);
-  fill_sys<float>(c, c->sys_f);
-  const void* req[] = {c->sys_d.atom_pos, c->sys_d.atom_charge, c->sys_d.shell_i, c->sys_d.shell_obj,
-                       c->sys_d.center_shells, c->sys_d.shell_cut,
-                       c->sys_d.spline, c->sys_d.spline64, c->sys_d.moc, c->sys_d.ee, c->sys_d.ee_like, c->sys_d.ee_unlike,
-                       c->sys_d.ei, c->sys_d.ei_first, c->sys_d.ei_count, c->sys_d.onebody, c->sys_d.tb_first,
-                       c->sys_d.tb_count, c->sys_d.pp_nchan, c->sys_d.pp_aip, c->sys_d.pp_cutoff,
-                       c->sys_d.pp_term_first, c->sys_d.pp_term, c->sys_d.pp_quad, c->sys_d.pp_w};
+  fill_sys<double>(c, c->sys_d, obj_base);
+  fill_sys<float>(c, c->sys_f, obj_base);
+  const void* req[] = {c->sys_d.shell_i, c->sys_d.shell_obj, c->sys_d.shell_cut, c->sys_d.spline,
+                       c->sys_d.spline64, c->sys_d.moc};
   for (const void* p : req)
     if (!p) throw std::runtime_error("internal: device table pointer left unset");
 }
@@ -263,19 +278,29 @@ static void make_layout(qwg_ctx* c) {
   L.gU = o; o = align16(o + 8 * 3 * N);
   L.lU = o; o = align16(o + 8 * N);
   L.state_bytes = o;
+  // scratch: the move/re-inversion phase and the pseudopotential phase are
+  // never live together, so their buffers share one region
+  const int s0 = o;
   L.bas = o; o = align16(o + rs * H.nbasis * 5);
   L.newcol = o; o = align16(o + rs * mm * 5);
-  // dG (move proposals) and Ue (pseudopotential) are never live together;
-  // nor are lu (re-inversion, Sherman-Morrison scratch) and the PP items
-  L.dG = o;
-  L.Ue = o;
-  o = align16(o + std::max(8 * 4 * N, 8 * N));
-  L.lu = o;
-  L.items = o;
-  o = align16(o + std::max(8 * mm * 2 * mm, (int)sizeof(PPItem) * N * A));
+  L.dG = o; o = align16(o + 8 * 4 * N);
+  L.lu = o; o = align16(o + 8 * mm * 2 * mm);
+  const int move_end = o;
+  o = s0;
+  L.items = o; o = align16(o + (int)sizeof(PPItem) * N * A);
+  L.Ue = o; o = align16(o + 8 * N);
   L.rot = o; o = align16(o + 8 * 9);
+  L.wproj = o;
+  // projected coefficients for a chunk of electrons: all of them if a walker
+  // still fits the budget of 4 walkers x 4 CTAs per SM, else as many as fit
+  // (at least 4)
+  const int budget = (227 * 1024 - 1024) / 16;
+  int room = std::max(budget - o, move_end - o);
+  L.wchunk = std::max(4, std::min(N, room / (rs * H.nbasis)));
+  o = align16(o + rs * H.nbasis * L.wchunk);
+  o = std::max(o, move_end);
   L.bytes = o;
-  const size_t moc_bytes = ((size_t)2 * H.nbasis * mm * rs + 15) / 16 * 16;
+  const size_t moc_bytes = 0;  // MO coefficients are read through L1, not staged
   // walkers per CTA: up to 4 while the CTA stays under ~110 KB (2 CTAs/SM)
   int wpc = 4;
   while (wpc > 1 && moc_bytes + (size_t)wpc * L.bytes > 110 * 1024) wpc--;
@@ -286,7 +311,7 @@ static void make_layout(qwg_ctx* c) {
 
 template <typename Real, int MM, int MODE>
 static void launch_mode(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int nwalk) {
-  auto kern = S.tb ? k_walkers<Real, MM, MODE, true> : k_walkers<Real, MM, MODE, false>;
+  auto kern = S.has_tb ? k_walkers<Real, MM, MODE, true> : k_walkers<Real, MM, MODE, false>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
   int grid = (nwalk + c->wpc - 1) / c->wpc;
   kern<<<grid, 32 * c->wpc, c->smem_bytes, c->stream>>>(S, c->L, P, io);

@@ -34,7 +34,7 @@ struct Walker {
   const DevSys<Real>& S;
   const WLayout& L;
   unsigned char* base;
-  const Real* moc_s;     // [2][nbasis][MMAX] in shared memory
+  const Real* moc_s;     // [2][nbasis][MMAX] MO coefficients (global, read through L1)
   int lane;
 
   __device__ double* R() const { return (double*)(base + L.R); }
@@ -50,6 +50,7 @@ struct Walker {
   __device__ double* lu() const { return (double*)(base + L.lu); }
   __device__ PPItem* items() const { return (PPItem*)(base + L.items); }
   __device__ double* rot() const { return (double*)(base + L.rot); }
+  __device__ Real* wproj() const { return (Real*)(base + L.wproj); }
 
   __device__ int spin(int e) const { return e < S.nup ? 0 : 1; }
   __device__ int eloc(int e) const { return e < S.nup ? e : e - S.nup; }
@@ -171,22 +172,21 @@ struct Walker {
       dg[0] = g0; dg[1] = g1; dg[2] = g2; dg[3] = l0;
     }
     // one-body terms: lanes over (atom, function) pairs
-    for (int a = 0; a < S.natoms; a++) {
-      const int f0 = S.ei_first[a], nf = S.ei_count[a];
-      if (lane >= nf) continue;
-      for (int k = lane; k < nf; k += 32) {
-        const double c = S.onebody[f0 + k];
-        if (c == 0.0) continue;
-        const double* ap = S.atom_pos + 3 * a;
-        double nx = px - ap[0], ny = py - ap[1], nz = pz - ap[2];
-        double qx = ox - ap[0], qy = oy - ap[1], qz = oz - ap[2];
-        double rn = sqrt(nx * nx + ny * ny + nz * nz), ro = sqrt(qx * qx + qy * qy + qz * qz);
-        double fnv, fnd, fnl;
-        radial_lap(S.ei[f0 + k], rn, fnv, fnd, fnl);
-        du += c * (fnv - radial_val(S.ei[f0 + k], ro));
-        ge[0] += c * fnd * nx; ge[1] += c * fnd * ny; ge[2] += c * fnd * nz;
-        le += c * fnl;
-      }
+    for (int idx = lane; idx < S.natoms * QWG_MAXEI; idx += 32) {
+      const int a = idx / QWG_MAXEI, k = idx - a * QWG_MAXEI;
+      const int t = S.atom_type[a];
+      if (k >= S.ei_n[t]) continue;
+      const double c = S.onebody[t][k];
+      if (c == 0.0) continue;
+      const double* ap = S.atom_pos[a];
+      double nx = px - ap[0], ny = py - ap[1], nz = pz - ap[2];
+      double qx = ox - ap[0], qy = oy - ap[1], qz = oz - ap[2];
+      double rn = sqrt(nx * nx + ny * ny + nz * nz), ro = sqrt(qx * qx + qy * qy + qz * qz);
+      double fnv, fnd, fnl;
+      radial_lap(S.ei[t][k], rn, fnv, fnd, fnl);
+      du += c * (fnv - radial_val(S.ei[t][k], ro));
+      ge[0] += c * fnd * nx; ge[1] += c * fnd * ny; ge[2] += c * fnd * nz;
+      le += c * fnl;
     }
     dU = warp_sum(du);
     double gu[3] = {warp_sum(ge[0]), warp_sum(ge[1]), warp_sum(ge[2])};
@@ -281,7 +281,7 @@ struct Walker {
     double v = 0;
     for (int idx = lane; idx < N * A; idx += 32) {
       int e = idx / A, a = idx - e * A;
-      const double* ap = S.atom_pos + 3 * a;
+      const double* ap = S.atom_pos[a];
       double dx = Rp[3 * e] - ap[0], dy = Rp[3 * e + 1] - ap[1], dz = Rp[3 * e + 2] - ap[2];
       v -= S.atom_charge[a] / sqrt(dx * dx + dy * dy + dz * dz);
     }
@@ -294,15 +294,14 @@ struct Walker {
     return warp_sum(v) + S.ion_ion;
   }
 
-  __device__ double pp_radial(int a, int l, double r) const {
+  __device__ double pp_radial(int t, int l, double r) const {
     double v = 0;
-    const int* tf = S.pp_term_first + 8 * a;
-    for (int t = tf[l]; t < tf[l + 1]; t++) {
-      const double* q = S.pp_term + 3 * t;
+    for (int n = S.pp_term_first[t][l]; n < S.pp_term_first[t][l + 1]; n++) {
+      const double* q = S.pp_term[t][n];
       double ex = fmin(q[1] * r * r, 60.0);
-      const double n = q[0];
-      const double rn = n == 0.0 ? 1.0 : n == -1.0 ? 1.0 / r : n == 1.0 ? r : n == -2.0 ? 1.0 / (r * r)
-                      : n == 2.0 ? r * r : pow(r, n);
+      const double pw = q[0];
+      const double rn = pw == 0.0 ? 1.0 : pw == -1.0 ? 1.0 / r : pw == 1.0 ? r : pw == -2.0 ? 1.0 / (r * r)
+                      : pw == 2.0 ? r * r : pow(r, pw);
       v += q[2] * rn * exp(-ex);
     }
     return v;
@@ -329,16 +328,17 @@ struct Walker {
       PPItem item;
       if (idx < N * A) {
         int e = idx / A, a = idx - e * A;
-        int nch = S.pp_nchan[a];
+        const int t = S.atom_type[a];
+        int nch = S.pp_nchan[t];
         if (nch > 0) {
-          const double* ap = S.atom_pos + 3 * a;
+          const double* ap = S.atom_pos[a];
           item.e = e; item.a = a;
           item.dx = Rp[3 * e] - ap[0]; item.dy = Rp[3 * e + 1] - ap[1]; item.dz = Rp[3 * e + 2] - ap[2];
           item.r = sqrt(item.dx * item.dx + item.dy * item.dy + item.dz * item.dz);
-          vloc += pp_radial(a, nch - 1, item.r);
-          for (int l = 0; l < 4; l++) item.vl[l] = (l < nch - 1) ? pp_radial(a, l, item.r) : 0.0;
+          vloc += pp_radial(t, nch - 1, item.r);
+          for (int l = 0; l < 4; l++) item.vl[l] = (l < nch - 1) ? pp_radial(t, l, item.r) : 0.0;
           if (deterministic) {
-            take = item.r < S.pp_cutoff[a];
+            take = item.r < S.pp_cutoff[t];
           } else {
             double strength = 0;
             for (int l = 0; l < nch - 1; l++) strength += 10.0 * (2 * l + 1) * fabs(item.vl[l]);
@@ -357,38 +357,56 @@ struct Walker {
     }
     __syncwarp();
     double vnl = 0;
-    int total = 0;
-    for (int k = 0; k < nitems; k++) total += S.pp_aip[it[k].a];
-    // lanes over (item, quadrature point)
-    int k = 0, qoff = 0;  // running item cursor for this lane's points
-    for (int p = lane; p < total; p += 32) {
-      while (p >= qoff + S.pp_aip[it[k].a]) { qoff += S.pp_aip[it[k].a]; k++; }
-      const PPItem& I = it[k];
-      const int q = p - qoff;
-      const double* q0 = S.pp_quad + ((size_t)I.a * S.max_aip + q) * 3;
-      double qx = q0[0] * rotm[0] + q0[1] * rotm[3] + q0[2] * rotm[6];
-      double qy = q0[0] * rotm[1] + q0[1] * rotm[4] + q0[2] * rotm[7];
-      double qz = q0[0] * rotm[2] + q0[1] * rotm[5] + q0[2] * rotm[8];
-      const double* ap = S.atom_pos + 3 * I.a;
-      double nx = ap[0] + qx * I.r, ny = ap[1] + qy * I.r, nz = ap[2] + qz * I.r;
-      const int s = spin(I.e), el = eloc(I.e), M = S.m[s];
-      Real phi[MMAX];
-      mo_val_lane<Real, MMAX>(S, mocs(s), nx, ny, nz, phi);
-      const Real* iv = inv(s) + el * MMAX;
-      Real rd = 0;
+    // electrons in chunks of L.wchunk: projected coefficients of the chunk,
+    // then lanes over the chunk's (item, quadrature point) pairs
+    const int CH = L.wchunk;
+    Real* w = wproj();
+    int kbeg = 0;
+    for (int e0 = 0; e0 < N && kbeg < nitems; e0 += CH) {
+      int kend = kbeg;
+      while (kend < nitems && it[kend].e < e0 + CH) kend++;
+      if (kend == kbeg) continue;
+      const int e1 = min(N, e0 + CH);
+      for (int idx = lane; idx < (e1 - e0) * S.nbasis; idx += 32) {
+        const int le = idx / S.nbasis, f = idx - le * S.nbasis;
+        const int e = e0 + le, s = spin(e), el = eloc(e), M = S.m[s];
+        const Real* cf = mocs(s) + (size_t)f * MMAX;
+        const Real* iv = inv(s) + el * MMAX;
+        Real acc = Real(0);
 #pragma unroll
-      for (int i = 0; i < MMAX; i++)
-        if (i < M) rd += iv[i] * phi[i];
-      const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);
-      double ratio = double(rd * exp(u - Real(Ue()[I.e]))) * S.pp_w[(size_t)I.a * S.max_aip + q];
-      // cos of the angle between the original and the quadrature direction
-      double ndx = nx - ap[0], ndy = ny - ap[1], ndz = nz - ap[2];
-      double nr = sqrt(ndx * ndx + ndy * ndy + ndz * ndz);
-      double c = (ndx * I.dx + ndy * I.dy + ndz * I.dz) / (nr * I.r);
-      double P[4] = {1.0, c, 0.5 * (3 * c * c - 1), 0.5 * (5 * c * c * c - 3 * c)};
-      double ts = 0;
-      for (int ll = 0; ll < 4; ll++) ts += (2 * ll + 1) * I.vl[ll] * P[ll];
-      vnl += ts * ratio;
+        for (int m = 0; m < MMAX; m++)
+          if (m < M) acc += cf[m] * iv[m];
+        w[le * S.nbasis + f] = acc;
+      }
+      __syncwarp();
+      int total = 0;
+      for (int k = kbeg; k < kend; k++) total += S.pp_aip[S.atom_type[it[k].a]];
+      int k = kbeg, qoff = 0;  // running item cursor for this lane's points
+      for (int p = lane; p < total; p += 32) {
+        while (p >= qoff + S.pp_aip[S.atom_type[it[k].a]]) { qoff += S.pp_aip[S.atom_type[it[k].a]]; k++; }
+        const PPItem& I = it[k];
+        const int q = p - qoff;
+        const int ty = S.atom_type[I.a];
+        const double* q0 = S.pp_quad[ty][q];
+        double qx = q0[0] * rotm[0] + q0[1] * rotm[3] + q0[2] * rotm[6];
+        double qy = q0[0] * rotm[1] + q0[1] * rotm[4] + q0[2] * rotm[7];
+        double qz = q0[0] * rotm[2] + q0[1] * rotm[5] + q0[2] * rotm[8];
+        const double* ap = S.atom_pos[I.a];
+        double nx = ap[0] + qx * I.r, ny = ap[1] + qy * I.r, nz = ap[2] + qz * I.r;
+        const Real rd = basis_dot_lane(S, nx, ny, nz, w + (I.e - e0) * S.nbasis);
+        const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);
+        double ratio = double(rd * exp(u - Real(Ue()[I.e]))) * S.pp_w[ty][q];
+        // cos of the angle between the original and the quadrature direction
+        double ndx = nx - ap[0], ndy = ny - ap[1], ndz = nz - ap[2];
+        double nr = sqrt(ndx * ndx + ndy * ndy + ndz * ndz);
+        double c = (ndx * I.dx + ndy * I.dy + ndz * I.dz) / (nr * I.r);
+        double P[4] = {1.0, c, 0.5 * (3 * c * c - 1), 0.5 * (5 * c * c * c - 3 * c)};
+        double ts = 0;
+        for (int ll = 0; ll < 4; ll++) ts += (2 * ll + 1) * I.vl[ll] * P[ll];
+        vnl += ts * ratio;
+      }
+      __syncwarp();
+      kbeg = kend;
     }
     return warp_sum(vloc) + warp_sum(vnl);
   }
@@ -417,15 +435,15 @@ __device__ __forceinline__ void random_rotation(const Rand4& r, double m[9]) {
 #define QWG_MIN_BLOCKS 4  // resident 128-thread CTAs per SM the register budget is sized for
 #endif
 template <typename Real, int MMAX, int mode, bool TB>
-__global__ void __launch_bounds__(128, QWG_MIN_BLOCKS) k_walkers(DevSys<Real> S, WLayout L, StepParams P, EvalIO io) {
+__global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
+    k_walkers(const __grid_constant__ DevSys<Real> S, const __grid_constant__ WLayout L, StepParams P, EvalIO io) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int wpc = blockDim.x / 32;
   const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
-  Real* moc_s = (Real*)smem;
-  const size_t moc_elems = (size_t)2 * S.nbasis * MMAX;
-  for (size_t i = threadIdx.x; i < moc_elems; i += blockDim.x) moc_s[i] = S.moc[i];
-  const size_t moc_bytes = (moc_elems * sizeof(Real) + 15) / 16 * 16;
-  __syncthreads();
+  // MO coefficients are read through L1 (a few kB shared by every walker);
+  // shared memory holds walker state only
+  const Real* moc_s = S.moc;
+  const size_t moc_bytes = 0;
   __shared__ double cta_acc[10];
   if (threadIdx.x < 10) cta_acc[threadIdx.x] = 0.0;
   __syncthreads();
