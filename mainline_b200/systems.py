@@ -212,10 +212,106 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
                 kind=name, seed=seed)
 
 
+DIAMOND_FRAC = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
+                         [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+
+
+def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff: float = 16.0,
+                   name: str = "diamond8", method: str | None = None) -> Deck:
+    """Simple-cubic 8-atom diamond-like cell (lattice constant ``a`` bohr) of
+    Z_eff=4 pseudo-atoms, 32 electrons (16 up, 16 down).  Per atom 13 periodic
+    Gaussians (4 S + 3 P shells, 3 primitives, exponents log-uniform in
+    [0.1, 5], AOSPLINE CUTOFF 16); image centers out to ``image_cutoff`` bohr
+    (CUTOFF_DIVIDER = a / image_cutoff); Ewald with EWALD_GMAX 8 (the
+    reference's alpha = 5 / smallest cell height); Jastrow with e-e
+    (CUTOFF_CUSP), e-n (POLYPADE, 4 coefficients) and e-e-n (8 coefficients)
+    terms, all cut off inside half the cell (3.3 bohr) so the minimum-image
+    Jastrow is smooth."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    label, charge, nup, ndown = "X", 4, 16, 16
+    shells = []
+    for sym, n in (("S", 4), ("P", 3)):
+        for _ in range(n):
+            ex = np.exp(rng.uniform(np.log(0.1), np.log(5.0), size=3))
+            shells.append((sym, ex, rng.uniform(0.1, 1.0, size=3)))
+    nper = sum(SHELL_NFUNC[s] for s, _, _ in shells)
+    natoms = len(DIAMOND_FRAC)
+    nb = natoms * nper
+    cup = _random_orthonormal(rng, nb, nup)
+    cdn = _random_orthonormal(rng, nb, ndown)
+    onebody = rng.normal(0.0, 0.1, size=4)
+    threebody = rng.normal(0.0, 0.05, size=8)
+    pp = _pseudo_text(rng, label, charge)
+    orb = os.path.join(outdir, f"{name}.orb")
+    _write_orb(orb, np.concatenate([cup, cdn], axis=1), [nper] * natoms)
+    pos = DIAMOND_FRAC * a
+    rc = 3.3
+    jas = "\n".join([
+        "JASTROW2",
+        "GROUP {",
+        f"  EEBASIS {{ EE CUTOFF_CUSP GAMMA 24.0 CUSP 1.0 CUTOFF {rc} }}",
+        f"  EEBASIS {{ EE CUTOFF_CUSP GAMMA 24.0 CUSP 1.0 CUTOFF {rc} }}",
+        "  TWOBODY_SPIN { FREEZE",
+        "    LIKE_COEFFICIENTS { 0.25 0.0 }",
+        "    UNLIKE_COEFFICIENTS { 0.0 0.5 }",
+        "  }",
+        "}",
+        "GROUP {",
+        f"  EEBASIS {{ EE POLYPADE BETA0 0.5 NFUNC 3 RCUT {rc} }}",
+        f"  EIBASIS {{ {label} POLYPADE BETA0 1.2 NFUNC 4 RCUT {rc} }}",
+        "  ONEBODY {",
+        f"    COEFFICIENTS {{ {label} " + " ".join(_fmt(c) for c in onebody) + " }",
+        "  }",
+        "  THREEBODY {",
+        f"    COEFFICIENTS {{ {label} " + " ".join(_fmt(c) for c in threebody) + " }",
+        "  }",
+        "}",
+    ])
+    states_up = " ".join(str(i + 1) for i in range(nup))
+    states_dn = " ".join(str(nup + i + 1) for i in range(ndown))
+    deck = "\n".join([
+        f"# seeded synthetic workload {name} (seed {seed})",
+        f"RANDOMSEED {{ {1 + seed % 100000} {7 + seed % 7919} }}",
+        "SYSTEM { PERIODIC",
+        f"  NSPIN {{ {nup} {ndown} }}",
+        f"  LATTICEVEC {{ {a} 0 0  0 {a} 0  0 0 {a} }}",
+        "  ORIGIN { 0 0 0 }",
+        f"  CUTOFF_DIVIDER {_fmt(a / image_cutoff)}",
+        "  EWALD_GMAX 8",
+    ] + [f"  ATOM {{ {label} {charge} COOR {_fmt(p[0])} {_fmt(p[1])} {_fmt(p[2])} }}" for p in pos] + [
+        "}",
+        pp,
+        "TRIALFUNC { SLATER-JASTROW",
+        "  WF1 { SLATER",
+        "    ORBITALS { BLAS_MO",
+        f"      NMO {nup + ndown}",
+        f"      ORBFILE {os.path.basename(orb)}",
+        _basis_text(label, shells, cutoff=16.0),
+        "      CENTERS { USEGLOBAL }",
+        "    }",
+        "    DETWT { 1.0 }",
+        f"    STATES {{ {states_up} {states_dn} }}",
+        "  }",
+        "  WF2 {",
+        jas,
+        "  }",
+        "}",
+        f"METHOD {{ {method} }}" if method else "",
+    ]) + "\n"
+    path = os.path.join(outdir, f"{name}.qw")
+    with open(path, "w") as fh:
+        fh.write(deck)
+    return Deck(path=path, orb_path=orb, nup=nup, ndown=ndown, natoms=natoms, nbasis=nb, kind=name, seed=seed,
+                extra={"a": a, "atoms": pos})
+
+
 def random_configs(deck: Deck, nconf: int, seed: int, spread: float = 1.2) -> np.ndarray:
     """Seeded electron configurations [nconf, nelec, 3]: each electron sits
     near a random atom with a Gaussian spread (bohr)."""
     rng = np.random.default_rng(seed)
+    if "a" in deck.extra:  # periodic cell: uniform in the cell
+        return rng.uniform(0.0, deck.extra["a"], size=(nconf, deck.nelec, 3))
     atoms = np.array([[0.0, 0.0, -1.0375], [0.0, 0.0, 1.0375]])
     which = rng.integers(0, len(atoms), size=(nconf, deck.nelec))
     return atoms[which] + rng.normal(0.0, spread, size=(nconf, deck.nelec, 3))

@@ -368,7 +368,8 @@ class System:
         self.deck_path = deck_path
         words = tokenize(deck_path)
         sysw = section(words, "SYSTEM")
-        assert sysw[0].upper() in ("MOLECULE", "MOLECULAR"), sysw[0]
+        self.periodic = sysw[0].upper() == "PERIODIC"
+        assert self.periodic or sysw[0].upper() in ("MOLECULE", "MOLECULAR"), sysw[0]
         ns = section(sysw, "NSPIN")
         self.nup, self.ndn = int(ns[0]), int(ns[1])
         self.nelec = self.nup + self.ndn
@@ -380,6 +381,8 @@ class System:
             pos.append([float(a[i + 1]), float(a[i + 2]), float(a[i + 3])])
         self.atoms = np.array(pos)
         self.charges = np.array(self.charges)
+        if self.periodic:
+            self._read_cell(sysw)
         tf = section(words, "TRIALFUNC")
         wf1 = section(tf, "WF1")
         wf2 = section(tf, "WF2")
@@ -394,10 +397,13 @@ class System:
         self.mo_kind = orbw[0].upper()
         self.nmo = int(value(orbw, "NMO", conv=int))
         self.basis = [SplineBasis(b) for b in sections(orbw, "BASIS")]
-        # centers = atoms (USEATOMS / USEGLOBAL for molecules)
+        # centers = atoms (USEATOMS / USEGLOBAL for molecules); a periodic cell
+        # sums each atom's functions over its image centers
         self.center_basis = []
         for lab in self.labels:
             self.center_basis.append([b for b in self.basis if b.label == lab])
+        if not self.periodic:
+            self.images = [self.atoms[a:a + 1] for a in range(len(self.atoms))]
         self.nfunc_center = [sum(b.nfunc for b in bl) for bl in self.center_basis]
         self.totbasis = sum(self.nfunc_center)
         orbfile = value(orbw, "ORBFILE", conv=str)
@@ -508,9 +514,11 @@ class System:
         P = np.asarray(P, dtype=float)
         vals = []
         for c, bl in enumerate(self.center_basis):
-            d = P - self.atoms[c]
             for b in bl:
-                v = b.eval_lap(d)
+                v = 0.0
+                for img in self.images[c]:
+                    d = P - img
+                    v = v + b.eval_lap(d)
                 keep = np.abs(v[..., 0]) > 1e-8
                 vals.append(np.where(keep[..., None], v, 0.0))
         B = np.concatenate(vals, axis=-2)          # [..., totbasis, 5]
@@ -556,7 +564,7 @@ class System:
             if "onebody" in grp or "threebody" in grp:
                 ei = {}
                 for a, lab in enumerate(self.labels):
-                    d = R - self.atoms[a]                         # [nc,N,3]
+                    d = self.min_image(R - self.atoms[a])         # [nc,N,3]
                     r = np.sqrt(np.sum(d * d, axis=-1))
                     fs = [b.eval(r) for b in grp["ei"] if b.label == lab]
                     F = np.concatenate(fs, axis=-2) if fs else np.zeros((nc, N, 0, 3))
@@ -574,7 +582,7 @@ class System:
             if "twobody_spin" in grp or "twobody" in grp or "threebody" in grp:
                 eef = []
                 iu, ju = np.triu_indices(N, 1)
-                d = R[:, iu] - R[:, ju]                            # r_i - r_j
+                d = self.min_image(R[:, iu] - R[:, ju])            # r_i - r_j
                 r = np.sqrt(np.sum(d * d, axis=-1))
                 E = np.concatenate([b.eval(r) for b in grp["ee"]], axis=-2)   # [nc,P,k,3]
                 if "twobody_spin" in grp or "twobody" in grp:
@@ -637,16 +645,18 @@ class System:
 
     def evaluate(self, R):
         """Full evaluation of configurations R [nc, N, 3]."""
-        R = np.asarray(R, dtype=float)
+        R = self.wrap(np.asarray(R, dtype=float))
         logd, sign, gD, lD, inv, mo = self.slater(R)
         U, gU, lU = self.jastrow(R)
         grad = gD + gU
         lap = lD + lU + np.sum(gU * gU, axis=-1) + 2 * np.sum(gD * gU, axis=-1)
         out = {"logpsi": logd + U, "sign": sign, "grad": grad, "lap": lap,
-               "kinetic": -0.5 * lap.sum(axis=1), "potential": self.coulomb(R)}
+               "kinetic": -0.5 * lap.sum(axis=1),
+               "potential": self.ewald(R) if self.periodic else self.coulomb(R)}
         return out
 
     def logpsi(self, R):
+        R = self.wrap(np.asarray(R, dtype=float))
         logd, sign, *_ = self.slater(R)
         U, _, _ = self.jastrow(R)
         return logd + U, sign
@@ -669,7 +679,7 @@ class System:
         """Deterministic semilocal PP (Pseudopotential.cpp:596-815): local
         channel plus Q-point quadrature of the nonlocal channels for every
         (electron, atom) pair with |r| < cutoff.  rot [nc,3,3] rows x,y,z."""
-        R = np.asarray(R, dtype=float)
+        R = self.wrap(np.asarray(R, dtype=float))
         nc, N, _ = R.shape
         tot = np.zeros(nc)
         lp0, sg0 = self.logpsi(R)
@@ -677,7 +687,7 @@ class System:
             p = self.pp.get(lab)
             if p is None:
                 continue
-            d = R - self.atoms[a]
+            d = self.min_image(R - self.atoms[a])
             r = np.sqrt(np.sum(d * d, axis=-1))
             vl = self._vl(p["chans"], r)
             nl = len(p["chans"])
@@ -689,7 +699,8 @@ class System:
                     continue
                 for iq in range(len(p["w"])):
                     Rn = R.copy()
-                    Rn[:, e] = self.atoms[a] + q[:, iq] * r[:, e:e + 1]
+                    # move relative to the nearest image of the atom
+                    Rn[:, e] = R[:, e] + q[:, iq] * r[:, e:e + 1] - d[:, e]
                     lp, sg = self.logpsi(Rn)
                     ratio = np.exp(lp - lp0) * sg * sg0 * p["w"][iq]
                     cosq = np.sum(q[:, iq] * d[:, e], axis=-1) / r[:, e]
@@ -708,6 +719,200 @@ class System:
         ev = self.evaluate(Rn)
         idx = np.arange(len(R))
         return ev["logpsi"] - lp0, ev["sign"] * s0, ev["grad"][idx, e], ev["lap"][idx, e]
+
+
+def _erfcm(x):
+    """Polynomial erfc approximation used by the Ewald sum (A&S 7.1.26,
+    system/Periodic_system.h:221-227)."""
+    p, a, b, c, d, e = .3275911, .254829592, -.284496736, 1.421413741, -1.453152027, 1.061405429
+    y = 1. / (1. + p * x)
+    return y * (a + y * (b + y * (c + y * (d + y * e)))) * np.exp(-x * x)
+
+
+def _cell_setup(self, sysw):
+    """Periodic_system::read (system/Periodic_system.cpp:106-413)."""
+    lv = np.array([float(x) for x in section(sysw, "LATTICEVEC")]).reshape(3, 3)
+    og = section(sysw, "ORIGIN")
+    self.origin = np.array([float(x) for x in og[:3]]) if og else np.zeros(3)
+    self.lat = lv
+    cross = np.array([np.cross(lv[1], lv[2]), np.cross(lv[2], lv[0]), np.cross(lv[0], lv[1])])
+    det = abs(np.linalg.det(lv))
+    self.volume = det
+    self.recip = cross / det
+    nv = cross.copy()
+    for i in range(3):
+        if np.dot(nv[i], lv[i]) < 0:
+            nv[i] = -nv[i]
+    self.normvec = nv
+    self.corners = self.origin[None, :] + lv
+    heights = [abs(np.dot(cross[i], lv[i])) / np.linalg.norm(cross[i]) for i in range(3)]
+    self.smallest = min(heights)
+    self.alpha = 5.0 / self.smallest
+    self.atoms = np.array([self._wrap1(a) for a in self.atoms])
+    self.lattice_basis = np.array([aa * lv[0] + bb * lv[1] + cc * lv[2]
+                                   for aa in (-1, 0, 1) for bb in (-1, 0, 1) for cc in (-1, 0, 1)])
+    div = value(sysw, "CUTOFF_DIVIDER", 2.000001)
+    gmax = int(value(sysw, "EWALD_GMAX", 200, int))
+    self._find_centers(div)
+    # G vectors: half space, weight 4 pi exp(-G^2 / 4 alpha^2) / (V G^2) > 1e-10
+    gs, ws = [], []
+    for ig in range(0, gmax + 1):
+        for jg in range(0 if ig == 0 else -gmax, gmax + 1):
+            for kg in range(0 if (ig == 0 and jg == 0) else -gmax, gmax + 1):
+                g = 2 * math.pi * (ig * self.recip[0] + jg * self.recip[1] + kg * self.recip[2])
+                g2 = float(np.dot(g, g))
+                if g2 > 1e-8:
+                    w = 4.0 * math.pi * math.exp(-g2 / (4 * self.alpha ** 2)) / (self.volume * g2)
+                    if w > 1e-10:
+                        gs.append(g)
+                        ws.append(w)
+    self.gvec = np.array(gs)
+    self.gw = np.array(ws)
+    # constant terms (constEwald, ewaldIon, Periodic_system.cpp:620-749)
+    N = self.nelec
+    q = self.charges
+    nion = len(q)
+    ionion = sum(q[i] * q[j] for i in range(nion) for j in range(i + 1, nion))
+    ionelec = float(np.sum(q)) * (-N)
+    sq = -.5 * (2 * self.alpha / math.sqrt(math.pi) + math.pi / (self.volume * self.alpha ** 2))
+    ij = -math.pi / (self.volume * self.alpha ** 2)
+    self.self_ii = ionion * ij + float(np.sum(q * q)) * sq
+    self.self_ei = ionelec * ij
+    self.self_ee = .5 * N * (N - 1) * ij + N * sq
+    real = 0.0
+    im5 = [aa * lv[0] + bb * lv[1] + cc * lv[2] for aa in range(-2, 3) for bb in range(-2, 3) for cc in range(-2, 3)]
+    for i in range(nion):
+        for j in range(i):
+            r1 = self.atoms[i] - self.atoms[j]
+            for v in im5:
+                r = float(np.linalg.norm(r1 + v))
+                real += q[i] * q[j] * _erfcm(self.alpha * r) / r
+    ph = self.atoms @ self.gvec.T                       # [nion, G]
+    self.ion_sin = (q[:, None] * np.sin(ph)).sum(0)
+    self.ion_cos = (q[:, None] * np.cos(ph)).sum(0)
+    self.ion_ewald = real + float(np.sum(self.gw * (self.ion_sin ** 2 + self.ion_cos ** 2) / 2)) * 2
+
+
+def _wrap1(self, p):
+    """Periodic_system::enforcePbc (system/Periodic_system.cpp:521-570)."""
+    p = np.array(p, dtype=float)
+    for i in range(3):
+        while True:
+            tooshort = float(np.dot(self.normvec[i], p - self.origin))
+            toofar = float(np.dot(self.normvec[i], p - self.corners[i]))
+            if tooshort < -1e-12:
+                p = p + self.lat[i]
+            elif toofar > 1e-12:
+                p = p - self.lat[i]
+            else:
+                break
+    return p
+
+
+def _find_centers(self, divider):
+    """Image centers of every atom (find_centers, system/Pbc_enforcer.cpp:205-420)."""
+    lv = self.lat
+    h = [abs(np.dot(lv[0], np.cross(lv[1], lv[2]))) / np.linalg.norm(np.cross(lv[1], lv[2])),
+         abs(np.dot(lv[1], np.cross(lv[0], lv[2]))) / np.linalg.norm(np.cross(lv[0], lv[2])),
+         abs(np.dot(lv[2], np.cross(lv[0], lv[1]))) / np.linalg.norm(np.cross(lv[0], lv[1]))]
+    cutoff = min(h) / divider
+    org = self.origin.copy()
+    piped = np.zeros((3, 3))
+    for i in range(3):
+        org = org - cutoff * lv[i] / h[i]
+        piped[i] = lv[i] * (1 + 2 * cutoff / h[i])
+    cm = self.origin + 0.5 * lv.sum(0)
+    diag1 = lv.sum(0)
+    radius = float(np.linalg.norm(diag1))
+    for j in range(3):
+        rad2 = float(np.linalg.norm(diag1 - 2 * lv[j]))
+        radius = max(radius, rad2)
+    radius = 0.5 * radius + cutoff
+    pc = np.array([np.cross(piped[1], piped[2]), np.cross(piped[2], piped[0]), np.cross(piped[0], piped[1])])
+    for i in range(3):
+        if np.dot(pc[i], piped[i]) < 0:
+            pc[i] = -pc[i]
+    corners = org[None, :] + piped
+    images = [[] for _ in range(len(self.atoms))]
+    n = 4
+    for ii in range(-n, n + 1):
+        for jj in range(-n, n + 1):
+            for kk in range(-n, n + 1):
+                for at in range(len(self.atoms)):
+                    pos = self.atoms[at] + lv[0] * ii + lv[1] * jj + lv[2] * kk
+                    inside = all(np.dot(pc[i], pos - org) >= 0 and np.dot(pc[i], pos - corners[i]) <= 0
+                                 for i in range(3))
+                    if inside and np.linalg.norm(pos - cm) < radius:
+                        images[at].append(pos)
+    self.images = [np.array(im) for im in images]
+
+
+def _min_image(self, dr):
+    """Periodic_sample::minimum_image (system/Periodic_sample.cpp:259-287),
+    vectorised over leading axes."""
+    if not self.periodic:
+        return dr
+    dr = np.asarray(dr, dtype=float)
+    h2 = self.smallest * self.smallest * .25
+    d2 = np.sum(dr * dr, axis=-1)
+    out = dr.copy()
+    flat = dr.reshape(-1, 3)
+    of = out.reshape(-1, 3)
+    for n, (v, dd) in enumerate(zip(flat, d2.reshape(-1))):
+        if dd < h2:
+            continue
+        best, bd = None, 1e99
+        for lb in self.lattice_basis:
+            t = v + lb
+            td = float(np.dot(t, t))
+            if td < bd:
+                best, bd = t, td
+                if td < h2:
+                    break
+            if td < h2:
+                break
+        of[n] = best
+    return out
+
+
+def _wrap(self, R):
+    if not self.periodic:
+        return R
+    R = np.array(R, dtype=float)
+    flat = R.reshape(-1, 3)
+    for n in range(len(flat)):
+        flat[n] = self._wrap1(flat[n])
+    return R
+
+
+def _ewald(self, R):
+    """Periodic_system::ewaldElectron + constants (Periodic_system.cpp:586-973)."""
+    nc, N, _ = R.shape
+    out = np.full(nc, self.ion_ewald + self.self_ii + self.self_ee + self.self_ei)
+    im3 = np.array([aa * self.lat[0] + bb * self.lat[1] + cc * self.lat[2]
+                    for aa in (-1, 0, 1) for bb in (-1, 0, 1) for cc in (-1, 0, 1)])
+    for a in range(len(self.atoms)):
+        d = self.min_image(R - self.atoms[a])                     # [nc,N,3]
+        r = np.linalg.norm(d[:, :, None, :] + im3[None, None], axis=-1)
+        out -= self.charges[a] * np.sum(_erfcm(self.alpha * r) / r, axis=(1, 2))
+    iu, ju = np.triu_indices(N, 1)
+    d = self.min_image(R[:, iu] - R[:, ju])
+    r = np.linalg.norm(d[:, :, None, :] + im3[None, None], axis=-1)
+    out += np.sum(_erfcm(self.alpha * r) / r, axis=(1, 2))
+    ph = R @ self.gvec.T                                          # [nc,N,G]
+    ss = np.sin(ph).sum(1)
+    cs = np.cos(ph).sum(1)
+    out += 2 * np.sum(-(self.ion_cos * cs + self.ion_sin * ss) * self.gw, axis=1)
+    out += 2 * np.sum((cs * cs + ss * ss) * self.gw / 2, axis=1)
+    return out
+
+
+System._read_cell = _cell_setup
+System._wrap1 = _wrap1
+System._find_centers = _find_centers
+System.min_image = _min_image
+System.wrap = _wrap
+System.ewald = _ewald
 
 
 def legendre(x, l):

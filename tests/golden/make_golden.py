@@ -26,16 +26,23 @@ import refrun  # noqa: E402
 
 NCONF = 256
 NMOVE = 2
-WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseudo=True), 12)]
+WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseudo=True), 12),
+             ("diamond8", dict(periodic=True), 13)]
 
 
 def make(name, kw, seed):
-    deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
-    R = systems.random_configs(deck, NCONF, seed=seed + 1000)
+    if kw.get("periodic"):
+        deck = systems.write_periodic(HERE, seed=seed, name=name)
+        nconf = 64
+    else:
+        deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
+        nconf = NCONF
+    R = systems.random_configs(deck, nconf, seed=seed + 1000)
+    NCONF_ = nconf
     rng = np.random.default_rng(seed + 2000)
-    rot = np.stack([systems.random_rotation(rng) for _ in range(NCONF)])
-    me = rng.integers(0, deck.nelec, size=(NCONF, NMOVE)).astype(np.int32)
-    mp = R[np.arange(NCONF)[:, None], me] + rng.normal(0.0, 0.4, size=(NCONF, NMOVE, 3))
+    rot = np.stack([systems.random_rotation(rng) for _ in range(NCONF_)])
+    me = rng.integers(0, deck.nelec, size=(NCONF_, NMOVE)).astype(np.int32)
+    mp = R[np.arange(NCONF_)[:, None], me] + rng.normal(0.0, 0.4, size=(NCONF_, NMOVE, 3))
     out = refrun.run_harness(deck.path, R, rot, me, mp)
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), R=R, rot=rot, move_e=me, move_pos=mp, **out)
     print(name, "logpsi[:3]", out["logpsi"][:3])
