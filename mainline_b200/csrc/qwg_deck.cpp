@@ -454,6 +454,198 @@ static double pp_radial(const PPAtom& P, int l, double r) {
   return v;
 }
 
+// ---------------------------------------------------------------------------
+// periodic cell: Periodic_system::read (system/Periodic_system.cpp:106-413),
+// enforcePbc (:521-570), find_centers (system/Pbc_enforcer.cpp:205-420),
+// constEwald / ewaldIon (Periodic_system.cpp:620-749)
+
+static void cross3(const double* a, const double* b, double* c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+static double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+static double erfc_poly(double x) {
+  const double p = .3275911, a = .254829592, b = -.284496736, c = 1.421413741, d = -1.453152027, e = 1.061405429;
+  double y = 1. / (1. + p * x);
+  return y * (a + y * (b + y * (c + y * (d + y * e)))) * std::exp(-x * x);
+}
+
+static void wrap_host(const HostSystem& S, double* p) {
+  for (int i = 0; i < 3; i++) {
+    for (int it = 0; it < 1000; it++) {
+      double too_short = 0, too_far = 0;
+      for (int j = 0; j < 3; j++) {
+        too_short += S.normvec[3 * i + j] * (p[j] - S.origin[j]);
+        too_far += S.normvec[3 * i + j] * (p[j] - S.corners[3 * i + j]);
+      }
+      if (too_short < -1e-12) for (int j = 0; j < 3; j++) p[j] += S.lat[3 * i + j];
+      else if (too_far > 1e-12) for (int j = 0; j < 3; j++) p[j] -= S.lat[3 * i + j];
+      else break;
+    }
+  }
+}
+
+static void setup_cell(HostSystem& S, const std::vector<std::string>& sysw) {
+  auto lv = get_section(sysw, "LATTICEVEC");
+  if (lv.size() != 9) throw InputError("LATTICEVEC must have exactly 9 values");
+  for (int i = 0; i < 9; i++) S.lat[i] = to_d(lv[i]);
+  size_t pos = 0;
+  std::vector<std::string> og;
+  if (find_section(sysw, "ORIGIN", pos, og)) {
+    if (og.size() < 3) throw InputError("ORIGIN section must have at least 3 elements");
+    for (int i = 0; i < 3; i++) S.origin[i] = to_d(og[i]);
+  }
+  pos = 0;
+  std::vector<std::string> kp;
+  if (find_section(sysw, "KPOINT", pos, kp))
+    for (auto& k : kp)
+      if (to_d(k) != 0.0) throw InputError("nonzero KPOINT (complex orbitals) is not supported");
+  const double divider = value_d(sysw, "CUTOFF_DIVIDER", 2.000001);
+  const int gmax = (int)value_d(sysw, "EWALD_GMAX", 200);
+  const double* a0 = S.lat;
+  const double* a1 = S.lat + 3;
+  const double* a2 = S.lat + 6;
+  double cr[9];
+  cross3(a1, a2, cr);
+  cross3(a2, a0, cr + 3);
+  cross3(a0, a1, cr + 6);
+  double det = std::fabs(dot3(a0, cr));
+  S.volume = det;
+  double recip[9];
+  for (int i = 0; i < 9; i++) recip[i] = cr[i] / det;
+  for (int i = 0; i < 3; i++) {
+    double d = dot3(cr + 3 * i, S.lat + 3 * i);
+    for (int j = 0; j < 3; j++) S.normvec[3 * i + j] = d < 0 ? -cr[3 * i + j] : cr[3 * i + j];
+    for (int j = 0; j < 3; j++) S.corners[3 * i + j] = S.origin[j] + S.lat[3 * i + j];
+  }
+  S.smallest_height = 1e99;
+  for (int i = 0; i < 3; i++) {
+    double h = std::fabs(dot3(cr + 3 * i, S.lat + 3 * i)) / std::sqrt(dot3(cr + 3 * i, cr + 3 * i));
+    S.smallest_height = std::min(S.smallest_height, h);
+  }
+  S.alpha = 5.0 / S.smallest_height;
+  for (int aa = -1; aa <= 1; aa++)
+    for (int bb = -1; bb <= 1; bb++)
+      for (int cc = -1; cc <= 1; cc++)
+        for (int d = 0; d < 3; d++) S.lattice_basis.push_back(aa * a0[d] + bb * a1[d] + cc * a2[d]);
+  // image centers within the cell enlarged by cutoff = min height / divider
+  double hgt[3];
+  {
+    double c12[3], c02[3], c01[3];
+    cross3(a1, a2, c12); cross3(a0, a2, c02); cross3(a0, a1, c01);
+    hgt[0] = std::fabs(dot3(a0, c12)) / std::sqrt(dot3(c12, c12));
+    hgt[1] = std::fabs(dot3(a1, c02)) / std::sqrt(dot3(c02, c02));
+    hgt[2] = std::fabs(dot3(a2, c01)) / std::sqrt(dot3(c01, c01));
+  }
+  const double cutoff = std::min(std::min(hgt[0], hgt[1]), hgt[2]) / divider;
+  double org[3] = {S.origin[0], S.origin[1], S.origin[2]}, piped[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      org[j] -= cutoff * S.lat[3 * i + j] / hgt[i];
+      piped[3 * i + j] = S.lat[3 * i + j] * (1 + 2 * cutoff / hgt[i]);
+    }
+  double cm[3], diag[3];
+  for (int i = 0; i < 3; i++) {
+    cm[i] = S.origin[i];
+    diag[i] = 0;
+    for (int j = 0; j < 3; j++) { cm[i] += 0.5 * S.lat[3 * j + i]; diag[i] += S.lat[3 * j + i]; }
+  }
+  double radius = std::sqrt(dot3(diag, diag));
+  for (int j = 0; j < 3; j++) {
+    double d2[3];
+    for (int i = 0; i < 3; i++) d2[i] = diag[i] - 2 * S.lat[3 * j + i];
+    radius = std::max(radius, std::sqrt(dot3(d2, d2)));
+  }
+  radius = 0.5 * radius + cutoff;
+  double pc[9];
+  cross3(piped + 3, piped + 6, pc);
+  cross3(piped + 6, piped, pc + 3);
+  cross3(piped, piped + 3, pc + 6);
+  for (int i = 0; i < 3; i++)
+    if (dot3(pc + 3 * i, piped + 3 * i) < 0)
+      for (int j = 0; j < 3; j++) pc[3 * i + j] = -pc[3 * i + j];
+  std::vector<std::vector<double>> img(S.natoms);
+  const int ns = 4;
+  for (int ii = -ns; ii <= ns; ii++)
+    for (int jj = -ns; jj <= ns; jj++)
+      for (int kk = -ns; kk <= ns; kk++)
+        for (int at = 0; at < S.natoms; at++) {
+          double p[3];
+          for (int i = 0; i < 3; i++) p[i] = S.atom_pos[3 * at + i] + a0[i] * ii + a1[i] * jj + a2[i] * kk;
+          bool inside = true;
+          for (int i = 0; i < 3 && inside; i++) {
+            double sh = 0, fa = 0;
+            for (int j = 0; j < 3; j++) {
+              sh += pc[3 * i + j] * (p[j] - org[j]);
+              fa += pc[3 * i + j] * (p[j] - (org[j] + piped[3 * i + j]));
+            }
+            if (sh < 0 || fa > 0) inside = false;
+          }
+          double dc[3] = {p[0] - cm[0], p[1] - cm[1], p[2] - cm[2]};
+          if (inside && std::sqrt(dot3(dc, dc)) < radius) img[at].insert(img[at].end(), p, p + 3);
+        }
+  for (int at = 0; at < S.natoms; at++) {
+    S.image_first.push_back((int)S.image_pos.size() / 3);
+    S.image_count.push_back((int)img[at].size() / 3);
+    S.image_pos.insert(S.image_pos.end(), img[at].begin(), img[at].end());
+  }
+  // the image centers come from the positions as given; the ions themselves
+  // are then put inside the cell (same order as the reference's read)
+  for (int a = 0; a < S.natoms; a++) wrap_host(S, &S.atom_pos[3 * a]);
+  // G vectors: half space, weight 4 pi exp(-G^2/4 alpha^2)/(V G^2) > 1e-10
+  for (int ig = 0; ig <= gmax; ig++)
+    for (int jg = (ig == 0 ? 0 : -gmax); jg <= gmax; jg++)
+      for (int kg = ((ig == 0 && jg == 0) ? 0 : -gmax); kg <= gmax; kg++) {
+        double g[3];
+        for (int i = 0; i < 3; i++) g[i] = 2 * M_PI * (ig * recip[i] + jg * recip[3 + i] + kg * recip[6 + i]);
+        double g2 = dot3(g, g);
+        if (g2 > 1e-8) {
+          double w = 4.0 * M_PI * std::exp(-g2 / (4 * S.alpha * S.alpha)) / (S.volume * g2);
+          if (w > 1e-10) { S.gvec.insert(S.gvec.end(), g, g + 3); S.gweight.push_back(w); }
+        }
+      }
+  const int ng = (int)S.gweight.size();
+  // constant terms
+  const int N = S.nelec, na = S.natoms;
+  double ionion = 0, ionelec = 0, q2 = 0;
+  for (int i = 0; i < na; i++) {
+    ionelec += S.atom_charge[i] * (-N);
+    q2 += S.atom_charge[i] * S.atom_charge[i];
+    for (int j = i + 1; j < na; j++) ionion += S.atom_charge[i] * S.atom_charge[j];
+  }
+  const double sq = -.5 * (2 * S.alpha / std::sqrt(M_PI) + M_PI / (S.volume * S.alpha * S.alpha));
+  const double ij = -M_PI / (S.volume * S.alpha * S.alpha);
+  const double self_ii = ionion * ij + q2 * sq;
+  const double self_ei = ionelec * ij;
+  const double self_ee = .5 * double(N) * (N - 1) * ij + N * sq;
+  double real = 0;
+  for (int i = 0; i < na; i++)
+    for (int j = 0; j < i; j++)
+      for (int kk = -2; kk <= 2; kk++)
+        for (int jj = -2; jj <= 2; jj++)
+          for (int ii = -2; ii <= 2; ii++) {
+            double r2[3];
+            for (int d = 0; d < 3; d++)
+              r2[d] = S.atom_pos[3 * i + d] - S.atom_pos[3 * j + d] + kk * a0[d] + jj * a1[d] + ii * a2[d];
+            double r = std::sqrt(dot3(r2, r2));
+            real += S.atom_charge[i] * S.atom_charge[j] * erfc_poly(S.alpha * r) / r;
+          }
+  S.ion_sin.assign(ng, 0.0);
+  S.ion_cos.assign(ng, 0.0);
+  double eion = 0;
+  for (int g = 0; g < ng; g++) {
+    for (int a = 0; a < na; a++) {
+      double dp = dot3(&S.atom_pos[3 * a], &S.gvec[3 * g]);
+      S.ion_sin[g] += S.atom_charge[a] * std::sin(dp);
+      S.ion_cos[g] += S.atom_charge[a] * std::cos(dp);
+    }
+    eion += S.gweight[g] * (S.ion_sin[g] * S.ion_sin[g] + S.ion_cos[g] * S.ion_cos[g]) / 2;
+  }
+  S.ewald_const = 2 * eion + real + self_ii + self_ee + self_ei;
+}
+
 HostSystem build_system(const std::string& deck_path) {
   HostSystem S;
   S.deck_path = deck_path;
@@ -462,8 +654,9 @@ HostSystem build_system(const std::string& deck_path) {
 
   // ---- SYSTEM
   auto sysw = get_section(words, "SYSTEM");
-  if (sysw.empty() || !(ieq(sysw[0], "MOLECULE") || ieq(sysw[0], "MOLECULAR")))
-    throw InputError("only SYSTEM { MOLECULE } is supported by this engine build");
+  if (sysw.empty() || !(ieq(sysw[0], "MOLECULE") || ieq(sysw[0], "MOLECULAR") || ieq(sysw[0], "PERIODIC")))
+    throw InputError("SYSTEM must be MOLECULE or PERIODIC");
+  S.periodic = ieq(sysw[0], "PERIODIC");
   auto ns = get_section(sysw, "NSPIN");
   if (ns.size() != 2) throw InputError("NSPIN needs two numbers");
   S.nup = to_i(ns[0]);
@@ -481,15 +674,21 @@ HostSystem build_system(const std::string& deck_path) {
   S.natoms = (int)S.labels.size();
   if (S.natoms == 0) throw InputError("no ATOM in SYSTEM");
   if (S.nelec <= 0 || S.nup < 0 || S.ndn < 0) throw InputError("bad NSPIN");
-  for (int i = 0; i < S.natoms; i++)
-    for (int j = 0; j < i; j++) {
-      double d2 = 0;
-      for (int d = 0; d < 3; d++) {
-        double t = S.atom_pos[3 * i + d] - S.atom_pos[3 * j + d];
-        d2 += t * t;
+  if (S.periodic) {
+    setup_cell(S, sysw);
+  } else {
+    for (int i = 0; i < S.natoms; i++)
+      for (int j = 0; j < i; j++) {
+        double d2 = 0;
+        for (int d = 0; d < 3; d++) {
+          double t = S.atom_pos[3 * i + d] - S.atom_pos[3 * j + d];
+          d2 += t * t;
+        }
+        S.ion_ion += S.atom_charge[i] * S.atom_charge[j] / std::sqrt(d2);
       }
-      S.ion_ion += S.atom_charge[i] * S.atom_charge[j] / std::sqrt(d2);
-    }
+    S.image_pos = S.atom_pos;
+    for (int a = 0; a < S.natoms; a++) { S.image_first.push_back(a); S.image_count.push_back(1); }
+  }
 
   // ---- TRIALFUNC
   auto tf = get_section(words, "TRIALFUNC");

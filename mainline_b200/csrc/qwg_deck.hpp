@@ -89,6 +89,16 @@ struct HostSystem {
   std::vector<double> onebody;       // per ei function (already per atom slice)
   std::vector<int> tb_first, tb_count;     // per atom slice into tb
   std::vector<ThreeBodyTerm> tb;
+  // periodic cell (SYSTEM { PERIODIC }); molecules keep periodic == false and
+  // one "image" per atom (the atom itself)
+  bool periodic = false;
+  double lat[9] = {0}, origin[3] = {0}, normvec[9] = {0}, corners[9] = {0};
+  double smallest_height = 0, alpha = 0, volume = 0;
+  std::vector<double> lattice_basis;   // [27][3] minimum-image search
+  std::vector<double> image_pos;       // [nimage][3] image centers of all atoms
+  std::vector<int> image_first, image_count;  // per atom slice of image_pos
+  std::vector<double> gvec, gweight, ion_sin, ion_cos;  // Ewald G-vectors [G][3], [G]
+  double ewald_const = 0;              // ion-ion Ewald + self/background terms
   // pseudopotential (per atom; nchan == 0 if none)
   std::vector<PPAtom> pp;
   bool has_pp = false;

@@ -97,7 +97,63 @@ struct DevSys {
   double pp_term[QWG_MAXT][QWG_MAXPPT][3];  // (n, a, c)
   double pp_quad[QWG_MAXT][QWG_MAXQ][3];
   double pp_w[QWG_MAXT][QWG_MAXQ];
+  // periodic cell (periodic == 0: molecule, one image per atom = the atom)
+  int periodic;
+  double lat[3][3], normvec[3][3], origin[3], corners[3][3];
+  double h2q;                    // (smallest cell height / 2)^2: minimum-image shortcut
+  double lattice_basis[27][3];
+  double alpha, ewald_const;
+  int2 atom_images[QWG_MAXA];    // (first, count) into image_pos
+  const double* image_pos;       // [nimage][3] basis centers (atoms and their images)
+  int ng;                        // Ewald G-vectors
+  const double* gvec;            // [ng][3]
+  const double* gweight;         // [ng]
+  const double* ion_sin;         // [ng]
+  const double* ion_cos;         // [ng]
 };
+
+// Minimum-image vector (Periodic_sample::minimum_image,
+// system/Periodic_sample.cpp:259-287); identity for molecules.
+template <typename Real>
+__device__ __forceinline__ void min_image(const DevSys<Real>& S, double& x, double& y, double& z) {
+  if (!S.periodic) return;
+  const double d2 = x * x + y * y + z * z;
+  if (d2 < S.h2q) return;
+  double bx = x, by = y, bz = z, bd = 1e99;
+  for (int a = 0; a < 27; a++) {
+    const double tx = x + S.lattice_basis[a][0], ty = y + S.lattice_basis[a][1], tz = z + S.lattice_basis[a][2];
+    const double td = tx * tx + ty * ty + tz * tz;
+    if (td < bd) {
+      bx = tx; by = ty; bz = tz; bd = td;
+      if (td < S.h2q) break;
+    }
+  }
+  x = bx; y = by; z = bz;
+}
+
+// Put a position inside the cell (Periodic_system::enforcePbc,
+// system/Periodic_system.cpp:521-570).  At most 64 shifts per direction.
+template <typename Real>
+__device__ __forceinline__ void wrap_pos(const DevSys<Real>& S, double& x, double& y, double& z) {
+  if (!S.periodic) return;
+  for (int i = 0; i < 3; i++) {
+    for (int it = 0; it < 64; it++) {
+      const double* n = S.normvec[i];
+      const double sh = n[0] * (x - S.origin[0]) + n[1] * (y - S.origin[1]) + n[2] * (z - S.origin[2]);
+      const double fa = n[0] * (x - S.corners[i][0]) + n[1] * (y - S.corners[i][1]) + n[2] * (z - S.corners[i][2]);
+      if (sh < -1e-12) { x += S.lat[i][0]; y += S.lat[i][1]; z += S.lat[i][2]; }
+      else if (fa > 1e-12) { x -= S.lat[i][0]; y -= S.lat[i][1]; z -= S.lat[i][2]; }
+      else break;
+    }
+  }
+}
+
+// erfc approximation of the Ewald sum (A&S 7.1.26, Periodic_system.h:221-227)
+__device__ __forceinline__ double erfc_poly(double x) {
+  const double p = .3275911, a = .254829592, b = -.284496736, c = 1.421413741, d = -1.453152027, e = 1.061405429;
+  double y = 1. / (1. + p * x);
+  return y * (a + y * (b + y * (c + y * (d + y * e)))) * exp(-x * x);
+}
 
 // Per-walker shared-memory layout (byte offsets, host computed).
 struct WLayout {
@@ -253,43 +309,52 @@ __device__ __forceinline__ T radial_val(const DRadial& q, T r) {
 // Orderings follow the GAMESS conventions of Cubic_spline_build.cpp:660-760.
 
 // Writes the 5 components of one function to out[0..4] (a basis row).
-template <typename Real>
+// ACC: add to out (image sums; the |value| rule is applied by the caller to
+// the sums) instead of storing with the |value| <= 1e-8 rule of the dense
+// evaluator (MO_matrix_blas.h:468-470).
+template <typename Real, bool ACC>
 __device__ __forceinline__ void put_lap(Real* out, double A, double ax, double ay, double az, double lapA, int l,
                                         double x, double y, double z, double f, double fd, double f2) {
   double v = A * f;
   double h = A * fd;
-  bool keep = fabs(v) > 1e-8;   // the dense evaluator drops |value| <= 1e-8
-  out[0] = Real(keep ? v : 0.0);
-  out[1] = Real(keep ? h * x + ax * f : 0.0);
-  out[2] = Real(keep ? h * y + ay * f : 0.0);
-  out[3] = Real(keep ? h * z + az * f : 0.0);
-  out[4] = Real(keep ? A * f2 + double(2 * l + 2) * h + lapA * f : 0.0);
+  double g0 = h * x + ax * f, g1 = h * y + ay * f, g2 = h * z + az * f;
+  double lp = A * f2 + double(2 * l + 2) * h + lapA * f;
+  if (ACC) {
+    out[0] += Real(v); out[1] += Real(g0); out[2] += Real(g1); out[3] += Real(g2); out[4] += Real(lp);
+  } else {
+    bool keep = fabs(v) > 1e-8;
+    out[0] = Real(keep ? v : 0.0);
+    out[1] = Real(keep ? g0 : 0.0);
+    out[2] = Real(keep ? g1 : 0.0);
+    out[3] = Real(keep ? g2 : 0.0);
+    out[4] = Real(keep ? lp : 0.0);
+  }
 }
 
-template <typename Real>
+template <typename Real, bool ACC>
 __device__ __forceinline__ void shell_lap_store(int sym, double x, double y, double z, double f, double fd, double f2,
                                                 Real* b /* [nf][5] */) {
   switch (sym) {
-    case 0: put_lap(b, 1.0, 0.0, 0.0, 0.0, 0.0, 0, x, y, z, f, fd, f2); break;
+    case 0: put_lap<Real, ACC>(b, 1.0, 0.0, 0.0, 0.0, 0.0, 0, x, y, z, f, fd, f2); break;
     case 1:
-      put_lap(b, x, 1.0, 0.0, 0.0, 0.0, 1, x, y, z, f, fd, f2);
-      put_lap(b + 5, y, 0.0, 1.0, 0.0, 0.0, 1, x, y, z, f, fd, f2);
-      put_lap(b + 10, z, 0.0, 0.0, 1.0, 0.0, 1, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b, x, 1.0, 0.0, 0.0, 0.0, 1, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 5, y, 0.0, 1.0, 0.0, 0.0, 1, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 10, z, 0.0, 0.0, 1.0, 0.0, 1, x, y, z, f, fd, f2);
       break;
     case 2:
-      put_lap(b, x * x, 2 * x, 0.0, 0.0, 2.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 5, y * y, 0.0, 2 * y, 0.0, 2.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 10, z * z, 0.0, 0.0, 2 * z, 2.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 15, x * y, y, x, 0.0, 0.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 20, x * z, z, 0.0, x, 0.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 25, y * z, 0.0, z, y, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b, x * x, 2 * x, 0.0, 0.0, 2.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 5, y * y, 0.0, 2 * y, 0.0, 2.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 10, z * z, 0.0, 0.0, 2 * z, 2.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 15, x * y, y, x, 0.0, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 20, x * z, z, 0.0, x, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 25, y * z, 0.0, z, y, 0.0, 2, x, y, z, f, fd, f2);
       break;
     default:
-      put_lap(b, 2 * z * z - x * x - y * y, -2 * x, -2 * y, 4 * z, 0.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 5, x * z, z, 0.0, x, 0.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 10, y * z, 0.0, z, y, 0.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 15, x * x - y * y, 2 * x, -2 * y, 0.0, 0.0, 2, x, y, z, f, fd, f2);
-      put_lap(b + 20, x * y, y, x, 0.0, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b, 2 * z * z - x * x - y * y, -2 * x, -2 * y, 4 * z, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 5, x * z, z, 0.0, x, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 10, y * z, 0.0, z, y, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 15, x * x - y * y, 2 * x, -2 * y, 0.0, 0.0, 2, x, y, z, f, fd, f2);
+      put_lap<Real, ACC>(b + 20, x * y, y, x, 0.0, 0.0, 2, x, y, z, f, fd, f2);
       break;
   }
 }
@@ -307,22 +372,47 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
   for (int s = lane; s < S.nshell; s += 32) {
     int4 si = S.shell_i[s];
     int2 so = S.shell_obj[s];
-    const double* ap = S.atom_pos[si.x];
-    double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
-    double r = sqrt(dx * dx + dy * dy + dz * dz);
     Real* b = bas + si.z * 5;
-    if (r < S.shell_cut[s]) {
-      int i = int(r * S.inv_spacing);
-      double h = r - double(i) * S.spacing;
-      const double2* c2p = reinterpret_cast<const double2*>(S.spline64 + ((size_t)so.x + (size_t)i * so.y + si.w) * 4);
-      double2 ca = __ldg(c2p), cb = __ldg(c2p + 1);
-      double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
-      double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
-      double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
-      shell_lap_store(si.y, dx, dy, dz, f, fd, f2, b);
+    const int nf = sym_nfunc(si.y);
+    const double cut = S.shell_cut[s];
+    if (!S.periodic) {
+      const double* ap = S.atom_pos[si.x];
+      double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      if (r < cut) {
+        int i = int(r * S.inv_spacing);
+        double h = r - double(i) * S.spacing;
+        const double2* c2p = reinterpret_cast<const double2*>(S.spline64 + ((size_t)so.x + (size_t)i * so.y + si.w) * 4);
+        double2 ca = __ldg(c2p), cb = __ldg(c2p + 1);
+        double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
+        double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
+        double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
+        shell_lap_store<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
+      } else {
+        for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
+      }
     } else {
-      const int nf = sym_nfunc(si.y);
+      // periodic: sum the shell over the atom's image centers, then apply the
+      // |value| <= 1e-8 rule to the sums (MO_matrix_blas.h:444-474)
       for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
+      const int2 im = S.atom_images[si.x];
+      for (int m = im.x; m < im.x + im.y; m++) {
+        const double* cp = S.image_pos + 3 * m;
+        double dx = px - cp[0], dy = py - cp[1], dz = pz - cp[2];
+        double r = sqrt(dx * dx + dy * dy + dz * dz);
+        if (!(r < cut)) continue;
+        int i = int(r * S.inv_spacing);
+        double h = r - double(i) * S.spacing;
+        const double2* c2p = reinterpret_cast<const double2*>(S.spline64 + ((size_t)so.x + (size_t)i * so.y + si.w) * 4);
+        double2 ca = __ldg(c2p), cb = __ldg(c2p + 1);
+        double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
+        double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
+        double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
+        shell_lap_store<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
+      }
+      for (int k = 0; k < nf; k++)
+        if (!(fabs(double(b[5 * k])) > 1e-8))
+          for (int c = 0; c < 5; c++) b[5 * k + c] = Real(0);
     }
   }
   __syncwarp();
@@ -409,6 +499,55 @@ __device__ __forceinline__ Real basis_dot_lane(const DevSys<Real>& S, double px,
   return acc;
 }
 
+// Periodic version of basis_dot_lane: each atom's functions are summed over
+// its image centers before the |value| rule and the dot with w.
+constexpr int QWG_MAXF_ATOM = 16;  // basis functions per atom on the periodic path
+template <typename Real>
+__device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, double px, double py, double pz,
+                                                        const Real* w) {
+  Real acc = Real(0);
+  for (int c = 0; c < S.natoms; c++) {
+    const int4 cs = S.center_seg[c];  // first shell, shells, object base, splines per row
+    if (cs.y == 0) continue;
+    Real fs[QWG_MAXF_ATOM];
+    int nfa = 0;
+    for (int k = 0; k < cs.y; k++) nfa += sym_nfunc(S.shell_pack[cs.x + k] & 0xf);
+    for (int q = 0; q < QWG_MAXF_ATOM; q++) fs[q] = Real(0);
+    const int fb0 = (S.shell_pack[cs.x] >> 4) & 0xffff;
+    const int2 im = S.atom_images[c];
+    const Real cut = Real(S.center_cut[c]);
+    for (int m = im.x; m < im.x + im.y; m++) {
+      const double* cp = S.image_pos + 3 * m;
+      const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
+      const Real rd = sqrt(x * x + y * y + z * z);
+      if (!(rd < cut)) continue;
+      const int i = int(rd * Real(S.inv_spacing));
+      const Real h = rd - Real(i) * Real(S.spacing);
+      const Real* row = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4;
+      for (int k = 0; k < cs.y; k++) {
+        const int pk = S.shell_pack[cs.x + k];
+        const int sym = pk & 0xf, fo = ((pk >> 4) & 0xffff) - fb0, kk = (pk >> 20) & 0xff;
+        const Real* cf = row + 4 * kk;
+        const Real f = __ldg(cf) + h * (__ldg(cf + 1) + h * (__ldg(cf + 2) + h * __ldg(cf + 3)));
+        switch (sym) {
+          case 0: fs[fo] += f; break;
+          case 1: fs[fo] += x * f; fs[fo + 1] += y * f; fs[fo + 2] += z * f; break;
+          case 2:
+            fs[fo] += x * x * f; fs[fo + 1] += y * y * f; fs[fo + 2] += z * z * f;
+            fs[fo + 3] += x * y * f; fs[fo + 4] += x * z * f; fs[fo + 5] += y * z * f;
+            break;
+          default:
+            fs[fo] += (Real(2) * z * z - x * x - y * y) * f; fs[fo + 1] += x * z * f; fs[fo + 2] += y * z * f;
+            fs[fo + 3] += (x * x - y * y) * f; fs[fo + 4] += x * y * f;
+            break;
+        }
+      }
+    }
+    for (int q = 0; q < nfa; q++) acc += (fabs(fs[q]) > Real(1e-8) ? fs[q] : Real(0)) * w[fb0 + q];
+  }
+  return acc;
+}
+
 // ---------------------------------------------------------------------------
 // Jastrow pieces (tables from the parameter bank; sums in double)
 
@@ -435,6 +574,7 @@ __device__ __forceinline__ void jas_onebody(const DevSys<Real>& S, double px, do
     const int t = S.atom_type[a];
     const double* ap = S.atom_pos[a];
     double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
+    min_image(S, dx, dy, dz);
     double r = sqrt(dx * dx + dy * dy + dz * dz);
     for (int k = 0; k < S.ei_n[t]; k++) {
       double c = S.onebody[t][k];
@@ -455,6 +595,7 @@ __device__ void jas_threebody_pair(const DevSys<Real>& S, const double pi[3], co
   u = 0; li = lj = 0;
   for (int d = 0; d < 3; d++) gi[d] = gj[d] = 0;
   double dij[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
+  min_image(S, dij[0], dij[1], dij[2]);
   double rij = sqrt(dij[0] * dij[0] + dij[1] * dij[1] + dij[2] * dij[2]);
   for (int a = 0; a < S.natoms; a++) {
     const int t = S.atom_type[a];
@@ -463,6 +604,8 @@ __device__ void jas_threebody_pair(const DevSys<Real>& S, const double pi[3], co
     const double* ap = S.atom_pos[a];
     double di[3] = {pi[0] - ap[0], pi[1] - ap[1], pi[2] - ap[2]};
     double dj[3] = {pj[0] - ap[0], pj[1] - ap[1], pj[2] - ap[2]};
+    min_image(S, di[0], di[1], di[2]);
+    min_image(S, dj[0], dj[1], dj[2]);
     double ri = sqrt(di[0] * di[0] + di[1] * di[1] + di[2] * di[2]);
     double rj = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
     for (int n = 0; n < nt; n++) {
@@ -509,6 +652,7 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
     double dx = px - R[3 * j], dy = py - R[3 * j + 1], dz = pz - R[3 * j + 2];
+    min_image(S, dx, dy, dz);
     double r = sqrt(dx * dx + dy * dy + dz * dz);
     double pu, pfd, pl;
     jas_pair_t<double>(S, si == (j < S.nup), r, pu, pfd, pl);
@@ -532,7 +676,9 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
   for (int a = 0; a < S.natoms; a++) {
     const int t = S.atom_type[a];
     const double* ap = S.atom_pos[a];
-    const T dx = T(px - ap[0]), dy = T(py - ap[1]), dz = T(pz - ap[2]);
+    double ex = px - ap[0], ey = py - ap[1], ez = pz - ap[2];
+    min_image(S, ex, ey, ez);
+    const T dx = T(ex), dy = T(ey), dz = T(ez);
     const T r = sqrt(dx * dx + dy * dy + dz * dz);
     for (int k = 0; k < S.ei_n[t]; k++) {
       const double c = S.onebody[t][k];
@@ -543,7 +689,9 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
   const double pi[3] = {px, py, pz};
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
-    const T dx = T(px - R[3 * j]), dy = T(py - R[3 * j + 1]), dz = T(pz - R[3 * j + 2]);
+    double ex = px - R[3 * j], ey = py - R[3 * j + 1], ez = pz - R[3 * j + 2];
+    min_image(S, ex, ey, ez);
+    const T dx = T(ex), dy = T(ey), dz = T(ez);
     const T r = sqrt(dx * dx + dy * dy + dz * dz);
     const bool same = si == (j < S.nup);
     for (int k = 0; k < S.nee; k++) {

@@ -71,6 +71,7 @@ struct qwg_ctx {
   long long launches = 0;
   // tables
   DevBuf d_shell_i, d_shell_obj, d_shell_cut, d_spline, d_spline64, d_moc;
+  DevBuf d_image_pos, d_gvec, d_gweight, d_ion_sin, d_ion_cos;
   DevSys<double> sys_d{};
   DevSys<float> sys_f{};
   WLayout L{};
@@ -161,6 +162,35 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     if (sh.first >= (1 << 16) || sh.k >= 256) throw InputError("basis too large for the shell table");
     S.shell_pack[k] = sh.sym | (sh.first << 4) | (sh.k << 20);
   }
+  // periodic cell and basis image centers
+  S.periodic = H.periodic ? 1 : 0;
+  for (int i = 0; i < 3; i++) {
+    S.origin[i] = H.origin[i];
+    for (int j = 0; j < 3; j++) {
+      S.lat[i][j] = H.lat[3 * i + j];
+      S.normvec[i][j] = H.normvec[3 * i + j];
+      S.corners[i][j] = H.corners[3 * i + j];
+    }
+  }
+  S.h2q = H.smallest_height * H.smallest_height * 0.25;
+  for (int k = 0; k < 27 && H.periodic; k++)
+    for (int d = 0; d < 3; d++) S.lattice_basis[k][d] = H.lattice_basis[3 * k + d];
+  S.alpha = H.alpha;
+  S.ewald_const = H.ewald_const;
+  for (int a = 0; a < H.natoms; a++) S.atom_images[a] = make_int2(H.image_first[a], H.image_count[a]);
+  S.image_pos = c->d_image_pos.as<double>();
+  S.ng = (int)H.gweight.size();
+  S.gvec = c->d_gvec.as<double>();
+  S.gweight = c->d_gweight.as<double>();
+  S.ion_sin = c->d_ion_sin.as<double>();
+  S.ion_cos = c->d_ion_cos.as<double>();
+  if (H.periodic)
+    for (int a = 0; a < H.natoms; a++) {
+      int nf = 0;
+      for (auto& sh : H.shells)
+        if (sh.center == a) nf += sh.nfunc;
+      if (nf > QWG_MAXF_ATOM) throw InputError("periodic cells support at most 16 basis functions per atom");
+    }
   // Jastrow
   S.nee = (int)H.ee.size();
   for (int k = 0; k < S.nee; k++) {
@@ -255,6 +285,11 @@ static void build_tables(qwg_ctx* c) {
     upload(c->d_spline, sf, st);
     upload(c->d_moc, mf, st);
   }
+  upload(c->d_image_pos, H.image_pos, st);
+  upload(c->d_gvec, H.gvec, st);
+  upload(c->d_gweight, H.gweight, st);
+  upload(c->d_ion_sin, H.ion_sin, st);
+  upload(c->d_ion_cos, H.ion_cos, st);
   fill_sys<double>(c, c->sys_d, obj_base);
   fill_sys<float>(c, c->sys_f, obj_base);
   const void* req[] = {c->sys_d.shell_i, c->sys_d.shell_obj, c->sys_d.shell_cut, c->sys_d.spline,

@@ -146,8 +146,10 @@ struct Walker {
       if (j == e) continue;
       const double* pj = Rp + 3 * j;
       const bool same = se == (j < S.nup);
-      const double nx = px - pj[0], ny = py - pj[1], nz = pz - pj[2];
-      const double qx = ox - pj[0], qy = oy - pj[1], qz = oz - pj[2];
+      double nx = px - pj[0], ny = py - pj[1], nz = pz - pj[2];
+      double qx = ox - pj[0], qy = oy - pj[1], qz = oz - pj[2];
+      min_image(S, nx, ny, nz);
+      min_image(S, qx, qy, qz);
       // pair functions in the working precision, sums in FP64
       const Real rn = sqrt(Real(nx * nx + ny * ny + nz * nz)), ro = sqrt(Real(qx * qx + qy * qy + qz * qz));
       double un, fn, ln, uo, fo, lo;
@@ -181,6 +183,8 @@ struct Walker {
       const double* ap = S.atom_pos[a];
       double nx = px - ap[0], ny = py - ap[1], nz = pz - ap[2];
       double qx = ox - ap[0], qy = oy - ap[1], qz = oz - ap[2];
+      min_image(S, nx, ny, nz);
+      min_image(S, qx, qy, qz);
       double rn = sqrt(nx * nx + ny * ny + nz * nz), ro = sqrt(qx * qx + qy * qy + qz * qz);
       double fnv, fnd, fnl;
       radial_lap(S.ei[t][k], rn, fnv, fnd, fnl);
@@ -274,8 +278,53 @@ struct Walker {
     return -0.5 * warp_sum(k);
   }
 
+  // Periodic_system::ewaldElectron + the constant ion/self terms
+  // (Periodic_system.cpp:586-973): real-space sums over the 27 images of the
+  // minimum-image vectors, reciprocal sum over the kept G-vectors.
+  __device__ double ewald() const {
+    const double* Rp = R();
+    const int N = S.nelec, A = S.natoms;
+    double v = 0;
+    for (int idx = lane; idx < N * A; idx += 32) {
+      const int e = idx / A, a = idx - e * A;
+      double dx = Rp[3 * e] - S.atom_pos[a][0], dy = Rp[3 * e + 1] - S.atom_pos[a][1], dz = Rp[3 * e + 2] - S.atom_pos[a][2];
+      min_image(S, dx, dy, dz);
+      double t = 0;
+      for (int k = 0; k < 27; k++) {
+        double x = dx + S.lattice_basis[k][0], y = dy + S.lattice_basis[k][1], z = dz + S.lattice_basis[k][2];
+        double r = sqrt(x * x + y * y + z * z);
+        t += erfc_poly(S.alpha * r) / r;
+      }
+      v -= S.atom_charge[a] * t;
+    }
+    for (int idx = lane; idx < N * N; idx += 32) {
+      const int i = idx / N, j = idx - i * N;
+      if (i >= j) continue;
+      double dx = Rp[3 * i] - Rp[3 * j], dy = Rp[3 * i + 1] - Rp[3 * j + 1], dz = Rp[3 * i + 2] - Rp[3 * j + 2];
+      min_image(S, dx, dy, dz);
+      for (int k = 0; k < 27; k++) {
+        double x = dx + S.lattice_basis[k][0], y = dy + S.lattice_basis[k][1], z = dz + S.lattice_basis[k][2];
+        double r = sqrt(x * x + y * y + z * z);
+        v += erfc_poly(S.alpha * r) / r;
+      }
+    }
+    for (int g = lane; g < S.ng; g += 32) {
+      const double* G = S.gvec + 3 * g;
+      double ss = 0, cs = 0;
+      for (int e = 0; e < N; e++) {
+        double sn, cn;
+        sincos(G[0] * Rp[3 * e] + G[1] * Rp[3 * e + 1] + G[2] * Rp[3 * e + 2], &sn, &cn);
+        ss += sn; cs += cn;
+      }
+      const double w = S.gweight[g];
+      v += 2.0 * (-(S.ion_cos[g] * cs + S.ion_sin[g] * ss) * w + (cs * cs + ss * ss) * w / 2);
+    }
+    return warp_sum(v) + S.ewald_const;
+  }
+
   // Molecular_system::calcLoc (Molecular_system.cpp:209-287), no field.
   __device__ double coulomb() const {
+    if (S.periodic) return ewald();
     const double* Rp = R();
     const int N = S.nelec, A = S.natoms;
     double v = 0;
@@ -334,6 +383,7 @@ struct Walker {
           const double* ap = S.atom_pos[a];
           item.e = e; item.a = a;
           item.dx = Rp[3 * e] - ap[0]; item.dy = Rp[3 * e + 1] - ap[1]; item.dz = Rp[3 * e + 2] - ap[2];
+          min_image(S, item.dx, item.dy, item.dz);
           item.r = sqrt(item.dx * item.dx + item.dy * item.dy + item.dz * item.dz);
           vloc += pp_radial(t, nch - 1, item.r);
           for (int l = 0; l < 4; l++) item.vl[l] = (l < nch - 1) ? pp_radial(t, l, item.r) : 0.0;
@@ -391,13 +441,18 @@ struct Walker {
         double qx = q0[0] * rotm[0] + q0[1] * rotm[3] + q0[2] * rotm[6];
         double qy = q0[0] * rotm[1] + q0[1] * rotm[4] + q0[2] * rotm[7];
         double qz = q0[0] * rotm[2] + q0[1] * rotm[5] + q0[2] * rotm[8];
-        const double* ap = S.atom_pos[I.a];
-        double nx = ap[0] + qx * I.r, ny = ap[1] + qy * I.r, nz = ap[2] + qz * I.r;
-        const Real rd = basis_dot_lane(S, nx, ny, nz, w + (I.e - e0) * S.nbasis);
+        // move relative to the nearest image of the atom, then into the cell
+        double nx = Rp[3 * I.e] + qx * I.r - I.dx, ny = Rp[3 * I.e + 1] + qy * I.r - I.dy,
+               nz = Rp[3 * I.e + 2] + qz * I.r - I.dz;
+        wrap_pos(S, nx, ny, nz);
+        const Real* wr = w + (I.e - e0) * S.nbasis;
+        const Real rd = S.periodic ? basis_dot_lane_periodic(S, nx, ny, nz, wr) : basis_dot_lane(S, nx, ny, nz, wr);
         const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);
         double ratio = double(rd * exp(u - Real(Ue()[I.e]))) * S.pp_w[ty][q];
         // cos of the angle between the original and the quadrature direction
+        const double* ap = S.atom_pos[I.a];
         double ndx = nx - ap[0], ndy = ny - ap[1], ndz = nz - ap[2];
+        min_image(S, ndx, ndy, ndz);
         double nr = sqrt(ndx * ndx + ndy * ndy + ndz * ndz);
         double c = (ndx * I.dx + ndy * I.dy + ndz * I.dz) / (nr * I.r);
         double P[4] = {1.0, c, 0.5 * (3 * c * c - 1), 0.5 * (5 * c * c * c - 3 * c)};
@@ -457,6 +512,9 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
     unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
     if (mode != KM_STEPS || P.refresh) {
       for (int i = lane; i < 3 * N; i += 32) Rp[i] = P.R[(size_t)wid * 3 * N + i];
+      __syncwarp();
+      if (S.periodic)
+        for (int e = lane; e < N; e += 32) wrap_pos(S, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2]);
       double keep_e = 0, keep_w = 1;
       if (mode == KM_STEPS) { keep_e = ((WScal*)(gstate + L.scal))->eold; keep_w = ((WScal*)(gstate + L.scal))->weight; }
       __syncwarp();
@@ -496,8 +554,10 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
     } else if constexpr (mode == KM_RATIO) {
       const int e = io.move_e[wid];
       const double* rn = io.move_r + 3 * (size_t)wid;
+      double mx = rn[0], my = rn[1], mz = rn[2];
+      wrap_pos(S, mx, my, mz);
       double ratioD, dU, g[3], l;
-      W.propose(e, rn[0], rn[1], rn[2], ratioD, dU, g, l);
+      W.propose(e, mx, my, mz, ratioD, dU, g, l);
       if (lane == 0) {
         io.logpsi[wid] = log(fabs(ratioD)) + dU;
         io.sign[wid] = ratioD < 0 ? -1.0 : 1.0;
@@ -528,8 +588,10 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
           double nx = ox + ga[0] * sqt + dv[0];
           double ny = oy + ga[1] * sqt + dv[1];
           double nz = oz + ga[2] * sqt + dv[2];
+          double wx = nx, wy = ny, wz = nz;  // the stored position is inside the cell
+          wrap_pos(S, wx, wy, wz);
           double ratioD, dU, g1[3], l1;
-          W.propose(e, nx, ny, nz, ratioD, dU, g1, l1);
+          W.propose(e, wx, wy, wz, ratioD, dU, g1, l1);
           // get_acceptance (Split_sample.cpp:302-373): psi ratio squared
           // times the ratio of drift-diffusion Green's functions
           double ratio = ratioD * exp(dU);
@@ -547,7 +609,7 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
           }
           natt += 1;
           if (acc + rb.u[0] > 1.0) {
-            W.accept(e, nx, ny, nz, ratioD, dU);
+            W.accept(e, wx, wy, wz, ratioD, dU);
             nacc += 1;
           }
         }

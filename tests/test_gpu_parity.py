@@ -15,7 +15,7 @@ from mainline_b200 import engine, systems
 
 pytestmark = pytest.mark.gpu
 
-NAMES = ["n2_allelectron", "n2_pseudo"]
+NAMES = ["n2_allelectron", "n2_pseudo", "diamond8"]
 FP64_TOL = 1e-10
 
 
@@ -95,8 +95,9 @@ def test_mixed_precision_error_per_configuration(golden):
     # configurations with electrons inside the tight (exponent up to 1e4)
     # shells, where |E_L| reaches 1e3-1e5 Ha.  Bounds: typical configuration
     # within 5e-5 Ha, relative error at FP32 level.
+    # periodic cells sum ~130 image centers per atom in FP32: 2e-6 relative
     assert np.median(err) < 5e-5
-    assert np.median(rel) < 1e-6
+    assert np.median(rel) < (2e-6 if name == "diamond8" else 1e-6)
     assert np.median(dlp) < 1e-5
 
 
