@@ -150,6 +150,13 @@ int qwg_vmc_block(qwg_ctx* ctx, int nstep, double timestep, uint64_t seed, int d
  * E_T), then run blocks on the device-resident population. */
 int qwg_dmc_init(qwg_ctx* ctx, const qwg_dmc_params* p);
 int qwg_dmc_block(qwg_ctx* ctx, qwg_block_stats* stats);
+/* The same block split in two: _async enqueues it on the context's stream
+ * (one CUDA graph launch: every feedback interval, branching and the E_ref/E_T
+ * update run on the device) and returns at once; _wait blocks until it is
+ * done and returns its statistics.  Blocks of several contexts on different
+ * streams overlap on the GPU (Dmc_method::runWithVariables, one block). */
+int qwg_dmc_block_async(qwg_ctx* ctx);
+int qwg_dmc_block_wait(qwg_ctx* ctx, qwg_block_stats* stats);
 
 /* VMC block that allocates no device memory.
  *

@@ -176,19 +176,36 @@ struct BlockAcc {   // per-launch reduction target (double atomics)
   double nonfinite, npts;
 };
 
+// Device-resident DMC scalars (dyn[]): the whole block runs without a host
+// round trip, so it can be replayed as one CUDA graph.
+enum DynSlot {
+  DYN_ETRIAL = 0,   // E_T
+  DYN_TEFF = 1,     // effective time step of the weights
+  DYN_SUMW = 2,     // sum of the walker weights after the last branching
+  DYN_PAIRS = 3,    // split/kill pairs so far
+  DYN_EREF = 4,     // E_ref (average of the block energies)
+  DYN_STEP = 5,     // global step counter (RNG counter)
+  DYN_BRANCH = 6,   // branching counter (RNG counter)
+  DYN_NBLOCK = 7,   // blocks completed
+  DYN_COUNT = 16
+};
+
 // Launch parameters shared by the step kernels.
 struct StepParams {
   int nwalk;
   int nsteps;
-  int refresh;          // 1: full recompute at start (else load state)
+  int refresh;          // 1: full recompute at start, 0: load state, 2: recompute when the
+                        //    chunk reaches a multiple of refresh_every steps (device counter)
+  int refresh_every;
   int dmc;              // 1: DMC weights + node restriction
+  int dyn_step;         // 1: take the step counter from etrial[DYN_STEP]
   int deterministic_pp;
   double tau;           // move time step
   double teff;          // DMC effective time step (weights)
-  const double* etrial; // device scalar
+  const double* etrial; // device scalars dyn[DYN_COUNT]
   double branch_start, branch_stop, max_weight;
   uint64_t seed;
-  uint64_t step0;       // global step counter of the first step
+  uint64_t step0;       // global step counter of the first step (dyn_step == 0)
   double* R;            // [W][N][3]
   unsigned char* state; // [W][state_bytes]
   BlockAcc* acc;

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -88,6 +89,12 @@ struct qwg_ctx {
   uint64_t branch_counter = 0;
   qwg_dmc_params dmc{};
   bool dmc_ready = false;
+  DevBuf d_hist, d_stats;
+  double* h_stats = nullptr;          // pinned block statistics
+  cudaGraph_t graph = nullptr;        // one DMC block
+  cudaGraphExec_t gexec = nullptr;
+  long long launches_per_block = 0;
+  bool block_pending = false;
   double eref = 0, branch_start = 0, branch_stop = 0;
   std::vector<double> block_energies, block_weights;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -95,13 +102,7 @@ struct qwg_ctx {
 
 namespace {
 
-// Host-side copy of the parameter-bank tables, filled once from HostSystem.
-struct ParamTables {
-  std::vector<int> atom_type;
-  std::vector<int4> center_seg;
-  std::vector<double> center_cut;
-  std::vector<int> shell_pack;
-};
+constexpr int kHistCap = 1 << 16;  // block energies kept on the device for E_ref
 
 static DRadial to_dradial(const Radial& r) {
   DRadial d{};
@@ -344,10 +345,25 @@ static void make_layout(qwg_ctx* c) {
   if (c->smem_bytes > 227 * 1024) throw InputError("system too large for the shared-memory walker kernel");
 }
 
+// Raise a kernel's dynamic shared-memory limit once to the largest size any
+// context asked for (never during a stream capture: callers make a plain
+// launch of every kernel before capturing it).
+template <class K>
+static void ensure_smem_attr(K kern, size_t bytes) {
+  static std::mutex mu;
+  static std::map<const void*, size_t> done;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& have = done[(const void*)kern];
+  if (bytes > have) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    have = bytes;
+  }
+}
+
 template <typename Real, int MM, int MODE>
 static void launch_mode(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int nwalk) {
   auto kern = S.has_tb ? k_walkers<Real, MM, MODE, true> : k_walkers<Real, MM, MODE, false>;
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_bytes));
+  ensure_smem_attr(kern, c->smem_bytes);
   int grid = (nwalk + c->wpc - 1) / c->wpc;
   kern<<<grid, 32 * c->wpc, c->smem_bytes, c->stream>>>(S, c->L, P, io);
   CK(cudaGetLastError());
@@ -440,17 +456,16 @@ static void run_chunk(qwg_ctx* c, int nsteps, double tau, uint64_t seed, int det
   c->step_counter += nsteps;
 }
 
-static void run_branch(qwg_ctx* c, const BlockAcc* acc) {
+static void run_branch(qwg_ctx* c, const BlockAcc* acc, int nsteps) {
   BranchParams B{};
   B.nwalk = c->nwalk;
   int p2 = 1;
   while (p2 < c->nwalk) p2 <<= 1;
   B.npow2 = p2;
-  B.eref = c->eref;
+  B.nsteps = nsteps;
   B.feedback = c->dmc.feedback;
   B.timestep = c->dmc.timestep;
   B.seed = c->dmc.seed ^ 0x5bd1e995ull;
-  B.counter = c->branch_counter++;
   B.state = c->d_state.as<unsigned char>();
   B.state_bytes = c->L.state_bytes;
   B.scal_off = c->L.scal;
@@ -459,7 +474,8 @@ static void run_branch(qwg_ctx* c, const BlockAcc* acc) {
   B.src_of = c->d_src.as<int>();
   B.new_w = c->d_neww.as<double>();
   size_t sm = (size_t)p2 * (8 + 4) + (size_t)c->nwalk * 4 + 16 + (size_t)c->nwalk * 8;
-  CK(cudaFuncSetAttribute(k_branch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  if (sm > 227 * 1024) throw InputError("population too large for the one-CTA branching kernel (max 8192 walkers)");
+  ensure_smem_attr(k_branch, sm);
   k_branch<<<1, 1024, sm, c->stream>>>(B);
   CK(cudaGetLastError());
   const int n3 = 3 * c->H.nelec;
@@ -469,8 +485,60 @@ static void run_branch(qwg_ctx* c, const BlockAcc* acc) {
                                             c->d_state2.as<unsigned char>());
   CK(cudaGetLastError());
   c->launches += 2;
-  std::swap(c->d_R.p, c->d_R2.p);
-  std::swap(c->d_state.p, c->d_state2.p);
+  // back into the primary buffers (keeps the buffers fixed for graph replay)
+  CK(cudaMemcpyAsync(c->d_R.p, c->d_R2.p, (size_t)c->nwalk * n3 * 8, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_state.p, c->d_state2.p, (size_t)c->nwalk * c->L.state_bytes, cudaMemcpyDeviceToDevice,
+                     c->stream));
+}
+
+// One DMC block on the stream, entirely device-driven: per feedback interval
+// the step kernel (step counter and refresh from dyn[]), then branching and
+// the population gather; at the end the block statistics and E_ref/E_T
+// update, and the statistics copied to pinned host memory.
+static void enqueue_dmc_block(qwg_ctx* c) {
+  const int nstep = c->dmc.nstep, fi = c->dmc.feedback_interval;
+  const int nchunk = (nstep + fi - 1) / fi;
+  BlockAcc* acc = c->d_acc.as<BlockAcc>();
+  CK(cudaMemsetAsync(acc, 0, sizeof(BlockAcc) * nchunk, c->stream));
+  for (int ch = 0, step = 0; ch < nchunk; ch++) {
+    const int np = std::min(fi, nstep - step);
+    StepParams P = base_params(c);
+    P.nsteps = np;
+    P.tau = c->dmc.timestep;
+    P.dmc = 1;
+    P.dyn_step = 1;
+    P.refresh = 2;
+    P.refresh_every = std::max(1, c->dmc.refresh_interval);
+    P.deterministic_pp = c->dmc.deterministic_pp;
+    P.seed = c->dmc.seed;
+    P.acc = acc + ch;
+    P.branch_start = c->branch_start;
+    P.branch_stop = c->branch_stop;
+    P.max_weight = c->dmc.max_poss_weight;
+    EvalIO io{};
+    launch_walkers(c, P, io, KM_STEPS, c->nwalk);
+    run_branch(c, acc + ch, np);
+    step += np;
+  }
+  k_block_end<<<1, 32, 0, c->stream>>>(acc, nchunk, c->d_dyn.as<double>(), c->d_hist.as<double>(), kHistCap,
+                                       c->dmc.feedback, c->nwalk, c->d_stats.as<double>());
+  CK(cudaGetLastError());
+  c->launches++;
+  CK(cudaMemcpyAsync(c->h_stats, c->d_stats.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+}
+
+static void stats_from_sums(const double* t, qwg_block_stats* s) {
+  memset(s, 0, sizeof(*s));
+  double W = t[0] > 0 ? t[0] : 1.0;
+  s->energy = t[1] / W;
+  s->kinetic = t[2] / W;
+  s->potential = t[3] / W;
+  s->nonlocal = t[4] / W;
+  s->energy_var = t[5] / W - s->energy * s->energy;
+  s->weight = t[9] > 0 ? t[0] / t[9] : 0.0;
+  s->acceptance = t[7] > 0 ? t[6] / t[7] : 0.0;
+  s->nonfinite = (int)t[8];
+  s->etrial = t[10];
 }
 
 static void acc_to_stats(const std::vector<BlockAcc>& v, qwg_block_stats* s) {
@@ -565,11 +633,14 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
     c->d_state.alloc((size_t)max_walkers * c->L.state_bytes);
     c->d_state2.alloc((size_t)max_walkers * c->L.state_bytes);
     c->d_acc.alloc(sizeof(BlockAcc) * 1024);
-    c->d_dyn.alloc(8 * 8);
-    CK(cudaMemsetAsync(c->d_dyn.p, 0, 64, c->stream));
+    c->d_dyn.alloc(DYN_COUNT * 8);
+    CK(cudaMemsetAsync(c->d_dyn.p, 0, DYN_COUNT * 8, c->stream));
     c->d_src.alloc((size_t)max_walkers * 4);
     c->d_neww.alloc((size_t)max_walkers * 8);
     c->d_energy.alloc((size_t)max_walkers * 8);
+    c->d_hist.alloc((size_t)kHistCap * 8);
+    c->d_stats.alloc(16 * 8);
+    CK(cudaMallocHost((void**)&c->h_stats, 16 * sizeof(double)));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
     CK(cudaStreamSynchronize(c->stream));
@@ -586,6 +657,9 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
 int qwg_destroy(qwg_ctx* ctx) {
   if (!ctx) return QWG_OK;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  if (ctx->h_stats) cudaFreeHost(ctx->h_stats);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   cudaStream_t st = ctx->own_stream ? ctx->stream : nullptr;
@@ -744,13 +818,12 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
     if (c->dmc.refresh_interval <= 0)
       c->dmc.refresh_interval = c->precision == QWG_FP64 ? c->dmc.feedback_interval : 32;
     const int W = c->nwalk;
-    // energies of the starting walkers: one gather step without moves is a
-    // zero-step launch, so run the local energy through KM_STEPS with
-    // nsteps = 0 ... simpler: evaluate with the stochastic PP like gatherData.
-    BlockAcc* acc = c->d_acc.as<BlockAcc>();
-    CK(cudaMemsetAsync(acc, 0, sizeof(BlockAcc), c->stream));
-    CK(cudaMemsetAsync(c->d_dyn.p, 0, 64, c->stream));
-    // evaluate E_L of each walker (deterministic PP for a clean start)
+    const int nchunk = (c->dmc.nstep + c->dmc.feedback_interval - 1) / c->dmc.feedback_interval;
+    if (nchunk > 1024) throw std::runtime_error("too many feedback intervals per block");
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+    // local energies of the starting walkers (gatherData for every walker in
+    // Dmc_method::restorecheckpoint; deterministic PP for a clean start)
     size_t n_g = (size_t)W * c->H.nelec * 3, n_l = (size_t)W * c->H.nelec;
     ensure_io(c, 8 * (5 * (size_t)W + n_g + n_l));
     double* base = c->d_io.as<double>();
@@ -782,74 +855,102 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
     c->branch_start = c->dmc.branch_start_cutoff * sigma;
     c->branch_stop = c->branch_start * 1.5;
     CK(cudaMemcpyAsync(c->d_energy.p, el.data(), 8 * W, cudaMemcpyHostToDevice, c->stream));
-    // state: weights 1, E_old = E_L; E_T = E_ref (start_feedback * log(1) = 0)
-    c->state_valid = false;
+    // resident state: one zero-step launch builds it; weights 1, E_old = E_L
     StepParams P2 = base_params(c);
     P2.nsteps = 0;
     P2.refresh = 1;
-    P2.acc = acc;
+    P2.acc = c->d_acc.as<BlockAcc>();
     EvalIO io2{};
-    launch_walkers(c, P2, io2, KM_STEPS, W);  // builds and stores the resident state
+    launch_walkers(c, P2, io2, KM_STEPS, W);
     k_init_weights<<<(W + 255) / 256, 256, 0, c->stream>>>(c->d_state.as<unsigned char>(), W, c->L.state_bytes,
                                                            c->L.scal, c->d_energy.as<double>());
     CK(cudaGetLastError());
     c->launches++;
-    double dyn0[4] = {c->eref, c->dmc.timestep, double(W), 0.0};
+    // device scalars: E_T = E_ref (start_feedback * log 1), counters
+    double dyn0[DYN_COUNT] = {0};
+    dyn0[DYN_ETRIAL] = c->eref;
+    dyn0[DYN_TEFF] = c->dmc.timestep;
+    dyn0[DYN_SUMW] = double(W);
+    dyn0[DYN_EREF] = c->eref;
+    dyn0[DYN_STEP] = double(c->step_counter);
+    dyn0[DYN_BRANCH] = double(c->branch_counter);
     CK(cudaMemcpyAsync(c->d_dyn.p, dyn0, sizeof(dyn0), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->state_valid = true;
+    // capture one block as a CUDA graph (every kernel in it has been
+    // launched before, so no attribute changes happen during the capture)
+    {
+      BlockAcc* acc = c->d_acc.as<BlockAcc>();
+      StepParams Pw = base_params(c);
+      Pw.nsteps = 0; Pw.refresh = 0; Pw.acc = acc;
+      EvalIO iw{};
+      launch_walkers(c, Pw, iw, KM_STEPS, W);  // same kernel variant as the block's chunks
+      CK(cudaStreamSynchronize(c->stream));
+    }
+    {
+      int p2 = 1;
+      while (p2 < W) p2 <<= 1;
+      size_t sm = (size_t)p2 * (8 + 4) + (size_t)W * 4 + 16 + (size_t)W * 8;
+      if (sm > 227 * 1024) throw InputError("population too large for the one-CTA branching kernel (max 8192 walkers)");
+      ensure_smem_attr(k_branch, sm);
+    }
+    const long long l0 = c->launches;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue_dmc_block(c);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(c->stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(c->stream, &c->graph));
+    CK(cudaGraphInstantiate(&c->gexec, c->graph, 0));
+    c->launches_per_block = c->launches - l0;
+    c->launches = l0;
     c->dmc_ready = true;
-    c->block_energies.clear();
-    c->block_weights.clear();
+    c->block_pending = false;
+    return QWG_OK;
+  });
+}
+
+int qwg_dmc_block_async(qwg_ctx* c) {
+  if (!c) return QWG_ERR_ARG;
+  if (!c->dmc_ready) return fail(c, QWG_ERR_STATE, "qwg_dmc_block_async: call qwg_dmc_init first");
+  if (c->block_pending) return fail(c, QWG_ERR_STATE, "qwg_dmc_block_async: previous block not collected");
+  return guarded(c, [&]() -> int {
+    CK(cudaEventRecord(c->ev0, c->stream));
+    CK(cudaGraphLaunch(c->gexec, c->stream));
+    CK(cudaEventRecord(c->ev1, c->stream));
+    c->launches += c->launches_per_block;
+    c->block_pending = true;
+    return QWG_OK;
+  });
+}
+
+int qwg_dmc_block_wait(qwg_ctx* c, qwg_block_stats* stats) {
+  if (!c) return QWG_ERR_ARG;
+  if (!c->block_pending) return fail(c, QWG_ERR_STATE, "qwg_dmc_block_wait: no block in flight");
+  return guarded(c, [&]() -> int {
+    CK(cudaEventSynchronize(c->ev1));
+    c->block_pending = false;
+    c->step_counter += c->dmc.nstep;
+    if (stats) {
+      stats_from_sums(c->h_stats, stats);
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+      stats->block_ms = ms;
+      stats->nsteps = c->dmc.nstep;
+      stats->nwalkers = c->nwalk;
+    }
     return QWG_OK;
   });
 }
 
 int qwg_dmc_block(qwg_ctx* c, qwg_block_stats* stats) {
-  if (!c) return QWG_ERR_ARG;
-  if (!c->dmc_ready) return fail(c, QWG_ERR_STATE, "qwg_dmc_block: call qwg_dmc_init first");
-  return guarded(c, [&]() -> int {
-    const int nstep = c->dmc.nstep, fi = c->dmc.feedback_interval;
-    const int nchunk = (nstep + fi - 1) / fi;
-    if (nchunk > 1024) throw std::runtime_error("too many feedback intervals per block");
-    BlockAcc* acc = c->d_acc.as<BlockAcc>();
-    CK(cudaMemsetAsync(acc, 0, sizeof(BlockAcc) * nchunk, c->stream));
-    CK(cudaEventRecord(c->ev0, c->stream));
-    for (int ch = 0, step = 0; ch < nchunk; ch++) {
-      int np = std::min(fi, nstep - step);
-      run_chunk(c, np, c->dmc.timestep, c->dmc.seed, c->dmc.deterministic_pp, true, acc + ch, nullptr);
-      run_branch(c, acc + ch);
-      step += np;
-    }
-    CK(cudaEventRecord(c->ev1, c->stream));
-    std::vector<BlockAcc> h(nchunk);
-    CK(cudaMemcpyAsync(h.data(), acc, sizeof(BlockAcc) * nchunk, cudaMemcpyDeviceToHost, c->stream));
-    double dyn[4];
-    CK(cudaMemcpyAsync(dyn, c->d_dyn.p, sizeof(dyn), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    qwg_block_stats s{};
-    acc_to_stats(h, &s);
-    // E_ref = average of the block energies so far (the first fifth of the
-    // blocks is treated as equilibration once there are more than five)
-    c->block_energies.push_back(s.energy);
-    size_t nb = c->block_energies.size(), b0 = nb > 5 ? nb / 5 : 0;
-    double se = 0;
-    for (size_t b = b0; b < nb; b++) se += c->block_energies[b];
-    c->eref = se / double(nb - b0);
-    k_set_etrial<<<1, 32, 0, c->stream>>>(c->d_dyn.as<double>(), c->eref, c->dmc.feedback, c->nwalk);
-    CK(cudaGetLastError());
-    c->launches++;
-    if (stats) {
-      *stats = s;
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-      stats->block_ms = ms;
-      stats->nsteps = nstep;
-      stats->nwalkers = c->nwalk;
-      stats->etrial = c->eref - c->dmc.feedback * std::log(dyn[2] / double(c->nwalk));
-    }
-    return QWG_OK;
-  });
+  int rc = qwg_dmc_block_async(c);
+  if (rc != QWG_OK) return rc;
+  return qwg_dmc_block_wait(c, stats);
 }
 
 // ---------------------------------------------------------------------------

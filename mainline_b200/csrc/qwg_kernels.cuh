@@ -510,7 +510,13 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
     const int N = S.nelec;
     double* Rp = W.R();
     unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
-    if (mode != KM_STEPS || P.refresh) {
+    const uint64_t step0 = P.dyn_step ? (uint64_t)P.etrial[DYN_STEP] : P.step0;
+    int refresh = P.refresh;
+    if (refresh == 2) {
+      const uint64_t R = (uint64_t)P.refresh_every, m = step0 % R;
+      refresh = (m == 0 || m + (uint64_t)P.nsteps > R) ? 1 : 0;
+    }
+    if (mode != KM_STEPS || refresh) {
       for (int i = lane; i < 3 * N; i += 32) Rp[i] = P.R[(size_t)wid * 3 * N + i];
       __syncwarp();
       if (S.periodic)
@@ -572,7 +578,7 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
       const double etr = P.dmc ? *P.etrial : 0.0;
       const double teff = P.dmc ? P.etrial[1] : 0.0;
       for (int st = 0; st < P.nsteps; st++) {
-        const uint64_t step = P.step0 + st;
+        const uint64_t step = step0 + st;
         for (int e = 0; e < N; e++) {
           // Split_sampler::split_driver depth 1 (Split_sample.cpp:380-478)
           double g0[3], l0;
@@ -673,8 +679,9 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
 // dyn[0] = E_T, dyn[1] = teff, dyn[2] = sum of weights, dyn[3] = branched pairs
 struct BranchParams {
   int nwalk, npow2;
-  double eref, feedback, timestep;
-  uint64_t seed, counter;
+  int nsteps;             // steps of the chunk just finished (advances the step counter)
+  double feedback, timestep;
+  uint64_t seed;
   const unsigned char* state;
   int state_bytes, scal_off;
   const BlockAcc* acc;    // running acceptance of this chunk
@@ -711,9 +718,9 @@ __global__ void __launch_bounds__(1024) k_branch(BranchParams B) {
     v = warp_sum(v);
     if (t == 0) {
       double acc_ratio = B.acc->attempted > 0 ? B.acc->accepted / B.acc->attempted : 1.0;
-      B.dyn[1] = B.timestep * acc_ratio;
-      B.dyn[0] = B.eref - B.feedback * log(v / double(B.nwalk));
-      B.dyn[2] = v;
+      B.dyn[DYN_TEFF] = B.timestep * acc_ratio;
+      B.dyn[DYN_ETRIAL] = B.dyn[DYN_EREF] - B.feedback * log(v / double(B.nwalk));
+      B.dyn[DYN_SUMW] = v;
     }
   }
   // bitonic sort ascending by weight (ties by index)
@@ -743,7 +750,7 @@ __global__ void __launch_bounds__(1024) k_branch(BranchParams B) {
       int wb = idx[big], ws = idx[k];
       double w1 = key[big], w2 = key[k];
       double weight1 = w1 / (w1 + w2);
-      Rand4 r = rand4(B.seed, (uint32_t)k, B.counter, 0u, 5u);
+      Rand4 r = rand4(B.seed, (uint32_t)k, (uint64_t)B.dyn[DYN_BRANCH], 0u, 5u);
       double merged = (w1 + w2) / 2.0;
       if (weight1 + r.u[0] >= 1.0) { cnt[wb] = 2; cnt[ws] = 0; nw[wb] = merged; }
       else { cnt[wb] = 0; cnt[ws] = 2; nw[ws] = merged; }
@@ -770,7 +777,12 @@ __global__ void __launch_bounds__(1024) k_branch(BranchParams B) {
       off++;
     }
   }
-  if (npair) atomicAdd(&B.dyn[3], double(npair));
+  if (npair) atomicAdd(&B.dyn[DYN_PAIRS], double(npair));
+  __syncthreads();
+  if (t == 0) {  // every thread has read the counters above
+    B.dyn[DYN_STEP] += double(B.nsteps);
+    B.dyn[DYN_BRANCH] += 1.0;
+  }
 }
 
 // Gather walkers into their new slots (positions + resident state).
@@ -787,8 +799,34 @@ __global__ void k_gather(int nwalk, int n3, int state_bytes, int scal_off, const
   if (threadIdx.x == 0) ((WScal*)(state2 + (size_t)w * state_bytes + scal_off))->weight = new_w[w];
 }
 
-__global__ void k_set_etrial(double* dyn, double eref, double feedback, int nwalk) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) dyn[0] = eref - feedback * log(dyn[2] / double(nwalk));
+// End of a DMC block: block averages from the per-chunk accumulators, the
+// block-energy history, E_ref = mean block energy (the first fifth of the
+// blocks dropped as equilibration once there are more than five), and E_T
+// (Dmc_method.cpp:475-530).  out[0..11]: sum w, sum wE, sum wT, sum wV,
+// sum wV_NL, sum wE^2, accepted, attempted, non-finite, points, E_T, E_ref.
+__global__ void k_block_end(const BlockAcc* acc, int nchunk, double* dyn, double* hist, int hist_cap,
+                            double feedback, int nwalk, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double t[10] = {0};
+  for (int c = 0; c < nchunk; c++) {
+    const double* a = (const double*)(acc + c);
+    for (int k = 0; k < 10; k++) t[k] += a[k];
+  }
+  const double eb = t[0] > 0 ? t[1] / t[0] : 0.0;
+  const int nb = (int)dyn[DYN_NBLOCK];
+  hist[nb % hist_cap] = eb;
+  const int n = nb + 1;
+  dyn[DYN_NBLOCK] = double(n);
+  const int b0 = n > 5 ? n / 5 : 0;
+  const int lo = max(b0, n - hist_cap);
+  double se = 0;
+  for (int b = lo; b < n; b++) se += hist[b % hist_cap];
+  const double eref = se / double(n - lo);
+  dyn[DYN_EREF] = eref;
+  dyn[DYN_ETRIAL] = eref - feedback * log(dyn[DYN_SUMW] / double(nwalk));
+  for (int k = 0; k < 10; k++) out[k] = t[k];
+  out[10] = dyn[DYN_ETRIAL];
+  out[11] = eref;
 }
 
 __global__ void k_init_weights(unsigned char* state, int nwalk, int state_bytes, int scal_off, const double* eloc) {

@@ -26,8 +26,8 @@ MIXED = 1
 EXPORTS = [
     "qwg_version", "qwg_last_error", "qwg_create", "qwg_destroy", "qwg_get_info", "qwg_inspect_deck",
     "qwg_inspect_spline", "qwg_set_walkers", "qwg_get_walkers", "qwg_set_walkers_device", "qwg_eval",
-    "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_vmc_block_noalloc", "qwg_launch_count",
-    "qwg_reset_launch_count",
+    "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
+    "qwg_vmc_block_noalloc", "qwg_launch_count", "qwg_reset_launch_count",
 ]
 
 
@@ -93,6 +93,8 @@ def load_library(path: str = LIB_PATH):
         "qwg_vmc_block": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_int, P(BlockStats)]),
         "qwg_dmc_init": (C.c_int, [C.c_void_p, P(DmcParams)]),
         "qwg_dmc_block": (C.c_int, [C.c_void_p, P(BlockStats)]),
+        "qwg_dmc_block_async": (C.c_int, [C.c_void_p]),
+        "qwg_dmc_block_wait": (C.c_int, [C.c_void_p, P(BlockStats)]),
         "qwg_vmc_block_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_uint64,
                                             C.c_int, C.c_void_p, C.c_void_p]),
         "qwg_launch_count": (C.c_longlong, [C.c_void_p]),
@@ -233,6 +235,15 @@ class Engine:
     def dmc_block(self) -> dict:
         st = BlockStats()
         self._check(self.lib.qwg_dmc_block(self.h, C.byref(st)), "qwg_dmc_block")
+        return st.as_dict()
+
+    def dmc_block_async(self):
+        """Enqueue one DMC block (one CUDA graph launch) without waiting."""
+        self._check(self.lib.qwg_dmc_block_async(self.h), "qwg_dmc_block_async")
+
+    def dmc_block_wait(self) -> dict:
+        st = BlockStats()
+        self._check(self.lib.qwg_dmc_block_wait(self.h, C.byref(st)), "qwg_dmc_block_wait")
         return st.as_dict()
 
     def launch_count(self) -> int:

@@ -127,3 +127,34 @@ def test_dmc_block_runs():
         assert np.isfinite(s["energy"]) and np.isfinite(s["etrial"])
         assert 0.9 < s["acceptance"] <= 1.0
         assert 0.2 < s["weight"] < 5.0
+
+
+def test_dmc_async_blocks_match_sync_and_overlap():
+    """Blocks enqueued asynchronously (one CUDA graph launch each) on two
+    contexts at once give the same statistics as the same contexts run
+    alone: per-context counter-based RNG, no cross-context state."""
+    deck = os.path.join(GOLDEN, "n2_pseudo.qw")
+    d = systems.Deck(deck, "", 7, 7, 2, 80, "n2_pseudo", 0)
+    R = systems.random_configs(d, 256, seed=8)
+
+    def make(seed):
+        E = engine.Engine(deck, engine.FP64, max_walkers=256)
+        E.set_walkers(R)
+        E.vmc_block(10, 0.3, seed=seed)
+        E.dmc_init(timestep=0.01, nstep=10, seed=seed + 1)
+        return E
+
+    alone = []
+    for seed in (21, 33):
+        E = make(seed)
+        alone.append([E.dmc_block()["energy"] for _ in range(3)])
+        E.close()
+    A, B = make(21), make(33)
+    mix = [[], []]
+    for _ in range(3):
+        A.dmc_block_async()
+        B.dmc_block_async()
+        mix[0].append(A.dmc_block_wait()["energy"])
+        mix[1].append(B.dmc_block_wait()["energy"])
+    for k in range(2):
+        assert np.allclose(mix[k], alone[k], rtol=1e-12, atol=0), (mix[k], alone[k])
