@@ -188,6 +188,22 @@ int qwg_dmc_block_wait(qwg_ctx* ctx, qwg_block_stats* stats);
 int qwg_vmc_block_noalloc(qwg_ctx* ctx, double* d_R, int nw, int nstep, double timestep, uint64_t seed,
                           int deterministic_pp, double* d_energy, double* d_sums);
 
+/* Batched uneven systems: one CUDA graph holding one DMC block of every
+ * context (each on its own stream, forked and joined inside the graph), so a
+ * single graph launch advances all systems concurrently.  Every context must
+ * have had qwg_dmc_init.  qwg_batch_block launches the graph, waits, and
+ * fills stats[i] for context i.  (Dmc_method::runWithVariables per system;
+ * QWalk runs independent systems as separate MPI groups, ooqmc.cpp:69-84.) */
+typedef struct qwg_batch qwg_batch;
+int qwg_batch_create(qwg_ctx* const* ctxs, int n, qwg_batch** out);
+int qwg_batch_block(qwg_batch* b, qwg_block_stats* stats);
+int qwg_batch_destroy(qwg_batch* b);
+
+/* Launch-shape autotuner: times the full evaluation of the resident walkers
+ * for each walkers-per-CTA choice that fits shared memory and keeps the
+ * fastest (call before qwg_dmc_init).  Returns the chosen value. */
+int qwg_autotune(qwg_ctx* ctx, int* walkers_per_cta);
+
 /* Number of kernel launches the context issued since the last reset. */
 long long qwg_launch_count(const qwg_ctx* ctx);
 void qwg_reset_launch_count(qwg_ctx* ctx);

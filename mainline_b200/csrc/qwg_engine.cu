@@ -1033,6 +1033,149 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
   });
 }
 
+// ---------------------------------------------------------------------------
+// batched systems: one graph, one block of every context
+
+}  // extern "C"
+
+struct qwg_batch {
+  std::vector<qwg_ctx*> ctxs;
+  cudaStream_t origin = nullptr;
+  std::vector<cudaEvent_t> events;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+};
+
+extern "C" {
+
+int qwg_batch_create(qwg_ctx* const* ctxs, int n, qwg_batch** out) {
+  if (!ctxs || n <= 0 || !out) return QWG_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<qwg_batch> b(new qwg_batch());
+  for (int i = 0; i < n; i++) {
+    if (!ctxs[i] || !ctxs[i]->dmc_ready) {
+      g_create_error = "qwg_batch_create: context " + std::to_string(i) + " has no qwg_dmc_init";
+      return QWG_ERR_STATE;
+    }
+    b->ctxs.push_back(ctxs[i]);
+  }
+  try {
+    CK(cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&b->ev0));
+    CK(cudaEventCreate(&b->ev1));
+    b->events.resize(n + 1);
+    for (auto& e : b->events) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto* c : b->ctxs) CK(cudaStreamSynchronize(c->stream));
+    CK(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+    CK(cudaEventRecord(b->events[n], b->origin));
+    for (int i = 0; i < n; i++) {
+      qwg_ctx* c = b->ctxs[i];
+      CK(cudaStreamWaitEvent(c->stream, b->events[n], 0));  // fork
+      enqueue_dmc_block(c);
+      CK(cudaEventRecord(b->events[i], c->stream));
+      CK(cudaStreamWaitEvent(b->origin, b->events[i], 0));   // join
+    }
+    CK(cudaStreamEndCapture(b->origin, &b->graph));
+    CK(cudaGraphInstantiate(&b->gexec, b->graph, 0));
+  } catch (const std::exception& e) {
+    g_create_error = std::string("qwg_batch_create: ") + e.what();
+    cudaGraph_t g = nullptr;
+    if (b->origin) {
+      cudaStreamCaptureStatus st;
+      if (cudaStreamIsCapturing(b->origin, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone)
+        cudaStreamEndCapture(b->origin, &g);
+    }
+    if (g) cudaGraphDestroy(g);
+    qwg_batch_destroy(b.release());
+    return QWG_ERR_CUDA;
+  }
+  for (auto* c : b->ctxs) c->launches -= c->launches_per_block;  // counted at capture
+  *out = b.release();
+  return QWG_OK;
+}
+
+int qwg_batch_block(qwg_batch* b, qwg_block_stats* stats) {
+  if (!b) return QWG_ERR_ARG;
+  for (auto* c : b->ctxs)
+    if (c->block_pending) { b->err = "qwg_batch_block: a context has a block in flight"; return QWG_ERR_STATE; }
+  try {
+    CK(cudaEventRecord(b->ev0, b->origin));
+    CK(cudaGraphLaunch(b->gexec, b->origin));
+    CK(cudaEventRecord(b->ev1, b->origin));
+    CK(cudaEventSynchronize(b->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    for (size_t i = 0; i < b->ctxs.size(); i++) {
+      qwg_ctx* c = b->ctxs[i];
+      c->launches += c->launches_per_block;
+      c->step_counter += c->dmc.nstep;
+      if (stats) {
+        stats_from_sums(c->h_stats, &stats[i]);
+        stats[i].block_ms = ms;
+        stats[i].nsteps = c->dmc.nstep;
+        stats[i].nwalkers = c->nwalk;
+      }
+    }
+  } catch (const std::exception& e) {
+    b->err = e.what();
+    return QWG_ERR_CUDA;
+  }
+  return QWG_OK;
+}
+
+int qwg_batch_destroy(qwg_batch* b) {
+  if (!b) return QWG_OK;
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto e : b->events)
+    if (e) cudaEventDestroy(e);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  delete b;
+  return QWG_OK;
+}
+
+int qwg_autotune(qwg_ctx* c, int* walkers_per_cta) {
+  if (!c) return QWG_ERR_ARG;
+  if (c->nwalk <= 0) return fail(c, QWG_ERR_STATE, "qwg_autotune: no walkers");
+  return guarded(c, [&]() -> int {
+    const int W = c->nwalk;
+    size_t n_g = (size_t)W * c->H.nelec * 3, n_l = (size_t)W * c->H.nelec;
+    ensure_io(c, 8 * (5 * (size_t)W + n_g + n_l));
+    double* base = c->d_io.as<double>();
+    EvalIO io{};
+    io.logpsi = base; io.sign = base + W; io.kinetic = base + 2 * W; io.potential = base + 3 * W;
+    io.nonlocal = base + 4 * W; io.grad = base + 5 * W; io.lap = io.grad + n_g;
+    const size_t per = (size_t)c->L.bytes;
+    int best = c->wpc;
+    float best_ms = 1e30f;
+    for (int cand : {1, 2, 4}) {
+      if ((size_t)cand * per > 227 * 1024) continue;
+      c->wpc = cand;
+      c->smem_bytes = (size_t)cand * per;
+      StepParams P = base_params(c);
+      launch_walkers(c, P, io, KM_EVAL, W);  // warm-up (and attribute)
+      CK(cudaEventRecord(c->ev0, c->stream));
+      for (int r = 0; r < 3; r++) launch_walkers(c, P, io, KM_EVAL, W);
+      CK(cudaEventRecord(c->ev1, c->stream));
+      CK(cudaEventSynchronize(c->ev1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+      if (ms < best_ms) { best_ms = ms; best = cand; }
+    }
+    c->wpc = best;
+    c->smem_bytes = (size_t)best * per;
+    c->state_valid = false;
+    c->dmc_ready = false;
+    if (walkers_per_cta) *walkers_per_cta = best;
+    return QWG_OK;
+  });
+}
+
 long long qwg_launch_count(const qwg_ctx* c) { return c ? c->launches : 0; }
 void qwg_reset_launch_count(qwg_ctx* c) { if (c) c->launches = 0; }
 

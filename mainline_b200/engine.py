@@ -27,7 +27,8 @@ EXPORTS = [
     "qwg_version", "qwg_last_error", "qwg_create", "qwg_destroy", "qwg_get_info", "qwg_inspect_deck",
     "qwg_inspect_spline", "qwg_set_walkers", "qwg_get_walkers", "qwg_set_walkers_device", "qwg_eval",
     "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
-    "qwg_vmc_block_noalloc", "qwg_launch_count", "qwg_reset_launch_count",
+    "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
+    "qwg_launch_count", "qwg_reset_launch_count",
 ]
 
 
@@ -97,6 +98,10 @@ def load_library(path: str = LIB_PATH):
         "qwg_dmc_block_wait": (C.c_int, [C.c_void_p, P(BlockStats)]),
         "qwg_vmc_block_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_uint64,
                                             C.c_int, C.c_void_p, C.c_void_p]),
+        "qwg_batch_create": (C.c_int, [P(C.c_void_p), C.c_int, P(C.c_void_p)]),
+        "qwg_batch_block": (C.c_int, [C.c_void_p, P(BlockStats)]),
+        "qwg_batch_destroy": (C.c_int, [C.c_void_p]),
+        "qwg_autotune": (C.c_int, [C.c_void_p, P(C.c_int)]),
         "qwg_launch_count": (C.c_longlong, [C.c_void_p]),
         "qwg_reset_launch_count": (None, [C.c_void_p]),
     }
@@ -246,8 +251,47 @@ class Engine:
         self._check(self.lib.qwg_dmc_block_wait(self.h, C.byref(st)), "qwg_dmc_block_wait")
         return st.as_dict()
 
+    def autotune(self) -> int:
+        """Pick the walkers-per-CTA launch shape by timing; before dmc_init."""
+        w = C.c_int(0)
+        self._check(self.lib.qwg_autotune(self.h, C.byref(w)), "qwg_autotune")
+        return w.value
+
     def launch_count(self) -> int:
         return int(self.lib.qwg_launch_count(self.h))
 
     def reset_launch_count(self):
         self.lib.qwg_reset_launch_count(self.h)
+
+
+class Batch:
+    """One CUDA graph that advances a DMC block of every engine at once
+    (batched uneven systems)."""
+
+    def __init__(self, engines):
+        self.lib = load_library()
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e.h for e in self.engines])
+        h = C.c_void_p()
+        rc = self.lib.qwg_batch_create(arr, len(self.engines), C.byref(h))
+        if rc != 0:
+            raise QwgError(f"qwg_batch_create failed ({rc}): {self.lib.qwg_last_error(None).decode()}")
+        self.h = h
+
+    def block(self) -> list:
+        st = (BlockStats * len(self.engines))()
+        rc = self.lib.qwg_batch_block(self.h, st)
+        if rc != 0:
+            raise QwgError(f"qwg_batch_block failed ({rc})")
+        return [s.as_dict() for s in st]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.qwg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

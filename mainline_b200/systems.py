@@ -306,13 +306,131 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
                 extra={"a": a, "atoms": pos})
 
 
+MAX_BATCH_ELECTRONS = 64  # the warp-per-walker kernels hold <= 32 electrons per spin
+
+
+def write_molecule(outdir: str, name: str, seed: int, nelec: int, max_atoms: int = 32) -> Deck:
+    """One seeded molecule of the batched-uneven workload: pseudo-atoms with
+    Z_eff 1-6 summing to ``nelec`` (neutral, 2..max_atoms atoms) at random
+    positions at least 1.5 bohr apart; 10 Gaussians per atom (4 S + 2 P,
+    exponents log-uniform in [0.1, 10]); random orthonormal MOs; Jastrow
+    e-e (CUTOFF_CUSP) + e-n (POLYPADE); semilocal pseudopotential per Z_eff
+    (as in the two-atom workload)."""
+    os.makedirs(outdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    natoms = int(np.clip(round(nelec / rng.uniform(2.5, 4.5)), 2, max_atoms))
+    natoms = min(natoms, nelec)
+    z = np.ones(natoms, dtype=int)
+    for _ in range(nelec - natoms):
+        cand = np.flatnonzero(z < 6)
+        z[rng.choice(cand)] += 1
+    radius = 1.2 * natoms ** (1.0 / 3.0) + 1.0
+    pos = []
+    while len(pos) < natoms:
+        p = rng.uniform(-radius, radius, size=3)
+        if np.linalg.norm(p) <= radius and all(np.linalg.norm(p - q) >= 1.5 for q in pos):
+            pos.append(p)
+    pos = np.array(pos)
+    types = sorted(set(int(v) for v in z))
+    shells = {t: _basis_shells(rng, {"S": 4, "P": 2}, hi=10.0) for t in types}
+    nper = {t: sum(SHELL_NFUNC[sy] for sy, _, _ in shells[t]) for t in types}
+    nb = sum(nper[int(v)] for v in z)
+    nup, ndn = (nelec + 1) // 2, nelec // 2
+    cup = _random_orthonormal(rng, nb, nup)
+    cdn = _random_orthonormal(rng, nb, ndn) if ndn else np.zeros((nb, 0))
+    orb = os.path.join(outdir, f"{name}.orb")
+    _write_orb(orb, np.concatenate([cup, cdn], axis=1), [nper[int(v)] for v in z])
+    label = {t: f"Z{t}" for t in types}
+    onebody = {t: rng.normal(0.0, 0.1, size=4) for t in types}
+    pp = "\n".join(_pseudo_text(rng, label[t], float(t)) for t in types)
+    jas = ["JASTROW2", "GROUP {",
+           "  EEBASIS { EE CUTOFF_CUSP GAMMA 24.0 CUSP 1.0 CUTOFF 7.5 }",
+           "  EEBASIS { EE CUTOFF_CUSP GAMMA 24.0 CUSP 1.0 CUTOFF 7.5 }",
+           "  TWOBODY_SPIN { FREEZE", "    LIKE_COEFFICIENTS { 0.25 0.0 }", "    UNLIKE_COEFFICIENTS { 0.0 0.5 }",
+           "  }", "}", "GROUP {"]
+    for t in types:
+        jas.append(f"  EIBASIS {{ {label[t]} POLYPADE BETA0 1.2 NFUNC 4 RCUT 7.5 }}")
+    jas.append("  ONEBODY {")
+    for t in types:
+        jas.append(f"    COEFFICIENTS {{ {label[t]} " + " ".join(_fmt(c) for c in onebody[t]) + " }")
+    jas += ["  }", "}"]
+    states_up = " ".join(str(i + 1) for i in range(nup))
+    states_dn = " ".join(str(nup + i + 1) for i in range(ndn))
+    deck = "\n".join([
+        f"# seeded synthetic molecule {name} (seed {seed})",
+        f"RANDOMSEED {{ {1 + seed % 100000} {7 + seed % 7919} }}",
+        "SYSTEM { MOLECULE",
+        f"  NSPIN {{ {nup} {ndn} }}",
+    ] + [f"  ATOM {{ {label[int(z[a])]} {int(z[a])} COOR {_fmt(pos[a, 0])} {_fmt(pos[a, 1])} {_fmt(pos[a, 2])} }}"
+         for a in range(natoms)] + [
+        "}",
+        pp,
+        "TRIALFUNC { SLATER-JASTROW",
+        "  WF1 { SLATER",
+        "    ORBITALS { BLAS_MO",
+        f"      NMO {nup + ndn}",
+        f"      ORBFILE {os.path.basename(orb)}",
+    ] + [_basis_text(label[t], shells[t]) for t in types] + [
+        "      CENTERS { USEATOMS }",
+        "    }",
+        "    DETWT { 1.0 }",
+        f"    STATES {{ {states_up} {states_dn} }}",
+        "  }",
+        "  WF2 {",
+        "\n".join(jas),
+        "  }",
+        "}",
+    ]) + "\n"
+    path = os.path.join(outdir, f"{name}.qw")
+    with open(path, "w") as fh:
+        fh.write(deck)
+    return Deck(path=path, orb_path=orb, nup=nup, ndown=ndn, natoms=natoms, nbasis=nb, kind=name, seed=seed,
+                extra={"atoms": pos})
+
+
+def write_batch(outdir: str, nsys: int = 64, seed: int = 777, emin: int = 8,
+                emax: int = MAX_BATCH_ELECTRONS) -> list:
+    """The batched-uneven workload: ``nsys`` seeded molecules with electron
+    counts log-uniform in [emin, emax] and 512-4096 walkers each (log-uniform);
+    returns [(deck, walkers)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nsys):
+        ne = int(round(np.exp(rng.uniform(np.log(emin), np.log(emax)))))
+        nw = int(round(np.exp(rng.uniform(np.log(512), np.log(4096)))))
+        d = write_molecule(outdir, f"mol{i:02d}", seed * 1000 + i, ne)
+        out.append((d, nw))
+    return out
+
+
+def read_deck(path: str) -> Deck:
+    """A Deck record for an existing molecule or cell file (sizes, atom
+    positions, lattice edge), enough to draw configurations for it."""
+    words = open(path).read().replace("{", " { ").replace("}", " } ").split()
+    nup = ndn = 0
+    atoms, a = [], None
+    for i, w in enumerate(words):
+        u = w.upper()
+        if u == "NSPIN":
+            nup, ndn = int(words[i + 2]), int(words[i + 3])
+        elif u == "COOR":
+            atoms.append([float(words[i + 1]), float(words[i + 2]), float(words[i + 3])])
+        elif u == "LATTICEVEC":
+            a = float(words[i + 2])
+    extra = {"atoms": np.array(atoms)}
+    if a is not None:
+        extra = {"a": a}
+    return Deck(path=path, orb_path="", nup=nup, ndown=ndn, natoms=len(atoms), nbasis=0,
+                kind=os.path.splitext(os.path.basename(path))[0], seed=0, extra=extra)
+
+
 def random_configs(deck: Deck, nconf: int, seed: int, spread: float = 1.2) -> np.ndarray:
     """Seeded electron configurations [nconf, nelec, 3]: each electron sits
     near a random atom with a Gaussian spread (bohr)."""
     rng = np.random.default_rng(seed)
     if "a" in deck.extra:  # periodic cell: uniform in the cell
         return rng.uniform(0.0, deck.extra["a"], size=(nconf, deck.nelec, 3))
-    atoms = np.array([[0.0, 0.0, -1.0375], [0.0, 0.0, 1.0375]])
+    atoms = deck.extra.get("atoms", np.array([[0.0, 0.0, -1.0375], [0.0, 0.0, 1.0375]]))
     which = rng.integers(0, len(atoms), size=(nconf, deck.nelec))
     return atoms[which] + rng.normal(0.0, spread, size=(nconf, deck.nelec, 3))
 

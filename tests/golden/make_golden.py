@@ -27,12 +27,15 @@ import refrun  # noqa: E402
 NCONF = 256
 NMOVE = 2
 WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseudo=True), 12),
-             ("diamond8", dict(periodic=True), 13)]
+             ("diamond8", dict(periodic=True), 13), ("mol43", dict(nelec=43), 14)]
 
 
 def make(name, kw, seed):
     if kw.get("periodic"):
         deck = systems.write_periodic(HERE, seed=seed, name=name)
+        nconf = 64
+    elif "nelec" in kw:  # one molecule of the batched-uneven workload (odd electron count)
+        deck = systems.write_molecule(HERE, name, seed, kw["nelec"])
         nconf = 64
     else:
         deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
@@ -51,5 +54,7 @@ def make(name, kw, seed):
 if __name__ == "__main__":
     if not refrun.harness_available():
         sys.exit("build the reference harness first: make -C oracle REF=<reference> -j8")
+    only = set(sys.argv[1:])
     for name, kw, seed in WORKLOADS:
-        make(name, kw, seed)
+        if not only or name in only:
+            make(name, kw, seed)
