@@ -128,6 +128,11 @@ int qwg_set_walkers(qwg_ctx* ctx, const double* R, int nw);
 int qwg_get_walkers(qwg_ctx* ctx, double* R, int nw);
 /* Device-buffer variants (pointers in device memory, stream-ordered). */
 int qwg_set_walkers_device(qwg_ctx* ctx, const double* dR, int nw);
+/* Per-walker scalars after the last VMC/DMC step: local energy and DMC weight
+ * (1 in VMC) of each walker, as Dmc_point keeps them (method/Dmc_method.h:62-82:
+ * prop.energy, weight).  energy / weight: host arrays of nw doubles, either
+ * may be NULL.  QWG_ERR_STATE before any block has run on these walkers. */
+int qwg_get_walker_scalars(qwg_ctx* ctx, double* energy, double* weight, int nw);
 
 /* Full evaluation of every resident walker.  rot: [nw][3][3] quadrature
  * rotations (rows x,y,z; Pseudopotential::rotateQuadrature) or NULL for the

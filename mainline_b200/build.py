@@ -25,6 +25,8 @@ NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--ex
 
 SOURCES_CU = ["qwg_engine.cu"]
 SOURCES_CXX = ["qwg_deck.cpp"]
+# walker-kernel families: qwg_walkers.cu once per (working precision, orbital capacity)
+FAMILIES = [(real, mm) for real in ("double", "float") for mm in (8, 16, 32, 0)]
 
 
 def _run(cmd):
@@ -46,22 +48,34 @@ def build(verbose: bool = False, extra_nvflags=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
     headers.append(os.path.join(ROOT, "include", "qwg.h"))
-    objs = []
+    objs, jobs = [], []
     for src in SOURCES_CXX:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if _stale(o, [s] + headers):
             _run(["g++", "-c", *CXXFLAGS, "-I" + os.path.join(ROOT, "include"), s, "-o", o])
         objs.append(o)
-    for src in SOURCES_CU:
-        s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src + ".o")
+    units = [(os.path.join(CSRC, src), os.path.join(BUILD, src + ".o"), []) for src in SOURCES_CU]
+    wsrc = os.path.join(CSRC, "qwg_walkers.cu")
+    for real, mm in FAMILIES:
+        units.append((wsrc, os.path.join(BUILD, f"qwg_walkers_{real}_{mm}.o"),
+                      [f"-DQWG_REAL={real}", f"-DQWG_MM={mm}"]))
+    for s, o, defs in units:
         if _stale(o, [s] + headers):
-            cmd = [NVCC, "-c", *NVFLAGS, *(extra_nvflags or []), s, "-o", o]
-            r = _run(cmd + (["-Xptxas", "-v"] if verbose else []))
-            if verbose:
-                sys.stderr.write(r.stderr)
+            cmd = [NVCC, "-c", *NVFLAGS, *defs, *(extra_nvflags or []), s, "-o", o]
+            cmd += ["-Xptxas", "-v"] if verbose else []
+            jobs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
         objs.append(o)
+    failed = None
+    for cmd, p in jobs:  # families compile in parallel
+        out, err = p.communicate()
+        if p.returncode != 0:
+            sys.stderr.write(out + err)
+            failed = cmd
+        elif verbose:
+            sys.stderr.write(err)
+    if failed:
+        raise RuntimeError("build step failed: " + " ".join(failed))
     if _stale(LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs])
     return LIB

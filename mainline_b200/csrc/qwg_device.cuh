@@ -87,6 +87,7 @@ struct DevSys {
   DRadial ei[QWG_MAXT][QWG_MAXEI];
   double onebody[QWG_MAXT][QWG_MAXEI];
   int tb_n[QWG_MAXT];
+  double tb_rc[QWG_MAXT];        // largest e-i cutoff the type's e-e-n terms use
   DTB tb[QWG_MAXT][QWG_MAXTB];
   int has_tb;
   // pseudopotential per type (nchan 0: none)
@@ -101,6 +102,7 @@ struct DevSys {
   int periodic;
   double lat[3][3], normvec[3][3], origin[3], corners[3][3];
   double h2q;                    // (smallest cell height / 2)^2: minimum-image shortcut
+  int ortho;                     // lattice vectors along x, y, z (orthorhombic cell)
   double lattice_basis[27][3];
   double alpha, ewald_const;
   int2 atom_images[QWG_MAXA];    // (first, count) into image_pos
@@ -119,6 +121,15 @@ __device__ __forceinline__ void min_image(const DevSys<Real>& S, double& x, doub
   if (!S.periodic) return;
   const double d2 = x * x + y * y + z * z;
   if (d2 < S.h2q) return;
+  if (S.ortho) {
+    // orthorhombic cell: the 27-image search reduces to one independent
+    // choice per axis among x - L, x, x + L (the same sums it would form)
+    const double lx = S.lat[0][0], ly = S.lat[1][1], lz = S.lat[2][2];
+    if (x > 0.5 * lx) x -= lx; else if (x < -0.5 * lx) x += lx;
+    if (y > 0.5 * ly) y -= ly; else if (y < -0.5 * ly) y += ly;
+    if (z > 0.5 * lz) z -= lz; else if (z < -0.5 * lz) z += lz;
+    return;
+  }
   double bx = x, by = y, bz = z, bd = 1e99;
   for (int a = 0; a < 27; a++) {
     const double tx = x + S.lattice_basis[a][0], ty = y + S.lattice_basis[a][1], tz = z + S.lattice_basis[a][2];
@@ -156,9 +167,17 @@ __device__ __forceinline__ double erfc_poly(double x) {
 }
 
 // Per-walker shared-memory layout (byte offsets, host computed).
+// Byte offsets of one walker's arrays.  R, inv, mov, gU, lU and scal are
+// offsets into the persistent state (state_bytes per walker); bas, newcol,
+// dG, lu, items, Ue, rot and wproj into the walker's scratch (scratch_bytes).
+// Walkers with <= 32 orbitals per spin keep state + scratch together in
+// shared memory (bytes = state_bytes + scratch_bytes per warp); larger ones
+// work in place in HBM with one scratch region per walker.
 struct WLayout {
   int R, inv, mov, gU, lU, scal, bas, newcol, dG, Ue, lu, items, rot, wproj, wchunk, bytes;
-  int state_bytes;  // prefix [0, state_bytes) is the persistent walker state
+  int state_bytes;    // persistent walker state
+  int scratch_bytes;  // per-walker scratch
+  int mstride;        // row stride of the inverse / MO-derivative rows (orbitals, padded)
 };
 
 // Persistent scalars of a walker (inside the state prefix).
@@ -208,6 +227,7 @@ struct StepParams {
   uint64_t step0;       // global step counter of the first step (dyn_step == 0)
   double* R;            // [W][N][3]
   unsigned char* state; // [W][state_bytes]
+  unsigned char* scratch;  // [W][scratch_bytes] (HBM-resident walkers only)
   BlockAcc* acc;
 };
 
@@ -433,6 +453,22 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
     }
   }
   __syncwarp();
+  if (M > 32) {
+    // many orbitals: lanes over MOs (coalesced coefficient rows), the basis
+    // values are warp-uniform reads
+    for (int mo = lane; mo < M; mo += 32) {
+      Real a0 = Real(0), a1 = Real(0), a2 = Real(0), a3 = Real(0), a4 = Real(0);
+      const Real* w = moc_s + mo;
+      for (int f = 0; f < S.nbasis; f++) {
+        const Real c = w[(size_t)f * S.mstride];
+        const Real* bb = bas + f * 5;
+        a0 += bb[0] * c; a1 += bb[1] * c; a2 += bb[2] * c; a3 += bb[3] * c; a4 += bb[4] * c;
+      }
+      out[mo * 5] = a0; out[mo * 5 + 1] = a1; out[mo * 5 + 2] = a2; out[mo * 5 + 3] = a3; out[mo * 5 + 4] = a4;
+    }
+    __syncwarp();
+    return;
+  }
   // contraction: lane (mo, chunk) sums the 5 components of one MO over a
   // slice of the basis (5 independent accumulators), then the slices of an
   // MO are added with shuffles
@@ -603,55 +639,106 @@ __device__ __forceinline__ void jas_onebody(const DevSys<Real>& S, double px, do
   }
 }
 
-// Three-body (e-e-n) contribution of the pair (i, j) at all atoms, with
-// gradients/laps for both electrons: sum_atom sum_terms c (a_k(i) a_l(j) +
-// a_l(i) a_k(j)) b_m(r_ij) (Jastrow2_three.cpp:138-404).
+// Atoms whose e-e-n terms can be nonzero for an electron at p: the e-i
+// radial functions vanish (value and derivatives) at and beyond their
+// cutoff, so an atom farther than tb_rc (the largest cutoff its e-e-n terms
+// use) from either electron of a pair contributes exactly zero.  Computed
+// once per position; n < 0 means more than QWG_NEAR atoms are in range and
+// the callers fall back to every atom.
+constexpr int QWG_NEAR = 12;
+struct NearSet {
+  int n;
+  int a[QWG_NEAR];
+  double d[QWG_NEAR][3];  // p - atom, minimum image
+  double r[QWG_NEAR];
+};
+
 template <typename Real>
-__device__ void jas_threebody_pair(const DevSys<Real>& S, const double pi[3], const double pj[3], double& u,
-                                   double gi[3], double& li, double gj[3], double& lj, bool need_derivs) {
-  u = 0; li = lj = 0;
-  for (int d = 0; d < 3; d++) gi[d] = gj[d] = 0;
-  double dij[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
-  min_image(S, dij[0], dij[1], dij[2]);
-  double rij = sqrt(dij[0] * dij[0] + dij[1] * dij[1] + dij[2] * dij[2]);
+__device__ __forceinline__ void near_atoms(const DevSys<Real>& S, const double p[3], NearSet& ns) {
+  ns.n = 0;
   for (int a = 0; a < S.natoms; a++) {
     const int t = S.atom_type[a];
-    const int nt = S.tb_n[t];
-    if (!nt) continue;
-    const double* ap = S.atom_pos[a];
-    double di[3] = {pi[0] - ap[0], pi[1] - ap[1], pi[2] - ap[2]};
-    double dj[3] = {pj[0] - ap[0], pj[1] - ap[1], pj[2] - ap[2]};
-    min_image(S, di[0], di[1], di[2]);
-    min_image(S, dj[0], dj[1], dj[2]);
-    double ri = sqrt(di[0] * di[0] + di[1] * di[1] + di[2] * di[2]);
-    double rj = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
-    for (int n = 0; n < nt; n++) {
-      const DTB& q = S.tb[t][n];
-      double aki, akdi, akli, akj, akdj, aklj, ali, aldi, alli, alj, aldj, allj, b, bd, bl;
-      radial_lap(S.ei[t][q.k], ri, aki, akdi, akli);
-      radial_lap(S.ei[t][q.k], rj, akj, akdj, aklj);
-      radial_lap(S.ei[t][q.l], ri, ali, aldi, alli);
-      radial_lap(S.ei[t][q.l], rj, alj, aldj, allj);
-      radial_lap(S.ee[q.m], rij, b, bd, bl);
-      double s = aki * alj + ali * akj;
-      u += q.c * s * b;
-      if (!need_derivs) continue;
-      double gsi[3], gsj[3], gb[3];
-      double dsi = 0, dsj = 0;
-      for (int d = 0; d < 3; d++) {
-        gsi[d] = akdi * di[d] * alj + aldi * di[d] * akj;
-        gsj[d] = aki * aldj * dj[d] + ali * akdj * dj[d];
-        gb[d] = bd * dij[d];
-        dsi += gsi[d] * gb[d];
-        dsj += gsj[d] * gb[d];
-      }
-      for (int d = 0; d < 3; d++) {
-        gi[d] += q.c * (gsi[d] * b + s * gb[d]);
-        gj[d] += q.c * (gsj[d] * b - s * gb[d]);
-      }
-      li += q.c * ((akli * alj + alli * akj) * b + s * bl + 2 * dsi);
-      lj += q.c * ((aki * allj + ali * aklj) * b + s * bl - 2 * dsj);
+    if (!S.tb_n[t]) continue;
+    double dx = p[0] - S.atom_pos[a][0], dy = p[1] - S.atom_pos[a][1], dz = p[2] - S.atom_pos[a][2];
+    min_image(S, dx, dy, dz);
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(r < S.tb_rc[t])) continue;
+    if (ns.n == QWG_NEAR) { ns.n = -1; return; }
+    ns.a[ns.n] = a;
+    ns.d[ns.n][0] = dx; ns.d[ns.n][1] = dy; ns.d[ns.n][2] = dz;
+    ns.r[ns.n] = r;
+    ns.n++;
+  }
+}
+
+// e-e-n terms of the pair (i, j) at one atom of type t (Jastrow2_three.cpp:
+// 138-404): sum_terms c (a_k(i) a_l(j) + a_l(i) a_k(j)) b_m(r_ij), with
+// gradients/laps for both electrons.
+template <typename Real>
+__device__ __forceinline__ void tb_atom(const DevSys<Real>& S, int t, const double di[3], double ri, const double dj[3],
+                                        double rj, const double dij[3], double rij, double& u, double gi[3],
+                                        double& li, double gj[3], double& lj, bool need_derivs) {
+  const int nt = S.tb_n[t];
+  for (int n = 0; n < nt; n++) {
+    const DTB& q = S.tb[t][n];
+    double aki, akdi, akli, akj, akdj, aklj, ali, aldi, alli, alj, aldj, allj, b, bd, bl;
+    radial_lap(S.ei[t][q.k], ri, aki, akdi, akli);
+    radial_lap(S.ei[t][q.k], rj, akj, akdj, aklj);
+    radial_lap(S.ei[t][q.l], ri, ali, aldi, alli);
+    radial_lap(S.ei[t][q.l], rj, alj, aldj, allj);
+    radial_lap(S.ee[q.m], rij, b, bd, bl);
+    double s = aki * alj + ali * akj;
+    u += q.c * s * b;
+    if (!need_derivs) continue;
+    double gsi[3], gsj[3], gb[3];
+    double dsi = 0, dsj = 0;
+    for (int d = 0; d < 3; d++) {
+      gsi[d] = akdi * di[d] * alj + aldi * di[d] * akj;
+      gsj[d] = aki * aldj * dj[d] + ali * akdj * dj[d];
+      gb[d] = bd * dij[d];
+      dsi += gsi[d] * gb[d];
+      dsj += gsj[d] * gb[d];
     }
+    for (int d = 0; d < 3; d++) {
+      gi[d] += q.c * (gsi[d] * b + s * gb[d]);
+      gj[d] += q.c * (gsj[d] * b - s * gb[d]);
+    }
+    li += q.c * ((akli * alj + alli * akj) * b + s * bl + 2 * dsi);
+    lj += q.c * ((aki * allj + ali * aklj) * b + s * bl - 2 * dsj);
+  }
+}
+
+// Three-body (e-e-n) contribution of the pair (i, j) summed over the atoms
+// (ns: the atoms in range of electron i, from near_atoms at pi).
+template <typename Real>
+__device__ void jas_threebody_pair(const DevSys<Real>& S, const NearSet& ns, const double pi[3], const double pj[3],
+                                   double& u, double gi[3], double& li, double gj[3], double& lj, bool need_derivs) {
+  u = 0; li = lj = 0;
+  for (int d = 0; d < 3; d++) gi[d] = gj[d] = 0;
+  if (ns.n == 0) return;
+  double dij[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
+  min_image(S, dij[0], dij[1], dij[2]);
+  const double rij = sqrt(dij[0] * dij[0] + dij[1] * dij[1] + dij[2] * dij[2]);
+  const int cnt = ns.n < 0 ? S.natoms : ns.n;
+  for (int q = 0; q < cnt; q++) {
+    const int a = ns.n < 0 ? q : ns.a[q];
+    const int t = S.atom_type[a];
+    if (!S.tb_n[t]) continue;
+    const double* ap = S.atom_pos[a];
+    double di[3], ri;
+    if (ns.n < 0) {
+      di[0] = pi[0] - ap[0]; di[1] = pi[1] - ap[1]; di[2] = pi[2] - ap[2];
+      min_image(S, di[0], di[1], di[2]);
+      ri = sqrt(di[0] * di[0] + di[1] * di[1] + di[2] * di[2]);
+    } else {
+      di[0] = ns.d[q][0]; di[1] = ns.d[q][1]; di[2] = ns.d[q][2];
+      ri = ns.r[q];
+    }
+    double dj[3] = {pj[0] - ap[0], pj[1] - ap[1], pj[2] - ap[2]};
+    min_image(S, dj[0], dj[1], dj[2]);
+    const double rj = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
+    if (!(rj < S.tb_rc[t]) || !(ri < S.tb_rc[t])) continue;  // every term vanishes
+    tb_atom(S, t, di, ri, dj, rj, dij, rij, u, gi, li, gj, lj, need_derivs);
   }
 }
 
@@ -666,6 +753,8 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
   for (int d = 0; d < 3; d++) g[d] = og[d];
   const bool si = i < S.nup;
   const double pi[3] = {px, py, pz};
+  NearSet ns;
+  if constexpr (TB) near_atoms(S, pi, ns);
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
     double dx = px - R[3 * j], dy = py - R[3 * j + 1], dz = pz - R[3 * j + 2];
@@ -677,7 +766,7 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
     g[0] += pfd * dx; g[1] += pfd * dy; g[2] += pfd * dz;
     if constexpr (TB) {  // e-e-n terms compiled in only when the deck has them
       double tu, tgi[3], tli, tgj[3], tlj;
-      jas_threebody_pair(S, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, need_derivs);
+      jas_threebody_pair(S, ns, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, need_derivs);
       u += tu; lap += tli;
       for (int d = 0; d < 3; d++) g[d] += tgi[d];
     }
@@ -704,6 +793,8 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
   }
   const bool si = i < S.nup;
   const double pi[3] = {px, py, pz};
+  NearSet ns;
+  if constexpr (TB) near_atoms(S, pi, ns);
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
     double ex = px - R[3 * j], ey = py - R[3 * j + 1], ez = pz - R[3 * j + 2];
@@ -717,7 +808,7 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
     }
     if constexpr (TB) {
       double tu, tgi[3], tli, tgj[3], tlj;
-      jas_threebody_pair(S, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false);
+      jas_threebody_pair(S, ns, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false);
       u += T(tu);
     }
   }
@@ -726,6 +817,84 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
 
 // ---------------------------------------------------------------------------
 // dense linear algebra in the warp
+
+// Gauss-Jordan inversion with partial pivoting for any M (the matrix lives in
+// HBM-resident scratch): lanes over columns; the pivot column is copied to
+// fcol[M] before each elimination so that no lane reads a factor another lane
+// is updating.  Same pivot rule, log|det| and sign as gj_inverse_warp.
+template <typename Real>
+__device__ void gj_inverse_warp_big(double* aug, double* fcol, int M, Real* invT, int invstride, double& logdet,
+                                    double& sign, int lane) {
+  const int W = 2 * M;
+  for (int idx = lane; idx < M * M; idx += 32) {
+    int i = idx / M, k = idx - i * M;
+    aug[i * W + M + k] = (i == k) ? 1.0 : 0.0;
+  }
+  __syncwarp();
+  double ld = 0.0, sg = 1.0;
+  bool singular = false;
+  for (int k = 0; k < M; k++) {
+    double best = -1.0;
+    int bi = k;
+    for (int i = k + lane; i < M; i += 32) {
+      double v = fabs(aug[i * W + k]);
+      if (v > best) { best = v; bi = i; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (!(best > 0.0)) { singular = true; break; }
+    if (bi != k) {
+      for (int c = lane; c < W; c += 32) {
+        double t = aug[k * W + c];
+        aug[k * W + c] = aug[bi * W + c];
+        aug[bi * W + c] = t;
+      }
+      sg = -sg;
+    }
+    __syncwarp();
+    const double piv = aug[k * W + k];
+    ld += log(fabs(piv));
+    if (piv < 0) sg = -sg;
+    const double inv = 1.0 / piv;
+    __syncwarp();
+    for (int c = lane; c < W; c += 32) aug[k * W + c] *= inv;
+    for (int i = lane; i < M; i += 32) fcol[i] = aug[i * W + k];
+    __syncwarp();
+    // columns k+1.. of the left half and the whole right half change; column k
+    // becomes the unit vector
+    for (int c = lane; c < W; c += 32) {
+      if (c < k) continue;
+      const double pk = aug[k * W + c];
+      if (c == k) {
+        for (int i = 0; i < M; i++)
+          if (i != k) aug[i * W + c] = 0.0;
+      } else {
+        for (int i = 0; i < M; i++)
+          if (i != k) aug[i * W + c] -= fcol[i] * pk;
+      }
+    }
+    __syncwarp();
+  }
+  if (singular) {
+    ld = -1e201;
+    for (int idx = lane; idx < M * M; idx += 32) {
+      int e = idx / M, i = idx - e * M;
+      invT[e * invstride + i] = Real(0);
+    }
+  } else {
+    for (int idx = lane; idx < M * M; idx += 32) {
+      int e = idx / M, i = idx - e * M;
+      invT[e * invstride + i] = Real(aug[i * W + M + e]);
+    }
+  }
+  __syncwarp();
+  logdet = ld;
+  sign = sg;
+}
 
 // Gauss-Jordan inversion with partial pivoting of A (M x M, M <= 32, row-major,
 // A[e][i] = phi_i(r_e)) held in aug[M][2M] (double).  Writes the transposed

@@ -13,7 +13,7 @@
 
 #include "../../include/qwg.h"
 #include "qwg_deck.hpp"
-#include "qwg_kernels.cuh"
+#include "qwg_launch.cuh"
 
 using namespace qwg;
 
@@ -50,10 +50,16 @@ static void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
   if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
 }
 
+// Kernel family for a system with m orbitals per spin: 8/16/32 select the
+// shared-memory walker kernels; 0 selects the HBM-resident kernels (up to
+// kMaxOrbHBM orbitals per spin); -1 is beyond this build.
+constexpr int kMaxOrbHBM = 256;
+static int mo_stride_for(int mmax, int nmo_max) { return mmax > 0 ? mmax : (nmo_max + 3) / 4 * 4; }
 static int mmax_for(int m) {
   if (m <= 8) return 8;
   if (m <= 16) return 16;
   if (m <= 32) return 32;
+  if (m <= kMaxOrbHBM) return 0;
   return -1;
 }
 
@@ -78,8 +84,9 @@ struct qwg_ctx {
   WLayout L{};
   size_t smem_bytes = 0;
   // walkers
-  DevBuf d_R, d_R2, d_state, d_state2;
+  DevBuf d_R, d_R2, d_state, d_state2, d_scratch;
   bool state_valid = false;
+  bool have_scalars = false;  // WScal.eold / weight written by a block
   // io scratch
   DevBuf d_io, d_acc, d_dyn, d_src, d_neww, d_energy;
   size_t io_bytes = 0;
@@ -122,7 +129,7 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
   S.nelec = H.nelec; S.nup = H.nup; S.ndn = H.ndn; S.natoms = H.natoms;
   S.nbasis = H.nbasis; S.nshell = (int)H.shells.size();
   S.m[0] = H.nmo[0]; S.m[1] = H.nmo[1];
-  S.mstride = c->mmax;
+  S.mstride = mo_stride_for(c->mmax, std::max(H.nmo[0], H.nmo[1]));
   S.ion_ion = H.ion_ion;
   S.shell_i = c->d_shell_i.as<int4>();
   S.shell_obj = c->d_shell_obj.as<int2>();
@@ -174,6 +181,10 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     }
   }
   S.h2q = H.smallest_height * H.smallest_height * 0.25;
+  S.ortho = 1;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      if (i != j && H.lat[3 * i + j] != 0.0) S.ortho = 0;
   for (int k = 0; k < 27 && H.periodic; k++)
     for (int d = 0; d < 3; d++) S.lattice_basis[k][d] = H.lattice_basis[3 * k + d];
   S.alpha = H.alpha;
@@ -214,9 +225,11 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     }
     if (H.tb_count[a] > QWG_MAXTB) throw InputError("more than 12 e-e-n terms on one atom");
     S.tb_n[t] = H.tb_count[a];
+    S.tb_rc[t] = 0.0;
     for (int n = 0; n < H.tb_count[a]; n++) {
       const ThreeBodyTerm& q = H.tb[H.tb_first[a] + n];
       S.tb[t][n] = DTB{q.k - H.ei_first[a], q.l - H.ei_first[a], q.m, q.c};
+      S.tb_rc[t] = std::max({S.tb_rc[t], S.ei[t][S.tb[t][n].k].rcut, S.ei[t][S.tb[t][n].l].rcut});
     }
     const PPAtom& P = H.pp[a];
     S.pp_nchan[t] = P.nchan;
@@ -270,8 +283,8 @@ static void build_tables(qwg_ctx* c) {
   upload(c->d_shell_i, si, st);
   upload(c->d_shell_obj, so, st);
   upload(c->d_shell_cut, sc, st);
-  // MO coefficients padded to MMAX columns, both spins
-  const int mm = c->mmax;
+  // MO coefficients padded to the orbital stride, both spins
+  const int mm = mo_stride_for(c->mmax, std::max(H.nmo[0], H.nmo[1]));
   std::vector<double> moc((size_t)2 * H.nbasis * mm, 0.0);
   for (int s = 0; s < 2; s++)
     for (int f = 0; f < H.nbasis; f++)
@@ -303,9 +316,12 @@ static int align16(int x) { return (x + 15) / 16 * 16; }
 
 static void make_layout(qwg_ctx* c) {
   const HostSystem& H = c->H;
-  const int N = H.nelec, mm = c->mmax, A = H.natoms;
+  const int N = H.nelec, A = H.natoms;
+  const bool hbm = c->mmax == 0;
+  const int mm = mo_stride_for(c->mmax, std::max(H.nmo[0], H.nmo[1]));
   const int rs = c->precision == QWG_FP64 ? 8 : 4;
   WLayout& L = c->L;
+  L.mstride = mm;
   int o = 0;
   L.scal = o; o = align16(o + (int)sizeof(WScal));
   L.R = o; o = align16(o + 8 * 3 * N);
@@ -314,34 +330,51 @@ static void make_layout(qwg_ctx* c) {
   L.gU = o; o = align16(o + 8 * 3 * N);
   L.lU = o; o = align16(o + 8 * N);
   L.state_bytes = o;
-  // scratch: the move/re-inversion phase and the pseudopotential phase are
-  // never live together, so their buffers share one region
-  const int s0 = o;
+  // scratch (offsets from its own start): the move/re-inversion phase and the
+  // pseudopotential phase are never live together, so their buffers share
+  // one region
+  o = 0;
   L.bas = o; o = align16(o + rs * H.nbasis * 5);
   L.newcol = o; o = align16(o + rs * mm * 5);
   L.dG = o; o = align16(o + 8 * 4 * N);
-  L.lu = o; o = align16(o + 8 * mm * 2 * mm);
+  L.lu = o; o = align16(o + 8 * (mm * 2 * mm + mm));
   const int move_end = o;
-  o = s0;
-  L.items = o; o = align16(o + (int)sizeof(PPItem) * N * A);
+  // pseudopotential phase for a chunk of wc electrons: items (wc x atoms),
+  // Jastrow values, rotation, projected coefficients (wc x nbasis)
+  auto pp_bytes = [&](int wc) {
+    int q = align16((int)sizeof(PPItem) * wc * A);
+    q = align16(q + 8 * N);
+    q = align16(q + 8 * 9);
+    return align16(q + rs * H.nbasis * wc);
+  };
+  if (hbm) {
+    L.wchunk = std::min(N, 64);
+  } else {
+    // all electrons in one chunk if a walker still fits the budget of 4
+    // walkers x 4 CTAs per SM, else as many as fit (at least 4)
+    const int budget = (227 * 1024 - 1024) / 16 - L.state_bytes;
+    const int room = std::max(budget, move_end);
+    int wc = N;
+    while (wc > 4 && pp_bytes(wc) > room) wc--;
+    L.wchunk = std::max(1, std::min(N, wc));
+  }
+  L.items = 0;
+  o = align16((int)sizeof(PPItem) * L.wchunk * A);
   L.Ue = o; o = align16(o + 8 * N);
   L.rot = o; o = align16(o + 8 * 9);
-  L.wproj = o;
-  // projected coefficients for a chunk of electrons: all of them if a walker
-  // still fits the budget of 4 walkers x 4 CTAs per SM, else as many as fit
-  // (at least 4)
-  const int budget = (227 * 1024 - 1024) / 16;
-  int room = std::max(budget - o, move_end - o);
-  L.wchunk = std::max(4, std::min(N, room / (rs * H.nbasis)));
-  o = align16(o + rs * H.nbasis * L.wchunk);
-  o = std::max(o, move_end);
-  L.bytes = o;
-  const size_t moc_bytes = 0;  // MO coefficients are read through L1, not staged
+  L.wproj = o; o = align16(o + rs * H.nbasis * L.wchunk);
+  L.scratch_bytes = std::max(o, move_end);
+  L.bytes = L.state_bytes + L.scratch_bytes;
+  if (hbm) {
+    c->wpc = 4;
+    c->smem_bytes = 0;
+    return;
+  }
   // walkers per CTA: up to 4 while the CTA stays under ~110 KB (2 CTAs/SM)
   int wpc = 4;
-  while (wpc > 1 && moc_bytes + (size_t)wpc * L.bytes > 110 * 1024) wpc--;
+  while (wpc > 1 && (size_t)wpc * L.bytes > 110 * 1024) wpc--;
   c->wpc = wpc;
-  c->smem_bytes = moc_bytes + (size_t)wpc * L.bytes;
+  c->smem_bytes = (size_t)wpc * L.bytes;
   if (c->smem_bytes > 227 * 1024) throw InputError("system too large for the shared-memory walker kernel");
 }
 
@@ -360,22 +393,11 @@ static void ensure_smem_attr(K kern, size_t bytes) {
   }
 }
 
-template <typename Real, int MM, int MODE>
-static void launch_mode(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int nwalk) {
-  auto kern = S.has_tb ? k_walkers<Real, MM, MODE, true> : k_walkers<Real, MM, MODE, false>;
-  ensure_smem_attr(kern, c->smem_bytes);
-  int grid = (nwalk + c->wpc - 1) / c->wpc;
-  kern<<<grid, 32 * c->wpc, c->smem_bytes, c->stream>>>(S, c->L, P, io);
-  CK(cudaGetLastError());
-  c->launches++;
-}
-
 template <typename Real, int MM>
 static void launch_walkers_t(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int mode,
                              int nwalk) {
-  if (mode == KM_EVAL) launch_mode<Real, MM, KM_EVAL>(c, S, P, io, nwalk);
-  else if (mode == KM_RATIO) launch_mode<Real, MM, KM_RATIO>(c, S, P, io, nwalk);
-  else launch_mode<Real, MM, KM_STEPS>(c, S, P, io, nwalk);
+  CK((launch_walker_kernels<Real, MM>(S, c->L, P, io, mode, nwalk, c->wpc, c->smem_bytes, c->stream)));
+  c->launches++;
 }
 
 static void launch_walkers(qwg_ctx* c, const StepParams& P, const EvalIO& io, int mode, int nwalk) {
@@ -383,13 +405,15 @@ static void launch_walkers(qwg_ctx* c, const StepParams& P, const EvalIO& io, in
     switch (c->mmax) {
       case 8: launch_walkers_t<double, 8>(c, c->sys_d, P, io, mode, nwalk); break;
       case 16: launch_walkers_t<double, 16>(c, c->sys_d, P, io, mode, nwalk); break;
-      default: launch_walkers_t<double, 32>(c, c->sys_d, P, io, mode, nwalk); break;
+      case 32: launch_walkers_t<double, 32>(c, c->sys_d, P, io, mode, nwalk); break;
+      default: launch_walkers_t<double, 0>(c, c->sys_d, P, io, mode, nwalk); break;
     }
   } else {
     switch (c->mmax) {
       case 8: launch_walkers_t<float, 8>(c, c->sys_f, P, io, mode, nwalk); break;
       case 16: launch_walkers_t<float, 16>(c, c->sys_f, P, io, mode, nwalk); break;
-      default: launch_walkers_t<float, 32>(c, c->sys_f, P, io, mode, nwalk); break;
+      case 32: launch_walkers_t<float, 32>(c, c->sys_f, P, io, mode, nwalk); break;
+      default: launch_walkers_t<float, 0>(c, c->sys_f, P, io, mode, nwalk); break;
     }
   }
 }
@@ -399,6 +423,7 @@ static StepParams base_params(qwg_ctx* c) {
   P.nwalk = c->nwalk;
   P.R = c->d_R.as<double>();
   P.state = c->d_state.as<unsigned char>();
+  P.scratch = c->d_scratch.p ? c->d_scratch.as<unsigned char>() : nullptr;
   P.acc = c->d_acc.as<BlockAcc>();
   P.etrial = c->d_dyn.as<double>();
   P.refresh = 1;
@@ -453,6 +478,7 @@ static void run_chunk(qwg_ctx* c, int nsteps, double tau, uint64_t seed, int det
   io.energy = energy_out;
   launch_walkers(c, P, io, KM_STEPS, c->nwalk);
   c->state_valid = true;
+  c->have_scalars = true;
   c->step_counter += nsteps;
 }
 
@@ -617,7 +643,7 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
   int rc = guarded(c.get(), [&]() -> int {
     c->H = build_system(deck_path);
     int mm = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
-    if (mm < 0) throw InputError("more than 32 electrons of one spin: beyond this engine build");
+    if (mm < 0) throw InputError("more than 256 electrons of one spin: beyond this engine build");
     c->mmax = mm;
     if (stream) {
       c->stream = (cudaStream_t)stream;
@@ -632,6 +658,7 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
     c->d_R2.alloc((size_t)max_walkers * 3 * N * 8);
     c->d_state.alloc((size_t)max_walkers * c->L.state_bytes);
     c->d_state2.alloc((size_t)max_walkers * c->L.state_bytes);
+    if (c->mmax == 0) c->d_scratch.alloc((size_t)max_walkers * c->L.scratch_bytes);
     c->d_acc.alloc(sizeof(BlockAcc) * 1024);
     c->d_dyn.alloc(DYN_COUNT * 8);
     CK(cudaMemsetAsync(c->d_dyn.p, 0, DYN_COUNT * 8, c->stream));
@@ -686,6 +713,7 @@ int qwg_set_walkers(qwg_ctx* c, const double* R, int nw) {
     CK(cudaMemcpyAsync(c->d_R.p, R, bytes, cudaMemcpyHostToDevice, c->stream));
     c->nwalk = nw;
     c->state_valid = false;
+    c->have_scalars = false;
     c->dmc_ready = false;
     return QWG_OK;
   });
@@ -697,6 +725,7 @@ int qwg_set_walkers_device(qwg_ctx* c, const double* dR, int nw) {
     CK(cudaMemcpyAsync(c->d_R.p, dR, (size_t)nw * 3 * c->H.nelec * 8, cudaMemcpyDeviceToDevice, c->stream));
     c->nwalk = nw;
     c->state_valid = false;
+    c->have_scalars = false;
     c->dmc_ready = false;
     return QWG_OK;
   });
@@ -707,6 +736,24 @@ int qwg_get_walkers(qwg_ctx* c, double* R, int nw) {
   return guarded(c, [&]() -> int {
     CK(cudaMemcpyAsync(R, c->d_R.p, (size_t)nw * 3 * c->H.nelec * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return QWG_OK;
+  });
+}
+
+int qwg_get_walker_scalars(qwg_ctx* c, double* energy, double* weight, int nw) {
+  if (!c || nw <= 0 || nw > c->nwalk) return fail(c, QWG_ERR_ARG, "qwg_get_walker_scalars: bad walker count");
+  if (!c->have_scalars) return fail(c, QWG_ERR_STATE, "qwg_get_walker_scalars: no block has run on these walkers");
+  return guarded(c, [&]() -> int {
+    // one strided copy of (eold, weight) out of every walker's state
+    std::vector<double> ew((size_t)nw * 2);
+    const unsigned char* src = c->d_state.as<unsigned char>() + c->L.scal + offsetof(WScal, eold);
+    static_assert(offsetof(WScal, weight) == offsetof(WScal, eold) + sizeof(double), "WScal layout");
+    CK(cudaMemcpy2DAsync(ew.data(), 16, src, c->L.state_bytes, 16, nw, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int w = 0; w < nw; w++) {
+      if (energy) energy[w] = ew[2 * (size_t)w];
+      if (weight) weight[w] = ew[2 * (size_t)w + 1];
+    }
     return QWG_OK;
   });
 }
@@ -866,6 +913,7 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
                                                            c->L.scal, c->d_energy.as<double>());
     CK(cudaGetLastError());
     c->launches++;
+    c->have_scalars = true;
     // device scalars: E_T = E_ref (start_feedback * log 1), counters
     double dyn0[DYN_COUNT] = {0};
     dyn0[DYN_ETRIAL] = c->eref;
@@ -996,9 +1044,12 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
     return fail(c, QWG_ERR_ARG, "qwg_vmc_block_noalloc: bad arguments");
   const size_t acc_bytes = 256;  // BlockAcc at the start, walker state after it
   static_assert(sizeof(BlockAcc) <= 256, "accumulator block exceeds its scratch slot");
-  const size_t need = acc_bytes + (size_t)nw * c->L.state_bytes;
+  // HBM-resident walkers (more than 32 orbitals per spin) also need their
+  // scratch region in the fixed buffer, after the walker states
+  const size_t per = (size_t)c->L.state_bytes + (c->mmax == 0 ? (size_t)c->L.scratch_bytes : 0);
+  const size_t need = acc_bytes + (size_t)nw * per;
   if (need > QWG_NOALLOC_SCRATCH_BYTES) {
-    const size_t maxw = (QWG_NOALLOC_SCRATCH_BYTES - acc_bytes) / c->L.state_bytes;
+    const size_t maxw = (QWG_NOALLOC_SCRATCH_BYTES - acc_bytes) / per;
     return fail(c, QWG_ERR_ARG, "qwg_vmc_block_noalloc: " + std::to_string(nw) + " walkers need " +
                                     std::to_string(need) + " bytes of scratch; the fixed scratch holds " +
                                     std::to_string(QWG_NOALLOC_SCRATCH_BYTES) + " bytes (at most " +
@@ -1022,6 +1073,7 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
     P.max_weight = 1.0;
     P.R = d_R;
     P.state = base + acc_bytes;
+    P.scratch = c->mmax == 0 ? base + acc_bytes + (size_t)nw * c->L.state_bytes : nullptr;
     P.acc = acc;
     P.etrial = c->d_dyn.as<double>();
     EvalIO io{};
@@ -1150,7 +1202,8 @@ int qwg_autotune(qwg_ctx* c, int* walkers_per_cta) {
     EvalIO io{};
     io.logpsi = base; io.sign = base + W; io.kinetic = base + 2 * W; io.potential = base + 3 * W;
     io.nonlocal = base + 4 * W; io.grad = base + 5 * W; io.lap = io.grad + n_g;
-    const size_t per = (size_t)c->L.bytes;
+    // shared memory per walker (none for HBM-resident walkers)
+    const size_t per = c->mmax == 0 ? 0 : (size_t)c->L.bytes;
     int best = c->wpc;
     float best_ms = 1e30f;
     for (int cand : {1, 2, 4}) {

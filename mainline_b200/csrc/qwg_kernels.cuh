@@ -29,32 +29,40 @@ struct PPItem {
   double vl[4];          // nonlocal channel radials (already scaled)
 };
 
+// MMAX > 0: at most MMAX orbitals per spin, state + scratch in shared
+// memory.  MMAX == 0: any count up to 256 per spin, arrays strided by
+// L.mstride and worked on in place in HBM.
 template <typename Real, int MMAX, bool TB>
 struct Walker {
   const DevSys<Real>& S;
   const WLayout& L;
-  unsigned char* base;
-  const Real* moc_s;     // [2][nbasis][MMAX] MO coefficients (global, read through L1)
+  unsigned char* base;   // persistent state
+  unsigned char* sbase;  // scratch
+  const Real* moc_s;     // [2][nbasis][mstride] MO coefficients (global, read through L1)
   int lane;
 
+  __device__ __forceinline__ int MS() const {
+    if constexpr (MMAX > 0) return MMAX;
+    else return L.mstride;
+  }
   __device__ double* R() const { return (double*)(base + L.R); }
-  __device__ Real* inv(int s) const { return (Real*)(base + L.inv) + s * MMAX * MMAX; }
+  __device__ Real* inv(int s) const { return (Real*)(base + L.inv) + (size_t)s * MS() * MS(); }
   __device__ Real* mov() const { return (Real*)(base + L.mov); }
   __device__ double* gU() const { return (double*)(base + L.gU); }
   __device__ double* lU() const { return (double*)(base + L.lU); }
   __device__ WScal* sc() const { return (WScal*)(base + L.scal); }
-  __device__ Real* bas() const { return (Real*)(base + L.bas); }
-  __device__ Real* newcol() const { return (Real*)(base + L.newcol); }
-  __device__ double* dG() const { return (double*)(base + L.dG); }
-  __device__ double* Ue() const { return (double*)(base + L.Ue); }
-  __device__ double* lu() const { return (double*)(base + L.lu); }
-  __device__ PPItem* items() const { return (PPItem*)(base + L.items); }
-  __device__ double* rot() const { return (double*)(base + L.rot); }
-  __device__ Real* wproj() const { return (Real*)(base + L.wproj); }
+  __device__ Real* bas() const { return (Real*)(sbase + L.bas); }
+  __device__ Real* newcol() const { return (Real*)(sbase + L.newcol); }
+  __device__ double* dG() const { return (double*)(sbase + L.dG); }
+  __device__ double* Ue() const { return (double*)(sbase + L.Ue); }
+  __device__ double* lu() const { return (double*)(sbase + L.lu); }
+  __device__ PPItem* items() const { return (PPItem*)(sbase + L.items); }
+  __device__ double* rot() const { return (double*)(sbase + L.rot); }
+  __device__ Real* wproj() const { return (Real*)(sbase + L.wproj); }
 
   __device__ int spin(int e) const { return e < S.nup ? 0 : 1; }
   __device__ int eloc(int e) const { return e < S.nup ? e : e - S.nup; }
-  __device__ const Real* mocs(int s) const { return moc_s + (size_t)s * S.nbasis * MMAX; }
+  __device__ const Real* mocs(int s) const { return moc_s + (size_t)s * S.nbasis * MS(); }
 
   // ---- full recompute: Slat_wf::calcLap (Slat_wf.h:948-1016) + the Jastrow
   // recomputation of every electron (Jastrow2_wf.cpp:988-1157).
@@ -71,14 +79,15 @@ struct Walker {
         mo_lap_warp(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], M, bas(), nc, lane);
         for (int i = lane; i < M; i += 32) {
           aug[el * 2 * M + i] = double(nc[i * 5]);
-          Real* mv = mov() + ((size_t)e * MMAX + i) * 4;
+          Real* mv = mov() + ((size_t)e * MS() + i) * 4;
           mv[0] = nc[i * 5 + 1]; mv[1] = nc[i * 5 + 2]; mv[2] = nc[i * 5 + 3]; mv[3] = nc[i * 5 + 4];
         }
         __syncwarp();
       }
       if (M > 0) {
         double ld, sg;
-        gj_inverse_warp(aug, M, inv(s), MMAX, ld, sg, lane);
+        if constexpr (MMAX > 0) gj_inverse_warp(aug, M, inv(s), MMAX, ld, sg, lane);
+        else gj_inverse_warp_big(aug, aug + 2 * M * M, M, inv(s), MS(), ld, sg, lane);
         if (lane == 0) { w->logdet[s] = ld; w->sign[s] = sg; }
       } else if (lane == 0) {
         w->logdet[s] = 0.0; w->sign[s] = 1.0;
@@ -104,8 +113,8 @@ struct Walker {
   // Slater gradient and Laplacian ratios of electron e at its position.
   __device__ void slater_gl(int e, double g[3], double& l) const {
     const int s = spin(e), el = eloc(e), M = S.m[s];
-    const Real* iv = inv(s) + el * MMAX;
-    const Real* mv = mov() + (size_t)e * MMAX * 4;
+    const Real* iv = inv(s) + (size_t)el * MS();
+    const Real* mv = mov() + (size_t)e * MS() * 4;
     double a0 = 0, a1 = 0, a2 = 0, a3 = 0;  // FP64 accumulation of the short dots
     for (int i = 0; i < M; i++) {
       double c = iv[i];
@@ -126,7 +135,7 @@ struct Walker {
     const double* Rp = R();
     Real* nc = newcol();
     mo_lap_warp(S, mocs(s), px, py, pz, M, bas(), nc, lane);
-    const Real* iv = inv(s) + el * MMAX;
+    const Real* iv = inv(s) + (size_t)el * MS();
     double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
     for (int i = 0; i < M; i++) {
       double c = iv[i];
@@ -140,6 +149,12 @@ struct Walker {
     const double ox = Rp[3 * e], oy = Rp[3 * e + 1], oz = Rp[3 * e + 2];
     const bool se = s == 0;
     constexpr bool has3 = TB;
+    NearSet nsn, nso;  // atoms in e-e-n range of the new and the old position
+    if constexpr (has3) {
+      const double pn[3] = {px, py, pz}, po[3] = {ox, oy, oz};
+      near_atoms(S, pn, nsn);
+      near_atoms(S, po, nso);
+    }
     double du = 0.0, ge[3] = {0, 0, 0}, le = 0.0;
     for (int j = lane; j < S.nelec; j += 32) {
       double* dg = dG() + 4 * j;
@@ -163,8 +178,8 @@ struct Walker {
       if constexpr (has3) {
         double pn[3] = {px, py, pz}, po[3] = {ox, oy, oz};
         double tu, tgi[3], tli, tgj[3], tlj, su, sgi[3], sli, sgj[3], slj;
-        jas_threebody_pair(S, pn, pj, tu, tgi, tli, tgj, tlj, true);
-        jas_threebody_pair(S, po, pj, su, sgi, sli, sgj, slj, true);
+        jas_threebody_pair(S, nsn, pn, pj, tu, tgi, tli, tgj, tlj, true);
+        jas_threebody_pair(S, nso, po, pj, su, sgi, sli, sgj, slj, true);
         du += tu - su;
         ge[0] += tgi[0]; ge[1] += tgi[1]; ge[2] += tgi[2];
         le += tli;
@@ -217,22 +232,23 @@ struct Walker {
     Real* nc = newcol();
     // scratch: wk[k] = sum_i phi'_i invT[k][i], rowe[i] = invT[el][i]
     Real* wk = (Real*)lu();
-    Real* rowe = wk + MMAX;
+    Real* rowe = wk + MS();
+    const int ms = MS();
     for (int k = lane; k < M; k += 32) {
       Real acc = 0;
-      for (int i = 0; i < M; i++) acc += nc[i * 5] * iv[k * MMAX + i];
+      for (int i = 0; i < M; i++) acc += nc[i * 5] * iv[(size_t)k * ms + i];
       wk[k] = acc;
-      rowe[k] = iv[el * MMAX + k];
+      rowe[k] = iv[(size_t)el * ms + k];
     }
     __syncwarp();
     const Real invr = Real(1.0 / ratioD);
     for (int idx = lane; idx < M * M; idx += 32) {
       int k = idx / M, i = idx - k * M;
-      if (k == el) iv[k * MMAX + i] = rowe[i] * invr;
-      else iv[k * MMAX + i] -= rowe[i] * wk[k] * invr;
+      if (k == el) iv[(size_t)k * ms + i] = rowe[i] * invr;
+      else iv[(size_t)k * ms + i] -= rowe[i] * wk[k] * invr;
     }
     for (int i = lane; i < M; i += 32) {
-      Real* mv = mov() + ((size_t)e * MMAX + i) * 4;
+      Real* mv = mov() + ((size_t)e * ms + i) * 4;
       mv[0] = nc[i * 5 + 1]; mv[1] = nc[i * 5 + 2]; mv[2] = nc[i * 5 + 3]; mv[3] = nc[i * 5 + 4];
     }
     for (int j = lane; j < S.nelec; j += 32) {
@@ -368,70 +384,72 @@ struct Walker {
     // per-electron Jastrow value at the current position
     for (int e = lane; e < N; e += 32)
       Ue()[e] = double(jas_electron_val<Real, TB>(S, Rp, e, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2]));
-    // item list
-    int nitems = 0;
-    PPItem* it = items();
-    for (int base0 = 0; base0 < N * A; base0 += 32) {
-      int idx = base0 + lane;
-      bool take = false;
-      PPItem item;
-      if (idx < N * A) {
-        int e = idx / A, a = idx - e * A;
-        const int t = S.atom_type[a];
-        int nch = S.pp_nchan[t];
-        if (nch > 0) {
-          const double* ap = S.atom_pos[a];
-          item.e = e; item.a = a;
-          item.dx = Rp[3 * e] - ap[0]; item.dy = Rp[3 * e + 1] - ap[1]; item.dz = Rp[3 * e + 2] - ap[2];
-          min_image(S, item.dx, item.dy, item.dz);
-          item.r = sqrt(item.dx * item.dx + item.dy * item.dy + item.dz * item.dz);
-          vloc += pp_radial(t, nch - 1, item.r);
-          for (int l = 0; l < 4; l++) item.vl[l] = (l < nch - 1) ? pp_radial(t, l, item.r) : 0.0;
-          if (deterministic) {
-            take = item.r < S.pp_cutoff[t];
-          } else {
-            double strength = 0;
-            for (int l = 0; l < nch - 1; l++) strength += 10.0 * (2 * l + 1) * fabs(item.vl[l]);
-            strength = fmin(1.0, strength);
-            Rand4 rr = rand4(seed, wid, step, (uint32_t)idx, 7u);
-            if (fabs(strength) > 0)
-              for (int l = 0; l < nch - 1; l++) item.vl[l] /= strength;
-            take = strength > rr.u[0];
-          }
-        }
-      }
-      unsigned m = __ballot_sync(0xffffffffu, take);
-      int pos = nitems + __popc(m & ((1u << lane) - 1u));
-      if (take) it[pos] = item;
-      nitems += __popc(m);
-    }
     __syncwarp();
     double vnl = 0;
-    // electrons in chunks of L.wchunk: projected coefficients of the chunk,
-    // then lanes over the chunk's (item, quadrature point) pairs
+    // electrons in chunks of L.wchunk: the (electron, atom) items of the
+    // chunk in electron-major order, the chunk's projected coefficients, then
+    // lanes over the chunk's (item, quadrature point) pairs
     const int CH = L.wchunk;
+    PPItem* it = items();
     Real* w = wproj();
-    int kbeg = 0;
-    for (int e0 = 0; e0 < N && kbeg < nitems; e0 += CH) {
-      int kend = kbeg;
-      while (kend < nitems && it[kend].e < e0 + CH) kend++;
-      if (kend == kbeg) continue;
+    for (int e0 = 0; e0 < N; e0 += CH) {
       const int e1 = min(N, e0 + CH);
+      int nitems = 0;
+      for (int base0 = e0 * A; base0 < e1 * A; base0 += 32) {
+        const int idx = base0 + lane;
+        bool take = false;
+        PPItem item;
+        if (idx < e1 * A) {
+          const int e = idx / A, a = idx - e * A;
+          const int t = S.atom_type[a];
+          const int nch = S.pp_nchan[t];
+          if (nch > 0) {
+            const double* ap = S.atom_pos[a];
+            item.e = e; item.a = a;
+            item.dx = Rp[3 * e] - ap[0]; item.dy = Rp[3 * e + 1] - ap[1]; item.dz = Rp[3 * e + 2] - ap[2];
+            min_image(S, item.dx, item.dy, item.dz);
+            item.r = sqrt(item.dx * item.dx + item.dy * item.dy + item.dz * item.dz);
+            vloc += pp_radial(t, nch - 1, item.r);
+            for (int l = 0; l < 4; l++) item.vl[l] = (l < nch - 1) ? pp_radial(t, l, item.r) : 0.0;
+            if (deterministic) {
+              take = item.r < S.pp_cutoff[t];
+            } else {
+              double strength = 0;
+              for (int l = 0; l < nch - 1; l++) strength += 10.0 * (2 * l + 1) * fabs(item.vl[l]);
+              strength = fmin(1.0, strength);
+              Rand4 rr = rand4(seed, wid, step, (uint32_t)idx, 7u);
+              if (fabs(strength) > 0)
+                for (int l = 0; l < nch - 1; l++) item.vl[l] /= strength;
+              take = strength > rr.u[0];
+            }
+          }
+        }
+        unsigned m = __ballot_sync(0xffffffffu, take);
+        int pos = nitems + __popc(m & ((1u << lane) - 1u));
+        if (take) it[pos] = item;
+        nitems += __popc(m);
+      }
+      __syncwarp();
+      if (nitems == 0) continue;
       for (int idx = lane; idx < (e1 - e0) * S.nbasis; idx += 32) {
         const int le = idx / S.nbasis, f = idx - le * S.nbasis;
         const int e = e0 + le, s = spin(e), el = eloc(e), M = S.m[s];
-        const Real* cf = mocs(s) + (size_t)f * MMAX;
-        const Real* iv = inv(s) + el * MMAX;
+        const Real* cf = mocs(s) + (size_t)f * MS();
+        const Real* iv = inv(s) + (size_t)el * MS();
         Real acc = Real(0);
+        if constexpr (MMAX > 0) {
 #pragma unroll
-        for (int m = 0; m < MMAX; m++)
-          if (m < M) acc += cf[m] * iv[m];
+          for (int m = 0; m < MMAX; m++)
+            if (m < M) acc += cf[m] * iv[m];
+        } else {
+          for (int m = 0; m < M; m++) acc += cf[m] * iv[m];
+        }
         w[le * S.nbasis + f] = acc;
       }
       __syncwarp();
       int total = 0;
-      for (int k = kbeg; k < kend; k++) total += S.pp_aip[S.atom_type[it[k].a]];
-      int k = kbeg, qoff = 0;  // running item cursor for this lane's points
+      for (int k = 0; k < nitems; k++) total += S.pp_aip[S.atom_type[it[k].a]];
+      int k = 0, qoff = 0;  // running item cursor for this lane's points
       for (int p = lane; p < total; p += 32) {
         while (p >= qoff + S.pp_aip[S.atom_type[it[k].a]]) { qoff += S.pp_aip[S.atom_type[it[k].a]]; k++; }
         const PPItem& I = it[k];
@@ -461,7 +479,6 @@ struct Walker {
         vnl += ts * ratio;
       }
       __syncwarp();
-      kbeg = kend;
     }
     return warp_sum(vloc) + warp_sum(vnl);
   }
@@ -504,12 +521,14 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
   __syncthreads();
 
   const int wid = blockIdx.x * wpc + warp;
+  constexpr bool HBM = MMAX == 0;  // walker worked on in place in HBM
   if (wid < P.nwalk) {
-    unsigned char* wb = smem + moc_bytes + (size_t)warp * L.bytes;
-    Walker<Real, MMAX, TB> W{S, L, wb, moc_s, lane};
+    unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
+    unsigned char* wb = HBM ? gstate : smem + moc_bytes + (size_t)warp * L.bytes;
+    unsigned char* sb = HBM ? P.scratch + (size_t)wid * L.scratch_bytes : wb + L.state_bytes;
+    Walker<Real, MMAX, TB> W{S, L, wb, sb, moc_s, lane};
     const int N = S.nelec;
     double* Rp = W.R();
-    unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
     const uint64_t step0 = P.dyn_step ? (uint64_t)P.etrial[DYN_STEP] : P.step0;
     int refresh = P.refresh;
     if (refresh == 2) {
@@ -527,7 +546,7 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
       W.recompute();
       if (lane == 0 && mode == KM_STEPS) { W.sc()->eold = keep_e; W.sc()->weight = keep_w; }
       __syncwarp();
-    } else {
+    } else if constexpr (!HBM) {
       // resident state: one coalesced copy HBM -> shared memory
       const int4* src = (const int4*)gstate;
       int4* dst = (int4*)wb;
@@ -659,9 +678,11 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
       // write back positions and the resident state
       __syncwarp();
       for (int i = lane; i < 3 * N; i += 32) P.R[(size_t)wid * 3 * N + i] = Rp[i];
-      int4* dst = (int4*)gstate;
-      const int4* src = (const int4*)wb;
-      for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
+      if constexpr (!HBM) {
+        int4* dst = (int4*)gstate;
+        const int4* src = (const int4*)wb;
+        for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
+      }
     }
   }
   if constexpr (mode == KM_STEPS) {
@@ -670,6 +691,7 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
   }
 }
 
+#ifndef QWG_WALKERS_ONLY  // population-control kernels live in the engine translation unit
 // ---------------------------------------------------------------------------
 // DMC population control on one CTA: E_T feedback (Dmc_method::updateEtrial,
 // :780-797), constant-population split/kill pairing (match_walkers,
@@ -836,5 +858,7 @@ __global__ void k_init_weights(unsigned char* state, int nwalk, int state_bytes,
   s->weight = 1.0;
   s->eold = eloc[w];
 }
+
+#endif  // QWG_WALKERS_ONLY
 
 }  // namespace qwg

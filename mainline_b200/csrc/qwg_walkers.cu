@@ -1,0 +1,58 @@
+// One walker-kernel family: compiled once per (QWG_REAL, QWG_MM) pair by the
+// build (e.g. -DQWG_REAL=float -DQWG_MM=32).
+#include <map>
+#include <mutex>
+
+#define QWG_WALKERS_ONLY
+#include "qwg_launch.cuh"
+
+#if !defined(QWG_REAL) || !defined(QWG_MM)
+#error "qwg_walkers.cu is compiled with -DQWG_REAL=<double|float> -DQWG_MM=<8|16|32|0>"
+#endif
+
+namespace qwg {
+namespace {
+
+// Raise a kernel's dynamic shared-memory limit once to the largest size any
+// context asked for (never during a stream capture: callers make a plain
+// launch of every kernel before capturing it).
+template <class K>
+cudaError_t ensure_smem_attr(K kern, size_t bytes) {
+  static std::mutex mu;
+  static std::map<const void*, size_t> done;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& have = done[(const void*)kern];
+  if (bytes > have) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    have = bytes;
+  }
+  return cudaSuccess;
+}
+
+template <typename Real, int MM, int MODE>
+cudaError_t launch_mode(const DevSys<Real>& S, const WLayout& L, const StepParams& P, const EvalIO& io, int nwalk,
+                        int wpc, size_t smem, cudaStream_t stream) {
+  auto kern = S.has_tb ? k_walkers<Real, MM, MODE, true> : k_walkers<Real, MM, MODE, false>;
+  cudaError_t e = ensure_smem_attr(kern, smem);
+  if (e != cudaSuccess) return e;
+  const int grid = (nwalk + wpc - 1) / wpc;
+  kern<<<grid, 32 * wpc, smem, stream>>>(S, L, P, io);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+template <typename Real, int MM>
+cudaError_t launch_walker_kernels(const DevSys<Real>& S, const WLayout& L, const StepParams& P, const EvalIO& io,
+                                  int mode, int nwalk, int wpc, size_t smem, cudaStream_t stream) {
+  if (mode == KM_EVAL) return launch_mode<Real, MM, KM_EVAL>(S, L, P, io, nwalk, wpc, smem, stream);
+  if (mode == KM_RATIO) return launch_mode<Real, MM, KM_RATIO>(S, L, P, io, nwalk, wpc, smem, stream);
+  return launch_mode<Real, MM, KM_STEPS>(S, L, P, io, nwalk, wpc, smem, stream);
+}
+
+template cudaError_t launch_walker_kernels<QWG_REAL, QWG_MM>(const DevSys<QWG_REAL>&, const WLayout&,
+                                                             const StepParams&, const EvalIO&, int, int, int, size_t,
+                                                             cudaStream_t);
+
+}  // namespace qwg

@@ -25,7 +25,8 @@ MIXED = 1
 
 EXPORTS = [
     "qwg_version", "qwg_last_error", "qwg_create", "qwg_destroy", "qwg_get_info", "qwg_inspect_deck",
-    "qwg_inspect_spline", "qwg_set_walkers", "qwg_get_walkers", "qwg_set_walkers_device", "qwg_eval",
+    "qwg_inspect_spline", "qwg_set_walkers", "qwg_get_walkers", "qwg_set_walkers_device",
+    "qwg_get_walker_scalars", "qwg_eval",
     "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
     "qwg_launch_count", "qwg_reset_launch_count",
@@ -89,6 +90,7 @@ def load_library(path: str = LIB_PATH):
         "qwg_set_walkers": (C.c_int, [C.c_void_p, dp, C.c_int]),
         "qwg_get_walkers": (C.c_int, [C.c_void_p, dp, C.c_int]),
         "qwg_set_walkers_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+        "qwg_get_walker_scalars": (C.c_int, [C.c_void_p, dp, dp, C.c_int]),
         "qwg_eval": (C.c_int, [C.c_void_p, dp, P(EvalOut)]),
         "qwg_ratio": (C.c_int, [C.c_void_p, P(C.c_int), dp, dp, dp, dp, dp]),
         "qwg_vmc_block": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_int, P(BlockStats)]),
@@ -200,6 +202,15 @@ class Engine:
         R = np.zeros((self.nwalk, self.nelec, 3))
         self._check(self.lib.qwg_get_walkers(self.h, _ptr(R), self.nwalk), "qwg_get_walkers")
         return R
+
+    def walker_scalars(self):
+        """(local energy, DMC weight) of every walker after the last step."""
+        e, w = np.zeros(self.nwalk), np.zeros(self.nwalk)
+        self._check(self.lib.qwg_get_walker_scalars(self.h, _ptr(e), _ptr(w), self.nwalk), "qwg_get_walker_scalars")
+        return e, w
+
+    def last_energies(self) -> np.ndarray:
+        return self.walker_scalars()[0]
 
     def eval(self, rot: np.ndarray | None = None) -> EvalResult:
         W, N = self.nwalk, self.nelec

@@ -217,7 +217,7 @@ DIAMOND_FRAC = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
 
 
 def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff: float = 16.0,
-                   name: str = "diamond8", method: str | None = None) -> Deck:
+                   name: str = "diamond8", method: str | None = None, supercell=(1, 1, 1)) -> Deck:
     """Simple-cubic 8-atom diamond-like cell (lattice constant ``a`` bohr) of
     Z_eff=4 pseudo-atoms, 32 electrons (16 up, 16 down).  Per atom 13 periodic
     Gaussians (4 S + 3 P shells, 3 primitives, exponents log-uniform in
@@ -226,17 +226,20 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
     reference's alpha = 5 / smallest cell height); Jastrow with e-e
     (CUTOFF_CUSP), e-n (POLYPADE, 4 coefficients) and e-e-n (8 coefficients)
     terms, all cut off inside half the cell (3.3 bohr) so the minimum-image
-    Jastrow is smooth."""
+    Jastrow is smooth.  ``supercell`` = (n1, n2, n3) repeats the cell along
+    the three axes (16 up + 16 down electrons per repeat), e.g. (2, 2, 2) is
+    the 64-atom, 512-electron cell with a = 13.48 bohr."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
-    label, charge, nup, ndown = "X", 4, 16, 16
+    ncell = int(np.prod(supercell))
+    label, charge, nup, ndown = "X", 4, 16 * ncell, 16 * ncell
     shells = []
     for sym, n in (("S", 4), ("P", 3)):
         for _ in range(n):
             ex = np.exp(rng.uniform(np.log(0.1), np.log(5.0), size=3))
             shells.append((sym, ex, rng.uniform(0.1, 1.0, size=3)))
     nper = sum(SHELL_NFUNC[s] for s, _, _ in shells)
-    natoms = len(DIAMOND_FRAC)
+    natoms = len(DIAMOND_FRAC) * ncell
     nb = natoms * nper
     cup = _random_orthonormal(rng, nb, nup)
     cdn = _random_orthonormal(rng, nb, ndown)
@@ -245,7 +248,9 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
     pp = _pseudo_text(rng, label, charge)
     orb = os.path.join(outdir, f"{name}.orb")
     _write_orb(orb, np.concatenate([cup, cdn], axis=1), [nper] * natoms)
-    pos = DIAMOND_FRAC * a
+    pos = np.concatenate([(DIAMOND_FRAC + np.array([i, j, k])) * a for i in range(supercell[0])
+                          for j in range(supercell[1]) for k in range(supercell[2])])
+    edge = [a * n for n in supercell]
     rc = 3.3
     jas = "\n".join([
         "JASTROW2",
@@ -275,9 +280,9 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
         f"RANDOMSEED {{ {1 + seed % 100000} {7 + seed % 7919} }}",
         "SYSTEM { PERIODIC",
         f"  NSPIN {{ {nup} {ndown} }}",
-        f"  LATTICEVEC {{ {a} 0 0  0 {a} 0  0 0 {a} }}",
+        f"  LATTICEVEC {{ {_fmt(edge[0])} 0 0  0 {_fmt(edge[1])} 0  0 0 {_fmt(edge[2])} }}",
         "  ORIGIN { 0 0 0 }",
-        f"  CUTOFF_DIVIDER {_fmt(a / image_cutoff)}",
+        f"  CUTOFF_DIVIDER {_fmt(min(edge) / image_cutoff)}",
         "  EWALD_GMAX 8",
     ] + [f"  ATOM {{ {label} {charge} COOR {_fmt(p[0])} {_fmt(p[1])} {_fmt(p[2])} }}" for p in pos] + [
         "}",
@@ -303,7 +308,7 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
     with open(path, "w") as fh:
         fh.write(deck)
     return Deck(path=path, orb_path=orb, nup=nup, ndown=ndown, natoms=natoms, nbasis=nb, kind=name, seed=seed,
-                extra={"a": a, "atoms": pos})
+                extra={"a": a, "cell": edge, "atoms": pos})
 
 
 MAX_BATCH_ELECTRONS = 64  # the warp-per-walker kernels hold <= 32 electrons per spin
@@ -408,7 +413,7 @@ def read_deck(path: str) -> Deck:
     positions, lattice edge), enough to draw configurations for it."""
     words = open(path).read().replace("{", " { ").replace("}", " } ").split()
     nup = ndn = 0
-    atoms, a = [], None
+    atoms, cell = [], None
     for i, w in enumerate(words):
         u = w.upper()
         if u == "NSPIN":
@@ -416,10 +421,11 @@ def read_deck(path: str) -> Deck:
         elif u == "COOR":
             atoms.append([float(words[i + 1]), float(words[i + 2]), float(words[i + 3])])
         elif u == "LATTICEVEC":
-            a = float(words[i + 2])
+            v = [float(x) for x in words[i + 2:i + 11]]
+            cell = [v[0], v[4], v[8]]
     extra = {"atoms": np.array(atoms)}
-    if a is not None:
-        extra = {"a": a}
+    if cell is not None:
+        extra = {"a": cell[0], "cell": cell}
     return Deck(path=path, orb_path="", nup=nup, ndown=ndn, natoms=len(atoms), nbasis=0,
                 kind=os.path.splitext(os.path.basename(path))[0], seed=0, extra=extra)
 
@@ -428,8 +434,9 @@ def random_configs(deck: Deck, nconf: int, seed: int, spread: float = 1.2) -> np
     """Seeded electron configurations [nconf, nelec, 3]: each electron sits
     near a random atom with a Gaussian spread (bohr)."""
     rng = np.random.default_rng(seed)
-    if "a" in deck.extra:  # periodic cell: uniform in the cell
-        return rng.uniform(0.0, deck.extra["a"], size=(nconf, deck.nelec, 3))
+    if "a" in deck.extra:  # periodic (orthorhombic) cell: uniform in the cell
+        edge = np.asarray(deck.extra.get("cell", [deck.extra["a"]] * 3), dtype=float)
+        return rng.uniform(0.0, 1.0, size=(nconf, deck.nelec, 3)) * edge
     atoms = deck.extra.get("atoms", np.array([[0.0, 0.0, -1.0375], [0.0, 0.0, 1.0375]]))
     which = rng.integers(0, len(atoms), size=(nconf, deck.nelec))
     return atoms[which] + rng.normal(0.0, spread, size=(nconf, deck.nelec, 3))

@@ -27,16 +27,18 @@ import refrun  # noqa: E402
 NCONF = 256
 NMOVE = 2
 WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseudo=True), 12),
-             ("diamond8", dict(periodic=True), 13), ("mol43", dict(nelec=43), 14)]
+             ("diamond8", dict(periodic=True), 13), ("mol43", dict(nelec=43), 14),
+             ("mol72", dict(nelec=72), 15), ("cell32", dict(periodic=True, supercell=(2, 2, 1)), 16)]
 
 
 def make(name, kw, seed):
     if kw.get("periodic"):
-        deck = systems.write_periodic(HERE, seed=seed, name=name)
-        nconf = 64
-    elif "nelec" in kw:  # one molecule of the batched-uneven workload (odd electron count)
+        sc = kw.get("supercell", (1, 1, 1))
+        deck = systems.write_periodic(HERE, seed=seed, name=name, supercell=sc)
+        nconf = 64 if sc == (1, 1, 1) else 16
+    elif "nelec" in kw:  # molecules of the batched-uneven workload (odd count; above 32 per spin)
         deck = systems.write_molecule(HERE, name, seed, kw["nelec"])
-        nconf = 64
+        nconf = 64 if kw["nelec"] < 64 else 32
     else:
         deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
         nconf = NCONF
