@@ -67,6 +67,7 @@ typedef struct {
   int precision;
   int walkers_per_cta; /* launch shape picked at create time */
   double ion_ion;      /* constant ion-ion energy */
+  unsigned long long device_bytes; /* device memory a context of max_walkers holds */
 } qwg_info;
 
 /* Per-walker outputs of qwg_eval (host arrays, caller-owned, sized by nw). */
@@ -119,6 +120,11 @@ int qwg_get_info(const qwg_ctx* ctx, qwg_info* info);
 /* Host-side table check without a GPU: parse the deck and build the device
  * tables on the host only; returns sizes through info.  Used by CPU tests. */
 int qwg_inspect_deck(const char* deck_path, qwg_info* info, char* err, int errlen);
+/* Device memory (bytes) qwg_create would hold for this deck, precision and
+ * walker count, computed on the host from the same layout (tables, walker
+ * state, scratch, DMC buffers).  No counterpart in the reference, which has
+ * no device memory; used for admission control. */
+int qwg_footprint(const char* deck_path, int precision, int max_walkers, unsigned long long* bytes);
 /* Radial spline table of basis shell s (host copy, [npts][4]); npts returned. */
 int qwg_inspect_spline(const char* deck_path, int shell, double* coef, int maxpts, int* npts,
                        double* spacing, double* cutoff);
@@ -162,6 +168,9 @@ int qwg_dmc_block(qwg_ctx* ctx, qwg_block_stats* stats);
  * streams overlap on the GPU (Dmc_method::runWithVariables, one block). */
 int qwg_dmc_block_async(qwg_ctx* ctx);
 int qwg_dmc_block_wait(qwg_ctx* ctx, qwg_block_stats* stats);
+/* 1 when the block in flight has finished (qwg_dmc_block_wait returns at
+ * once), 0 while it runs; negative error code otherwise.  Does not block. */
+int qwg_dmc_block_ready(qwg_ctx* ctx);
 
 /* VMC block that allocates no device memory.
  *

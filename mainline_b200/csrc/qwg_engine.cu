@@ -378,6 +378,22 @@ static void make_layout(qwg_ctx* c) {
   if (c->smem_bytes > 227 * 1024) throw InputError("system too large for the shared-memory walker kernel");
 }
 
+// Device bytes a context holds for max_walkers walkers (the allocations of
+// qwg_create plus the evaluation buffers qwg_dmc_init sizes).
+static size_t footprint_bytes(const qwg_ctx* c, int max_walkers) {
+  const HostSystem& H = c->H;
+  const size_t rs = c->precision == QWG_FP64 ? 8 : 4, N = H.nelec, W = max_walkers;
+  size_t total4 = 0;
+  for (size_t o = 0; o < H.obj_first.size(); o++) total4 += (size_t)H.spline_npts * H.obj_count[o];
+  const size_t ms = mo_stride_for(c->mmax, std::max(H.nmo[0], H.nmo[1]));
+  size_t b = total4 * 4 * (8 + rs) + 2 * (size_t)H.nbasis * ms * rs + H.shells.size() * 32 +
+             H.image_pos.size() * 8 + H.gvec.size() * 8 + 3 * H.gweight.size() * 8;
+  b += W * (2 * 3 * N * 8 + 2 * (size_t)c->L.state_bytes + (c->mmax == 0 ? (size_t)c->L.scratch_bytes : 0) + 20);
+  b += W * 8 * (9 + 5 + 4 * N);  // evaluation outputs (qwg_eval / qwg_dmc_init)
+  b += sizeof(BlockAcc) * 1024 + DYN_COUNT * 8 + (size_t)kHistCap * 8 + 16 * 8;
+  return b;
+}
+
 // Raise a kernel's dynamic shared-memory limit once to the largest size any
 // context asked for (never during a stream capture: callers make a plain
 // launch of every kernel before capturing it).
@@ -615,6 +631,23 @@ int qwg_inspect_deck(const char* deck_path, qwg_info* info, char* err, int errle
   }
 }
 
+int qwg_footprint(const char* deck_path, int precision, int max_walkers, unsigned long long* bytes) {
+  if (!deck_path || !bytes || max_walkers <= 0) return QWG_ERR_ARG;
+  if (precision != QWG_FP64 && precision != QWG_MIXED) return QWG_ERR_ARG;
+  try {
+    std::unique_ptr<qwg_ctx> c(new qwg_ctx());
+    c->precision = precision;
+    c->H = build_system(deck_path);
+    c->mmax = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
+    if (c->mmax < 0) return QWG_ERR_INPUT;
+    make_layout(c.get());
+    *bytes = footprint_bytes(c.get(), max_walkers);
+    return QWG_OK;
+  } catch (const std::exception&) {
+    return QWG_ERR_INPUT;
+  }
+}
+
 int qwg_inspect_spline(const char* deck_path, int shell, double* coef, int maxpts, int* npts, double* spacing,
                        double* cutoff) {
   try {
@@ -703,6 +736,7 @@ int qwg_get_info(const qwg_ctx* c, qwg_info* info) {
   info->nbasis = H.nbasis; info->nshell = (int)H.shells.size(); info->nmo_up = H.nmo[0]; info->nmo_down = H.nmo[1];
   info->has_pseudo = H.has_pp; info->max_walkers = c->max_walkers; info->precision = c->precision;
   info->walkers_per_cta = c->wpc; info->ion_ion = H.ion_ion;
+  info->device_bytes = footprint_bytes(c, c->max_walkers);
   return QWG_OK;
 }
 
@@ -993,6 +1027,15 @@ int qwg_dmc_block_wait(qwg_ctx* c, qwg_block_stats* stats) {
     }
     return QWG_OK;
   });
+}
+
+int qwg_dmc_block_ready(qwg_ctx* c) {
+  if (!c) return QWG_ERR_ARG;
+  if (!c->block_pending) return fail(c, QWG_ERR_STATE, "qwg_dmc_block_ready: no block in flight");
+  cudaError_t e = cudaEventQuery(c->ev1);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) return 0;
+  return fail(c, QWG_ERR_CUDA, std::string("qwg_dmc_block_ready: ") + cudaGetErrorString(e));
 }
 
 int qwg_dmc_block(qwg_ctx* c, qwg_block_stats* stats) {

@@ -29,7 +29,9 @@ EXPORTS = [
     "qwg_get_walker_scalars", "qwg_eval",
     "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
-    "qwg_launch_count", "qwg_reset_launch_count",
+    "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready",
+    "qwg_server_create", "qwg_server_destroy", "qwg_server_submit", "qwg_server_progress",
+    "qwg_server_get_status", "qwg_server_last_error",
 ]
 
 
@@ -41,7 +43,7 @@ class Info(C.Structure):
     _fields_ = [("nelec", C.c_int), ("nup", C.c_int), ("ndown", C.c_int), ("natoms", C.c_int),
                 ("nbasis", C.c_int), ("nshell", C.c_int), ("nmo_up", C.c_int), ("nmo_down", C.c_int),
                 ("has_pseudo", C.c_int), ("max_walkers", C.c_int), ("precision", C.c_int),
-                ("walkers_per_cta", C.c_int), ("ion_ion", C.c_double)]
+                ("walkers_per_cta", C.c_int), ("ion_ion", C.c_double), ("device_bytes", C.c_ulonglong)]
 
 
 class EvalOut(C.Structure):
@@ -64,6 +66,23 @@ class DmcParams(C.Structure):
                 ("feedback", C.c_double), ("max_poss_weight", C.c_double),
                 ("branch_start_cutoff", C.c_double), ("refresh_interval", C.c_int),
                 ("deterministic_pp", C.c_int), ("seed", C.c_uint64)]
+
+
+class JobDesc(C.Structure):
+    _fields_ = [("deck", C.c_char_p), ("precision", C.c_int), ("nwalkers", C.c_int), ("nblocks", C.c_int),
+                ("vmc_blocks", C.c_int), ("vmc_steps", C.c_int), ("vmc_timestep", C.c_double),
+                ("vmc_seed", C.c_uint64), ("R", C.POINTER(C.c_double)), ("dmc", DmcParams)]
+
+
+class BlockEvent(C.Structure):
+    _fields_ = [("job", C.c_int), ("block", C.c_int), ("latency_ms", C.c_double), ("queue_ms", C.c_double),
+                ("stats", BlockStats)]
+
+
+class ServerStatus(C.Structure):
+    _fields_ = [("queued", C.c_int), ("active", C.c_int), ("finished", C.c_int), ("failed", C.c_int),
+                ("bytes_in_use", C.c_ulonglong), ("budget_bytes", C.c_ulonglong), ("blocks_done", C.c_longlong),
+                ("walker_steps", C.c_double)]
 
 
 _lib = None
@@ -106,6 +125,14 @@ def load_library(path: str = LIB_PATH):
         "qwg_autotune": (C.c_int, [C.c_void_p, P(C.c_int)]),
         "qwg_launch_count": (C.c_longlong, [C.c_void_p]),
         "qwg_reset_launch_count": (None, [C.c_void_p]),
+        "qwg_footprint": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P(C.c_ulonglong)]),
+        "qwg_dmc_block_ready": (C.c_int, [C.c_void_p]),
+        "qwg_server_create": (C.c_int, [C.c_ulonglong, C.c_int, P(C.c_void_p)]),
+        "qwg_server_destroy": (C.c_int, [C.c_void_p]),
+        "qwg_server_submit": (C.c_int, [C.c_void_p, P(JobDesc), P(C.c_int)]),
+        "qwg_server_progress": (C.c_int, [C.c_void_p, P(BlockEvent), C.c_int, P(C.c_int)]),
+        "qwg_server_get_status": (C.c_int, [C.c_void_p, P(ServerStatus)]),
+        "qwg_server_last_error": (C.c_char_p, [C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -299,6 +326,79 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             self.lib.qwg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def footprint(deck_path: str, precision: int, walkers: int) -> int:
+    """Device bytes a context of this deck, precision and walker count holds."""
+    lib = load_library()
+    b = C.c_ulonglong(0)
+    rc = lib.qwg_footprint(deck_path.encode(), precision, walkers, C.byref(b))
+    if rc != 0:
+        raise QwgError(f"qwg_footprint failed ({rc}) for {deck_path}")
+    return int(b.value)
+
+
+class Server:
+    """Continuous-batching DMC job server (include/qwg_server.h)."""
+
+    def __init__(self, budget_bytes: int, max_active: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.qwg_server_create(budget_bytes, max_active, C.byref(h))
+        if rc != 0:
+            raise QwgError(f"qwg_server_create failed ({rc})")
+        self.h = h
+        self._ev = (BlockEvent * 256)()
+
+    def submit(self, deck: str, R: np.ndarray, precision: int, nblocks: int, dmc: dict,
+               vmc_blocks: int = 2, vmc_steps: int = 10, vmc_timestep: float = 0.3, vmc_seed: int = 1) -> int:
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        p = DmcParams()
+        d = dict(timestep=0.01, nstep=10, feedback_interval=5, feedback=1.0, max_poss_weight=7.0,
+                 branch_start_cutoff=10.0, refresh_interval=32, deterministic_pp=0, seed=1)
+        d.update(dmc)
+        for k, v in d.items():
+            setattr(p, k, v)
+        j = JobDesc(deck=deck.encode(), precision=precision, nwalkers=R.shape[0], nblocks=nblocks,
+                    vmc_blocks=vmc_blocks, vmc_steps=vmc_steps, vmc_timestep=vmc_timestep, vmc_seed=vmc_seed,
+                    R=_ptr(R), dmc=p)
+        jid = C.c_int(-1)
+        rc = self.lib.qwg_server_submit(self.h, C.byref(j), C.byref(jid))
+        if rc != 0:
+            raise QwgError(f"qwg_server_submit failed ({rc}): {self.lib.qwg_server_last_error(self.h).decode()}")
+        return jid.value
+
+    def progress(self) -> list:
+        """One scheduling pass; returns the finished blocks as dicts."""
+        out = []
+        while True:
+            n = C.c_int(0)
+            rc = self.lib.qwg_server_progress(self.h, self._ev, len(self._ev), C.byref(n))
+            if rc != 0:
+                raise QwgError(f"qwg_server_progress failed ({rc}): {self.lib.qwg_server_last_error(self.h).decode()}")
+            for i in range(n.value):
+                e = self._ev[i]
+                d = e.stats.as_dict()
+                d.update(job=e.job, block=e.block, latency_ms=e.latency_ms, queue_ms=e.queue_ms)
+                out.append(d)
+            if n.value < len(self._ev):
+                return out
+
+    def status(self) -> dict:
+        st = ServerStatus()
+        self.lib.qwg_server_get_status(self.h, C.byref(st))
+        return {k: getattr(st, k) for k, _ in ServerStatus._fields_}
+
+    def close(self):
+        if self.h:
+            self.lib.qwg_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

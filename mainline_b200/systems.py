@@ -311,7 +311,7 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
                 extra={"a": a, "cell": edge, "atoms": pos})
 
 
-MAX_BATCH_ELECTRONS = 64  # the warp-per-walker kernels hold <= 32 electrons per spin
+MAX_BATCH_ELECTRONS = 192  # 32 atoms of Z_eff <= 6
 
 
 def write_molecule(outdir: str, name: str, seed: int, nelec: int, max_atoms: int = 32) -> Deck:
@@ -397,7 +397,8 @@ def write_batch(outdir: str, nsys: int = 64, seed: int = 777, emin: int = 8,
                 emax: int = MAX_BATCH_ELECTRONS) -> list:
     """The batched-uneven workload: ``nsys`` seeded molecules with electron
     counts log-uniform in [emin, emax] and 512-4096 walkers each (log-uniform);
-    returns [(deck, walkers)]."""
+    returns [(deck, walkers)].  With 2-32 atoms of Z_eff 1-6 a neutral
+    molecule has at most 192 electrons, the default upper end."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(nsys):

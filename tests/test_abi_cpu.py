@@ -1,5 +1,5 @@
 """CPU-side checks of the C-ABI library: it loads without a GPU, exports every
-symbol include/qwg.h declares, and its host table builder (deck parser +
+symbol include/*.h declares, and its host table builder (deck parser +
 spline fit) reproduces the oracle's tables."""
 import os
 import re
@@ -11,11 +11,12 @@ from conftest import GOLDEN, ROOT
 import qworacle
 from mainline_b200 import engine
 
-HEADER = os.path.join(ROOT, "include", "qwg.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in sorted(os.listdir(os.path.join(ROOT, "include")))
+           if h.endswith(".h")]
 
 
 def _declared():
-    txt = open(HEADER).read()
+    txt = "".join(open(h).read() for h in HEADERS)
     return sorted(set(re.findall(r"\b(qwg_[a-z_]+)\s*\(", txt)))
 
 
