@@ -96,6 +96,15 @@ def make_workload(tmpdir):
     return deck, R0
 
 
+def _traffic_per_launch():
+    """DRAM bytes (read + write) of one walker-step kernel launch of this
+    workload, from the committed ncu summary (profiles/traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    return json.load(open(p)).get("k_walkers_mixed_dmc", {}).get("dram_bytes_per_launch")
+
+
 def algorithmic_bytes_per_walker_step(N, M, nb, precision_bytes):
     """Resident walker state read + written once per step (positions, both
     inverse matrices, MO gradient/Laplacian rows, Jastrow sums, scalars)."""
@@ -112,7 +121,10 @@ def run_engine(args, rank, world):
     deck, R0 = make_workload(tmp)
     stream = torch.cuda.Stream(device=dev)
     results = {}
-    for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
+    arms = (("fp64", engine.FP64), ("mixed", engine.MIXED))
+    if args.precision != "both":
+        arms = tuple(a for a in arms if a[0] == args.precision)
+    for label, prec in arms:
         E = engine.Engine(deck.path, prec, max_walkers=NWALK, stream=stream.cuda_stream)
         E.set_walkers(R0)
         for b in range(3):  # VMC equilibration from the seeded start
@@ -174,6 +186,74 @@ def run_engine(args, rank, world):
     return results, e2e_ms, steps, deck
 
 
+def run_extras(stream, dev, seconds=30.0):
+    """Bounded samples of the other workloads, mixed precision vs FP64:
+    the periodic cell (DMC), a batch of uneven molecules advanced by one
+    graph per block, and the Poisson job stream through the job server."""
+    import torch
+    from mainline_b200 import engine, serving, systems
+    tmp = tempfile.mkdtemp(prefix="qwg_extra_")
+    out = {}
+    # periodic: 8-atom cell, 32 electrons, tau 0.005, 16384 walkers
+    cell = systems.write_periodic(tmp, seed=13, name="diamond8_bench")
+    Rc = systems.random_configs(cell, 16384, seed=SEED)
+    per = {}
+    for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
+        E = engine.Engine(cell.path, prec, max_walkers=16384, stream=stream.cuda_stream)
+        E.set_walkers(Rc)
+        E.vmc_block(5, 0.3, seed=SEED + 1)
+        E.dmc_init(timestep=0.005, nstep=10, seed=SEED + 2)
+        E.dmc_block()
+        st = E.dmc_block()
+        per[label] = {"walker_steps_per_s": 16384 * 10 / (st["block_ms"] / 1e3), "block_ms": st["block_ms"],
+                      "energy": st["energy"]}
+        E.close()
+    per["mixed_vs_fp64"] = per["mixed"]["walker_steps_per_s"] / per["fp64"]["walker_steps_per_s"]
+    per["config"] = "8 Z_eff=4 atoms, a=6.74 bohr, 32 electrons, 104 basis fns + images, Ewald, e-e-n Jastrow; " \
+                    "16384 walkers, tau=0.005, 10-step blocks"
+    out["periodic"] = per
+    # batched uneven molecules: 16 systems, 8-192 electrons, 512-4096 walkers
+    mols = systems.write_batch(os.path.join(tmp, "batch"), nsys=16, seed=SEED % 1000)
+    bat = {}
+    for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
+        engines = []
+        for i, (d, nw) in enumerate(mols):
+            E = engine.Engine(d.path, prec, max_walkers=nw)
+            E.set_walkers(systems.random_configs(d, nw, seed=SEED + i))
+            E.vmc_block(3, 0.3, seed=SEED + i)
+            E.dmc_init(timestep=0.01, nstep=5, seed=SEED + 100 + i)
+            engines.append(E)
+        B = engine.Batch(engines)
+        B.block()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        sts = B.block()
+        wall = time.perf_counter() - t0
+        ws = sum(s["nwalkers"] * s["nsteps"] for s in sts)
+        bat[label] = {"walker_steps_per_s": ws / wall, "block_wall_ms": wall * 1e3}
+        B.close()
+        for E in engines:
+            E.close()
+    bat["mixed_vs_fp64"] = bat["mixed"]["walker_steps_per_s"] / bat["fp64"]["walker_steps_per_s"]
+    bat["config"] = ("16 seeded molecules, 2-32 atoms Z_eff 1-6, electrons log-uniform 8-192 (" +
+                     ",".join(str(d.nelec) for d, _ in mols) + "), 512-4096 walkers, one 5-step DMC block of "
+                     "every system per graph launch; host wall time")
+    out["batched"] = bat
+    # serving: Poisson 2 jobs/s, bounded window
+    jobs = serving.workload(os.path.join(tmp, "serve"), njobs=12, seed=SEED % 997, emin=16, emax=64)
+    srv = {}
+    for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
+        r = serving.run(jobs, prec, budget_bytes=120 << 30, nstep=5, time_limit=seconds)
+        r.pop("events")
+        srv[label] = r
+    srv["mixed_vs_fp64"] = srv["mixed"]["walker_steps_per_s"] / srv["fp64"]["walker_steps_per_s"]
+    srv["config"] = (f"12 jobs, Poisson 2/s, seeded molecules and 8-atom cells of 16-64 electrons, 1024-8192 "
+                     f"walkers, 20-100 blocks of 5 steps, 120 GiB admission budget; first {seconds:.0f} s of the "
+                     "stream (jobs still running at the limit are counted up to it)")
+    out["serving"] = srv
+    return out
+
+
 def cpu_reference(deck_path, seconds_target=20.0, cores=None):
     """Reference qwalk (oracle/_ref/qwalk-Linux, shipped -O3 -ffast-math flags)
     on the host cores: one process per core, DMC on the same deck.  Per-block
@@ -218,6 +298,9 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--latency-blocks", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="only the headline workload")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
+                    help="arms of the headline workload (profiling runs use one)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -248,6 +331,11 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     results, e2e_ms, steps, deck = run_engine(args, rank, world)
+    if args.precision != "both":  # profiling run: no report line
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     mx = results["mixed"]
     fp = results["fp64"]
     # max over ranks of the device time
@@ -293,11 +381,15 @@ def main():
         "e2e": {"value": NWALK * steps / (e2e_ms / 1e3), "unit": "walker-steps/s",
                 "h2d_bytes_per_step": NWALK * N * 3 * 8 / steps, "d2h_bytes_per_step": (NWALK * N * 3 * 8 + 96) / steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": src, "traffic": None,
+                     "peak_source": src, "traffic": _traffic_per_launch(),
                      "note": "walker-step kernel; algorithmic bytes = resident state read+write per walker-step"},
         "gpu_launches": mx["launches"],
         "clocks": mx["clocks"],
     }
+    if not args.no_extras and world == 1:
+        import torch
+        dev = torch.device("cuda", 0)
+        line["workloads"] = run_extras(torch.cuda.Stream(device=dev), dev)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(os.path.abspath(deck.path))
     print(json.dumps(line))

@@ -175,6 +175,7 @@ __device__ __forceinline__ double erfc_poly(double x) {
 // work in place in HBM with one scratch region per walker.
 struct WLayout {
   int R, inv, mov, gU, lU, scal, bas, newcol, dG, Ue, lu, items, rot, wproj, wchunk, bytes;
+  int sweep_bytes;    // state + the move-phase scratch (shared memory per walker of the sweep kernel)
   int state_bytes;    // persistent walker state
   int scratch_bytes;  // per-walker scratch
   int mstride;        // row stride of the inverse / MO-derivative rows (orbitals, padded)
@@ -213,6 +214,7 @@ enum DynSlot {
 struct StepParams {
   int nwalk;
   int nsteps;
+  int st;               // KM_SWEEP / KM_ELOC: step of the chunk this launch performs
   int refresh;          // 1: full recompute at start, 0: load state, 2: recompute when the
                         //    chunk reaches a multiple of refresh_every steps (device counter)
   int refresh_every;

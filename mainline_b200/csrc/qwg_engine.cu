@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -73,6 +74,9 @@ struct qwg_ctx {
   int nwalk = 0;
   int mmax = 8;
   int wpc = 4;
+  int wpc_sweep = 4;        // walkers per CTA of the move-phase kernel (KM_SWEEP)
+  size_t smem_sweep = 0;
+  bool split = true;        // DMC steps as sweep + local-energy launches (else one fused launch per chunk)
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   long long launches = 0;
@@ -84,7 +88,7 @@ struct qwg_ctx {
   WLayout L{};
   size_t smem_bytes = 0;
   // walkers
-  DevBuf d_R, d_R2, d_state, d_state2, d_scratch;
+  DevBuf d_R, d_R2, d_state, d_state2, d_scratch, d_branch;
   bool state_valid = false;
   bool have_scalars = false;  // WScal.eold / weight written by a block
   // io scratch
@@ -365,11 +369,14 @@ static void make_layout(qwg_ctx* c) {
   L.wproj = o; o = align16(o + rs * H.nbasis * L.wchunk);
   L.scratch_bytes = std::max(o, move_end);
   L.bytes = L.state_bytes + L.scratch_bytes;
+  L.sweep_bytes = L.state_bytes + move_end;
   if (hbm) {
-    c->wpc = 4;
-    c->smem_bytes = 0;
+    c->wpc = c->wpc_sweep = 4;
+    c->smem_bytes = c->smem_sweep = 0;
     return;
   }
+  c->wpc_sweep = 4;
+  c->smem_sweep = (size_t)c->wpc_sweep * L.sweep_bytes;
   // walkers per CTA: up to 4 while the CTA stays under ~110 KB (2 CTAs/SM)
   int wpc = 4;
   while (wpc > 1 && (size_t)wpc * L.bytes > 110 * 1024) wpc--;
@@ -377,6 +384,17 @@ static void make_layout(qwg_ctx* c) {
   c->smem_bytes = (size_t)wpc * L.bytes;
   if (c->smem_bytes > 227 * 1024) throw InputError("system too large for the shared-memory walker kernel");
 }
+
+// Dynamic shared memory of the branching kernel for W walkers, or 0 when the
+// sort runs in global memory (populations above kBranchSmemMax walkers).
+constexpr int kBranchSmemMax = 8192;
+constexpr int kMaxDmcWalkers = 1 << 18;
+static size_t branch_bytes(int W) {
+  int p2 = 1;
+  while (p2 < W) p2 <<= 1;
+  return (size_t)p2 * (8 + 4) + (size_t)W * 4 + 16 + (size_t)W * 8;
+}
+static size_t branch_smem(int W) { return W <= kBranchSmemMax ? branch_bytes(W) : 0; }
 
 // Device bytes a context holds for max_walkers walkers (the allocations of
 // qwg_create plus the evaluation buffers qwg_dmc_init sizes).
@@ -391,6 +409,7 @@ static size_t footprint_bytes(const qwg_ctx* c, int max_walkers) {
   b += W * (2 * 3 * N * 8 + 2 * (size_t)c->L.state_bytes + (c->mmax == 0 ? (size_t)c->L.scratch_bytes : 0) + 20);
   b += W * 8 * (9 + 5 + 4 * N);  // evaluation outputs (qwg_eval / qwg_dmc_init)
   b += sizeof(BlockAcc) * 1024 + DYN_COUNT * 8 + (size_t)kHistCap * 8 + 16 * 8;
+  if (max_walkers > kBranchSmemMax) b += branch_bytes(max_walkers);
   return b;
 }
 
@@ -412,8 +431,10 @@ static void ensure_smem_attr(K kern, size_t bytes) {
 template <typename Real, int MM>
 static void launch_walkers_t(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int mode,
                              int nwalk) {
-  CK((launch_walker_kernels<Real, MM>(S, c->L, P, io, mode, nwalk, c->wpc, c->smem_bytes, c->stream)));
-  c->launches++;
+  const bool sw = mode == KM_SWEEP;
+  CK((launch_walker_kernels<Real, MM>(S, c->L, P, io, mode, nwalk, sw ? c->wpc_sweep : c->wpc,
+                                      sw ? c->smem_sweep : c->smem_bytes, c->stream)));
+  if (nwalk > 0) c->launches++;
 }
 
 static void launch_walkers(qwg_ctx* c, const StepParams& P, const EvalIO& io, int mode, int nwalk) {
@@ -515,9 +536,15 @@ static void run_branch(qwg_ctx* c, const BlockAcc* acc, int nsteps) {
   B.dyn = c->d_dyn.as<double>();
   B.src_of = c->d_src.as<int>();
   B.new_w = c->d_neww.as<double>();
-  size_t sm = (size_t)p2 * (8 + 4) + (size_t)c->nwalk * 4 + 16 + (size_t)c->nwalk * 8;
-  if (sm > 227 * 1024) throw InputError("population too large for the one-CTA branching kernel (max 8192 walkers)");
-  ensure_smem_attr(k_branch, sm);
+  size_t sm = branch_smem(c->nwalk);
+  if (sm == 0) {  // large population: keys and counts in the context's global buffer
+    B.gkey = c->d_branch.as<double>();
+    B.gidx = (int*)(B.gkey + p2);
+    B.gcnt = B.gidx + p2;
+    B.gnw = (double*)(((uintptr_t)(B.gcnt + c->nwalk) + 15) & ~(uintptr_t)15);
+  } else {
+    ensure_smem_attr(k_branch, sm);
+  }
   k_branch<<<1, 1024, sm, c->stream>>>(B);
   CK(cudaGetLastError());
   const int n3 = 3 * c->H.nelec;
@@ -558,7 +585,15 @@ static void enqueue_dmc_block(qwg_ctx* c) {
     P.branch_stop = c->branch_stop;
     P.max_weight = c->dmc.max_poss_weight;
     EvalIO io{};
-    launch_walkers(c, P, io, KM_STEPS, c->nwalk);
+    if (c->split) {
+      for (int st = 0; st < np; st++) {
+        P.st = st;
+        launch_walkers(c, P, io, KM_SWEEP, c->nwalk);
+        launch_walkers(c, P, io, KM_ELOC, c->nwalk);
+      }
+    } else {
+      launch_walkers(c, P, io, KM_STEPS, c->nwalk);
+    }
     run_branch(c, acc + ch, np);
     step += np;
   }
@@ -678,6 +713,7 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
     int mm = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
     if (mm < 0) throw InputError("more than 256 electrons of one spin: beyond this engine build");
     c->mmax = mm;
+    if (const char* sched = getenv("QWG_DMC_SCHEDULE")) c->split = strcmp(sched, "fused") != 0;
     if (stream) {
       c->stream = (cudaStream_t)stream;
     } else {
@@ -967,14 +1003,15 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
       Pw.nsteps = 0; Pw.refresh = 0; Pw.acc = acc;
       EvalIO iw{};
       launch_walkers(c, Pw, iw, KM_STEPS, W);  // same kernel variant as the block's chunks
+      launch_walkers(c, Pw, iw, KM_SWEEP, 0);  // shared-memory attributes of the split kernels
+      launch_walkers(c, Pw, iw, KM_ELOC, 0);
       CK(cudaStreamSynchronize(c->stream));
     }
-    {
-      int p2 = 1;
-      while (p2 < W) p2 <<= 1;
-      size_t sm = (size_t)p2 * (8 + 4) + (size_t)W * 4 + 16 + (size_t)W * 8;
-      if (sm > 227 * 1024) throw InputError("population too large for the one-CTA branching kernel (max 8192 walkers)");
-      ensure_smem_attr(k_branch, sm);
+    if (W > kMaxDmcWalkers) throw InputError("DMC populations above 262144 walkers are beyond this engine build");
+    if (branch_smem(W)) {
+      ensure_smem_attr(k_branch, branch_smem(W));
+    } else if (c->d_branch.n < branch_bytes(W)) {
+      c->d_branch.alloc(branch_bytes(W));
     }
     const long long l0 = c->launches;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));

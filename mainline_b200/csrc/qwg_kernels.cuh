@@ -6,7 +6,11 @@
 
 namespace qwg {
 
-enum KMode { KM_EVAL = 0, KM_RATIO = 1, KM_STEPS = 2 };
+// KM_STEPS runs whole steps (moves + local energy + weight) in one launch;
+// KM_SWEEP and KM_ELOC split one step into its two phases (the electron
+// moves; the local energy and weight), one launch each, with the same
+// arithmetic and random streams, so the two schedules give identical walks.
+enum KMode { KM_EVAL = 0, KM_RATIO = 1, KM_STEPS = 2, KM_SWEEP = 3, KM_ELOC = 4 };
 
 struct EvalIO {
   const double* rot;     // [W][9] quadrature rotations (KM_EVAL) or nullptr
@@ -524,7 +528,8 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
   constexpr bool HBM = MMAX == 0;  // walker worked on in place in HBM
   if (wid < P.nwalk) {
     unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
-    unsigned char* wb = HBM ? gstate : smem + moc_bytes + (size_t)warp * L.bytes;
+    constexpr bool SWEEP_ONLY = mode == KM_SWEEP;
+    unsigned char* wb = HBM ? gstate : smem + moc_bytes + (size_t)warp * (SWEEP_ONLY ? L.sweep_bytes : L.bytes);
     unsigned char* sb = HBM ? P.scratch + (size_t)wid * L.scratch_bytes : wb + L.state_bytes;
     Walker<Real, MMAX, TB> W{S, L, wb, sb, moc_s, lane};
     const int N = S.nelec;
@@ -535,16 +540,18 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
       const uint64_t R = (uint64_t)P.refresh_every, m = step0 % R;
       refresh = (m == 0 || m + (uint64_t)P.nsteps > R) ? 1 : 0;
     }
-    if (mode != KM_STEPS || refresh) {
+    if (mode == KM_ELOC || (mode == KM_SWEEP && P.st > 0)) refresh = 0;  // only a chunk's first sweep
+    constexpr bool STEPS = mode == KM_STEPS || mode == KM_SWEEP || mode == KM_ELOC;
+    if (!STEPS || refresh) {
       for (int i = lane; i < 3 * N; i += 32) Rp[i] = P.R[(size_t)wid * 3 * N + i];
       __syncwarp();
       if (S.periodic)
         for (int e = lane; e < N; e += 32) wrap_pos(S, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2]);
       double keep_e = 0, keep_w = 1;
-      if (mode == KM_STEPS) { keep_e = ((WScal*)(gstate + L.scal))->eold; keep_w = ((WScal*)(gstate + L.scal))->weight; }
+      if (STEPS) { keep_e = ((WScal*)(gstate + L.scal))->eold; keep_w = ((WScal*)(gstate + L.scal))->weight; }
       __syncwarp();
       W.recompute();
-      if (lane == 0 && mode == KM_STEPS) { W.sc()->eold = keep_e; W.sc()->weight = keep_w; }
+      if (lane == 0 && STEPS) { W.sc()->eold = keep_e; W.sc()->weight = keep_w; }
       __syncwarp();
     } else if constexpr (!HBM) {
       // resident state: one coalesced copy HBM -> shared memory
@@ -590,102 +597,118 @@ __global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
         io.lap[wid] = l;
       }
     } else {
-      // ---- VMC / DMC steps
+      // ---- VMC / DMC steps (KM_STEPS: P.nsteps steps; KM_SWEEP / KM_ELOC:
+      // one phase of step P.st)
       const double sqt = sqrt(P.tau);
       double nacc = 0, natt = 0;
-      double sw = 0, swe = 0, swk = 0, swv = 0, swnl = 0, swe2 = 0, nbad = 0;
+      double sw = 0, swe = 0, swk = 0, swv = 0, swnl = 0, swe2 = 0, nbad = 0, npts = 0;
       const double etr = P.dmc ? *P.etrial : 0.0;
       const double teff = P.dmc ? P.etrial[1] : 0.0;
-      for (int st = 0; st < P.nsteps; st++) {
+      const int st0 = mode == KM_STEPS ? 0 : P.st, st1 = mode == KM_STEPS ? P.nsteps : P.st + 1;
+      for (int st = st0; st < st1; st++) {
         const uint64_t step = step0 + st;
-        for (int e = 0; e < N; e++) {
-          // Split_sampler::split_driver depth 1 (Split_sample.cpp:380-478)
-          double g0[3], l0;
-          W.electron_grad(e, g0, l0);
-          double dv[3];
-          lim_drift(g0, P.tau, dv);
-          Rand4 ra = rand4(P.seed, wid, step, e, 1u);
-          Rand4 rb = rand4(P.seed, wid, step, e, 2u);
-          double ga[4];
-          box_muller(ra.u[0], ra.u[1], ga[0], ga[1]);
-          box_muller(ra.u[2], ra.u[3], ga[2], ga[3]);
-          const double ox = Rp[3 * e], oy = Rp[3 * e + 1], oz = Rp[3 * e + 2];
-          double nx = ox + ga[0] * sqt + dv[0];
-          double ny = oy + ga[1] * sqt + dv[1];
-          double nz = oz + ga[2] * sqt + dv[2];
-          double wx = nx, wy = ny, wz = nz;  // the stored position is inside the cell
-          wrap_pos(S, wx, wy, wz);
-          double ratioD, dU, g1[3], l1;
-          W.propose(e, wx, wy, wz, ratioD, dU, g1, l1);
-          // get_acceptance (Split_sample.cpp:302-373): psi ratio squared
-          // times the ratio of drift-diffusion Green's functions
-          double ratio = ratioD * exp(dU);
-          double acc;
-          if (P.dmc && ratio < 0) acc = 0;  // node restriction
-          else {
-            double bd[3];
-            lim_drift(g1, P.tau, bd);
-            double fw = 0, bw = 0;
-            fw -= (nx - ox - dv[0]) * (nx - ox - dv[0]) + (ny - oy - dv[1]) * (ny - oy - dv[1]) +
-                  (nz - oz - dv[2]) * (nz - oz - dv[2]);
-            bw -= (ox - nx - bd[0]) * (ox - nx - bd[0]) + (oy - ny - bd[1]) * (oy - ny - bd[1]) +
-                  (oz - nz - bd[2]) * (oz - nz - bd[2]);
-            acc = fmin(1.0, ratio * ratio * exp((bw - fw) / (2.0 * P.tau)));
-          }
-          natt += 1;
-          if (acc + rb.u[0] > 1.0) {
-            W.accept(e, wx, wy, wz, ratioD, dU);
-            nacc += 1;
+        if constexpr (mode != KM_ELOC) {
+          for (int e = 0; e < N; e++) {
+            // Split_sampler::split_driver depth 1 (Split_sample.cpp:380-478)
+            double g0[3], l0;
+            W.electron_grad(e, g0, l0);
+            double dv[3];
+            lim_drift(g0, P.tau, dv);
+            Rand4 ra = rand4(P.seed, wid, step, e, 1u);
+            Rand4 rb = rand4(P.seed, wid, step, e, 2u);
+            double ga[4];
+            box_muller(ra.u[0], ra.u[1], ga[0], ga[1]);
+            box_muller(ra.u[2], ra.u[3], ga[2], ga[3]);
+            const double ox = Rp[3 * e], oy = Rp[3 * e + 1], oz = Rp[3 * e + 2];
+            double nx = ox + ga[0] * sqt + dv[0];
+            double ny = oy + ga[1] * sqt + dv[1];
+            double nz = oz + ga[2] * sqt + dv[2];
+            double wx = nx, wy = ny, wz = nz;  // the stored position is inside the cell
+            wrap_pos(S, wx, wy, wz);
+            double ratioD, dU, g1[3], l1;
+            W.propose(e, wx, wy, wz, ratioD, dU, g1, l1);
+            // get_acceptance (Split_sample.cpp:302-373): psi ratio squared
+            // times the ratio of drift-diffusion Green's functions
+            double ratio = ratioD * exp(dU);
+            double acc;
+            if (P.dmc && ratio < 0) acc = 0;  // node restriction
+            else {
+              double bd[3];
+              lim_drift(g1, P.tau, bd);
+              double fw = 0, bw = 0;
+              fw -= (nx - ox - dv[0]) * (nx - ox - dv[0]) + (ny - oy - dv[1]) * (ny - oy - dv[1]) +
+                    (nz - oz - dv[2]) * (nz - oz - dv[2]);
+              bw -= (ox - nx - bd[0]) * (ox - nx - bd[0]) + (oy - ny - bd[1]) * (oy - ny - bd[1]) +
+                    (oz - nz - bd[2]) * (oz - nz - bd[2]);
+              acc = fmin(1.0, ratio * ratio * exp((bw - fw) / (2.0 * P.tau)));
+            }
+            natt += 1;
+            if (acc + rb.u[0] > 1.0) {
+              W.accept(e, wx, wy, wz, ratioD, dU);
+              nacc += 1;
+            }
           }
         }
-        // gatherData (Properties_gather.cpp:40-74)
-        Rand4 rr = rand4(P.seed, wid, step, 0xffffu, 3u);
-        double rm[9];
-        random_rotation(rr, rm);
-        double kin = W.kinetic();
-        double pot = W.coulomb();
-        double nl = S.has_pp ? W.pseudo(rm, P.deterministic_pp != 0, P.seed, wid, step) : 0.0;
-        double el = kin + pot + nl;
-        WScal* w = W.sc();
-        double wt = 1.0;
-        if (P.dmc) {
-          // Dmc_method::getWeight (Dmc_method.cpp:801-824) + weight clamp
-          double eold = w->eold;
-          double teffac = teff / 2.0;
-          double fbet = fmax(etr - el, etr - eold);
-          if (fbet > P.branch_stop) teffac = 0;
-          else if (fbet > P.branch_start)
-            teffac = teffac * (1. - (fbet - P.branch_start) / (P.branch_stop - P.branch_start));
-          wt = w->weight * exp(teffac * (etr * 2 - el - eold));
-          if (wt > P.max_weight) wt = P.max_weight;
-          if (!isfinite(el) || !isfinite(wt)) { nbad += 1; wt = 0.0; el = etr; }
-          __syncwarp();
-          if (lane == 0) { w->weight = wt; w->eold = el; }
-          __syncwarp();
-        } else {
-          if (!isfinite(el)) { nbad += 1; el = 0.0; wt = 0.0; }
-          if (lane == 0) w->eold = el;
+        if constexpr (mode != KM_SWEEP) {
+          // gatherData (Properties_gather.cpp:40-74)
+          Rand4 rr = rand4(P.seed, wid, step, 0xffffu, 3u);
+          double rm[9];
+          random_rotation(rr, rm);
+          double kin = W.kinetic();
+          double pot = W.coulomb();
+          double nl = S.has_pp ? W.pseudo(rm, P.deterministic_pp != 0, P.seed, wid, step) : 0.0;
+          double el = kin + pot + nl;
+          WScal* w = W.sc();
+          double wt = 1.0;
+          if (P.dmc) {
+            // Dmc_method::getWeight (Dmc_method.cpp:801-824) + weight clamp
+            double eold = w->eold;
+            double teffac = teff / 2.0;
+            double fbet = fmax(etr - el, etr - eold);
+            if (fbet > P.branch_stop) teffac = 0;
+            else if (fbet > P.branch_start)
+              teffac = teffac * (1. - (fbet - P.branch_start) / (P.branch_stop - P.branch_start));
+            wt = w->weight * exp(teffac * (etr * 2 - el - eold));
+            if (wt > P.max_weight) wt = P.max_weight;
+            if (!isfinite(el) || !isfinite(wt)) { nbad += 1; wt = 0.0; el = etr; }
+            __syncwarp();
+            if (lane == 0) { w->weight = wt; w->eold = el; }
+            __syncwarp();
+          } else {
+            if (!isfinite(el)) { nbad += 1; el = 0.0; wt = 0.0; }
+            if (lane == 0) w->eold = el;
+          }
+          sw += wt; swe += wt * el; swk += wt * kin; swv += wt * pot; swnl += wt * nl; swe2 += wt * el * el;
+          npts += 1;
         }
-        sw += wt; swe += wt * el; swk += wt * kin; swv += wt * pot; swnl += wt * nl; swe2 += wt * el * el;
       }
       if (lane == 0) {
-        atomicAdd(&cta_acc[0], sw); atomicAdd(&cta_acc[1], swe); atomicAdd(&cta_acc[2], swk);
-        atomicAdd(&cta_acc[3], swv); atomicAdd(&cta_acc[4], swnl); atomicAdd(&cta_acc[5], swe2);
-        atomicAdd(&cta_acc[6], nacc); atomicAdd(&cta_acc[7], natt); atomicAdd(&cta_acc[8], nbad);
-        atomicAdd(&cta_acc[9], double(P.nsteps));
-        if (io.energy) io.energy[wid] = W.sc()->eold;
+        if (mode != KM_ELOC) { atomicAdd(&cta_acc[6], nacc); atomicAdd(&cta_acc[7], natt); }
+        if (mode != KM_SWEEP) {
+          atomicAdd(&cta_acc[0], sw); atomicAdd(&cta_acc[1], swe); atomicAdd(&cta_acc[2], swk);
+          atomicAdd(&cta_acc[3], swv); atomicAdd(&cta_acc[4], swnl); atomicAdd(&cta_acc[5], swe2);
+          atomicAdd(&cta_acc[8], nbad);
+          atomicAdd(&cta_acc[9], npts);
+          if (io.energy) io.energy[wid] = W.sc()->eold;
+        }
       }
-      // write back positions and the resident state
+      // write back: positions and the resident state after moves; only the
+      // walker scalars after a local-energy pass
       __syncwarp();
-      for (int i = lane; i < 3 * N; i += 32) P.R[(size_t)wid * 3 * N + i] = Rp[i];
+      if (mode != KM_ELOC)
+        for (int i = lane; i < 3 * N; i += 32) P.R[(size_t)wid * 3 * N + i] = Rp[i];
       if constexpr (!HBM) {
         int4* dst = (int4*)gstate;
         const int4* src = (const int4*)wb;
-        for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
+        if (mode == KM_ELOC) {
+          for (int i = lane; i < (int)sizeof(WScal) / 16; i += 32) ((int4*)(gstate + L.scal))[i] = ((const int4*)(wb + L.scal))[i];
+        } else {
+          for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
+        }
       }
     }
   }
-  if constexpr (mode == KM_STEPS) {
+  if constexpr (mode == KM_STEPS || mode == KM_SWEEP || mode == KM_ELOC) {
     __syncthreads();
     if (threadIdx.x < 10) atomicAdd(&((double*)P.acc)[threadIdx.x], cta_acc[threadIdx.x]);
   }
@@ -710,14 +733,20 @@ struct BranchParams {
   double* dyn;
   int* src_of;            // [W] output mapping
   double* new_w;          // [W] weight of the slot after branching
+  // sort keys and counts in global memory (large populations); null: in
+  // dynamic shared memory
+  double* gkey;           // [npow2]
+  int* gidx;              // [npow2]
+  int* gcnt;              // [nwalk]
+  double* gnw;            // [nwalk]
 };
 
 __global__ void __launch_bounds__(1024) k_branch(BranchParams B) {
   extern __shared__ __align__(16) unsigned char sm[];
-  double* key = (double*)sm;                 // [npow2]
-  int* idx = (int*)(key + B.npow2);          // [npow2]
-  int* cnt = idx + B.npow2;                  // [nwalk]
-  double* nw = (double*)(((uintptr_t)(cnt + B.nwalk) + 15) & ~(uintptr_t)15);  // [nwalk]
+  double* key = B.gkey ? B.gkey : (double*)sm;                 // [npow2]
+  int* idx = B.gkey ? B.gidx : (int*)(key + B.npow2);          // [npow2]
+  int* cnt = B.gkey ? B.gcnt : idx + B.npow2;                  // [nwalk]
+  double* nw = B.gkey ? B.gnw : (double*)(((uintptr_t)(cnt + B.nwalk) + 15) & ~(uintptr_t)15);  // [nwalk]
   __shared__ double red[32];
   const int t = threadIdx.x, nt = blockDim.x;
   double local = 0;

@@ -36,6 +36,7 @@ cudaError_t launch_mode(const DevSys<Real>& S, const WLayout& L, const StepParam
   auto kern = S.has_tb ? k_walkers<Real, MM, MODE, true> : k_walkers<Real, MM, MODE, false>;
   cudaError_t e = ensure_smem_attr(kern, smem);
   if (e != cudaSuccess) return e;
+  if (nwalk <= 0) return cudaSuccess;  // attribute set only (before a stream capture)
   const int grid = (nwalk + wpc - 1) / wpc;
   kern<<<grid, 32 * wpc, smem, stream>>>(S, L, P, io);
   return cudaGetLastError();
@@ -48,6 +49,8 @@ cudaError_t launch_walker_kernels(const DevSys<Real>& S, const WLayout& L, const
                                   int mode, int nwalk, int wpc, size_t smem, cudaStream_t stream) {
   if (mode == KM_EVAL) return launch_mode<Real, MM, KM_EVAL>(S, L, P, io, nwalk, wpc, smem, stream);
   if (mode == KM_RATIO) return launch_mode<Real, MM, KM_RATIO>(S, L, P, io, nwalk, wpc, smem, stream);
+  if (mode == KM_SWEEP) return launch_mode<Real, MM, KM_SWEEP>(S, L, P, io, nwalk, wpc, smem, stream);
+  if (mode == KM_ELOC) return launch_mode<Real, MM, KM_ELOC>(S, L, P, io, nwalk, wpc, smem, stream);
   return launch_mode<Real, MM, KM_STEPS>(S, L, P, io, nwalk, wpc, smem, stream);
 }
 
