@@ -96,20 +96,24 @@ def make_workload(tmpdir):
     return deck, R0
 
 
-def _traffic_per_launch():
-    """DRAM bytes (read + write) of one walker-step kernel launch of this
+def _traffic_per_launch(kernel):
+    """DRAM bytes (read + write) of one launch of the given kernel of this
     workload, from the committed ncu summary (profiles/traffic.json), or None."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
-    return json.load(open(p)).get("k_walkers_mixed_dmc", {}).get("dram_bytes_per_launch")
+    return json.load(open(p)).get(kernel, {}).get("dram_bytes_per_launch")
+
+
+def walker_state_bytes(N, M, precision_bytes):
+    """Resident walker state: positions, both inverse matrices, MO
+    gradient/Laplacian rows, Jastrow gradients/Laplacians, scalars."""
+    return 8 * 3 * N + precision_bytes * (2 * M * M + N * M * 4) + 8 * 4 * N + 64
 
 
 def algorithmic_bytes_per_walker_step(N, M, nb, precision_bytes):
-    """Resident walker state read + written once per step (positions, both
-    inverse matrices, MO gradient/Laplacian rows, Jastrow sums, scalars)."""
-    state = 8 * 3 * N + precision_bytes * (2 * M * M + N * M * 4) + 8 * 4 * N + 64
-    return 2 * state
+    """Resident walker state read + written once per step."""
+    return 2 * walker_state_bytes(N, M, precision_bytes)
 
 
 def run_engine(args, rank, world):
@@ -150,6 +154,9 @@ def run_engine(args, rank, world):
             torch.cuda.synchronize(dev)
         ms = e0.elapsed_time(e1)
         launches = E.launch_count()
+        # per-kernel durations (move kernel, local-energy kernel), CUDA events
+        # around individual launches of the same kernels the block graph holds
+        sweep_ms, eloc_ms = E.time_kernels(5)
         # block latency: several shorter blocks (20 steps), host wall time from
         # block start to block statistics on the host
         E.dmc_init(timestep=TAU, nstep=20, seed=SEED + 99 + rank)
@@ -160,7 +167,8 @@ def run_engine(args, rank, world):
             lat.append((time.perf_counter() - t0) * 1e3)
             energies.append(s2["energy"])
         results[label] = {"ms": ms, "steps": steps, "stats": st, "launches": launches, "clocks": cs.summary(),
-                          "lat": lat, "energies": energies, "kernel_ms": st["block_ms"]}
+                          "lat": lat, "energies": energies, "kernel_ms": st["block_ms"], "sweep_ms": sweep_ms,
+                          "eloc_ms": eloc_ms}
         E.close()
     # end-to-end through the C-ABI with host buffers: upload walkers, run the
     # block, download walkers + statistics, every step amortised
@@ -355,10 +363,13 @@ def main():
         return
     N, M, nb = 14, 7, 80
     hbm, src = _peaks()
-    # dominant kernel: the walker-step kernel; algorithmic bytes per launch =
-    # walkers x steps-per-launch x resident-state read+write per walker-step
-    bytes_launch = NWALK * FEEDBACK_INTERVAL * algorithmic_bytes_per_walker_step(N, M, nb, 4)
-    kern_ms_per_launch = mx["kernel_ms"] / (steps / FEEDBACK_INTERVAL)
+    # dominant kernel: the move kernel (one launch = one sweep of every
+    # walker); algorithmic bytes per launch = walkers x resident state read +
+    # written once.  The local-energy kernel reads the state and writes 16 B.
+    sb = walker_state_bytes(N, M, 4)
+    kern = {"sweep": (mx["sweep_ms"], NWALK * 2 * sb), "eloc": (mx["eloc_ms"], NWALK * (sb + 16))}
+    dom = max(kern, key=lambda k: kern[k][0])
+    kern_ms_per_launch, bytes_launch = kern[dom]
     achieved = bytes_launch / (kern_ms_per_launch / 1e3) / 1e9
     lat = np.array(mx["lat"])
     line = {
@@ -381,8 +392,12 @@ def main():
         "e2e": {"value": NWALK * steps / (e2e_ms / 1e3), "unit": "walker-steps/s",
                 "h2d_bytes_per_step": NWALK * N * 3 * 8 / steps, "d2h_bytes_per_step": (NWALK * N * 3 * 8 + 96) / steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": src, "traffic": _traffic_per_launch(),
-                     "note": "walker-step kernel; algorithmic bytes = resident state read+write per walker-step"},
+                     "peak_source": src, "traffic": _traffic_per_launch(dom),
+                     "kernel": {"sweep": "k_walkers<float,8,KM_SWEEP>", "eloc": "k_walkers<float,8,KM_ELOC>"}[dom],
+                     "kernel_ms": {"sweep": mx["sweep_ms"], "eloc": mx["eloc_ms"]},
+                     "algorithmic_bytes_per_launch": bytes_launch,
+                     "note": "per launch every walker's resident state is read (and, for the move kernel, "
+                             "written) once; the state fits L2, so the kernel is latency/issue-bound, not HBM-bound"},
         "gpu_launches": mx["launches"],
         "clocks": mx["clocks"],
     }

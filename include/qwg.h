@@ -218,6 +218,13 @@ int qwg_batch_destroy(qwg_batch* b);
  * fastest (call before qwg_dmc_init).  Returns the chosen value. */
 int qwg_autotune(qwg_ctx* ctx, int* walkers_per_cta);
 
+/* Kernel timing for rooflines: runs nstep DMC steps of the resident
+ * population as individual launches of the move kernel and the local-energy
+ * kernel (no branching; the walk and the weights advance) with CUDA events
+ * around each launch, and returns the mean duration of each in ms.  Requires
+ * qwg_dmc_init and no block in flight. */
+int qwg_time_kernels(qwg_ctx* ctx, int nstep, double* sweep_ms, double* eloc_ms);
+
 /* Number of kernel launches the context issued since the last reset. */
 long long qwg_launch_count(const qwg_ctx* ctx);
 void qwg_reset_launch_count(qwg_ctx* ctx);

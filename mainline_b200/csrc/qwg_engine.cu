@@ -375,8 +375,10 @@ static void make_layout(qwg_ctx* c) {
     c->smem_bytes = c->smem_sweep = 0;
     return;
   }
-  c->wpc_sweep = 4;
-  c->smem_sweep = (size_t)c->wpc_sweep * L.sweep_bytes;
+  int wps = 4;  // same rule for the move kernel's smaller footprint
+  while (wps > 1 && (size_t)wps * L.sweep_bytes > 110 * 1024) wps--;
+  c->wpc_sweep = wps;
+  c->smem_sweep = (size_t)wps * L.sweep_bytes;
   // walkers per CTA: up to 4 while the CTA stays under ~110 KB (2 CTAs/SM)
   int wpc = 4;
   while (wpc > 1 && (size_t)wpc * L.bytes > 110 * 1024) wpc--;
@@ -493,6 +495,20 @@ static void ensure_io(qwg_ctx* c, size_t bytes) {
 }
 
 // One chunk of steps on the resident population (plus DMC branching).
+// P.nsteps steps of every walker: one fused launch, or (split schedule) a
+// move launch and a local-energy launch per step.
+static void launch_steps(qwg_ctx* c, StepParams P, const EvalIO& io, int nwalk) {
+  if (!c->split) {
+    launch_walkers(c, P, io, KM_STEPS, nwalk);
+    return;
+  }
+  for (int st = 0; st < P.nsteps; st++) {
+    P.st = st;
+    launch_walkers(c, P, io, KM_SWEEP, nwalk);
+    launch_walkers(c, P, io, KM_ELOC, nwalk);
+  }
+}
+
 static void run_chunk(qwg_ctx* c, int nsteps, double tau, uint64_t seed, int det_pp, bool dmc, BlockAcc* acc,
                       double* energy_out) {
   StepParams P = base_params(c);
@@ -513,7 +529,7 @@ static void run_chunk(qwg_ctx* c, int nsteps, double tau, uint64_t seed, int det
   if (P.refresh) c->last_refresh = c->step_counter;
   EvalIO io{};
   io.energy = energy_out;
-  launch_walkers(c, P, io, KM_STEPS, c->nwalk);
+  launch_steps(c, P, io, c->nwalk);
   c->state_valid = true;
   c->have_scalars = true;
   c->step_counter += nsteps;
@@ -585,15 +601,7 @@ static void enqueue_dmc_block(qwg_ctx* c) {
     P.branch_stop = c->branch_stop;
     P.max_weight = c->dmc.max_poss_weight;
     EvalIO io{};
-    if (c->split) {
-      for (int st = 0; st < np; st++) {
-        P.st = st;
-        launch_walkers(c, P, io, KM_SWEEP, c->nwalk);
-        launch_walkers(c, P, io, KM_ELOC, c->nwalk);
-      }
-    } else {
-      launch_walkers(c, P, io, KM_STEPS, c->nwalk);
-    }
+    launch_steps(c, P, io, c->nwalk);
     run_branch(c, acc + ch, np);
     step += np;
   }
@@ -1158,7 +1166,7 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
     P.etrial = c->d_dyn.as<double>();
     EvalIO io{};
     io.energy = d_energy;
-    launch_walkers(c, P, io, KM_STEPS, nw);
+    launch_steps(c, P, io, nw);
     CK(cudaMemcpyAsync(d_sums, acc, 10 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     c->step_counter += nstep;
     return QWG_OK;
@@ -1269,6 +1277,51 @@ int qwg_batch_destroy(qwg_batch* b) {
   if (b->origin) cudaStreamDestroy(b->origin);
   delete b;
   return QWG_OK;
+}
+
+int qwg_time_kernels(qwg_ctx* c, int nstep, double* sweep_ms, double* eloc_ms) {
+  if (!c || nstep <= 0) return QWG_ERR_ARG;
+  if (!c->dmc_ready) return fail(c, QWG_ERR_STATE, "qwg_time_kernels: call qwg_dmc_init first");
+  if (c->block_pending) return fail(c, QWG_ERR_STATE, "qwg_time_kernels: a block is in flight");
+  return guarded(c, [&]() -> int {
+    BlockAcc* acc = c->d_acc.as<BlockAcc>();
+    CK(cudaMemsetAsync(acc, 0, sizeof(BlockAcc), c->stream));
+    StepParams P = base_params(c);
+    P.nsteps = nstep;
+    P.tau = c->dmc.timestep;
+    P.dmc = 1;
+    P.dyn_step = 1;
+    P.refresh = 0;
+    P.deterministic_pp = c->dmc.deterministic_pp;
+    P.seed = c->dmc.seed ^ 0x7157ull;  // a stream of its own
+    P.acc = acc;
+    P.branch_start = c->branch_start;
+    P.branch_stop = c->branch_stop;
+    P.max_weight = c->dmc.max_poss_weight;
+    EvalIO io{};
+    std::vector<cudaEvent_t> ev(3 * nstep);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int st = 0; st < nstep; st++) {
+      P.st = st;
+      CK(cudaEventRecord(ev[3 * st], c->stream));
+      launch_walkers(c, P, io, KM_SWEEP, c->nwalk);
+      CK(cudaEventRecord(ev[3 * st + 1], c->stream));
+      launch_walkers(c, P, io, KM_ELOC, c->nwalk);
+      CK(cudaEventRecord(ev[3 * st + 2], c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    double ts = 0, te = 0;
+    for (int st = 0; st < nstep; st++) {
+      float a = 0, b = 0;
+      CK(cudaEventElapsedTime(&a, ev[3 * st], ev[3 * st + 1]));
+      CK(cudaEventElapsedTime(&b, ev[3 * st + 1], ev[3 * st + 2]));
+      ts += a; te += b;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (sweep_ms) *sweep_ms = ts / nstep;
+    if (eloc_ms) *eloc_ms = te / nstep;
+    return QWG_OK;
+  });
 }
 
 int qwg_autotune(qwg_ctx* c, int* walkers_per_cta) {

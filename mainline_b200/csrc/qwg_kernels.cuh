@@ -507,11 +507,26 @@ __device__ __forceinline__ void random_rotation(const Rand4& r, double m[9]) {
   m[6] = 2 * (x * z + y * w);     m[7] = 2 * (y * z - x * w);     m[8] = 1 - 2 * (x * x + y * y);
 }
 
+// Resident 128-thread CTAs per SM the register budget of each kernel mode is
+// sized for (the move and local-energy kernels are smaller than the fused one).
 #ifndef QWG_MIN_BLOCKS
-#define QWG_MIN_BLOCKS 4  // resident 128-thread CTAs per SM the register budget is sized for
+#define QWG_MIN_BLOCKS 4
 #endif
+#ifndef QWG_MIN_BLOCKS_SWEEP
+#define QWG_MIN_BLOCKS_SWEEP 4
+#endif
+#ifndef QWG_MIN_BLOCKS_ELOC
+#define QWG_MIN_BLOCKS_ELOC 4
+#endif
+template <int mode>
+struct MinBlocks { static constexpr int value = QWG_MIN_BLOCKS; };
+template <>
+struct MinBlocks<KM_SWEEP> { static constexpr int value = QWG_MIN_BLOCKS_SWEEP; };
+template <>
+struct MinBlocks<KM_ELOC> { static constexpr int value = QWG_MIN_BLOCKS_ELOC; };
+
 template <typename Real, int MMAX, int mode, bool TB>
-__global__ void __launch_bounds__(128, QWG_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, MinBlocks<mode>::value)
     k_walkers(const __grid_constant__ DevSys<Real> S, const __grid_constant__ WLayout L, StepParams P, EvalIO io) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int wpc = blockDim.x / 32;

@@ -18,7 +18,7 @@ from dataclasses import dataclass
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libqwg.so")
+LIB_PATH = os.environ.get("QWG_LIBRARY", os.path.join(HERE, "libqwg.so"))
 
 FP64 = 0
 MIXED = 1
@@ -29,7 +29,7 @@ EXPORTS = [
     "qwg_get_walker_scalars", "qwg_eval",
     "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
-    "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready",
+    "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready", "qwg_time_kernels",
     "qwg_server_create", "qwg_server_destroy", "qwg_server_submit", "qwg_server_progress",
     "qwg_server_get_status", "qwg_server_last_error",
 ]
@@ -127,6 +127,7 @@ def load_library(path: str = LIB_PATH):
         "qwg_reset_launch_count": (None, [C.c_void_p]),
         "qwg_footprint": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P(C.c_ulonglong)]),
         "qwg_dmc_block_ready": (C.c_int, [C.c_void_p]),
+        "qwg_time_kernels": (C.c_int, [C.c_void_p, C.c_int, dp, dp]),
         "qwg_server_create": (C.c_int, [C.c_ulonglong, C.c_int, P(C.c_void_p)]),
         "qwg_server_destroy": (C.c_int, [C.c_void_p]),
         "qwg_server_submit": (C.c_int, [C.c_void_p, P(JobDesc), P(C.c_int)]),
@@ -294,6 +295,13 @@ class Engine:
         w = C.c_int(0)
         self._check(self.lib.qwg_autotune(self.h, C.byref(w)), "qwg_autotune")
         return w.value
+
+    def time_kernels(self, nstep: int = 5):
+        """Mean device ms of the move kernel and the local-energy kernel over
+        nstep DMC steps launched one by one (advances the walk)."""
+        a, b = C.c_double(0), C.c_double(0)
+        self._check(self.lib.qwg_time_kernels(self.h, nstep, C.byref(a), C.byref(b)), "qwg_time_kernels")
+        return a.value, b.value
 
     def launch_count(self) -> int:
         return int(self.lib.qwg_launch_count(self.h))
