@@ -435,10 +435,13 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
       // |value| <= 1e-8 rule to the sums (MO_matrix_blas.h:444-474)
       for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
       const int2 im = S.atom_images[si.x];
+      const double cut2 = cut * cut * (1.0 + 1e-12);  // beyond it r < cut is certainly false
       for (int m = im.x; m < im.x + im.y; m++) {
         const double* cp = S.image_pos + 3 * m;
         double dx = px - cp[0], dy = py - cp[1], dz = pz - cp[2];
-        double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 < cut2)) continue;
+        double r = sqrt(r2);
         if (!(r < cut)) continue;
         int i = int(r * S.inv_spacing);
         double h = r - double(i) * S.spacing;
@@ -571,10 +574,13 @@ __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, d
     const int fb0 = (S.shell_pack[cs.x] >> 4) & 0xffff;
     const int2 im = S.atom_images[c];
     const Real cut = Real(S.center_cut[c]);
+    const Real cut2 = cut * cut * Real(1.000001);  // beyond it rd < cut is certainly false
     for (int m = im.x; m < im.x + im.y; m++) {
       const double* cp = S.image_pos + 3 * m;
       const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
-      const Real rd = sqrt(x * x + y * y + z * z);
+      const Real rd2 = x * x + y * y + z * z;
+      if (!(rd2 < cut2)) continue;
+      const Real rd = sqrt(rd2);
       if (!(rd < cut)) continue;
       const int i = int(rd * Real(S.inv_spacing));
       const Real h = rd - Real(i) * Real(S.spacing);

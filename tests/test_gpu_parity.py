@@ -103,7 +103,7 @@ def test_mixed_precision_error_per_configuration(golden):
     nelec = g["R"].shape[1]
     assert np.median(err) / nelec < 4e-6
     assert np.median(rel) < 5e-6
-    assert np.median(dlp) < 1e-5
+    assert np.median(dlp) / nelec < 2e-7  # ln|det| sums one FP32-rounded pivot per electron
 
 
 def test_vmc_block_runs():
