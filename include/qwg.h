@@ -92,6 +92,11 @@ typedef struct {
   double block_ms;        /* device time of the block (CUDA events)     */
   int nsteps, nwalkers;
   int nonfinite;          /* walkers whose E_L or weight went non-finite */
+  /* Point statistics of the block as Properties_manager::endBlock keeps them
+   * for the log (properties/Properties.cpp:574-640): npoints = walker-steps,
+   * var_* = unweighted sample variance over those points, n/(n-1) corrected. */
+  double npoints;
+  double var_energy, var_kinetic, var_potential, var_nonlocal, var_weight;
 } qwg_block_stats;
 
 /* DMC parameters (Dmc_method::read defaults, method/Dmc_method.cpp:33-160). */
@@ -217,6 +222,20 @@ int qwg_batch_destroy(qwg_batch* b);
  * for each walkers-per-CTA choice that fits shared memory and keeps the
  * fastest (call before qwg_dmc_init).  Returns the chosen value. */
 int qwg_autotune(qwg_ctx* ctx, int* walkers_per_cta);
+
+/* QWalk log files (runid.log), host only.  qwg_log_header appends the run
+ * banner of Dmc_method::run / Vmc_method::run (method/Dmc_method.cpp:307-317,
+ * method/Vmc_method.cpp:333-340) and the "init" entry of
+ * Properties_manager::initializeLog (properties/Properties.cpp:1022-1036);
+ * qwg_log_block appends one "block { ... }" entry with the fields and
+ * precision of Properties_manager::endBlock + Properties_block::storeToLog
+ * (properties/Properties.cpp:628-636, properties/Properties_block.cpp:73-136),
+ * so the reference's gosling analyser reads and reblocks engine runs.
+ * method: "DMC" or "VMC"; label: the block label (e.g. "dmc"); nconfig and
+ * nstep appear in the VMC banner only. */
+int qwg_log_header(const char* path, const char* method, const char* label, double timestep, int nconfig,
+                   int nstep);
+int qwg_log_block(const char* path, const char* label, const qwg_block_stats* stats);
 
 /* Kernel timing for rooflines: runs nstep DMC steps of the resident
  * population as individual launches of the move kernel and the local-energy

@@ -194,7 +194,11 @@ struct WScal {
 struct BlockAcc {   // per-launch reduction target (double atomics)
   double sum_w, sum_we, sum_wk, sum_wv, sum_wnl, sum_we2, accepted, attempted;
   double nonfinite, npts;
+  // unweighted point sums for the block variances of the log
+  // (Properties_manager::insertPoint / endBlock, Properties.cpp:437-640)
+  double sum_e, sum_e2, sum_k, sum_k2, sum_v, sum_v2, sum_nl, sum_nl2, sum_wt, sum_wt2;
 };
+constexpr int QWG_NACC = 20;  // doubles in BlockAcc
 
 // Device-resident DMC scalars (dyn[]): the whole block runs without a host
 // round trip, so it can be replayed as one CUDA graph.

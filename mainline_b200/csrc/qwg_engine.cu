@@ -114,6 +114,7 @@ struct qwg_ctx {
 namespace {
 
 constexpr int kHistCap = 1 << 16;  // block energies kept on the device for E_ref
+constexpr int kStatsLen = QWG_NACC + 2;  // block sums, E_T, E_ref (k_block_end output)
 
 static DRadial to_dradial(const Radial& r) {
   DRadial d{};
@@ -410,7 +411,7 @@ static size_t footprint_bytes(const qwg_ctx* c, int max_walkers) {
              H.image_pos.size() * 8 + H.gvec.size() * 8 + 3 * H.gweight.size() * 8;
   b += W * (2 * 3 * N * 8 + 2 * (size_t)c->L.state_bytes + (c->mmax == 0 ? (size_t)c->L.scratch_bytes : 0) + 20);
   b += W * 8 * (9 + 5 + 4 * N);  // evaluation outputs (qwg_eval / qwg_dmc_init)
-  b += sizeof(BlockAcc) * 1024 + DYN_COUNT * 8 + (size_t)kHistCap * 8 + 16 * 8;
+  b += sizeof(BlockAcc) * 1024 + DYN_COUNT * 8 + (size_t)kHistCap * 8 + kStatsLen * 8;
   if (max_walkers > kBranchSmemMax) b += branch_bytes(max_walkers);
   return b;
 }
@@ -609,9 +610,13 @@ static void enqueue_dmc_block(qwg_ctx* c) {
                                        c->dmc.feedback, c->nwalk, c->d_stats.as<double>());
   CK(cudaGetLastError());
   c->launches++;
-  CK(cudaMemcpyAsync(c->h_stats, c->d_stats.p, 16 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_stats, c->d_stats.p, kStatsLen * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
 }
 
+// Block statistics from the BlockAcc sums t[0..QWG_NACC-1]: weighted averages
+// as Properties_manager::endBlock (Properties.cpp:578-640), and the point
+// variances of its log entry: (mean x^2 - mean^2) n / (n - 1) over the
+// block's walker-steps, unweighted (condense_variance, :574-577).
 static void stats_from_sums(const double* t, qwg_block_stats* s) {
   memset(s, 0, sizeof(*s));
   double W = t[0] > 0 ? t[0] : 1.0;
@@ -623,25 +628,28 @@ static void stats_from_sums(const double* t, qwg_block_stats* s) {
   s->weight = t[9] > 0 ? t[0] / t[9] : 0.0;
   s->acceptance = t[7] > 0 ? t[6] / t[7] : 0.0;
   s->nonfinite = (int)t[8];
-  s->etrial = t[10];
+  s->npoints = t[9];
+  const double n = t[9];
+  auto pvar = [&](double sx, double sx2) {
+    if (n < 2) return 0.0;
+    const double m = sx / n;
+    return (sx2 / n - m * m) * (n / (n - 1.0));
+  };
+  s->var_energy = pvar(t[10], t[11]);
+  s->var_kinetic = pvar(t[12], t[13]);
+  s->var_potential = pvar(t[14], t[15]);
+  s->var_nonlocal = pvar(t[16], t[17]);
+  s->var_weight = pvar(t[18], t[19]);
+  s->etrial = t[QWG_NACC];
 }
 
 static void acc_to_stats(const std::vector<BlockAcc>& v, qwg_block_stats* s) {
-  BlockAcc t{};
+  double t[QWG_NACC + 2] = {0};
   for (auto& a : v) {
-    t.sum_w += a.sum_w; t.sum_we += a.sum_we; t.sum_wk += a.sum_wk; t.sum_wv += a.sum_wv; t.sum_wnl += a.sum_wnl;
-    t.sum_we2 += a.sum_we2; t.accepted += a.accepted; t.attempted += a.attempted; t.nonfinite += a.nonfinite;
-    t.npts += a.npts;
+    const double* p = (const double*)&a;
+    for (int k = 0; k < QWG_NACC; k++) t[k] += p[k];
   }
-  double W = t.sum_w > 0 ? t.sum_w : 1.0;
-  s->energy = t.sum_we / W;
-  s->kinetic = t.sum_wk / W;
-  s->potential = t.sum_wv / W;
-  s->nonlocal = t.sum_wnl / W;
-  s->energy_var = t.sum_we2 / W - s->energy * s->energy;
-  s->weight = t.npts > 0 ? t.sum_w / t.npts : 0.0;
-  s->acceptance = t.attempted > 0 ? t.accepted / t.attempted : 0.0;
-  s->nonfinite = (int)t.nonfinite;
+  stats_from_sums(t, s);
 }
 
 }  // namespace
@@ -743,8 +751,8 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
     c->d_neww.alloc((size_t)max_walkers * 8);
     c->d_energy.alloc((size_t)max_walkers * 8);
     c->d_hist.alloc((size_t)kHistCap * 8);
-    c->d_stats.alloc(16 * 8);
-    CK(cudaMallocHost((void**)&c->h_stats, 16 * sizeof(double)));
+    c->d_stats.alloc(kStatsLen * 8);
+    CK(cudaMallocHost((void**)&c->h_stats, kStatsLen * sizeof(double)));
     CK(cudaEventCreate(&c->ev0));
     CK(cudaEventCreate(&c->ev1));
     CK(cudaStreamSynchronize(c->stream));

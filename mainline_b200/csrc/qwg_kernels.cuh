@@ -535,8 +535,8 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
   // shared memory holds walker state only
   const Real* moc_s = S.moc;
   const size_t moc_bytes = 0;
-  __shared__ double cta_acc[10];
-  if (threadIdx.x < 10) cta_acc[threadIdx.x] = 0.0;
+  __shared__ double cta_acc[QWG_NACC];
+  if (threadIdx.x < QWG_NACC) cta_acc[threadIdx.x] = 0.0;
   __syncthreads();
 
   const int wid = blockIdx.x * wpc + warp;
@@ -617,6 +617,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       const double sqt = sqrt(P.tau);
       double nacc = 0, natt = 0;
       double sw = 0, swe = 0, swk = 0, swv = 0, swnl = 0, swe2 = 0, nbad = 0, npts = 0;
+      double u[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // unweighted sums of E, E^2, T, T^2, V, V^2, NL, NL^2, w, w^2
       const double etr = P.dmc ? *P.etrial : 0.0;
       const double teff = P.dmc ? P.etrial[1] : 0.0;
       const int st0 = mode == KM_STEPS ? 0 : P.st, st1 = mode == KM_STEPS ? P.nsteps : P.st + 1;
@@ -694,6 +695,8 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
             if (lane == 0) w->eold = el;
           }
           sw += wt; swe += wt * el; swk += wt * kin; swv += wt * pot; swnl += wt * nl; swe2 += wt * el * el;
+          u[0] += el; u[1] += el * el; u[2] += kin; u[3] += kin * kin; u[4] += pot; u[5] += pot * pot;
+          u[6] += nl; u[7] += nl * nl; u[8] += wt; u[9] += wt * wt;
           npts += 1;
         }
       }
@@ -704,6 +707,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
           atomicAdd(&cta_acc[3], swv); atomicAdd(&cta_acc[4], swnl); atomicAdd(&cta_acc[5], swe2);
           atomicAdd(&cta_acc[8], nbad);
           atomicAdd(&cta_acc[9], npts);
+          for (int k = 0; k < 10; k++) atomicAdd(&cta_acc[10 + k], u[k]);
           if (io.energy) io.energy[wid] = W.sc()->eold;
         }
       }
@@ -725,7 +729,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
   }
   if constexpr (mode == KM_STEPS || mode == KM_SWEEP || mode == KM_ELOC) {
     __syncthreads();
-    if (threadIdx.x < 10) atomicAdd(&((double*)P.acc)[threadIdx.x], cta_acc[threadIdx.x]);
+    if (threadIdx.x < QWG_NACC) atomicAdd(&((double*)P.acc)[threadIdx.x], cta_acc[threadIdx.x]);
   }
 }
 
@@ -868,15 +872,15 @@ __global__ void k_gather(int nwalk, int n3, int state_bytes, int scal_off, const
 // End of a DMC block: block averages from the per-chunk accumulators, the
 // block-energy history, E_ref = mean block energy (the first fifth of the
 // blocks dropped as equilibration once there are more than five), and E_T
-// (Dmc_method.cpp:475-530).  out[0..11]: sum w, sum wE, sum wT, sum wV,
-// sum wV_NL, sum wE^2, accepted, attempted, non-finite, points, E_T, E_ref.
+// (Dmc_method.cpp:475-530).  out[0..QWG_NACC-1]: the BlockAcc sums of the
+// block; out[QWG_NACC] = E_T, out[QWG_NACC + 1] = E_ref.
 __global__ void k_block_end(const BlockAcc* acc, int nchunk, double* dyn, double* hist, int hist_cap,
                             double feedback, int nwalk, double* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double t[10] = {0};
+  double t[QWG_NACC] = {0};
   for (int c = 0; c < nchunk; c++) {
     const double* a = (const double*)(acc + c);
-    for (int k = 0; k < 10; k++) t[k] += a[k];
+    for (int k = 0; k < QWG_NACC; k++) t[k] += a[k];
   }
   const double eb = t[0] > 0 ? t[1] / t[0] : 0.0;
   const int nb = (int)dyn[DYN_NBLOCK];
@@ -890,9 +894,9 @@ __global__ void k_block_end(const BlockAcc* acc, int nchunk, double* dyn, double
   const double eref = se / double(n - lo);
   dyn[DYN_EREF] = eref;
   dyn[DYN_ETRIAL] = eref - feedback * log(dyn[DYN_SUMW] / double(nwalk));
-  for (int k = 0; k < 10; k++) out[k] = t[k];
-  out[10] = dyn[DYN_ETRIAL];
-  out[11] = eref;
+  for (int k = 0; k < QWG_NACC; k++) out[k] = t[k];
+  out[QWG_NACC] = dyn[DYN_ETRIAL];
+  out[QWG_NACC + 1] = eref;
 }
 
 __global__ void k_init_weights(unsigned char* state, int nwalk, int state_bytes, int scal_off, const double* eloc) {

@@ -30,6 +30,7 @@ EXPORTS = [
     "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
     "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready", "qwg_time_kernels",
+    "qwg_log_header", "qwg_log_block",
     "qwg_server_create", "qwg_server_destroy", "qwg_server_submit", "qwg_server_progress",
     "qwg_server_get_status", "qwg_server_last_error",
 ]
@@ -55,7 +56,9 @@ class BlockStats(C.Structure):
     _fields_ = [("energy", C.c_double), ("kinetic", C.c_double), ("potential", C.c_double),
                 ("nonlocal", C.c_double), ("weight", C.c_double), ("energy_var", C.c_double),
                 ("acceptance", C.c_double), ("etrial", C.c_double), ("block_ms", C.c_double),
-                ("nsteps", C.c_int), ("nwalkers", C.c_int), ("nonfinite", C.c_int)]
+                ("nsteps", C.c_int), ("nwalkers", C.c_int), ("nonfinite", C.c_int),
+                ("npoints", C.c_double), ("var_energy", C.c_double), ("var_kinetic", C.c_double),
+                ("var_potential", C.c_double), ("var_nonlocal", C.c_double), ("var_weight", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -128,6 +131,8 @@ def load_library(path: str = LIB_PATH):
         "qwg_footprint": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P(C.c_ulonglong)]),
         "qwg_dmc_block_ready": (C.c_int, [C.c_void_p]),
         "qwg_time_kernels": (C.c_int, [C.c_void_p, C.c_int, dp, dp]),
+        "qwg_log_header": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_double, C.c_int, C.c_int]),
+        "qwg_log_block": (C.c_int, [C.c_char_p, C.c_char_p, P(BlockStats)]),
         "qwg_server_create": (C.c_int, [C.c_ulonglong, C.c_int, P(C.c_void_p)]),
         "qwg_server_destroy": (C.c_int, [C.c_void_p]),
         "qwg_server_submit": (C.c_int, [C.c_void_p, P(JobDesc), P(C.c_int)]),
@@ -414,3 +419,22 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def log_header(path: str, method: str, label: str, timestep: float, nconfig: int = 0, nstep: int = 0) -> None:
+    """Append the run banner and init entry of a QWalk log file (runid.log)."""
+    rc = load_library().qwg_log_header(path.encode(), method.encode(), label.encode(), timestep, nconfig, nstep)
+    if rc != 0:
+        raise QwgError(f"qwg_log_header failed ({rc}) for {path}")
+
+
+def log_block(path: str, label: str, stats: dict) -> None:
+    """Append one block entry (as returned by vmc_block / dmc_block) in the
+    format the reference's gosling analyser reads."""
+    st = BlockStats()
+    for k, _ in BlockStats._fields_:
+        if k in stats:
+            setattr(st, k, stats[k])
+    rc = load_library().qwg_log_block(path.encode(), label.encode(), C.byref(st))
+    if rc != 0:
+        raise QwgError(f"qwg_log_block failed ({rc}) for {path}")
