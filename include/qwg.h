@@ -237,6 +237,23 @@ int qwg_log_header(const char* path, const char* method, const char* label, doub
                    int nstep);
 int qwg_log_block(const char* path, const char* label, const qwg_block_stats* stats);
 
+/* Walker configuration files (STORECONFIG / READCONFIG), host only, in the
+ * text layout of write_configurations / read_configurations
+ * (program_utils/qmc_io.h:371-470) with Config_save_point positions
+ * (system/Sample_point.cpp:120-148) and, for DMC, the Dmc_point weight and
+ * sign section (method/Dmc_method.cpp:1228-1267).  qwg_write_configs renames
+ * an existing file to <path>.backup first, as the reference does; weight NULL
+ * writes VMC walkers (positions only), sign NULL writes sign 1.
+ * qwg_read_configs fills up to maxw walkers (weight and sign 1 where a walker
+ * has no DMC section) and fails with QWG_ERR_INPUT on a malformed file or an
+ * electron count other than nelec.  qwg_store_configs writes the context's
+ * resident walkers (with weights and signs if dmc != 0). */
+int qwg_write_configs(const char* path, const double* R, const double* weight, const double* sign, int nw,
+                      int nelec);
+int qwg_count_configs(const char* path, int* nw, int* nelec);
+int qwg_read_configs(const char* path, double* R, double* weight, double* sign, int maxw, int nelec, int* nw_read);
+int qwg_store_configs(qwg_ctx* ctx, const char* path, int dmc);
+
 /* Kernel timing for rooflines: runs nstep DMC steps of the resident
  * population as individual launches of the move kernel and the local-energy
  * kernel (no branching; the walk and the weights advance) with CUDA events

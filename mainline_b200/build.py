@@ -24,7 +24,7 @@ NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--ex
                   "-I" + os.path.join(ROOT, "include")]
 
 SOURCES_CU = ["qwg_engine.cu"]
-SOURCES_CXX = ["qwg_deck.cpp", "qwg_server.cpp", "qwg_log.cpp"]
+SOURCES_CXX = ["qwg_deck.cpp", "qwg_server.cpp", "qwg_log.cpp", "qwg_configs.cpp"]
 # walker-kernel families: qwg_walkers.cu once per (working precision, orbital capacity)
 FAMILIES = [(real, mm) for real in ("double", "float") for mm in (8, 16, 32, 0)]
 

@@ -844,6 +844,34 @@ int qwg_get_walker_scalars(qwg_ctx* c, double* energy, double* weight, int nw) {
   });
 }
 
+int qwg_store_configs(qwg_ctx* c, const char* path, int dmc) {
+  if (!c || !path) return QWG_ERR_ARG;
+  if (c->nwalk <= 0) return fail(c, QWG_ERR_STATE, "qwg_store_configs: no walkers");
+  if (dmc && !c->have_scalars) return fail(c, QWG_ERR_STATE, "qwg_store_configs: no DMC weights yet");
+  return guarded(c, [&]() -> int {
+    const int W = c->nwalk, N = c->H.nelec;
+    std::vector<double> R((size_t)W * N * 3), wt, sg;
+    CK(cudaMemcpyAsync(R.data(), c->d_R.p, R.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (dmc) {
+      // weight and both determinant signs out of every walker's scalars
+      std::vector<WScal> sc(W);
+      CK(cudaMemcpy2DAsync(sc.data(), sizeof(WScal), c->d_state.as<unsigned char>() + c->L.scal, c->L.state_bytes,
+                           sizeof(WScal), W, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      wt.resize(W);
+      sg.resize(W);
+      for (int w = 0; w < W; w++) {
+        wt[w] = sc[w].weight;
+        sg[w] = sc[w].sign[0] * sc[w].sign[1];
+      }
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    const int rc = qwg_write_configs(path, R.data(), dmc ? wt.data() : nullptr, dmc ? sg.data() : nullptr, W, N);
+    if (rc != QWG_OK) return fail(c, rc, std::string("qwg_store_configs: cannot write ") + path);
+    return QWG_OK;
+  });
+}
+
 int qwg_eval(qwg_ctx* c, const double* rot, qwg_eval_out* out) {
   if (!c || !out) return QWG_ERR_ARG;
   if (c->nwalk <= 0) return fail(c, QWG_ERR_STATE, "qwg_eval: no walkers");

@@ -30,7 +30,8 @@ EXPORTS = [
     "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
     "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready", "qwg_time_kernels",
-    "qwg_log_header", "qwg_log_block",
+    "qwg_log_header", "qwg_log_block", "qwg_write_configs", "qwg_count_configs", "qwg_read_configs",
+    "qwg_store_configs",
     "qwg_server_create", "qwg_server_destroy", "qwg_server_submit", "qwg_server_progress",
     "qwg_server_get_status", "qwg_server_last_error",
 ]
@@ -133,6 +134,10 @@ def load_library(path: str = LIB_PATH):
         "qwg_time_kernels": (C.c_int, [C.c_void_p, C.c_int, dp, dp]),
         "qwg_log_header": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_double, C.c_int, C.c_int]),
         "qwg_log_block": (C.c_int, [C.c_char_p, C.c_char_p, P(BlockStats)]),
+        "qwg_write_configs": (C.c_int, [C.c_char_p, dp, dp, dp, C.c_int, C.c_int]),
+        "qwg_count_configs": (C.c_int, [C.c_char_p, P(C.c_int), P(C.c_int)]),
+        "qwg_read_configs": (C.c_int, [C.c_char_p, dp, dp, dp, C.c_int, C.c_int, P(C.c_int)]),
+        "qwg_store_configs": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
         "qwg_server_create": (C.c_int, [C.c_ulonglong, C.c_int, P(C.c_void_p)]),
         "qwg_server_destroy": (C.c_int, [C.c_void_p]),
         "qwg_server_submit": (C.c_int, [C.c_void_p, P(JobDesc), P(C.c_int)]),
@@ -308,6 +313,10 @@ class Engine:
         self._check(self.lib.qwg_time_kernels(self.h, nstep, C.byref(a), C.byref(b)), "qwg_time_kernels")
         return a.value, b.value
 
+    def store_configs(self, path: str, dmc: bool = False):
+        """Write the resident walkers as a QWalk configuration file."""
+        self._check(self.lib.qwg_store_configs(self.h, path.encode(), int(dmc)), "qwg_store_configs")
+
     def launch_count(self) -> int:
         return int(self.lib.qwg_launch_count(self.h))
 
@@ -438,3 +447,30 @@ def log_block(path: str, label: str, stats: dict) -> None:
     rc = load_library().qwg_log_block(path.encode(), label.encode(), C.byref(st))
     if rc != 0:
         raise QwgError(f"qwg_log_block failed ({rc}) for {path}")
+
+
+def write_configs(path: str, R: np.ndarray, weight=None, sign=None) -> None:
+    """Write walkers [W, N, 3] (and DMC weights/signs) as a QWalk configuration file."""
+    R = np.ascontiguousarray(R, dtype=np.float64)
+    W, N = R.shape[0], R.shape[1]
+    w = None if weight is None else np.ascontiguousarray(weight, dtype=np.float64)
+    sg = None if sign is None else np.ascontiguousarray(sign, dtype=np.float64)
+    rc = load_library().qwg_write_configs(path.encode(), _ptr(R), _ptr(w) if w is not None else None,
+                                          _ptr(sg) if sg is not None else None, W, N)
+    if rc != 0:
+        raise QwgError(f"qwg_write_configs failed ({rc}) for {path}")
+
+
+def read_configs(path: str):
+    """Read a QWalk configuration file: (R [W, N, 3], weight [W], sign [W])."""
+    lib = load_library()
+    nw, ne = C.c_int(0), C.c_int(0)
+    if lib.qwg_count_configs(path.encode(), C.byref(nw), C.byref(ne)) != 0:
+        raise QwgError(f"malformed configuration file {path}")
+    R = np.zeros((nw.value, ne.value, 3))
+    w, sg = np.zeros(nw.value), np.zeros(nw.value)
+    n = C.c_int(0)
+    if nw.value and lib.qwg_read_configs(path.encode(), _ptr(R), _ptr(w), _ptr(sg), nw.value, ne.value,
+                                         C.byref(n)) != 0:
+        raise QwgError(f"malformed configuration file {path}")
+    return R, w, sg

@@ -52,3 +52,24 @@ def test_dmc_log_read_by_gosling(tmp_path):
     assert "4 total blocks" in out
     m = re.search(r"total_energy0\s+(\S+)", out)
     assert m and min(energies) - 1e-6 <= float(m.group(1)) <= max(energies) + 1e-6
+
+
+def test_store_configs_round_trip(tmp_path):
+    """The resident DMC walkers written as a QWalk configuration file read
+    back as the same positions, weights and signs."""
+    deck = os.path.join(GOLDEN, "n2_pseudo.qw")
+    nw = 256
+    E = engine.Engine(deck, engine.FP64, max_walkers=nw)
+    E.set_walkers(systems.random_configs(systems.read_deck(deck), nw, seed=8))
+    E.vmc_block(5, 0.3, seed=9)
+    E.dmc_init(timestep=0.01, nstep=10, seed=10)
+    E.dmc_block()
+    p = str(tmp_path / "run.config")
+    E.store_configs(p, dmc=True)
+    R, w, sg = engine.read_configs(p)
+    assert np.allclose(R, E.get_walkers(), rtol=1e-14, atol=1e-14)
+    assert np.allclose(w, E.walker_scalars()[1], rtol=1e-14)
+    assert set(np.unique(sg)) <= {-1.0, 1.0}
+    E2 = engine.Engine(deck, engine.FP64, max_walkers=nw)
+    E2.set_walkers(R)
+    assert np.all(np.isfinite(E2.eval().energy))
