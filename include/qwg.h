@@ -110,6 +110,9 @@ typedef struct {
   int refresh_interval;   /* steps between full recomputes (MIXED: LU refresh) */
   int deterministic_pp;   /* 1: evaluate every pair inside the cutoff   */
   uint64_t seed;
+  int tmoves;             /* 0: locality approximation; 1: TMOVES (one T-move per
+                             walker per step); 2: TMOVESSC (size-consistent, one per
+                             electron) -- Dmc_method::doTmove, method/Dmc_method.cpp:850-906 */
 } qwg_dmc_params;
 
 const char* qwg_version(void);
@@ -253,6 +256,16 @@ int qwg_write_configs(const char* path, const double* R, const double* weight, c
 int qwg_count_configs(const char* path, int* nw, int* nelec);
 int qwg_read_configs(const char* path, double* R, double* weight, double* sign, int maxw, int nelec, int* nw_read);
 int qwg_store_configs(qwg_ctx* ctx, const char* path, int dmc);
+
+/* T-move selection without moving (Pseudopotential::calcNonlocTmove +
+ * the selection of Dmc_method::doTmove, system/Pseudopotential.cpp:371-389,
+ * method/Dmc_method.cpp:850-906) for the resident walkers, with the
+ * deterministic pseudopotential and the quadrature rotations rot ([nw][3][3]
+ * or NULL): mode 1 or 2 as qwg_dmc_params.tmoves, tau the time step.  For
+ * electron e of walker w, moved[w][e] = 1 and pos[w][e][0..2] its target when
+ * a move is selected, else moved = 0. */
+int qwg_tmove_select(qwg_ctx* ctx, const double* rot, int mode, double tau, uint64_t seed, int* moved,
+                     double* pos);
 
 /* Kernel timing for rooflines: runs nstep DMC steps of the resident
  * population as individual launches of the move kernel and the local-energy

@@ -235,6 +235,12 @@ struct StepParams {
   unsigned char* state; // [W][state_bytes]
   unsigned char* scratch;  // [W][scratch_bytes] (HBM-resident walkers only)
   BlockAcc* acc;
+  // T-moves (Dmc_method::doTmove, Dmc_method.cpp:850-906): 0 off, 1 one move
+  // per walker (TMOVES), 2 one per electron (TMOVESSC)
+  int tmoves;
+  int tm_cap;           // quadrature terms per walker the candidate buffer holds
+  double* tm_cand;      // [W][tm_cap] the current electron chunk's point terms
+  double* tm_moves;     // [W][N][4] selected targets (x, y, z, 1) or flag 0
 };
 
 // ---------------------------------------------------------------------------

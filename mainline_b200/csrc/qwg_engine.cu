@@ -88,7 +88,7 @@ struct qwg_ctx {
   WLayout L{};
   size_t smem_bytes = 0;
   // walkers
-  DevBuf d_R, d_R2, d_state, d_state2, d_scratch, d_branch;
+  DevBuf d_R, d_R2, d_state, d_state2, d_scratch, d_branch, d_tm_cand, d_tm_moves;
   bool state_valid = false;
   bool have_scalars = false;  // WScal.eold / weight written by a block
   // io scratch
@@ -434,7 +434,7 @@ static void ensure_smem_attr(K kern, size_t bytes) {
 template <typename Real, int MM>
 static void launch_walkers_t(qwg_ctx* c, const DevSys<Real>& S, const StepParams& P, const EvalIO& io, int mode,
                              int nwalk) {
-  const bool sw = mode == KM_SWEEP;
+  const bool sw = mode == KM_SWEEP || mode == KM_TMOVE;  // move-phase shared-memory layout
   CK((launch_walker_kernels<Real, MM>(S, c->L, P, io, mode, nwalk, sw ? c->wpc_sweep : c->wpc,
                                       sw ? c->smem_sweep : c->smem_bytes, c->stream)));
   if (nwalk > 0) c->launches++;
@@ -496,6 +496,21 @@ static void ensure_io(qwg_ctx* c, size_t bytes) {
 }
 
 // One chunk of steps on the resident population (plus DMC branching).
+// Candidate and target buffers of the T-moves for nw walkers.
+static int tmove_cap(const qwg_ctx* c) { return c->L.wchunk * c->H.natoms * QWG_MAXQ; }
+static void ensure_tmove_buffers(qwg_ctx* c, int nw) {
+  const size_t cand = (size_t)nw * tmove_cap(c) * 8, mv = (size_t)nw * c->H.nelec * 4 * 8;
+  if (c->d_tm_cand.n < cand) c->d_tm_cand.alloc(cand);
+  if (c->d_tm_moves.n < mv) c->d_tm_moves.alloc(mv);
+}
+static void set_tmoves(qwg_ctx* c, StepParams& P) {
+  P.tmoves = c->dmc.tmoves;
+  if (!P.tmoves) return;
+  P.tm_cap = tmove_cap(c);
+  P.tm_cand = c->d_tm_cand.as<double>();
+  P.tm_moves = c->d_tm_moves.as<double>();
+}
+
 // P.nsteps steps of every walker: one fused launch, or (split schedule) a
 // move launch and a local-energy launch per step.
 static void launch_steps(qwg_ctx* c, StepParams P, const EvalIO& io, int nwalk) {
@@ -507,6 +522,7 @@ static void launch_steps(qwg_ctx* c, StepParams P, const EvalIO& io, int nwalk) 
     P.st = st;
     launch_walkers(c, P, io, KM_SWEEP, nwalk);
     launch_walkers(c, P, io, KM_ELOC, nwalk);
+    if (P.tmoves) launch_walkers(c, P, io, KM_TMOVE, nwalk);
   }
 }
 
@@ -601,6 +617,7 @@ static void enqueue_dmc_block(qwg_ctx* c) {
     P.branch_start = c->branch_start;
     P.branch_stop = c->branch_stop;
     P.max_weight = c->dmc.max_poss_weight;
+    set_tmoves(c, P);
     EvalIO io{};
     launch_steps(c, P, io, c->nwalk);
     run_branch(c, acc + ch, np);
@@ -978,6 +995,10 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
     if (c->dmc.branch_start_cutoff <= 0) c->dmc.branch_start_cutoff = 10.0;
     if (c->dmc.refresh_interval <= 0)
       c->dmc.refresh_interval = c->precision == QWG_FP64 ? c->dmc.feedback_interval : 32;
+    if (c->dmc.tmoves < 0 || c->dmc.tmoves > 2) throw InputError("tmoves must be 0, 1 or 2");
+    if (c->dmc.tmoves && !c->H.has_pp) throw InputError("T-moves need a pseudopotential");
+    if (c->dmc.tmoves && !c->split) throw InputError("T-moves need the split step schedule");
+    if (c->dmc.tmoves) ensure_tmove_buffers(c, c->nwalk);
     const int W = c->nwalk;
     const int nchunk = (c->dmc.nstep + c->dmc.feedback_interval - 1) / c->dmc.feedback_interval;
     if (nchunk > 1024) throw std::runtime_error("too many feedback intervals per block");
@@ -1049,6 +1070,7 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
       launch_walkers(c, Pw, iw, KM_STEPS, W);  // same kernel variant as the block's chunks
       launch_walkers(c, Pw, iw, KM_SWEEP, 0);  // shared-memory attributes of the split kernels
       launch_walkers(c, Pw, iw, KM_ELOC, 0);
+      launch_walkers(c, Pw, iw, KM_TMOVE, 0);
       CK(cudaStreamSynchronize(c->stream));
     }
     if (W > kMaxDmcWalkers) throw InputError("DMC populations above 262144 walkers are beyond this engine build");
@@ -1313,6 +1335,44 @@ int qwg_batch_destroy(qwg_batch* b) {
   if (b->origin) cudaStreamDestroy(b->origin);
   delete b;
   return QWG_OK;
+}
+
+int qwg_tmove_select(qwg_ctx* c, const double* rot, int mode, double tau, uint64_t seed, int* moved, double* pos) {
+  if (!c || !moved || !pos || (mode != 1 && mode != 2) || !(tau > 0)) return QWG_ERR_ARG;
+  if (c->nwalk <= 0) return fail(c, QWG_ERR_STATE, "qwg_tmove_select: no walkers");
+  if (!c->H.has_pp) return fail(c, QWG_ERR_INPUT, "qwg_tmove_select: the deck has no pseudopotential");
+  return guarded(c, [&]() -> int {
+    const int W = c->nwalk, N = c->H.nelec;
+    ensure_tmove_buffers(c, W);
+    const size_t n_rot = (size_t)W * 9, n_g = (size_t)W * N * 3, n_l = (size_t)W * N;
+    ensure_io(c, 8 * (n_rot + 5 * (size_t)W + n_g + n_l));
+    double* base = c->d_io.as<double>();
+    EvalIO io{};
+    io.logpsi = base; io.sign = base + W; io.kinetic = base + 2 * W; io.potential = base + 3 * W;
+    io.nonlocal = base + 4 * W; io.grad = base + 5 * W; io.lap = io.grad + n_g;
+    if (rot) {
+      double* drot = io.lap + n_l;
+      CK(cudaMemcpyAsync(drot, rot, 8 * n_rot, cudaMemcpyHostToDevice, c->stream));
+      io.rot = drot;
+    }
+    StepParams P = base_params(c);
+    P.tmoves = mode;
+    P.tau = tau;
+    P.seed = seed;
+    P.tm_cap = tmove_cap(c);
+    P.tm_cand = c->d_tm_cand.as<double>();
+    P.tm_moves = c->d_tm_moves.as<double>();
+    launch_walkers(c, P, io, KM_EVAL, W);
+    std::vector<double> mv((size_t)W * N * 4);
+    CK(cudaMemcpyAsync(mv.data(), P.tm_moves, mv.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t k = 0; k < (size_t)W * N; k++) {
+      moved[k] = mv[4 * k + 3] != 0.0 ? 1 : 0;
+      for (int d = 0; d < 3; d++) pos[3 * k + d] = mv[4 * k + d];
+    }
+    c->state_valid = false;  // the evaluation used the resident state slots as scratch
+    return QWG_OK;
+  });
 }
 
 int qwg_time_kernels(qwg_ctx* c, int nstep, double* sweep_ms, double* eloc_ms) {

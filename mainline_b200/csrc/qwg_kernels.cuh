@@ -10,7 +10,8 @@ namespace qwg {
 // KM_SWEEP and KM_ELOC split one step into its two phases (the electron
 // moves; the local energy and weight), one launch each, with the same
 // arithmetic and random streams, so the two schedules give identical walks.
-enum KMode { KM_EVAL = 0, KM_RATIO = 1, KM_STEPS = 2, KM_SWEEP = 3, KM_ELOC = 4 };
+// KM_TMOVE applies the T-moves the local-energy kernel selected.
+enum KMode { KM_EVAL = 0, KM_RATIO = 1, KM_STEPS = 2, KM_SWEEP = 3, KM_ELOC = 4, KM_TMOVE = 5 };
 
 struct EvalIO {
   const double* rot;     // [W][9] quadrature rotations (KM_EVAL) or nullptr
@@ -381,10 +382,21 @@ struct Walker {
   // Q-point quadrature of the nonlocal channels for the pairs selected
   // deterministically (r < cutoff) or stochastically (rand < strength, with
   // the nonlocal radials divided by the strength).  rot: 3x3 rows x,y,z.
-  __device__ double pseudo(const double* rotm, bool deterministic, uint64_t seed, uint32_t wid, uint64_t step) {
+  // T-moves: the quadrature terms v_xx of every point go to cand; with
+  // tmoves == 2 every electron then moves to one of its points of negative
+  // v_xx with probability tau |v_xx| / (1 + tau sum |v_xx|), with tmoves == 1
+  // at most one electron of the walker moves, chosen over all such points
+  // (Dmc_method::doTmove, Dmc_method.cpp:850-906; Pseudopotential.cpp:740-763).
+  // The energy keeps every term.  Selected targets go to moves[N][4].
+  __device__ double pseudo(const double* rotm, bool deterministic, uint64_t seed, uint32_t wid, uint64_t step,
+                           int tmoves = 0, double tm_tau = 0.0, double* cand = nullptr, double* moves = nullptr) {
     const double* Rp = R();
     const int N = S.nelec, A = S.natoms;
     double vloc = 0;
+    if (tmoves)
+      for (int e = lane; e < N; e += 32) moves[4 * e + 3] = 0.0;
+    double res_total = 1.0, res_x = 0, res_y = 0, res_z = 0;  // one-move-per-walker reservoir
+    int res_e = -1;
     // per-electron Jastrow value at the current position
     for (int e = lane; e < N; e += 32)
       Ue()[e] = double(jas_electron_val<Real, TB>(S, Rp, e, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2]));
@@ -481,9 +493,81 @@ struct Walker {
         double ts = 0;
         for (int ll = 0; ll < 4; ll++) ts += (2 * ll + 1) * I.vl[ll] * P[ll];
         vnl += ts * ratio;
+        if (tmoves) cand[p] = ts * ratio;
       }
       __syncwarp();
+      if (tmoves) {
+        // target of point p of this chunk (the same arithmetic as above)
+        auto point_pos = [&](int p, double& x, double& y, double& z) {
+          int kk = 0, qo = 0;
+          while (p >= qo + S.pp_aip[S.atom_type[it[kk].a]]) { qo += S.pp_aip[S.atom_type[it[kk].a]]; kk++; }
+          const PPItem& I = it[kk];
+          const double* q0 = S.pp_quad[S.atom_type[I.a]][p - qo];
+          const double qx = q0[0] * rotm[0] + q0[1] * rotm[3] + q0[2] * rotm[6];
+          const double qy = q0[0] * rotm[1] + q0[1] * rotm[4] + q0[2] * rotm[7];
+          const double qz = q0[0] * rotm[2] + q0[1] * rotm[5] + q0[2] * rotm[8];
+          x = Rp[3 * I.e] + qx * I.r - I.dx; y = Rp[3 * I.e + 1] + qy * I.r - I.dy; z = Rp[3 * I.e + 2] + qz * I.r - I.dz;
+          wrap_pos(S, x, y, z);
+        };
+        if (tmoves == 2) {
+          // size-consistent: lanes over the chunk's electrons; the points of
+          // one electron are contiguous (items are in electron order)
+          for (int e = e0 + lane; e < e1; e += 32) {
+            int pb = 0, k = 0;
+            for (; k < nitems && it[k].e < e; k++) pb += S.pp_aip[S.atom_type[it[k].a]];
+            int pe = pb;
+            for (; k < nitems && it[k].e == e; k++) pe += S.pp_aip[S.atom_type[it[k].a]];
+            if (pe == pb) continue;
+            double sum = 1.0;
+            for (int p = pb; p < pe; p++)
+              if (cand[p] < 0) sum -= tm_tau * cand[p];
+            const double x = rand4(seed, wid, step, (uint32_t)e, 8u).u[0] * sum;
+            if (!(x > 1.0)) continue;
+            double sel = 1.0;
+            for (int p = pb; p < pe; p++) {
+              if (!(cand[p] < 0)) continue;
+              sel -= tm_tau * cand[p];
+              if (x < sel) {
+                point_pos(p, moves[4 * e], moves[4 * e + 1], moves[4 * e + 2]);
+                moves[4 * e + 3] = 1.0;
+                break;
+              }
+            }
+          }
+        } else {
+          // one move per walker over all electrons: a weighted reservoir
+          // across the chunks (same distribution as one draw over all terms)
+          double tc = 0.0;
+          for (int p = 0; p < total; p++)
+            if (cand[p] < 0) tc -= tm_tau * cand[p];
+          if (tc > 0) {
+            const Rand4 r = rand4(seed, wid, step, 0x10000u + (uint32_t)e0, 9u);
+            res_total += tc;
+            if (r.u[1] * res_total < tc) {
+              const double x = r.u[0] * tc;
+              double sel = 0.0;
+              for (int p = 0; p < total; p++) {
+                if (!(cand[p] < 0)) continue;
+                sel -= tm_tau * cand[p];
+                if (x < sel || p == total - 1) {
+                  int kk = 0, qo = 0;
+                  while (p >= qo + S.pp_aip[S.atom_type[it[kk].a]]) { qo += S.pp_aip[S.atom_type[it[kk].a]]; kk++; }
+                  res_e = it[kk].e;
+                  point_pos(p, res_x, res_y, res_z);
+                  break;
+                }
+              }
+            }
+          }
+        }
+        __syncwarp();
+      }
     }
+    if (tmoves == 1 && res_e >= 0 && lane == 0) {
+      moves[4 * res_e] = res_x; moves[4 * res_e + 1] = res_y; moves[4 * res_e + 2] = res_z;
+      moves[4 * res_e + 3] = 1.0;
+    }
+    __syncwarp();
     return warp_sum(vloc) + warp_sum(vnl);
   }
 };
@@ -543,7 +627,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
   constexpr bool HBM = MMAX == 0;  // walker worked on in place in HBM
   if (wid < P.nwalk) {
     unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
-    constexpr bool SWEEP_ONLY = mode == KM_SWEEP;
+    constexpr bool SWEEP_ONLY = mode == KM_SWEEP || mode == KM_TMOVE;  // move-phase shared memory only
     unsigned char* wb = HBM ? gstate : smem + moc_bytes + (size_t)warp * (SWEEP_ONLY ? L.sweep_bytes : L.bytes);
     unsigned char* sb = HBM ? P.scratch + (size_t)wid * L.scratch_bytes : wb + L.state_bytes;
     Walker<Real, MMAX, TB> W{S, L, wb, sb, moc_s, lane};
@@ -555,8 +639,8 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       const uint64_t R = (uint64_t)P.refresh_every, m = step0 % R;
       refresh = (m == 0 || m + (uint64_t)P.nsteps > R) ? 1 : 0;
     }
-    if (mode == KM_ELOC || (mode == KM_SWEEP && P.st > 0)) refresh = 0;  // only a chunk's first sweep
-    constexpr bool STEPS = mode == KM_STEPS || mode == KM_SWEEP || mode == KM_ELOC;
+    if (mode == KM_ELOC || mode == KM_TMOVE || (mode == KM_SWEEP && P.st > 0)) refresh = 0;  // a chunk's first sweep only
+    constexpr bool STEPS = mode == KM_STEPS || mode == KM_SWEEP || mode == KM_ELOC || mode == KM_TMOVE;
     if (!STEPS || refresh) {
       for (int i = lane; i < 3 * N; i += 32) Rp[i] = P.R[(size_t)wid * 3 * N + i];
       __syncwarp();
@@ -589,7 +673,11 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       }
       double kin = W.kinetic();
       double pot = W.coulomb();
-      double nl = S.has_pp ? W.pseudo(rm, true, 0, wid, 0) : 0.0;
+      // P.tmoves here: T-move selection for qwg_tmove_select (no move is made)
+      double nl = S.has_pp ? W.pseudo(rm, true, P.seed, wid, 0, P.tmoves, P.tau,
+                                      P.tmoves ? P.tm_cand + (size_t)wid * P.tm_cap : nullptr,
+                                      P.tmoves ? P.tm_moves + (size_t)wid * N * 4 : nullptr)
+                           : 0.0;
       if (lane == 0) {
         WScal* w = W.sc();
         io.logpsi[wid] = w->logdet[0] + w->logdet[1] + w->U;
@@ -610,6 +698,24 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
         io.sign[wid] = ratioD < 0 ? -1.0 : 1.0;
         io.grad[3 * (size_t)wid] = g[0]; io.grad[3 * (size_t)wid + 1] = g[1]; io.grad[3 * (size_t)wid + 2] = g[2];
         io.lap[wid] = l;
+      }
+    } else if constexpr (mode == KM_TMOVE) {
+      // the T-moves selected by the last local-energy pass: each chosen
+      // electron moves to its quadrature point (Sample_point::translateElectron)
+      const double* mv = P.tm_moves + (size_t)wid * N * 4;
+      for (int e = 0; e < N; e++) {
+        if (mv[4 * e + 3] == 0.0) continue;
+        const double px = mv[4 * e], py = mv[4 * e + 1], pz = mv[4 * e + 2];
+        double ratioD, dU, g[3], l;
+        W.propose(e, px, py, pz, ratioD, dU, g, l);
+        if (isfinite(ratioD) && ratioD != 0.0 && isfinite(dU)) W.accept(e, px, py, pz, ratioD, dU);
+      }
+      __syncwarp();
+      for (int i = lane; i < 3 * N; i += 32) P.R[(size_t)wid * 3 * N + i] = Rp[i];
+      if constexpr (!HBM) {
+        int4* dst = (int4*)gstate;
+        const int4* src = (const int4*)wb;
+        for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
       }
     } else {
       // ---- VMC / DMC steps (KM_STEPS: P.nsteps steps; KM_SWEEP / KM_ELOC:
@@ -672,7 +778,10 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
           random_rotation(rr, rm);
           double kin = W.kinetic();
           double pot = W.coulomb();
-          double nl = S.has_pp ? W.pseudo(rm, P.deterministic_pp != 0, P.seed, wid, step) : 0.0;
+          double nl = S.has_pp ? W.pseudo(rm, P.deterministic_pp != 0, P.seed, wid, step, P.tmoves, P.tau,
+                                          P.tmoves ? P.tm_cand + (size_t)wid * P.tm_cap : nullptr,
+                                          P.tmoves ? P.tm_moves + (size_t)wid * N * 4 : nullptr)
+                               : 0.0;
           double el = kin + pot + nl;
           WScal* w = W.sc();
           double wt = 1.0;

@@ -31,7 +31,7 @@ EXPORTS = [
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
     "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready", "qwg_time_kernels",
     "qwg_log_header", "qwg_log_block", "qwg_write_configs", "qwg_count_configs", "qwg_read_configs",
-    "qwg_store_configs",
+    "qwg_store_configs", "qwg_tmove_select",
     "qwg_server_create", "qwg_server_destroy", "qwg_server_submit", "qwg_server_progress",
     "qwg_server_get_status", "qwg_server_last_error",
 ]
@@ -69,7 +69,7 @@ class DmcParams(C.Structure):
     _fields_ = [("timestep", C.c_double), ("nstep", C.c_int), ("feedback_interval", C.c_int),
                 ("feedback", C.c_double), ("max_poss_weight", C.c_double),
                 ("branch_start_cutoff", C.c_double), ("refresh_interval", C.c_int),
-                ("deterministic_pp", C.c_int), ("seed", C.c_uint64)]
+                ("deterministic_pp", C.c_int), ("seed", C.c_uint64), ("tmoves", C.c_int)]
 
 
 class JobDesc(C.Structure):
@@ -138,6 +138,7 @@ def load_library(path: str = LIB_PATH):
         "qwg_count_configs": (C.c_int, [C.c_char_p, P(C.c_int), P(C.c_int)]),
         "qwg_read_configs": (C.c_int, [C.c_char_p, dp, dp, dp, C.c_int, C.c_int, P(C.c_int)]),
         "qwg_store_configs": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+        "qwg_tmove_select": (C.c_int, [C.c_void_p, dp, C.c_int, C.c_double, C.c_uint64, P(C.c_int), dp]),
         "qwg_server_create": (C.c_int, [C.c_ulonglong, C.c_int, P(C.c_void_p)]),
         "qwg_server_destroy": (C.c_int, [C.c_void_p]),
         "qwg_server_submit": (C.c_int, [C.c_void_p, P(JobDesc), P(C.c_int)]),
@@ -281,9 +282,9 @@ class Engine:
 
     def dmc_init(self, timestep: float, nstep: int = 0, seed: int = 1, feedback_interval: int = 5,
                  feedback: float = 1.0, max_poss_weight: float = 7.0, branch_start_cutoff: float = 10.0,
-                 refresh_interval: int = 0, deterministic_pp: bool = False):
+                 refresh_interval: int = 0, deterministic_pp: bool = False, tmoves: int = 0):
         p = DmcParams(timestep, nstep, feedback_interval, feedback, max_poss_weight, branch_start_cutoff,
-                      refresh_interval, int(deterministic_pp), seed)
+                      refresh_interval, int(deterministic_pp), seed, tmoves)
         self._check(self.lib.qwg_dmc_init(self.h, C.byref(p)), "qwg_dmc_init")
 
     def dmc_block(self) -> dict:
@@ -312,6 +313,18 @@ class Engine:
         a, b = C.c_double(0), C.c_double(0)
         self._check(self.lib.qwg_time_kernels(self.h, nstep, C.byref(a), C.byref(b)), "qwg_time_kernels")
         return a.value, b.value
+
+    def tmove_select(self, mode: int, tau: float, seed: int = 1, rot: np.ndarray | None = None):
+        """T-move selection (deterministic PP) without moving: (moved [W, N]
+        int, target [W, N, 3])."""
+        W, N = self.nwalk, self.nelec
+        moved = np.zeros((W, N), dtype=np.int32)
+        pos = np.zeros((W, N, 3))
+        r = None if rot is None else np.ascontiguousarray(rot, dtype=np.float64)
+        self._check(self.lib.qwg_tmove_select(self.h, _ptr(r) if r is not None else None, mode, tau, seed,
+                                              moved.ctypes.data_as(C.POINTER(C.c_int)), _ptr(pos)),
+                    "qwg_tmove_select")
+        return moved, pos
 
     def store_configs(self, path: str, dmc: bool = False):
         """Write the resident walkers as a QWalk configuration file."""

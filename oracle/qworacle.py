@@ -710,6 +710,39 @@ class System:
                     tot += np.where(acc, ts * ratio, 0.0)
         return tot
 
+    def tmove_terms(self, R, rot):
+        """Per quadrature point terms of the deterministic nonlocal PP for one
+        configuration R [N,3] and rotation rot [3,3]: list of (electron,
+        target position, v_xx) with v_xx = sum_l (2l+1) v_l(r) P_l(cos) *
+        psi(target)/psi(R) * w_q, the T-move matrix elements of
+        Pseudopotential::calcNonlocWithAllvariables (Pseudopotential.cpp:740-763)."""
+        R = self.wrap(np.asarray(R, dtype=float)[None])
+        N = R.shape[1]
+        lp0, sg0 = self.logpsi(R)
+        out = []
+        for a, lab in enumerate(self.labels):
+            p = self.pp.get(lab)
+            if p is None:
+                continue
+            d = self.min_image(R - self.atoms[a])
+            r = np.sqrt(np.sum(d * d, axis=-1))
+            vl = self._vl(p["chans"], r)
+            nl = len(p["chans"])
+            q = p["quad"] @ np.asarray(rot, dtype=float)
+            for e in range(N):
+                if not r[0, e] < p["cutoff"]:
+                    continue
+                for iq in range(len(p["w"])):
+                    Rn = R.copy()
+                    Rn[:, e] = R[:, e] + q[iq] * r[:, e:e + 1] - d[:, e]
+                    Rn = self.wrap(Rn)
+                    lp, sg = self.logpsi(Rn)
+                    ratio = np.exp(lp - lp0) * sg * sg0 * p["w"][iq]
+                    cosq = np.sum(q[iq] * d[0, e]) / r[0, e]
+                    ts = sum((2 * l + 1) * vl[l][0, e] * legendre(cosq, l) for l in range(nl - 1))
+                    out.append((e, Rn[0, e].copy(), float(ts * ratio[0])))
+        return out
+
     def move_ratio(self, R, e, rnew):
         """ln|psi(R')| - ln|psi(R)|, sign ratio, grad and lap of electron e at R'."""
         R = np.asarray(R, dtype=float)
