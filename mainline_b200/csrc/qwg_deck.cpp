@@ -703,6 +703,7 @@ HostSystem build_system(const std::string& deck_path) {
   auto detwt = get_section(wf1, "DETWT");
   if (detwt.size() != 1) throw InputError("only single-determinant SLATER is supported");
   if (has_section(wf1, "CSF")) throw InputError("CSF expansions are not supported");
+  if (has_section(wf1, "CORBITALS")) throw InputError("complex orbitals (CORBITALS) are not supported");
   auto orbw = get_section(wf1, "ORBITALS");
   if (!orbw.empty() && (ieq(orbw[0], "CUTOFF_MO") || ieq(orbw[0], "EINSPLINE_MO") || ieq(orbw[0], "BASFUNC_MO")))
     throw InputError("ORBITALS type " + orbw[0] + " not supported (the dense BLAS_MO evaluator is used)");

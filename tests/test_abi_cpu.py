@@ -65,3 +65,21 @@ def test_bad_deck_reports_error(lib, tmp_path):
     p.write_text("SYSTEM { MOLECULE NSPIN { 1 0 } ATOM { H 1 COOR 0 0 0 } }\nTRIALFUNC { SLATER }\n")
     with pytest.raises(engine.QwgError, match="SLATER-JASTROW"):
         engine.inspect_deck(str(p))
+
+
+@pytest.mark.parametrize("edit,msg", [
+    (lambda t: t.replace("DETWT { 1.0 }", "DETWT { 0.9 0.1 }"), "single-determinant"),
+    (lambda t: t.replace("ORBITALS { BLAS_MO", "CORBITALS { BLAS_MO"), "complex orbitals"),
+])
+def test_unsupported_wavefunctions_are_rejected(lib, tmp_path, edit, msg):
+    """Multi-determinant expansions and complex orbitals are outside this
+    engine: the deck is rejected with a clear message, not run wrongly."""
+    import shutil
+    src = os.path.join(GOLDEN, "n2_pseudo.qw")
+    shutil.copy(os.path.join(GOLDEN, "n2_pseudo.orb"), tmp_path)
+    text = open(src).read()
+    assert "DETWT { 1.0 }" in text and "ORBITALS { BLAS_MO" in text
+    p = tmp_path / "x.qw"
+    p.write_text(edit(text))
+    with pytest.raises(engine.QwgError, match=msg):
+        engine.inspect_deck(str(p))
