@@ -521,7 +521,7 @@ static void launch_steps(qwg_ctx* c, StepParams P, const EvalIO& io, int nwalk) 
   for (int st = 0; st < P.nsteps; st++) {
     P.st = st;
     launch_walkers(c, P, io, KM_SWEEP, nwalk);
-    launch_walkers(c, P, io, KM_ELOC, nwalk);
+    launch_walkers(c, P, io, P.tmoves ? KM_ELOC_TM : KM_ELOC, nwalk);
     if (P.tmoves) launch_walkers(c, P, io, KM_TMOVE, nwalk);
   }
 }
@@ -1070,6 +1070,7 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
       launch_walkers(c, Pw, iw, KM_STEPS, W);  // same kernel variant as the block's chunks
       launch_walkers(c, Pw, iw, KM_SWEEP, 0);  // shared-memory attributes of the split kernels
       launch_walkers(c, Pw, iw, KM_ELOC, 0);
+      launch_walkers(c, Pw, iw, KM_ELOC_TM, 0);
       launch_walkers(c, Pw, iw, KM_TMOVE, 0);
       CK(cudaStreamSynchronize(c->stream));
     }

@@ -11,7 +11,8 @@ namespace qwg {
 // moves; the local energy and weight), one launch each, with the same
 // arithmetic and random streams, so the two schedules give identical walks.
 // KM_TMOVE applies the T-moves the local-energy kernel selected.
-enum KMode { KM_EVAL = 0, KM_RATIO = 1, KM_STEPS = 2, KM_SWEEP = 3, KM_ELOC = 4, KM_TMOVE = 5 };
+// KM_ELOC_TM is KM_ELOC with the T-move selection compiled in.
+enum KMode { KM_EVAL = 0, KM_RATIO = 1, KM_STEPS = 2, KM_SWEEP = 3, KM_ELOC = 4, KM_TMOVE = 5, KM_ELOC_TM = 6 };
 
 struct EvalIO {
   const double* rot;     // [W][9] quadrature rotations (KM_EVAL) or nullptr
@@ -388,8 +389,10 @@ struct Walker {
   // at most one electron of the walker moves, chosen over all such points
   // (Dmc_method::doTmove, Dmc_method.cpp:850-906; Pseudopotential.cpp:740-763).
   // The energy keeps every term.  Selected targets go to moves[N][4].
+  template <bool TMV = false>
   __device__ double pseudo(const double* rotm, bool deterministic, uint64_t seed, uint32_t wid, uint64_t step,
-                           int tmoves = 0, double tm_tau = 0.0, double* cand = nullptr, double* moves = nullptr) {
+                           int tmoves_ = 0, double tm_tau = 0.0, double* cand = nullptr, double* moves = nullptr) {
+    const int tmoves = TMV ? tmoves_ : 0;  // T-move code only in the TMV instantiation
     const double* Rp = R();
     const int N = S.nelec, A = S.natoms;
     double vloc = 0;
@@ -608,6 +611,8 @@ template <>
 struct MinBlocks<KM_SWEEP> { static constexpr int value = QWG_MIN_BLOCKS_SWEEP; };
 template <>
 struct MinBlocks<KM_ELOC> { static constexpr int value = QWG_MIN_BLOCKS_ELOC; };
+template <>
+struct MinBlocks<KM_ELOC_TM> { static constexpr int value = QWG_MIN_BLOCKS_ELOC; };
 
 template <typename Real, int MMAX, int mode, bool TB>
 __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
@@ -639,8 +644,9 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       const uint64_t R = (uint64_t)P.refresh_every, m = step0 % R;
       refresh = (m == 0 || m + (uint64_t)P.nsteps > R) ? 1 : 0;
     }
-    if (mode == KM_ELOC || mode == KM_TMOVE || (mode == KM_SWEEP && P.st > 0)) refresh = 0;  // a chunk's first sweep only
-    constexpr bool STEPS = mode == KM_STEPS || mode == KM_SWEEP || mode == KM_ELOC || mode == KM_TMOVE;
+    constexpr bool ELOCM = mode == KM_ELOC || mode == KM_ELOC_TM;  // local-energy phase
+    if (ELOCM || mode == KM_TMOVE || (mode == KM_SWEEP && P.st > 0)) refresh = 0;  // a chunk's first sweep only
+    constexpr bool STEPS = mode == KM_STEPS || mode == KM_SWEEP || ELOCM || mode == KM_TMOVE;
     if (!STEPS || refresh) {
       for (int i = lane; i < 3 * N; i += 32) Rp[i] = P.R[(size_t)wid * 3 * N + i];
       __syncwarp();
@@ -674,10 +680,14 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       double kin = W.kinetic();
       double pot = W.coulomb();
       // P.tmoves here: T-move selection for qwg_tmove_select (no move is made)
-      double nl = S.has_pp ? W.pseudo(rm, true, P.seed, wid, 0, P.tmoves, P.tau,
-                                      P.tmoves ? P.tm_cand + (size_t)wid * P.tm_cap : nullptr,
-                                      P.tmoves ? P.tm_moves + (size_t)wid * N * 4 : nullptr)
-                           : 0.0;
+      double nl = 0.0;
+      if (S.has_pp) {
+        if (P.tmoves)
+          nl = W.template pseudo<true>(rm, true, P.seed, wid, 0, P.tmoves, P.tau, P.tm_cand + (size_t)wid * P.tm_cap,
+                                       P.tm_moves + (size_t)wid * N * 4);
+        else
+          nl = W.pseudo(rm, true, 0, wid, 0);
+      }
       if (lane == 0) {
         WScal* w = W.sc();
         io.logpsi[wid] = w->logdet[0] + w->logdet[1] + w->U;
@@ -729,7 +739,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       const int st0 = mode == KM_STEPS ? 0 : P.st, st1 = mode == KM_STEPS ? P.nsteps : P.st + 1;
       for (int st = st0; st < st1; st++) {
         const uint64_t step = step0 + st;
-        if constexpr (mode != KM_ELOC) {
+        if constexpr (!ELOCM) {
           for (int e = 0; e < N; e++) {
             // Split_sampler::split_driver depth 1 (Split_sample.cpp:380-478)
             double g0[3], l0;
@@ -778,10 +788,14 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
           random_rotation(rr, rm);
           double kin = W.kinetic();
           double pot = W.coulomb();
-          double nl = S.has_pp ? W.pseudo(rm, P.deterministic_pp != 0, P.seed, wid, step, P.tmoves, P.tau,
-                                          P.tmoves ? P.tm_cand + (size_t)wid * P.tm_cap : nullptr,
-                                          P.tmoves ? P.tm_moves + (size_t)wid * N * 4 : nullptr)
-                               : 0.0;
+          double nl = 0.0;
+          if (S.has_pp) {
+            if constexpr (mode == KM_ELOC_TM)
+              nl = W.template pseudo<true>(rm, P.deterministic_pp != 0, P.seed, wid, step, P.tmoves, P.tau,
+                                           P.tm_cand + (size_t)wid * P.tm_cap, P.tm_moves + (size_t)wid * N * 4);
+            else
+              nl = W.pseudo(rm, P.deterministic_pp != 0, P.seed, wid, step);
+          }
           double el = kin + pot + nl;
           WScal* w = W.sc();
           double wt = 1.0;
@@ -810,7 +824,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
         }
       }
       if (lane == 0) {
-        if (mode != KM_ELOC) { atomicAdd(&cta_acc[6], nacc); atomicAdd(&cta_acc[7], natt); }
+        if (!ELOCM) { atomicAdd(&cta_acc[6], nacc); atomicAdd(&cta_acc[7], natt); }
         if (mode != KM_SWEEP) {
           atomicAdd(&cta_acc[0], sw); atomicAdd(&cta_acc[1], swe); atomicAdd(&cta_acc[2], swk);
           atomicAdd(&cta_acc[3], swv); atomicAdd(&cta_acc[4], swnl); atomicAdd(&cta_acc[5], swe2);
@@ -823,12 +837,12 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       // write back: positions and the resident state after moves; only the
       // walker scalars after a local-energy pass
       __syncwarp();
-      if (mode != KM_ELOC)
+      if (!ELOCM)
         for (int i = lane; i < 3 * N; i += 32) P.R[(size_t)wid * 3 * N + i] = Rp[i];
       if constexpr (!HBM) {
         int4* dst = (int4*)gstate;
         const int4* src = (const int4*)wb;
-        if (mode == KM_ELOC) {
+        if (ELOCM) {
           for (int i = lane; i < (int)sizeof(WScal) / 16; i += 32) ((int4*)(gstate + L.scal))[i] = ((const int4*)(wb + L.scal))[i];
         } else {
           for (int i = lane; i < L.state_bytes / 16; i += 32) dst[i] = src[i];
@@ -836,7 +850,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       }
     }
   }
-  if constexpr (mode == KM_STEPS || mode == KM_SWEEP || mode == KM_ELOC) {
+  if constexpr (mode == KM_STEPS || mode == KM_SWEEP || mode == KM_ELOC || mode == KM_ELOC_TM) {
     __syncthreads();
     if (threadIdx.x < QWG_NACC) atomicAdd(&((double*)P.acc)[threadIdx.x], cta_acc[threadIdx.x]);
   }

@@ -52,6 +52,7 @@ cudaError_t launch_walker_kernels(const DevSys<Real>& S, const WLayout& L, const
   if (mode == KM_SWEEP) return launch_mode<Real, MM, KM_SWEEP>(S, L, P, io, nwalk, wpc, smem, stream);
   if (mode == KM_ELOC) return launch_mode<Real, MM, KM_ELOC>(S, L, P, io, nwalk, wpc, smem, stream);
   if (mode == KM_TMOVE) return launch_mode<Real, MM, KM_TMOVE>(S, L, P, io, nwalk, wpc, smem, stream);
+  if (mode == KM_ELOC_TM) return launch_mode<Real, MM, KM_ELOC_TM>(S, L, P, io, nwalk, wpc, smem, stream);
   return launch_mode<Real, MM, KM_STEPS>(S, L, P, io, nwalk, wpc, smem, stream);
 }
 
