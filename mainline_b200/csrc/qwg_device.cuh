@@ -415,7 +415,9 @@ __device__ __forceinline__ int sym_nfunc(int sym) { return sym == 0 ? 1 : sym ==
 // Laplacian of the tight shells cancels strongly), basis rows go to bas
 // [nbasis][5] as Real, then lanes split the (MO, component) outputs of the
 // contraction with the MO coefficients moc_s [nbasis][mstride].
-template <typename Real>
+// PER: 0 molecule, 1 periodic cell (compiled for that case only), 2 decided
+// at run time from S.periodic.
+template <typename Real, int PER>
 __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz, int M,
                             Real* bas, Real* out, int lane) {
   for (int s = lane; s < S.nshell; s += 32) {
@@ -424,7 +426,7 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
     Real* b = bas + si.z * 5;
     const int nf = sym_nfunc(si.y);
     const double cut = S.shell_cut[s];
-    if (!S.periodic) {
+    if (PER == 0 || (PER == 2 && !S.periodic)) {
       const double* ap = S.atom_pos[si.x];
       double dx = px - ap[0], dy = py - ap[1], dz = pz - ap[2];
       double r = sqrt(dx * dx + dy * dy + dz * dz);

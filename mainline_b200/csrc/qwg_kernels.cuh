@@ -38,7 +38,9 @@ struct PPItem {
 // MMAX > 0: at most MMAX orbitals per spin, state + scratch in shared
 // memory.  MMAX == 0: any count up to 256 per spin, arrays strided by
 // L.mstride and worked on in place in HBM.
-template <typename Real, int MMAX, bool TB>
+// PER: 0 molecule, 1 periodic cell, 2 either (decided at run time); the
+// local-energy kernels are compiled per case, the others check at run time.
+template <typename Real, int MMAX, bool TB, int PER>
 struct Walker {
   const DevSys<Real>& S;
   const WLayout& L;
@@ -82,7 +84,7 @@ struct Walker {
       const int e0 = s == 0 ? 0 : S.nup;
       for (int el = 0; el < M; el++) {
         const int e = e0 + el;
-        mo_lap_warp(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], M, bas(), nc, lane);
+        mo_lap_warp<Real, PER>(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], M, bas(), nc, lane);
         for (int i = lane; i < M; i += 32) {
           aug[el * 2 * M + i] = double(nc[i * 5]);
           Real* mv = mov() + ((size_t)e * MS() + i) * 4;
@@ -140,7 +142,7 @@ struct Walker {
     const int s = spin(e), el = eloc(e), M = S.m[s];
     const double* Rp = R();
     Real* nc = newcol();
-    mo_lap_warp(S, mocs(s), px, py, pz, M, bas(), nc, lane);
+    mo_lap_warp<Real, PER>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
     const Real* iv = inv(s) + (size_t)el * MS();
     double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
     for (int i = 0; i < M; i++) {
@@ -346,7 +348,7 @@ struct Walker {
 
   // Molecular_system::calcLoc (Molecular_system.cpp:209-287), no field.
   __device__ double coulomb() const {
-    if (S.periodic) return ewald();
+    if (PER == 1 || (PER == 2 && S.periodic)) return ewald();
     const double* Rp = R();
     const int N = S.nelec, A = S.natoms;
     double v = 0;
@@ -483,7 +485,9 @@ struct Walker {
                nz = Rp[3 * I.e + 2] + qz * I.r - I.dz;
         wrap_pos(S, nx, ny, nz);
         const Real* wr = w + (I.e - e0) * S.nbasis;
-        const Real rd = S.periodic ? basis_dot_lane_periodic(S, nx, ny, nz, wr) : basis_dot_lane(S, nx, ny, nz, wr);
+        Real rd;
+        if (PER == 1 || (PER == 2 && S.periodic)) rd = basis_dot_lane_periodic(S, nx, ny, nz, wr);
+        else rd = basis_dot_lane(S, nx, ny, nz, wr);
         const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);
         double ratio = double(rd * exp(u - Real(Ue()[I.e]))) * S.pp_w[ty][q];
         // cos of the angle between the original and the quadrature direction
@@ -614,7 +618,7 @@ struct MinBlocks<KM_ELOC> { static constexpr int value = QWG_MIN_BLOCKS_ELOC; };
 template <>
 struct MinBlocks<KM_ELOC_TM> { static constexpr int value = QWG_MIN_BLOCKS_ELOC; };
 
-template <typename Real, int MMAX, int mode, bool TB>
+template <typename Real, int MMAX, int mode, bool TB, int PER>
 __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
     k_walkers(const __grid_constant__ DevSys<Real> S, const __grid_constant__ WLayout L, StepParams P, EvalIO io) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -635,7 +639,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
     constexpr bool SWEEP_ONLY = mode == KM_SWEEP || mode == KM_TMOVE;  // move-phase shared memory only
     unsigned char* wb = HBM ? gstate : smem + moc_bytes + (size_t)warp * (SWEEP_ONLY ? L.sweep_bytes : L.bytes);
     unsigned char* sb = HBM ? P.scratch + (size_t)wid * L.scratch_bytes : wb + L.state_bytes;
-    Walker<Real, MMAX, TB> W{S, L, wb, sb, moc_s, lane};
+    Walker<Real, MMAX, TB, PER> W{S, L, wb, sb, moc_s, lane};
     const int N = S.nelec;
     double* Rp = W.R();
     const uint64_t step0 = P.dyn_step ? (uint64_t)P.etrial[DYN_STEP] : P.step0;
