@@ -699,9 +699,10 @@ HostSystem build_system(const std::string& deck_path) {
   if (wf1.empty() || !ieq(wf1[0], "SLATER")) throw InputError("WF1 must be SLATER");
   if (wf2.empty() || !ieq(wf2[0], "JASTROW2")) throw InputError("WF2 must be JASTROW2");
 
-  // Slater: single determinant
+  // Slater: one or more determinants (DETWT weights, STATES per determinant)
   auto detwt = get_section(wf1, "DETWT");
-  if (detwt.size() != 1) throw InputError("only single-determinant SLATER is supported");
+  if (detwt.empty()) throw InputError("Need DETWT in SLATER section");
+  if (detwt.size() > 64) throw InputError("more than 64 determinants: beyond this engine build");
   if (has_section(wf1, "CSF")) throw InputError("CSF expansions are not supported");
   if (has_section(wf1, "CORBITALS")) throw InputError("complex orbitals (CORBITALS) are not supported");
   auto orbw = get_section(wf1, "ORBITALS");
@@ -758,17 +759,41 @@ HostSystem build_system(const std::string& deck_path) {
   std::vector<double> moc_all;
   read_orb(orbfile, nmo, nfunc_center, moc_all);
   auto states = get_section(wf1, "STATES");
-  if ((int)states.size() != S.nelec) throw InputError("STATES must list nup+ndown orbitals");
+  const int ndet = (int)detwt.size();
+  if ((int)states.size() != ndet * S.nelec)
+    throw InputError("STATES must list nup+ndown orbitals for every determinant");
+  S.nel_s[0] = S.nup; S.nel_s[1] = S.ndn;
+  S.detwt.resize(ndet);
+  S.det_ud.assign((size_t)ndet * 2, 0);
   for (int s = 0; s < 2; s++) {
-    int ne = s == 0 ? S.nup : S.ndn, off = s == 0 ? 0 : S.nup;
-    S.nmo[s] = ne;
-    S.moc[s].assign((size_t)S.nbasis * std::max(ne, 1), 0.0);
-    for (int i = 0; i < ne; i++) {
-      int mo = to_i(states[off + i]) - 1;
-      if (mo < 0 || mo >= nmo) throw InputError("STATES entry beyond NMO");
-      for (int f = 0; f < S.nbasis; f++) S.moc[s][(size_t)f * ne + i] = moc_all[(size_t)f * nmo + mo];
+    const int ne = S.nel_s[s];
+    std::vector<int> uni;                     // union of this spin's orbitals, first-use order
+    std::vector<std::vector<int>> uorbs;      // distinct spin-determinants (MO lists)
+    for (int k = 0; k < ndet; k++) {
+      std::vector<int> orbs(ne);
+      for (int i = 0; i < ne; i++) {
+        int mo = to_i(states[(size_t)k * S.nelec + (s == 0 ? 0 : S.nup) + i]) - 1;
+        if (mo < 0 || mo >= nmo) throw InputError("STATES entry beyond NMO");
+        orbs[i] = mo;
+        if (std::find(uni.begin(), uni.end(), mo) == uni.end()) uni.push_back(mo);
+      }
+      int u = (int)(std::find(uorbs.begin(), uorbs.end(), orbs) - uorbs.begin());
+      if (u == (int)uorbs.size()) uorbs.push_back(orbs);
+      S.det_ud[2 * k + s] = u;
+    }
+    if (uorbs.size() > 16) throw InputError("more than 16 distinct determinants of one spin: beyond this engine build");
+    S.nmo[s] = (int)uni.size();
+    S.moc[s].assign((size_t)S.nbasis * std::max(S.nmo[s], 1), 0.0);
+    for (int j = 0; j < S.nmo[s]; j++)
+      for (int f = 0; f < S.nbasis; f++) S.moc[s][(size_t)f * S.nmo[s] + j] = moc_all[(size_t)f * nmo + uni[j]];
+    S.udet_cols[s].clear();
+    for (auto& o : uorbs) {
+      std::vector<int> cols(ne);
+      for (int i = 0; i < ne; i++) cols[i] = (int)(std::find(uni.begin(), uni.end(), o[i]) - uni.begin());
+      S.udet_cols[s].push_back(cols);
     }
   }
+  for (int k = 0; k < ndet; k++) S.detwt[k] = to_d(detwt[k]);
 
   // ---- Jastrow groups
   S.ei_first.assign(S.natoms, 0);

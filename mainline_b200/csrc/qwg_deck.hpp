@@ -78,9 +78,18 @@ struct HostSystem {
   double spline_spacing = 0.02;
   std::vector<double> spline_coef;   // [nspline][npts][4]
   std::vector<int> obj_first, obj_count;   // per basis object: its splines
-  // molecular orbitals per spin: [nbasis][m_s]
+  // molecular orbitals per spin: [nbasis][nmo_s], the union of the orbitals
+  // the determinants of that spin occupy (one determinant: its occupied
+  // orbitals in STATES order)
   int nmo[2] = {0, 0};
   std::vector<double> moc[2];
+  // determinant expansion sum_k detwt[k] D_up(det_ud[k][0]) D_down(det_ud[k][1])
+  // over the distinct spin-determinants; udet_cols[s][u] = the union columns
+  // of spin-determinant u in STATES order (Slat_wf_data.cpp:34-303)
+  int nel_s[2] = {0, 0};             // electrons per spin
+  std::vector<double> detwt;         // [ndet]
+  std::vector<int> det_ud;           // [ndet][2]
+  std::vector<std::vector<int>> udet_cols[2];
   // Jastrow
   std::vector<Radial> ee;            // global e-e function list
   std::vector<double> ee_like, ee_unlike;  // two-body coefficients per ee function

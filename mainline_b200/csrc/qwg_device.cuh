@@ -49,6 +49,8 @@ constexpr int QWG_MAXTB = 12;      // e-e-n terms per type
 constexpr int QWG_MAXPPT = 16;     // pseudopotential Gaussian terms per type
 constexpr int QWG_MAXQ = 12;       // quadrature points
 constexpr int QWG_MAXSHELL = 1024; // basis shells
+constexpr int QWG_MAXDET = 64;     // determinants of an expansion
+constexpr int QWG_MAXUD = 16;      // distinct determinants of one spin
 
 // System tables.  Large tables (splines, MO coefficients, the per-shell
 // arrays read by lanes that each take a different shell) live in HBM; the
@@ -58,8 +60,18 @@ constexpr int QWG_MAXSHELL = 1024; // basis shells
 template <typename Real>
 struct DevSys {
   int nelec, nup, ndn, natoms, nbasis, nshell;
-  int m[2];                      // MOs per spin (= electrons per spin)
+  int m[2];                      // electrons per spin (Slater matrix size)
   int mstride;                   // padded MO stride of moc rows (= MMAX)
+  // determinant expansion (HBM-resident kernels only when ndet > 1):
+  // psi_D = sum_k det_c[k] D_up(det_ud[2k]) D_down(det_ud[2k+1]); nmo_u[s]
+  // orbitals per spin (union), ud_cols[(s * QWG_MAXUD + u) * mstride + i] =
+  // union column of orbital i of spin-determinant u
+  int ndet;
+  int nud[2];
+  int nmo_u[2];
+  const double* det_c;
+  const int* det_ud;
+  const int* ud_cols;
   double ion_ion;
   const int4* shell_i;           // (center, sym, first, k) per shell, sorted by center
   const int2* shell_obj;         // (table base in 4-tuples, splines in the object)
@@ -179,6 +191,11 @@ struct WLayout {
   int state_bytes;    // persistent walker state
   int scratch_bytes;  // per-walker scratch
   int mstride;        // row stride of the inverse / MO-derivative rows (orbitals, padded)
+  // determinant expansions: nud distinct determinants per spin (1 for a single
+  // determinant); state: udl [2][nud][2] (log|D|, sign), mdt [QWG_MAXDET + 2 +
+  // 2 * QWG_MAXUD] (weights t_k, W, log reference, per-spin weight sums);
+  // scratch: mdv [mstride][mstride] orbital values, mdr [QWG_MAXUD][5] ratios
+  int nud, udl, mdt, mdv, mdr;
 };
 
 // Persistent scalars of a walker (inside the state prefix).
@@ -567,6 +584,51 @@ __device__ __forceinline__ Real basis_dot_lane(const DevSys<Real>& S, double px,
     }
   }
   return acc;
+}
+
+// basis_dot_lane for several projected-coefficient vectors at once (the
+// distinct spin-determinants of an expansion): acc[u] = sum_f b_f(p) w[u *
+// wstride + f] for u < nu (molecules).
+template <typename Real>
+__device__ __forceinline__ void basis_dot_lane_multi(const DevSys<Real>& S, double px, double py, double pz,
+                                                     const Real* w, int wstride, int nu, Real* acc) {
+#pragma unroll
+  for (int u = 0; u < QWG_MAXUD; u++) acc[u] = Real(0);
+  auto add = [&](int f, Real v) {
+    const Real vv = fabs(v) > Real(1e-8) ? v : Real(0);
+#pragma unroll
+    for (int u = 0; u < QWG_MAXUD; u++)
+      if (u < nu) acc[u] += vv * w[(size_t)u * wstride + f];
+  };
+  for (int c = 0; c < S.natoms; c++) {
+    const int4 cs = S.center_seg[c];
+    if (cs.y == 0) continue;
+    const double* ap = S.atom_pos[c];
+    const Real x = Real(px - ap[0]), y = Real(py - ap[1]), z = Real(pz - ap[2]);
+    const Real rd = sqrt(x * x + y * y + z * z);
+    if (!(rd < Real(S.center_cut[c]))) continue;
+    const int i = int(rd * Real(S.inv_spacing));
+    const Real h = rd - Real(i) * Real(S.spacing);
+    const Real* row = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4;
+    for (int k0 = 0; k0 < cs.y; k0++) {
+      const int pk = S.shell_pack[cs.x + k0];
+      const int sym = pk & 0xf, fb = (pk >> 4) & 0xffff, kk = (pk >> 20) & 0xff;
+      const Real* cf = row + 4 * kk;
+      const Real f = __ldg(cf) + h * (__ldg(cf + 1) + h * (__ldg(cf + 2) + h * __ldg(cf + 3)));
+      switch (sym) {
+        case 0: add(fb, f); break;
+        case 1: add(fb, x * f); add(fb + 1, y * f); add(fb + 2, z * f); break;
+        case 2:
+          add(fb, x * x * f); add(fb + 1, y * y * f); add(fb + 2, z * z * f);
+          add(fb + 3, x * y * f); add(fb + 4, x * z * f); add(fb + 5, y * z * f);
+          break;
+        default:
+          add(fb, (Real(2) * z * z - x * x - y * y) * f); add(fb + 1, x * z * f); add(fb + 2, y * z * f);
+          add(fb + 3, (x * x - y * y) * f); add(fb + 4, x * y * f);
+          break;
+      }
+    }
+  }
 }
 
 // Periodic version of basis_dot_lane: each atom's functions are summed over

@@ -83,6 +83,7 @@ struct qwg_ctx {
   // tables
   DevBuf d_shell_i, d_shell_obj, d_shell_cut, d_spline, d_spline64, d_moc;
   DevBuf d_image_pos, d_gvec, d_gweight, d_ion_sin, d_ion_cos;
+  DevBuf d_det_c, d_det_ud, d_ud_cols;  // determinant expansion tables
   DevSys<double> sys_d{};
   DevSys<float> sys_f{};
   WLayout L{};
@@ -133,8 +134,13 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
   memset(&S, 0, sizeof(S));
   S.nelec = H.nelec; S.nup = H.nup; S.ndn = H.ndn; S.natoms = H.natoms;
   S.nbasis = H.nbasis; S.nshell = (int)H.shells.size();
-  S.m[0] = H.nmo[0]; S.m[1] = H.nmo[1];
+  S.m[0] = H.nel_s[0]; S.m[1] = H.nel_s[1];
   S.mstride = mo_stride_for(c->mmax, std::max(H.nmo[0], H.nmo[1]));
+  S.ndet = (int)H.detwt.size();
+  for (int s = 0; s < 2; s++) { S.nud[s] = (int)H.udet_cols[s].size(); S.nmo_u[s] = H.nmo[s]; }
+  S.det_c = c->d_det_c.as<double>();
+  S.det_ud = c->d_det_ud.as<int>();
+  S.ud_cols = c->d_ud_cols.as<int>();
   S.ion_ion = H.ion_ion;
   S.shell_i = c->d_shell_i.as<int4>();
   S.shell_obj = c->d_shell_obj.as<int2>();
@@ -294,6 +300,15 @@ static void build_tables(qwg_ctx* c) {
   for (int s = 0; s < 2; s++)
     for (int f = 0; f < H.nbasis; f++)
       for (int i = 0; i < H.nmo[s]; i++) moc[((size_t)s * H.nbasis + f) * mm + i] = H.moc[s][(size_t)f * H.nmo[s] + i];
+  // determinant expansion: weights, (up, down) spin-determinant of each
+  // determinant, union columns of every distinct spin-determinant
+  upload(c->d_det_c, H.detwt, st);
+  upload(c->d_det_ud, H.det_ud, st);
+  std::vector<int> ucols((size_t)2 * QWG_MAXUD * mm, 0);
+  for (int s = 0; s < 2; s++)
+    for (size_t u = 0; u < H.udet_cols[s].size(); u++)
+      for (size_t i = 0; i < H.udet_cols[s][u].size(); i++) ucols[((size_t)s * QWG_MAXUD + u) * mm + i] = H.udet_cols[s][u][i];
+  upload(c->d_ud_cols, ucols, st);
   upload(c->d_spline64, il, st);
   if (c->precision == QWG_FP64) {
     upload(c->d_spline, il, st);
@@ -330,10 +345,16 @@ static void make_layout(qwg_ctx* c) {
   int o = 0;
   L.scal = o; o = align16(o + (int)sizeof(WScal));
   L.R = o; o = align16(o + 8 * 3 * N);
-  L.inv = o; o = align16(o + rs * 2 * mm * mm);
+  L.nud = std::max<int>(1, (int)std::max(H.udet_cols[0].size(), H.udet_cols[1].size()));
+  L.inv = o; o = align16(o + rs * 2 * L.nud * mm * mm);
   L.mov = o; o = align16(o + rs * N * mm * 4);
   L.gU = o; o = align16(o + 8 * 3 * N);
   L.lU = o; o = align16(o + 8 * N);
+  L.udl = L.mdt = L.mdv = L.mdr = 0;
+  if (H.detwt.size() > 1) {
+    L.udl = o; o = align16(o + 8 * 2 * L.nud * 2);
+    L.mdt = o; o = align16(o + 8 * (QWG_MAXDET + 2 + 2 * QWG_MAXUD));
+  }
   L.state_bytes = o;
   // scratch (offsets from its own start): the move/re-inversion phase and the
   // pseudopotential phase are never live together, so their buffers share
@@ -343,6 +364,10 @@ static void make_layout(qwg_ctx* c) {
   L.newcol = o; o = align16(o + rs * mm * 5);
   L.dG = o; o = align16(o + 8 * 4 * N);
   L.lu = o; o = align16(o + 8 * (mm * 2 * mm + mm));
+  if (H.detwt.size() > 1) {
+    L.mdv = o; o = align16(o + 8 * mm * mm);
+    L.mdr = o; o = align16(o + 8 * QWG_MAXUD * 5);
+  }
   const int move_end = o;
   // pseudopotential phase for a chunk of wc electrons: items (wc x atoms),
   // Jastrow values, rotation, projected coefficients (wc x nbasis)
@@ -367,7 +392,7 @@ static void make_layout(qwg_ctx* c) {
   o = align16((int)sizeof(PPItem) * L.wchunk * A);
   L.Ue = o; o = align16(o + 8 * N);
   L.rot = o; o = align16(o + 8 * 9);
-  L.wproj = o; o = align16(o + rs * H.nbasis * L.wchunk);
+  L.wproj = o; o = align16(o + rs * H.nbasis * L.wchunk * L.nud);
   L.scratch_bytes = std::max(o, move_end);
   L.bytes = L.state_bytes + L.scratch_bytes;
   L.sweep_bytes = L.state_bytes + move_end;
@@ -708,6 +733,7 @@ int qwg_footprint(const char* deck_path, int precision, int max_walkers, unsigne
     c->H = build_system(deck_path);
     c->mmax = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
     if (c->mmax < 0) return QWG_ERR_INPUT;
+    if (c->H.detwt.size() > 1) c->mmax = 0;  // expansions run on the HBM-resident kernels
     make_layout(c.get());
     *bytes = footprint_bytes(c.get(), max_walkers);
     return QWG_OK;
@@ -744,7 +770,11 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
   int rc = guarded(c.get(), [&]() -> int {
     c->H = build_system(deck_path);
     int mm = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
-    if (mm < 0) throw InputError("more than 256 electrons of one spin: beyond this engine build");
+    if (mm < 0) throw InputError("more than 256 electrons (or expansion orbitals) of one spin: beyond this engine build");
+    if (c->H.detwt.size() > 1) {
+      if (c->H.periodic) throw InputError("determinant expansions are supported for molecules only");
+      mm = 0;  // expansions run on the HBM-resident kernels
+    }
     c->mmax = mm;
     if (const char* sched = getenv("QWG_DMC_SCHEDULE")) c->split = strcmp(sched, "fused") != 0;
     if (stream) {

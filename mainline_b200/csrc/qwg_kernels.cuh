@@ -54,7 +54,56 @@ struct Walker {
     else return L.mstride;
   }
   __device__ double* R() const { return (double*)(base + L.R); }
-  __device__ Real* inv(int s) const { return (Real*)(base + L.inv) + (size_t)s * MS() * MS(); }
+  __device__ Real* inv(int s) const {
+    if constexpr (MMAX > 0) return (Real*)(base + L.inv) + (size_t)s * MS() * MS();
+    else return (Real*)(base + L.inv) + (size_t)s * L.nud * MS() * MS();
+  }
+  // ---- determinant expansions (HBM-resident kernels, S.ndet > 1)
+  __device__ bool multi() const {
+    if constexpr (MMAX > 0) return false;
+    else return S.ndet > 1;
+  }
+  __device__ Real* inv_u(int s, int u) const { return (Real*)(base + L.inv) + ((size_t)s * L.nud + u) * MS() * MS(); }
+  __device__ double* udl() const { return (double*)(base + L.udl); }
+  __device__ double* mdt() const { return (double*)(base + L.mdt); }
+  __device__ double* mdv() const { return (double*)(sbase + L.mdv); }
+  __device__ double* mdr() const { return (double*)(sbase + L.mdr); }
+  __device__ const int* cols(int s, int u) const { return S.ud_cols + ((size_t)s * QWG_MAXUD + u) * MS(); }
+  // t_k = c_k sign_k exp(L_k - Lref) with L_k = log|D_up| + log|D_down|;
+  // W = sum_k t_k (psi_D = W exp(Lref)); T[s][u] = sum of t_k over the
+  // determinants whose spin-s factor is u.  mdt = [t_0..t_K-1, W, Lref, T[2][MAXUD]]
+  __device__ void md_weights() {
+    const double* ld = udl();
+    double* t = mdt();
+    const int K = S.ndet, nu = L.nud;
+    double lref = -1e300;
+    for (int k = 0; k < K; k++)
+      lref = fmax(lref, ld[(0 * nu + S.det_ud[2 * k]) * 2] + ld[(1 * nu + S.det_ud[2 * k + 1]) * 2]);
+    for (int k = lane; k < K; k += 32) {
+      const int a = S.det_ud[2 * k], b = S.det_ud[2 * k + 1];
+      const double lk = ld[(0 * nu + a) * 2] + ld[(1 * nu + b) * 2];
+      t[k] = S.det_c[k] * ld[(0 * nu + a) * 2 + 1] * ld[(1 * nu + b) * 2 + 1] * exp(lk - lref);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      double W = 0;
+      double* T = t + QWG_MAXDET + 2;
+      for (int q = 0; q < 2 * QWG_MAXUD; q++) T[q] = 0.0;
+      for (int k = 0; k < K; k++) {
+        W += t[k];
+        T[S.det_ud[2 * k]] += t[k];
+        T[QWG_MAXUD + S.det_ud[2 * k + 1]] += t[k];
+      }
+      t[QWG_MAXDET] = W;
+      t[QWG_MAXDET + 1] = lref;
+    }
+    __syncwarp();
+  }
+  __device__ double md_logpsi_d(double& sign) const {
+    const double W = mdt()[QWG_MAXDET];
+    sign = W < 0 ? -1.0 : 1.0;
+    return mdt()[QWG_MAXDET + 1] + log(fabs(W));
+  }
   __device__ Real* mov() const { return (Real*)(base + L.mov); }
   __device__ double* gU() const { return (double*)(base + L.gU); }
   __device__ double* lU() const { return (double*)(base + L.lU); }
@@ -79,7 +128,39 @@ struct Walker {
     Real* nc = newcol();
     double* aug = lu();
     WScal* w = sc();
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < 2 && multi(); s++) {
+      // every orbital of the spin's union at every electron, then one
+      // inversion per distinct spin-determinant (Slat_wf::calcLap for all
+      // determinants, Slat_wf.h:948-1016)
+      const int M = S.m[s], NU = S.nmo_u[s], ms = MS();
+      const int e0 = s == 0 ? 0 : S.nup;
+      double* vals = mdv();
+      for (int el = 0; el < M; el++) {
+        const int e = e0 + el;
+        mo_lap_warp<Real, PER>(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], NU, bas(), nc, lane);
+        for (int j = lane; j < NU; j += 32) {
+          vals[(size_t)el * ms + j] = double(nc[j * 5]);
+          Real* mv = mov() + ((size_t)e * ms + j) * 4;
+          mv[0] = nc[j * 5 + 1]; mv[1] = nc[j * 5 + 2]; mv[2] = nc[j * 5 + 3]; mv[3] = nc[j * 5 + 4];
+        }
+        __syncwarp();
+      }
+      for (int u = 0; u < S.nud[s]; u++) {
+        const int* cu = cols(s, u);
+        for (int idx = lane; idx < M * M; idx += 32) {
+          const int el = idx / M, i = idx - el * M;
+          aug[el * 2 * M + i] = vals[(size_t)el * ms + cu[i]];
+        }
+        __syncwarp();
+        double ld = 0.0, sg = 1.0;
+        if (M > 0) gj_inverse_warp_big(aug, aug + 2 * M * M, M, inv_u(s, u), ms, ld, sg, lane);
+        if (lane == 0) { udl()[((size_t)s * L.nud + u) * 2] = ld; udl()[((size_t)s * L.nud + u) * 2 + 1] = sg; }
+        __syncwarp();
+      }
+      if (lane == 0) { w->logdet[s] = udl()[((size_t)s * L.nud) * 2]; w->sign[s] = udl()[((size_t)s * L.nud) * 2 + 1]; }
+    }
+    if (multi()) md_weights();
+    for (int s = 0; s < 2 && !multi(); s++) {
       const int M = S.m[s];
       const int e0 = s == 0 ? 0 : S.nup;
       for (int el = 0; el < M; el++) {
@@ -120,6 +201,27 @@ struct Walker {
 
   // Slater gradient and Laplacian ratios of electron e at its position.
   __device__ void slater_gl(int e, double g[3], double& l) const {
+    if (multi()) {
+      // sum over distinct spin-determinants u of T[s][u] (grad D_u / D_u) / W
+      const int s = spin(e), el = eloc(e), M = S.m[s], ms = MS();
+      const double* T = mdt() + QWG_MAXDET + 2 + s * QWG_MAXUD;
+      const double W = mdt()[QWG_MAXDET];
+      const Real* mvb = mov() + (size_t)e * ms * 4;
+      double b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+      for (int u = 0; u < S.nud[s]; u++) {
+        const Real* iv = inv_u(s, u) + (size_t)el * ms;
+        const int* cu = cols(s, u);
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (int i = 0; i < M; i++) {
+          const double c = iv[i];
+          const Real* mv = mvb + 4 * cu[i];
+          a0 += c * double(mv[0]); a1 += c * double(mv[1]); a2 += c * double(mv[2]); a3 += c * double(mv[3]);
+        }
+        b0 += T[u] * a0; b1 += T[u] * a1; b2 += T[u] * a2; b3 += T[u] * a3;
+      }
+      g[0] = b0 / W; g[1] = b1 / W; g[2] = b2 / W; l = b3 / W;
+      return;
+    }
     const int s = spin(e), el = eloc(e), M = S.m[s];
     const Real* iv = inv(s) + (size_t)el * MS();
     const Real* mv = mov() + (size_t)e * MS() * 4;
@@ -142,13 +244,39 @@ struct Walker {
     const int s = spin(e), el = eloc(e), M = S.m[s];
     const double* Rp = R();
     Real* nc = newcol();
-    mo_lap_warp<Real, PER>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
-    const Real* iv = inv(s) + (size_t)el * MS();
     double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
-    for (int i = 0; i < M; i++) {
-      double c = iv[i];
-      r0 += c * double(nc[i * 5]); r1 += c * double(nc[i * 5 + 1]); r2 += c * double(nc[i * 5 + 2]);
-      r3 += c * double(nc[i * 5 + 3]); r4 += c * double(nc[i * 5 + 4]);
+    if (multi()) {
+      // ratios of every distinct spin-determinant (kept in mdr for accept),
+      // combined with the expansion weights
+      mo_lap_warp<Real, PER>(S, mocs(s), px, py, pz, S.nmo_u[s], bas(), nc, lane);
+      double* rr = mdr();
+      for (int u = lane; u < S.nud[s]; u += 32) {
+        const Real* iv = inv_u(s, u) + (size_t)el * MS();
+        const int* cu = cols(s, u);
+        double a[5] = {0, 0, 0, 0, 0};
+        for (int i = 0; i < M; i++) {
+          const double c = iv[i];
+          const Real* v = nc + 5 * cu[i];
+          for (int q = 0; q < 5; q++) a[q] += c * double(v[q]);
+        }
+        for (int q = 0; q < 5; q++) rr[u * 5 + q] = a[q];
+      }
+      __syncwarp();
+      const double* T = mdt() + QWG_MAXDET + 2 + s * QWG_MAXUD;
+      const double W = mdt()[QWG_MAXDET];
+      for (int u = 0; u < S.nud[s]; u++) {
+        r0 += T[u] * rr[u * 5]; r1 += T[u] * rr[u * 5 + 1]; r2 += T[u] * rr[u * 5 + 2];
+        r3 += T[u] * rr[u * 5 + 3]; r4 += T[u] * rr[u * 5 + 4];
+      }
+      r0 /= W; r1 /= W; r2 /= W; r3 /= W; r4 /= W;
+    } else {
+      mo_lap_warp<Real, PER>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
+      const Real* iv = inv(s) + (size_t)el * MS();
+      for (int i = 0; i < M; i++) {
+        double c = iv[i];
+        r0 += c * double(nc[i * 5]); r1 += c * double(nc[i * 5 + 1]); r2 += c * double(nc[i * 5 + 2]);
+        r3 += c * double(nc[i * 5 + 3]); r4 += c * double(nc[i * 5 + 4]);
+      }
     }
     ratioD = double(r0);
     double gD[3] = {double(r1) / ratioD, double(r2) / ratioD, double(r3) / ratioD};
@@ -242,7 +370,45 @@ struct Walker {
     Real* wk = (Real*)lu();
     Real* rowe = wk + MS();
     const int ms = MS();
-    for (int k = lane; k < M; k += 32) {
+    if (multi()) {
+      // Sherman-Morrison update of every distinct spin-determinant with its
+      // own ratio (from propose), then the stored rows of every union orbital
+      for (int u = 0; u < S.nud[s]; u++) {
+        const double ru = mdr()[u * 5];
+        Real* ivu = inv_u(s, u);
+        const int* cu = cols(s, u);
+        if (!(ru != 0.0) || !isfinite(ru)) {
+          if (lane == 0) udl()[((size_t)s * L.nud + u) * 2] = -1e201;  // became singular
+          __syncwarp();
+          continue;
+        }
+        for (int k = lane; k < M; k += 32) {
+          Real acc = 0;
+          for (int i = 0; i < M; i++) acc += nc[cu[i] * 5] * ivu[(size_t)k * ms + i];
+          wk[k] = acc;
+          rowe[k] = ivu[(size_t)el * ms + k];
+        }
+        __syncwarp();
+        const Real invr = Real(1.0 / ru);
+        for (int idx = lane; idx < M * M; idx += 32) {
+          int k = idx / M, i = idx - k * M;
+          if (k == el) ivu[(size_t)k * ms + i] = rowe[i] * invr;
+          else ivu[(size_t)k * ms + i] -= rowe[i] * wk[k] * invr;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          double* d = udl() + ((size_t)s * L.nud + u) * 2;
+          d[0] += log(fabs(ru));
+          if (ru < 0) d[1] = -d[1];
+        }
+        __syncwarp();
+      }
+      for (int j = lane; j < S.nmo_u[s]; j += 32) {
+        Real* mv = mov() + ((size_t)e * ms + j) * 4;
+        mv[0] = nc[j * 5 + 1]; mv[1] = nc[j * 5 + 2]; mv[2] = nc[j * 5 + 3]; mv[3] = nc[j * 5 + 4];
+      }
+    }
+    for (int k = lane; k < M && !multi(); k += 32) {
       Real acc = 0;
       for (int i = 0; i < M; i++) acc += nc[i * 5] * iv[(size_t)k * ms + i];
       wk[k] = acc;
@@ -250,12 +416,12 @@ struct Walker {
     }
     __syncwarp();
     const Real invr = Real(1.0 / ratioD);
-    for (int idx = lane; idx < M * M; idx += 32) {
+    for (int idx = lane; idx < M * M && !multi(); idx += 32) {
       int k = idx / M, i = idx - k * M;
       if (k == el) iv[(size_t)k * ms + i] = rowe[i] * invr;
       else iv[(size_t)k * ms + i] -= rowe[i] * wk[k] * invr;
     }
-    for (int i = lane; i < M; i += 32) {
+    for (int i = lane; i < M && !multi(); i += 32) {
       Real* mv = mov() + ((size_t)e * ms + i) * 4;
       mv[0] = nc[i * 5 + 1]; mv[1] = nc[i * 5 + 2]; mv[2] = nc[i * 5 + 3]; mv[3] = nc[i * 5 + 4];
     }
@@ -276,6 +442,7 @@ struct Walker {
       w->U += dU;
     }
     __syncwarp();
+    if (multi()) md_weights();
   }
 
   __device__ void electron_grad(int e, double g[3], double& lap) const {
@@ -452,7 +619,21 @@ struct Walker {
       }
       __syncwarp();
       if (nitems == 0) continue;
-      for (int idx = lane; idx < (e1 - e0) * S.nbasis; idx += 32) {
+      const int nproj = multi() ? L.nud : 1;  // projected-coefficient sets per electron
+      for (int idx = lane; idx < (e1 - e0) * S.nbasis * nproj && multi(); idx += 32) {
+        // one set per distinct spin-determinant u: w_f = sum_i C[f][col_u(i)] (A_u^-1)[i][e]
+        const int u = idx / ((e1 - e0) * S.nbasis), r = idx - u * (e1 - e0) * S.nbasis;
+        const int le = r / S.nbasis, f = r - le * S.nbasis;
+        const int e = e0 + le, s = spin(e), el = eloc(e), M = S.m[s];
+        if (u >= S.nud[s]) continue;
+        const Real* cf = mocs(s) + (size_t)f * MS();
+        const Real* iv = inv_u(s, u) + (size_t)el * MS();
+        const int* cu = cols(s, u);
+        Real acc = Real(0);
+        for (int m = 0; m < M; m++) acc += cf[cu[m]] * iv[m];
+        w[((size_t)u * CH + le) * S.nbasis + f] = acc;
+      }
+      for (int idx = lane; idx < (e1 - e0) * S.nbasis && !multi(); idx += 32) {
         const int le = idx / S.nbasis, f = idx - le * S.nbasis;
         const int e = e0 + le, s = spin(e), el = eloc(e), M = S.m[s];
         const Real* cf = mocs(s) + (size_t)f * MS();
@@ -486,8 +667,20 @@ struct Walker {
         wrap_pos(S, nx, ny, nz);
         const Real* wr = w + (I.e - e0) * S.nbasis;
         Real rd;
-        if (PER == 1 || (PER == 2 && S.periodic)) rd = basis_dot_lane_periodic(S, nx, ny, nz, wr);
-        else rd = basis_dot_lane(S, nx, ny, nz, wr);
+        if (PER == 1 || (PER == 2 && S.periodic)) {
+          rd = basis_dot_lane_periodic(S, nx, ny, nz, wr);
+        } else if (multi()) {
+          // sum over distinct spin-determinants of T[s][u] R_u / W
+          const int s = spin(I.e);
+          Real ru[QWG_MAXUD];
+          basis_dot_lane_multi(S, nx, ny, nz, wr, CH * S.nbasis, S.nud[s], ru);
+          const double* T = mdt() + QWG_MAXDET + 2 + s * QWG_MAXUD;
+          double acc = 0.0;
+          for (int u = 0; u < S.nud[s]; u++) acc += T[u] * double(ru[u]);
+          rd = Real(acc / mdt()[QWG_MAXDET]);
+        } else {
+          rd = basis_dot_lane(S, nx, ny, nz, wr);
+        }
         const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);
         double ratio = double(rd * exp(u - Real(Ue()[I.e]))) * S.pp_w[ty][q];
         // cos of the angle between the original and the quadrature direction
@@ -694,8 +887,14 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       }
       if (lane == 0) {
         WScal* w = W.sc();
-        io.logpsi[wid] = w->logdet[0] + w->logdet[1] + w->U;
-        io.sign[wid] = w->sign[0] * w->sign[1];
+        if (W.multi()) {
+          double sgn;
+          io.logpsi[wid] = W.md_logpsi_d(sgn) + w->U;
+          io.sign[wid] = sgn;
+        } else {
+          io.logpsi[wid] = w->logdet[0] + w->logdet[1] + w->U;
+          io.sign[wid] = w->sign[0] * w->sign[1];
+        }
         io.kinetic[wid] = kin;
         io.potential[wid] = pot;
         io.nonlocal[wid] = nl;

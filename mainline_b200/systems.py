@@ -155,10 +155,13 @@ def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
 
 
 def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | None = None,
-             name: str | None = None) -> Deck:
+             name: str | None = None, expansion=None) -> Deck:
     """Two-atom molecule of the all-electron (``pseudo=False``) or Z_eff=5
     pseudopotential (``pseudo=True``) workload.  ``method`` is an optional
-    METHOD section body written into the deck (e.g. ``"VMC NBLOCK 50 ..."``)."""
+    METHOD section body written into the deck (e.g. ``"VMC NBLOCK 50 ..."``).
+    ``expansion``: optional determinant expansion [(weight, up orbitals,
+    down orbitals)], orbitals numbered from 1 within each spin (7 occupied
+    plus virtual orbitals up to the largest index used)."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     label = "N"
@@ -170,15 +173,19 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
     shells = _basis_shells(rng, {"S": 10, "P": 6, "6D": 2}, hi=10.0 if pseudo else 1e4)
     nper = sum(SHELL_NFUNC[s] for s, _, _ in shells)
     nb = 2 * nper
-    cup = _random_orthonormal(rng, nb, nup)
-    cdn = _random_orthonormal(rng, nb, ndown)
+    nspin_mo = nup if not expansion else max(max(max(u), max(d)) for _, u, d in expansion)
+    cup = _random_orthonormal(rng, nb, nspin_mo)
+    cdn = _random_orthonormal(rng, nb, nspin_mo)
     onebody = rng.normal(0.0, 0.1, size=4)
     pp = _pseudo_text(rng, label, charge) if pseudo else ""
     name = name or ("n2_pseudo" if pseudo else "n2_allelectron")
     orb = os.path.join(outdir, f"{name}.orb")
     _write_orb(orb, np.concatenate([cup, cdn], axis=1), [nper, nper])
-    states_up = " ".join(str(i + 1) for i in range(nup))
-    states_dn = " ".join(str(nup + i + 1) for i in range(ndown))
+    if not expansion:
+        expansion = [(1.0, list(range(1, nup + 1)), list(range(1, ndown + 1)))]
+    detwt = " ".join(_fmt(w) for w, _, _ in expansion)
+    states = "\n      ".join(" ".join(str(i) for i in u) + " " + " ".join(str(nspin_mo + i) for i in d)
+                              for _, u, d in expansion)
     deck = "\n".join([
         f"# seeded synthetic workload {name} (seed {seed})",
         f"RANDOMSEED {{ {1 + seed % 100000} {7 + seed % 7919} }}",
@@ -191,13 +198,13 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
         "TRIALFUNC { SLATER-JASTROW",
         "  WF1 { SLATER",
         "    ORBITALS { BLAS_MO",
-        f"      NMO {nup + ndown}",
+        f"      NMO {2 * nspin_mo}",
         f"      ORBFILE {os.path.basename(orb)}",
         _basis_text(label, shells),
         "      CENTERS { USEATOMS }",
         "    }",
-        "    DETWT { 1.0 }",
-        f"    STATES {{ {states_up} {states_dn} }}",
+        f"    DETWT {{ {detwt} }}",
+        f"    STATES {{ {states} }}",
         "  }",
         "  WF2 {",
         _jastrow_text(label, onebody),

@@ -28,7 +28,15 @@ NCONF = 256
 NMOVE = 2
 WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseudo=True), 12),
              ("diamond8", dict(periodic=True), 13), ("mol43", dict(nelec=43), 14),
-             ("mol72", dict(nelec=72), 15), ("cell32", dict(periodic=True, supercell=(2, 2, 1)), 16)]
+             ("mol72", dict(nelec=72), 15), ("cell32", dict(periodic=True, supercell=(2, 2, 1)), 16),
+             ("n2_multidet", dict(pseudo=True, expansion=[
+                 (0.9, [1, 2, 3, 4, 5, 6, 7], [1, 2, 3, 4, 5, 6, 7]),
+                 (-0.25, [1, 2, 3, 4, 5, 6, 8], [1, 2, 3, 4, 5, 6, 7]),
+                 (-0.25, [1, 2, 3, 4, 5, 6, 7], [1, 2, 3, 4, 5, 6, 8]),
+                 (0.12, [1, 2, 3, 4, 5, 6, 8], [1, 2, 3, 4, 5, 6, 8]),
+                 (0.08, [1, 2, 3, 4, 5, 7, 9], [1, 2, 3, 4, 5, 6, 7]),
+                 (0.08, [1, 2, 3, 4, 5, 6, 7], [1, 2, 3, 4, 5, 7, 9]),
+                 (-0.05, [1, 2, 3, 4, 6, 8, 9], [2, 3, 4, 5, 6, 7, 8])]), 17)]
 
 
 def make(name, kw, seed):
@@ -41,7 +49,7 @@ def make(name, kw, seed):
         nconf = 64 if kw["nelec"] < 64 else 32
     else:
         deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
-        nconf = NCONF
+        nconf = NCONF if "expansion" not in kw else 64
     R = systems.random_configs(deck, nconf, seed=seed + 1000)
     NCONF_ = nconf
     rng = np.random.default_rng(seed + 2000)

@@ -68,12 +68,12 @@ def test_bad_deck_reports_error(lib, tmp_path):
 
 
 @pytest.mark.parametrize("edit,msg", [
-    (lambda t: t.replace("DETWT { 1.0 }", "DETWT { 0.9 0.1 }"), "single-determinant"),
+    (lambda t: t.replace("DETWT { 1.0 }", "DETWT { 0.9 0.1 }"), "every determinant"),
     (lambda t: t.replace("ORBITALS { BLAS_MO", "CORBITALS { BLAS_MO"), "complex orbitals"),
 ])
 def test_unsupported_wavefunctions_are_rejected(lib, tmp_path, edit, msg):
-    """Multi-determinant expansions and complex orbitals are outside this
-    engine: the deck is rejected with a clear message, not run wrongly."""
+    """Malformed determinant expansions and complex orbitals (outside this
+    engine) are rejected with a clear message, not run wrongly."""
     import shutil
     src = os.path.join(GOLDEN, "n2_pseudo.qw")
     shutil.copy(os.path.join(GOLDEN, "n2_pseudo.orb"), tmp_path)

@@ -15,7 +15,7 @@ from mainline_b200 import engine, systems
 
 pytestmark = pytest.mark.gpu
 
-NAMES = ["n2_allelectron", "n2_pseudo", "diamond8", "mol43", "mol72", "cell32"]
+NAMES = ["n2_allelectron", "n2_pseudo", "diamond8", "mol43", "mol72", "cell32", "n2_multidet"]
 FP64_TOL = 1e-10
 
 
@@ -261,3 +261,41 @@ def test_dmc_split_schedule_matches_fused(prec, monkeypatch):
         # may be contracted to FMAs differently (1-ulp differences), which can
         # flip a rare accept/reject decision; the walks agree to 1e-3 Ha
         assert np.max(np.abs(np.subtract(out["split"], out["fused"]))) < 1e-3, out
+
+
+def test_multideterminant_dmc_runs():
+    """A 7-determinant expansion (3 distinct determinants per spin, 9
+    orbitals per spin) through VMC and DMC blocks: finite energies and
+    weights."""
+    deck = os.path.join(GOLDEN, "n2_multidet.qw")
+    d = systems.read_deck(deck)
+    for prec in (engine.FP64, engine.MIXED):
+        E = engine.Engine(deck, prec, max_walkers=512)
+        E.set_walkers(systems.random_configs(d, 512, seed=12))
+        s = E.vmc_block(10, 0.3, seed=13)
+        assert s["nonfinite"] == 0 and 0.2 < s["acceptance"] <= 1.0
+        E.dmc_init(timestep=0.01, nstep=10, seed=14)
+        for _ in range(2):
+            st = E.dmc_block()
+            # the random-orbital expansion is a poor trial function: weights swing widely
+            assert np.isfinite(st["energy"]) and st["nonfinite"] == 0 and 0.0 < st["weight"] < 8.0
+
+
+def test_multideterminant_moves_track_state(tmp_path):
+    """After a VMC block of single-electron moves, the local energy computed
+    from the Sherman-Morrison-updated inverses of every distinct
+    spin-determinant and the expansion weights equals a fresh evaluation at
+    the final positions (bare Coulomb copy of the deck, so no quadrature
+    rotation enters)."""
+    deck = os.path.join(GOLDEN, "n2_multidet.qw")
+    d = systems.read_deck(deck)
+    bare = _strip_pseudo(deck, str(tmp_path))
+    nw = 256
+    E = engine.Engine(bare, engine.FP64, max_walkers=nw)
+    E.set_walkers(systems.random_configs(d, nw, seed=21))
+    s = E.vmc_block(4, 0.1, seed=22)
+    assert s["nonfinite"] == 0
+    e_moves = E.last_energies()
+    E2 = engine.Engine(bare, engine.FP64, max_walkers=nw)
+    E2.set_walkers(E.get_walkers())
+    assert _rel(e_moves, E2.eval().energy) < 1e-8
