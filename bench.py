@@ -28,6 +28,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from mainline_b200.replicas import aggregate_rate, max_over_ranks, replica_seed  # noqa: E402
+
 NWALK = 4096
 TAU = 0.01
 FEEDBACK_INTERVAL = 5
@@ -132,9 +134,9 @@ def run_engine(args, rank, world):
         E = engine.Engine(deck.path, prec, max_walkers=NWALK, stream=stream.cuda_stream)
         E.set_walkers(R0)
         for b in range(3):  # VMC equilibration from the seeded start
-            E.vmc_block(20, 0.3, seed=SEED + 17 * rank + b)
+            E.vmc_block(20, 0.3, seed=replica_seed(SEED, rank) + 17 * b)
         steps = max(FEEDBACK_INTERVAL, (args.steps // FEEDBACK_INTERVAL) * FEEDBACK_INTERVAL)
-        E.dmc_init(timestep=TAU, nstep=steps, seed=SEED + rank)
+        E.dmc_init(timestep=TAU, nstep=steps, seed=replica_seed(SEED, rank))
         for _ in range(max(args.warmup, 3) // 1):
             E.dmc_block()  # warm-up blocks (untimed)
         # timed: one block of `steps` steps, CUDA events on the engine's stream
@@ -159,7 +161,7 @@ def run_engine(args, rank, world):
         sweep_ms, eloc_ms = E.time_kernels(5)
         # block latency: several shorter blocks (20 steps), host wall time from
         # block start to block statistics on the host
-        E.dmc_init(timestep=TAU, nstep=20, seed=SEED + 99 + rank)
+        E.dmc_init(timestep=TAU, nstep=20, seed=replica_seed(SEED + 99, rank))
         energies = []
         for b in range(args.latency_blocks):
             t0 = time.perf_counter()
@@ -346,16 +348,10 @@ def main():
         return
     mx = results["mixed"]
     fp = results["fp64"]
-    # max over ranks of the device time
-    ms = mx["ms"]
-    if world > 1:
-        import torch
-        import torch.distributed as dist
-        t = torch.tensor([ms, e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
-    ws = NWALK * steps * world / (ms / 1e3)
-    ws64 = NWALK * fp["steps"] * world / (fp["ms"] / 1e3)
+    # max over ranks of the device times (every rank takes part)
+    ms, ms64, e2e_ms = max_over_ranks([mx["ms"], fp["ms"], e2e_ms], "cuda")
+    ws = aggregate_rate(NWALK * steps, world, ms)
+    ws64 = aggregate_rate(NWALK * fp["steps"], world, ms64)
     if rank != 0:
         if world > 1:
             import torch.distributed as dist
@@ -381,7 +377,7 @@ def main():
                    "walkers_per_gpu": NWALK, "tau": TAU, "feedback_interval": FEEDBACK_INTERVAL,
                    "parallelism": f"replicas x{world}", "l2": "walker state resident (working set < L2); "
                    "256 MiB buffer written before the timed block"},
-        "fp64": {"value": ws64, "unit": "walker-steps/s", "ms_per_step": fp["ms"] / fp["steps"],
+        "fp64": {"value": ws64, "unit": "walker-steps/s", "ms_per_step": ms64 / fp["steps"],
                  "block_energy_mean": float(np.mean(fp["energies"])),
                  "block_energy_sem": float(np.std(fp["energies"]) / np.sqrt(len(fp["energies"])))},
         "mixed_vs_fp64": ws / ws64,
@@ -389,7 +385,7 @@ def main():
                                "sem": float(np.std(mx["energies"]) / np.sqrt(len(mx["energies"])))},
         "block_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                              "steps_per_block": 20, "walkers": NWALK},
-        "e2e": {"value": NWALK * steps / (e2e_ms / 1e3), "unit": "walker-steps/s",
+        "e2e": {"value": aggregate_rate(NWALK * steps, world, e2e_ms), "unit": "walker-steps/s",
                 "h2d_bytes_per_step": NWALK * N * 3 * 8 / steps, "d2h_bytes_per_step": (NWALK * N * 3 * 8 + 96) / steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": src, "traffic": _traffic_per_launch(dom),
