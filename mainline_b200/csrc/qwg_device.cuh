@@ -100,6 +100,8 @@ struct DevSys {
   double onebody[QWG_MAXT][QWG_MAXEI];
   int tb_n[QWG_MAXT];
   double tb_rc[QWG_MAXT];        // largest e-i cutoff the type's e-e-n terms use
+  double ee_rc2;                 // (largest e-e cutoff)^2 (1 + 1e-12): every pair term (two- and
+                                 // three-body) vanishes for electrons at least that far apart
   DTB tb[QWG_MAXT][QWG_MAXTB];
   int has_tb;
   // pseudopotential per type (nchan 0: none)
@@ -841,7 +843,9 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
     if (j == i) continue;
     double dx = px - R[3 * j], dy = py - R[3 * j + 1], dz = pz - R[3 * j + 2];
     min_image(S, dx, dy, dz);
-    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    if (!(r2 < S.ee_rc2)) continue;  // beyond every e-e cutoff: no pair term
+    double r = sqrt(r2);
     double pu, pfd, pl;
     jas_pair_t<double>(S, si == (j < S.nup), r, pu, pfd, pl);
     u += pu; lap += pl;
@@ -882,7 +886,9 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
     double ex = px - R[3 * j], ey = py - R[3 * j + 1], ez = pz - R[3 * j + 2];
     min_image(S, ex, ey, ez);
     const T dx = T(ex), dy = T(ey), dz = T(ez);
-    const T r = sqrt(dx * dx + dy * dy + dz * dz);
+    const T r2 = dx * dx + dy * dy + dz * dz;
+    if (!(r2 < T(S.ee_rc2))) continue;  // beyond every e-e cutoff: no pair term
+    const T r = sqrt(r2);
     const bool same = si == (j < S.nup);
     for (int k = 0; k < S.nee; k++) {
       const double c = same ? S.ee_like[k] : S.ee_unlike[k];

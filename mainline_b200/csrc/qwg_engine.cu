@@ -216,6 +216,9 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     }
   // Jastrow
   S.nee = (int)H.ee.size();
+  double ee_rc = 0.0;
+  for (const Radial& r : H.ee) ee_rc = std::max(ee_rc, r.rcut);
+  S.ee_rc2 = ee_rc * ee_rc * (1.0 + 1e-12);
   for (int k = 0; k < S.nee; k++) {
     S.ee[k] = to_dradial(H.ee[k]);
     S.ee_like[k] = H.ee_like[k];

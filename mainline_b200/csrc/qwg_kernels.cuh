@@ -301,6 +301,10 @@ struct Walker {
       double qx = ox - pj[0], qy = oy - pj[1], qz = oz - pj[2];
       min_image(S, nx, ny, nz);
       min_image(S, qx, qy, qz);
+      if (!(nx * nx + ny * ny + nz * nz < S.ee_rc2) && !(qx * qx + qy * qy + qz * qz < S.ee_rc2)) {
+        dg[0] = dg[1] = dg[2] = dg[3] = 0.0;  // beyond every e-e cutoff before and after the move
+        continue;
+      }
       // pair functions in the working precision, sums in FP64
       const Real rn = sqrt(Real(nx * nx + ny * ny + nz * nz)), ro = sqrt(Real(qx * qx + qy * qy + qz * qz));
       double un, fn, ln, uo, fo, lo;
