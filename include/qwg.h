@@ -68,14 +68,15 @@ typedef struct {
   int walkers_per_cta; /* launch shape picked at create time */
   double ion_ion;      /* constant ion-ion energy */
   unsigned long long device_bytes; /* device memory a context of max_walkers holds */
+  int complex_orbitals; /* 1: complex-orbital kernels (CORBITALS, or a nonzero KPOINT) */
 } qwg_info;
 
 /* Per-walker outputs of qwg_eval (host arrays, caller-owned, sized by nw). */
 typedef struct {
   double* logpsi;      /* [nw]          ln|psi|                        */
-  double* sign;        /* [nw]          sign of psi                    */
+  double* sign;        /* [nw]          sign of psi; complex orbitals: arg psi (radians) */
   double* grad;        /* [nw][nelec][3] grad ln|psi| per electron     */
-  double* lap;         /* [nw][nelec]   (lap psi)/psi per electron     */
+  double* lap;         /* [nw][nelec]   Re (lap psi)/psi per electron  */
   double* kinetic;     /* [nw]  -1/2 sum_e lap                         */
   double* potential;   /* [nw]  Coulomb e-e, e-i, i-i                  */
   double* nonlocal;    /* [nw]  pseudopotential (local + nonlocal)     */
@@ -154,7 +155,8 @@ int qwg_get_walker_scalars(qwg_ctx* ctx, double* energy, double* weight, int nw)
 int qwg_eval(qwg_ctx* ctx, const double* rot, qwg_eval_out* out);
 
 /* Single-electron move per walker: electron e[w] to Rnew[w][3].  Returns
- * ln|psi'|-ln|psi|, sign ratio, grad ln psi' [nw][3] and lap psi'/psi' of
+ * ln|psi'|-ln|psi|, sign ratio (complex orbitals: the phase change
+ * arg(psi'/psi) in radians), grad ln|psi'| [nw][3] and Re lap psi'/psi' of
  * the moved electron. */
 int qwg_ratio(qwg_ctx* ctx, const int* e, const double* Rnew, double* dlogpsi, double* sign,
               double* grad, double* lap);

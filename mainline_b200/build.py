@@ -26,7 +26,7 @@ NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--ex
 SOURCES_CU = ["qwg_engine.cu"]
 SOURCES_CXX = ["qwg_deck.cpp", "qwg_server.cpp", "qwg_log.cpp", "qwg_configs.cpp"]
 # walker-kernel families: qwg_walkers.cu once per (working precision, orbital capacity)
-FAMILIES = [(real, mm) for real in ("double", "float") for mm in (8, 16, 32, 0)]
+FAMILIES = [(real, mm) for real in ("double", "float") for mm in (8, 16, 32, 0, -1)]  # -1: complex orbitals
 
 
 def _run(cmd):
@@ -58,7 +58,7 @@ def build(verbose: bool = False, extra_nvflags=None) -> str:
     units = [(os.path.join(CSRC, src), os.path.join(BUILD, src + ".o"), []) for src in SOURCES_CU]
     wsrc = os.path.join(CSRC, "qwg_walkers.cu")
     for real, mm in FAMILIES:
-        units.append((wsrc, os.path.join(BUILD, f"qwg_walkers_{real}_{mm}.o"),
+        units.append((wsrc, os.path.join(BUILD, f"qwg_walkers_{real}_{'cpx' if mm < 0 else mm}.o"),
                       [f"-DQWG_REAL={real}", f"-DQWG_MM={mm}"]))
     for s, o, defs in units:
         if _stale(o, [s] + headers):

@@ -341,8 +341,10 @@ static BasisObj read_aospline(const std::vector<std::string>& w, HostSystem& S,
 
 // ORB file: "mo basis center label" records until COEFFICIENTS, then the
 // coefficient list; each (mo, center, basis) entry points at a label.
+// Complex coefficients (CORBITALS) are written "(re,im)" (or a plain real);
+// moc_im receives their imaginary parts when given.
 static void read_orb(const std::string& path, int nmo, const std::vector<int>& nfunc_center,
-                     std::vector<double>& moc /* [nbasis][nmo] */) {
+                     std::vector<double>& moc /* [nbasis][nmo] */, std::vector<double>* moc_im = nullptr) {
   std::ifstream in(path);
   if (!in) throw InputError("cannot open ORBFILE " + path);
   int ncent = (int)nfunc_center.size();
@@ -365,20 +367,35 @@ static void read_orb(const std::string& path, int nmo, const std::vector<int>& n
     }
     maxlabel = std::max(maxlabel, l + 1);
   }
-  std::vector<double> coef(maxlabel);
+  std::vector<double> coef(maxlabel), coef_im(maxlabel, 0.0);
   for (long i = 0; i < maxlabel; i++) {
     if (!(in >> t)) throw InputError("ORBFILE " + path + ": too few coefficients");
-    coef[i] = to_d(t);
+    if (!t.empty() && t[0] == '(') {
+      if (!moc_im) throw InputError("ORBFILE " + path + ": complex coefficient in real ORBITALS");
+      // "(re,im)" or "(re)"; a space may follow the comma
+      while (t.back() != ')') {
+        std::string more;
+        if (!(in >> more)) throw InputError("ORBFILE " + path + ": unterminated complex coefficient");
+        t += more;
+      }
+      const size_t comma = t.find(',');
+      coef[i] = to_d(t.substr(1, (comma == std::string::npos ? t.size() - 1 : comma) - 1));
+      if (comma != std::string::npos) coef_im[i] = to_d(t.substr(comma + 1, t.size() - comma - 2));
+    } else {
+      coef[i] = to_d(t);
+    }
   }
   int nbasis = 0;
   for (int v : nfunc_center) nbasis += v;
   moc.assign((size_t)nbasis * nmo, 0.0);
+  if (moc_im) moc_im->assign((size_t)nbasis * nmo, 0.0);
   int row = 0;
   for (int c = 0; c < ncent; c++)
     for (int f = 0; f < nfunc_center[c]; f++, row++)
       for (int mo = 0; mo < nmo; mo++) {
         long l = cm[((size_t)mo * ncent + c) * maxb + f];
         moc[(size_t)row * nmo + mo] = l >= 0 ? coef[l] : 0.0;
+        if (moc_im) (*moc_im)[(size_t)row * nmo + mo] = l >= 0 ? coef_im[l] : 0.0;
       }
 }
 
@@ -499,9 +516,10 @@ static void setup_cell(HostSystem& S, const std::vector<std::string>& sysw) {
   }
   pos = 0;
   std::vector<std::string> kp;
-  if (find_section(sysw, "KPOINT", pos, kp))
-    for (auto& k : kp)
-      if (to_d(k) != 0.0) throw InputError("nonzero KPOINT (complex orbitals) is not supported");
+  if (find_section(sysw, "KPOINT", pos, kp)) {
+    if (kp.size() != 3) throw InputError("KPOINT must have 3 elements");
+    for (int d = 0; d < 3; d++) S.kpt[d] = to_d(kp[d]);
+  }
   const double divider = value_d(sysw, "CUTOFF_DIVIDER", 2.000001);
   const int gmax = (int)value_d(sysw, "EWALD_GMAX", 200);
   const double* a0 = S.lat;
@@ -567,6 +585,7 @@ static void setup_cell(HostSystem& S, const std::vector<std::string>& sysw) {
     if (dot3(pc + 3 * i, piped + 3 * i) < 0)
       for (int j = 0; j < 3; j++) pc[3 * i + j] = -pc[3 * i + j];
   std::vector<std::vector<double>> img(S.natoms);
+  std::vector<std::vector<int>> shift(S.natoms);
   const int ns = 4;
   for (int ii = -ns; ii <= ns; ii++)
     for (int jj = -ns; jj <= ns; jj++)
@@ -584,12 +603,16 @@ static void setup_cell(HostSystem& S, const std::vector<std::string>& sysw) {
             if (sh < 0 || fa > 0) inside = false;
           }
           double dc[3] = {p[0] - cm[0], p[1] - cm[1], p[2] - cm[2]};
-          if (inside && std::sqrt(dot3(dc, dc)) < radius) img[at].insert(img[at].end(), p, p + 3);
+          if (inside && std::sqrt(dot3(dc, dc)) < radius) {
+            img[at].insert(img[at].end(), p, p + 3);
+            shift[at].insert(shift[at].end(), {ii, jj, kk});
+          }
         }
   for (int at = 0; at < S.natoms; at++) {
     S.image_first.push_back((int)S.image_pos.size() / 3);
     S.image_count.push_back((int)img[at].size() / 3);
     S.image_pos.insert(S.image_pos.end(), img[at].begin(), img[at].end());
+    S.image_shift.insert(S.image_shift.end(), shift[at].begin(), shift[at].end());
   }
   // the image centers come from the positions as given; the ions themselves
   // are then put inside the cell (same order as the reference's read)
@@ -687,6 +710,7 @@ HostSystem build_system(const std::string& deck_path) {
         S.ion_ion += S.atom_charge[i] * S.atom_charge[j] / std::sqrt(d2);
       }
     S.image_pos = S.atom_pos;
+    S.image_shift.assign((size_t)3 * S.natoms, 0);
     for (int a = 0; a < S.natoms; a++) { S.image_first.push_back(a); S.image_count.push_back(1); }
   }
 
@@ -704,8 +728,11 @@ HostSystem build_system(const std::string& deck_path) {
   if (detwt.empty()) throw InputError("Need DETWT in SLATER section");
   if (detwt.size() > 64) throw InputError("more than 64 determinants: beyond this engine build");
   if (has_section(wf1, "CSF")) throw InputError("CSF expansions are not supported");
-  if (has_section(wf1, "CORBITALS")) throw InputError("complex orbitals (CORBITALS) are not supported");
-  auto orbw = get_section(wf1, "ORBITALS");
+  // CORBITALS: complex orbitals (Slat_wf_data.cpp:130-147)
+  S.complex_orbitals = has_section(wf1, "CORBITALS");
+  if (S.complex_orbitals && has_section(wf1, "ORBITALS")) throw InputError("both ORBITALS and CORBITALS given");
+  auto orbw = get_section(wf1, S.complex_orbitals ? "CORBITALS" : "ORBITALS");
+  if (orbw.empty()) throw InputError("Need ORBITALS or CORBITALS section in SLATER wave function");
   if (!orbw.empty() && (ieq(orbw[0], "CUTOFF_MO") || ieq(orbw[0], "EINSPLINE_MO") || ieq(orbw[0], "BASFUNC_MO")))
     throw InputError("ORBITALS type " + orbw[0] + " not supported (the dense BLAS_MO evaluator is used)");
   std::string tmp;
@@ -756,8 +783,11 @@ HostSystem build_system(const std::string& deck_path) {
   std::string orbfile;
   if (!find_value(orbw, "ORBFILE", orbfile)) throw InputError("Must specify ORBFILE for MO matrix");
   if (orbfile[0] != '/' && !file_exists(orbfile)) orbfile = base + "/" + orbfile;
-  std::vector<double> moc_all;
-  read_orb(orbfile, nmo, nfunc_center, moc_all);
+  std::vector<double> moc_all, moc_all_im;
+  read_orb(orbfile, nmo, nfunc_center, moc_all, S.complex_orbitals ? &moc_all_im : nullptr);
+  const bool kpt_nonzero = S.kpt[0] != 0.0 || S.kpt[1] != 0.0 || S.kpt[2] != 0.0;
+  if ((S.complex_orbitals || kpt_nonzero) && detwt.size() > 1)
+    throw InputError("determinant expansions need real orbitals at the Gamma point");
   auto states = get_section(wf1, "STATES");
   const int ndet = (int)detwt.size();
   if ((int)states.size() != ndet * S.nelec)
@@ -786,6 +816,11 @@ HostSystem build_system(const std::string& deck_path) {
     S.moc[s].assign((size_t)S.nbasis * std::max(S.nmo[s], 1), 0.0);
     for (int j = 0; j < S.nmo[s]; j++)
       for (int f = 0; f < S.nbasis; f++) S.moc[s][(size_t)f * S.nmo[s] + j] = moc_all[(size_t)f * nmo + uni[j]];
+    S.moc_im[s].assign(S.moc[s].size(), 0.0);
+    if (S.complex_orbitals)
+      for (int j = 0; j < S.nmo[s]; j++)
+        for (int f = 0; f < S.nbasis; f++)
+          S.moc_im[s][(size_t)f * S.nmo[s] + j] = moc_all_im[(size_t)f * nmo + uni[j]];
     S.udet_cols[s].clear();
     for (auto& o : uorbs) {
       std::vector<int> cols(ne);

@@ -83,6 +83,12 @@ struct HostSystem {
   // orbitals in STATES order)
   int nmo[2] = {0, 0};
   std::vector<double> moc[2];
+  // complex orbitals (CORBITALS, Slat_wf<dcomplex>): imaginary parts of moc,
+  // same layout; real orbitals with a nonzero k-point also run on the complex
+  // kernels (moc_im zero, real k-point factors)
+  bool complex_orbitals = false;
+  std::vector<double> moc_im[2];
+  double kpt[3] = {0, 0, 0};         // KPOINT (units of pi / lattice vector)
   // determinant expansion sum_k detwt[k] D_up(det_ud[k][0]) D_down(det_ud[k][1])
   // over the distinct spin-determinants; udet_cols[s][u] = the union columns
   // of spin-determinant u in STATES order (Slat_wf_data.cpp:34-303)
@@ -106,6 +112,7 @@ struct HostSystem {
   std::vector<double> lattice_basis;   // [27][3] minimum-image search
   std::vector<double> image_pos;       // [nimage][3] image centers of all atoms
   std::vector<int> image_first, image_count;  // per atom slice of image_pos
+  std::vector<int> image_shift;        // [nimage][3] lattice translation of each image center
   std::vector<double> gvec, gweight, ion_sin, ion_cos;  // Ewald G-vectors [G][3], [G]
   double ewald_const = 0;              // ion-ion Ewald + self/background terms
   // pseudopotential (per atom; nchan == 0 if none)

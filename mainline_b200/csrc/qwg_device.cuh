@@ -24,6 +24,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 namespace qwg {
 
@@ -121,6 +122,17 @@ struct DevSys {
   double alpha, ewald_const;
   int2 atom_images[QWG_MAXA];    // (first, count) into image_pos
   const double* image_pos;       // [nimage][3] basis centers (atoms and their images)
+  // complex-orbital kernels (CORBITALS, or real orbitals at a nonzero k-point):
+  // planar complex tables (imaginary plane of the MO coefficients in moc_im,
+  // same layout as moc); image_kfac[m] = k-point factor of image center m,
+  // e^{i pi k.n} for complex orbitals and cos(pi k.n) for real ones, n its
+  // lattice translation (MO_matrix.h:333-342, MO_matrix_blas.h:179-188)
+  const Real* moc_im;
+  const double* image_kfac;      // [nimage][2]
+  double kpt[3];                 // KPOINT
+  int kint;                      // every k component an integer: the overall sign
+                                 // cos(pi k.n) of a wrap enters node checks and PP signs
+  int real_orb;                  // orbitals real (ORBITALS at a nonzero k-point)
   int ng;                        // Ewald G-vectors
   const double* gvec;            // [ng][3]
   const double* gweight;         // [ng]
@@ -173,6 +185,27 @@ __device__ __forceinline__ void wrap_pos(const DevSys<Real>& S, double& x, doubl
   }
 }
 
+// wrap_pos that also returns the lattice translations applied (nshift[i] +1
+// for each +L_i, Periodic_system::enforcePbc, Periodic_system.cpp:521-570);
+// their k-point phase pi k.n enters the pseudopotential ratios
+// (Periodic_sample::translateElectron, Periodic_sample.cpp:388-420).
+template <typename Real>
+__device__ __forceinline__ double wrap_pos_kphase(const DevSys<Real>& S, double& x, double& y, double& z) {
+  if (!S.periodic) return 0.0;
+  int ns[3] = {0, 0, 0};
+  for (int i = 0; i < 3; i++) {
+    for (int it = 0; it < 64; it++) {
+      const double* n = S.normvec[i];
+      const double sh = n[0] * (x - S.origin[0]) + n[1] * (y - S.origin[1]) + n[2] * (z - S.origin[2]);
+      const double fa = n[0] * (x - S.corners[i][0]) + n[1] * (y - S.corners[i][1]) + n[2] * (z - S.corners[i][2]);
+      if (sh < -1e-12) { x += S.lat[i][0]; y += S.lat[i][1]; z += S.lat[i][2]; ns[i]++; }
+      else if (fa > 1e-12) { x -= S.lat[i][0]; y -= S.lat[i][1]; z -= S.lat[i][2]; ns[i]--; }
+      else break;
+    }
+  }
+  return CUDART_PI * (S.kpt[0] * ns[0] + S.kpt[1] * ns[1] + S.kpt[2] * ns[2]);
+}
+
 // erfc approximation of the Ewald sum (A&S 7.1.26, Periodic_system.h:221-227)
 __device__ __forceinline__ double erfc_poly(double x) {
   const double p = .3275911, a = .254829592, b = -.284496736, c = 1.421413741, d = -1.453152027, e = 1.061405429;
@@ -207,7 +240,7 @@ struct WScal {
   double U;
   double eold;      // previous local energy (DMC weight)
   double weight;
-  double pad;
+  double phase;     // arg psi_D (complex-orbital kernels; 0 otherwise)
 };
 
 struct BlockAcc {   // per-launch reduction target (double atomics)
@@ -686,6 +719,143 @@ __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, d
 }
 
 // ---------------------------------------------------------------------------
+// Complex orbitals (MO_matrix_blas<dcomplex>, MO_matrix_blas.h:336-491).
+// Complex arrays are planar: the real plane, then the imaginary plane.
+
+// Spline value f, f'/r and f'' of one shell at distance r (r < cutoff).
+template <typename Real>
+__device__ __forceinline__ void shell_radial64(const DevSys<Real>& S, int2 so, int k, double r, double& f, double& fd,
+                                               double& f2) {
+  const int i = int(r * S.inv_spacing);
+  const double h = r - double(i) * S.spacing;
+  const double2* c2p = reinterpret_cast<const double2*>(S.spline64 + ((size_t)so.x + (size_t)i * so.y + k) * 4);
+  const double2 ca = __ldg(c2p), cb = __ldg(c2p + 1);
+  f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
+  fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
+  f2 = 2.0 * cb.x + 6.0 * h * cb.y;
+}
+
+// MO values, gradients and Laplacians of one position: each shell summed
+// over its atom's image centers times the image's k-point factor, the
+// |value| <= 1e-8 rule on the modulus of the sums (MO_matrix_blas.h:444-474),
+// then the complex contraction with the coefficients.  Molecules have one
+// image per atom (the atom, factor 1).  bas: [nbasis][5] + imaginary plane at
+// bas + 5 nbasis; out: [M][5] + imaginary plane at out + 5 ms.
+template <typename Real>
+__device__ void mo_lap_warp_cpx(const DevSys<Real>& S, const Real* moc_re, const Real* moc_im, double px, double py,
+                                double pz, int M, int ms, Real* bas, Real* out, int lane) {
+  const int nb5 = 5 * S.nbasis;
+  for (int s = lane; s < S.nshell; s += 32) {
+    const int4 si = S.shell_i[s];
+    const int2 so = S.shell_obj[s];
+    Real* br = bas + si.z * 5;
+    Real* bi = br + nb5;
+    const int nf = sym_nfunc(si.y);
+    for (int k = 0; k < 5 * nf; k++) br[k] = bi[k] = Real(0);
+    const double cut = S.shell_cut[s];
+    const double cut2 = cut * cut * (1.0 + 1e-12);
+    const int2 im = S.atom_images[si.x];
+    for (int m = im.x; m < im.x + im.y; m++) {
+      const double* cp = S.image_pos + 3 * m;
+      const double dx = px - cp[0], dy = py - cp[1], dz = pz - cp[2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (!(r2 < cut2)) continue;
+      const double r = sqrt(r2);
+      if (!(r < cut)) continue;
+      double f, fd, f2;
+      shell_radial64(S, so, si.w, r, f, fd, f2);
+      const double kc = S.image_kfac[2 * m], ks = S.image_kfac[2 * m + 1];
+      shell_lap_store<Real, true>(si.y, dx, dy, dz, f * kc, fd * kc, f2 * kc, br);
+      if (ks != 0.0) shell_lap_store<Real, true>(si.y, dx, dy, dz, f * ks, fd * ks, f2 * ks, bi);
+    }
+    for (int k = 0; k < nf; k++) {
+      const double vr = double(br[5 * k]), vi = double(bi[5 * k]);
+      if (!(sqrt(vr * vr + vi * vi) > 1e-8))
+        for (int c = 0; c < 5; c++) br[5 * k + c] = bi[5 * k + c] = Real(0);
+    }
+  }
+  __syncwarp();
+  for (int mo = lane; mo < M; mo += 32) {
+    Real ar[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)}, ai[5] = {Real(0), Real(0), Real(0), Real(0), Real(0)};
+    for (int f = 0; f < S.nbasis; f++) {
+      const Real cr = moc_re[(size_t)f * ms + mo], ci = moc_im[(size_t)f * ms + mo];
+      const Real* b = bas + f * 5;
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        const Real xr = b[q], xi = b[nb5 + q];
+        ar[q] += cr * xr - ci * xi;
+        ai[q] += cr * xi + ci * xr;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 5; q++) { out[mo * 5 + q] = ar[q]; out[5 * ms + mo * 5 + q] = ai[q]; }
+  }
+  __syncwarp();
+}
+
+// Determinant ratio of one electron moved to p, by the calling lane, with
+// the projected coefficients w (complex, planar with imaginary plane at
+// w_im): sum_f b_f(p) w_f over the k-phased image sums of every shell.
+template <typename Real>
+__device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double px, double py, double pz,
+                                                   const Real* w_re, const Real* w_im, Real& out_re, Real& out_im) {
+  Real acr = Real(0), aci = Real(0);
+  for (int c = 0; c < S.natoms; c++) {
+    const int4 cs = S.center_seg[c];  // first shell, shells, object base, splines per row
+    if (cs.y == 0) continue;
+    const int2 im = S.atom_images[c];
+    const Real cut = Real(S.center_cut[c]);
+    const Real cut2 = cut * cut * Real(1.000001);
+    for (int k = 0; k < cs.y; k++) {
+      const int pk = S.shell_pack[cs.x + k];
+      const int sym = pk & 0xf, fb = (pk >> 4) & 0xffff, kk = (pk >> 20) & 0xff;
+      Real fr[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
+      Real fi[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
+      for (int m = im.x; m < im.x + im.y; m++) {
+        const double* cp = S.image_pos + 3 * m;
+        const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
+        const Real rd2 = x * x + y * y + z * z;
+        if (!(rd2 < cut2)) continue;
+        const Real rd = sqrt(rd2);
+        if (!(rd < cut)) continue;
+        const int i = int(rd * Real(S.inv_spacing));
+        const Real h = rd - Real(i) * Real(S.spacing);
+        const Real* cf = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4 + 4 * kk;
+        const Real f = __ldg(cf) + h * (__ldg(cf + 1) + h * (__ldg(cf + 2) + h * __ldg(cf + 3)));
+        Real a[6];
+        int n;
+        switch (sym) {
+          case 0: a[0] = f; n = 1; break;
+          case 1: a[0] = x * f; a[1] = y * f; a[2] = z * f; n = 3; break;
+          case 2:
+            a[0] = x * x * f; a[1] = y * y * f; a[2] = z * z * f; a[3] = x * y * f; a[4] = x * z * f; a[5] = y * z * f;
+            n = 6;
+            break;
+          default:
+            a[0] = (Real(2) * z * z - x * x - y * y) * f; a[1] = x * z * f; a[2] = y * z * f;
+            a[3] = (x * x - y * y) * f; a[4] = x * y * f; n = 5;
+            break;
+        }
+        const Real kc = Real(S.image_kfac[2 * m]), ks = Real(S.image_kfac[2 * m + 1]);
+#pragma unroll
+        for (int q = 0; q < 6; q++)
+          if (q < n) { fr[q] += kc * a[q]; fi[q] += ks * a[q]; }
+      }
+      const int n = sym_nfunc(sym);
+#pragma unroll
+      for (int q = 0; q < 6; q++)
+        if (q < n && sqrt(fr[q] * fr[q] + fi[q] * fi[q]) > Real(1e-8)) {
+          const Real wr = w_re[fb + q], wi = w_im[fb + q];
+          acr += fr[q] * wr - fi[q] * wi;
+          aci += fr[q] * wi + fi[q] * wr;
+        }
+    }
+  }
+  out_re = acr;
+  out_im = aci;
+}
+
+// ---------------------------------------------------------------------------
 // Jastrow pieces (tables from the parameter bank; sums in double)
 
 // Two-body u(r) for a pair of given spins: value, f'/r, lap (precision T).
@@ -1058,6 +1228,89 @@ __device__ void gj_inverse_warp(double* aug, int M, Real* invT, int invstride, d
   __syncwarp();
   logdet = ld;
   sign = sg;
+}
+
+// Complex Gauss-Jordan inversion with partial pivoting on the modulus (the
+// complex counterpart of gj_inverse_warp_big, TransposeInverseMatrix for
+// dcomplex, MatrixAlgebrac.cpp:316-421): aug holds the real plane [M][2M],
+// then the imaginary plane [M][2M], then the pivot column (real M, imaginary
+// M).  Writes the transposed inverse (planar, imaginary plane at inv_im) and
+// returns log|det A| and arg det A.
+template <typename Real>
+__device__ void gj_inverse_warp_cpx(double* aug, int M, Real* inv_re, Real* inv_im, int invstride, double& logdet,
+                                    double& phase, int lane) {
+  const int W = 2 * M;
+  double* ar = aug;
+  double* ai = aug + (size_t)M * W;
+  double* fr = ai + (size_t)M * W;
+  double* fi = fr + M;
+  for (int idx = lane; idx < M * M; idx += 32) {
+    int i = idx / M, k = idx - i * M;
+    ar[i * W + M + k] = (i == k) ? 1.0 : 0.0;
+    ai[i * W + M + k] = 0.0;
+  }
+  __syncwarp();
+  double ld = 0.0, ph = 0.0;
+  bool singular = false;
+  for (int k = 0; k < M; k++) {
+    double best = -1.0;
+    int bi = k;
+    for (int i = k + lane; i < M; i += 32) {
+      const double v = hypot(ar[i * W + k], ai[i * W + k]);
+      if (v > best) { best = v; bi = i; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if (!(best > 0.0)) { singular = true; break; }
+    if (bi != k) {
+      for (int c = lane; c < W; c += 32) {
+        double t = ar[k * W + c]; ar[k * W + c] = ar[bi * W + c]; ar[bi * W + c] = t;
+        t = ai[k * W + c]; ai[k * W + c] = ai[bi * W + c]; ai[bi * W + c] = t;
+      }
+      ph += CUDART_PI;
+    }
+    __syncwarp();
+    const double pr = ar[k * W + k], pi = ai[k * W + k];
+    const double m2 = pr * pr + pi * pi;
+    ld += 0.5 * log(m2);
+    ph += atan2(pi, pr);
+    const double qr = pr / m2, qi = -pi / m2;  // 1 / pivot
+    __syncwarp();
+    for (int c = lane; c < W; c += 32) {
+      const double xr = ar[k * W + c], xi = ai[k * W + c];
+      ar[k * W + c] = xr * qr - xi * qi;
+      ai[k * W + c] = xr * qi + xi * qr;
+    }
+    for (int i = lane; i < M; i += 32) { fr[i] = ar[i * W + k]; fi[i] = ai[i * W + k]; }
+    __syncwarp();
+    for (int c = lane; c < W; c += 32) {
+      if (c < k) continue;
+      const double pkr = ar[k * W + c], pki = ai[k * W + c];
+      if (c == k) {
+        for (int i = 0; i < M; i++)
+          if (i != k) { ar[i * W + c] = 0.0; ai[i * W + c] = 0.0; }
+      } else {
+        for (int i = 0; i < M; i++)
+          if (i != k) {
+            ar[i * W + c] -= fr[i] * pkr - fi[i] * pki;
+            ai[i * W + c] -= fr[i] * pki + fi[i] * pkr;
+          }
+      }
+    }
+    __syncwarp();
+  }
+  for (int idx = lane; idx < M * M; idx += 32) {
+    int e = idx / M, i = idx - e * M;
+    inv_re[e * invstride + i] = singular ? Real(0) : Real(ar[i * W + M + e]);
+    inv_im[e * invstride + i] = singular ? Real(0) : Real(ai[i * W + M + e]);
+  }
+  __syncwarp();
+  logdet = singular ? -1e201 : ld;
+  phase = ph;
 }
 
 }  // namespace qwg

@@ -56,6 +56,13 @@ static void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
 // kMaxOrbHBM orbitals per spin); -1 is beyond this build.
 constexpr int kMaxOrbHBM = 256;
 static int mo_stride_for(int mmax, int nmo_max) { return mmax > 0 ? mmax : (nmo_max + 3) / 4 * 4; }
+// -1: the HBM-resident kernels with complex orbitals (CORBITALS, or real
+// orbitals at a nonzero k-point)
+constexpr int kComplexFamily = -1;
+static bool hbm_family(int mmax) { return mmax <= 0; }
+static bool needs_complex(const HostSystem& H) {
+  return H.complex_orbitals || H.kpt[0] != 0.0 || H.kpt[1] != 0.0 || H.kpt[2] != 0.0;
+}
 static int mmax_for(int m) {
   if (m <= 8) return 8;
   if (m <= 16) return 16;
@@ -81,7 +88,7 @@ struct qwg_ctx {
   bool own_stream = false;
   long long launches = 0;
   // tables
-  DevBuf d_shell_i, d_shell_obj, d_shell_cut, d_spline, d_spline64, d_moc;
+  DevBuf d_shell_i, d_shell_obj, d_shell_cut, d_spline, d_spline64, d_moc, d_moc_im, d_image_kfac;
   DevBuf d_image_pos, d_gvec, d_gweight, d_ion_sin, d_ion_cos;
   DevBuf d_det_c, d_det_ud, d_ud_cols;  // determinant expansion tables
   DevSys<double> sys_d{};
@@ -148,6 +155,13 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
   S.spline = c->d_spline.as<Real>();
   S.spline64 = c->d_spline64.as<double>();
   S.moc = c->d_moc.as<Real>();
+  S.moc_im = c->d_moc_im.as<Real>();
+  S.image_kfac = c->d_image_kfac.as<double>();
+  for (int d = 0; d < 3; d++) S.kpt[d] = H.kpt[d];
+  S.kint = 1;
+  for (int d = 0; d < 3; d++)
+    if (H.kpt[d] != std::floor(H.kpt[d])) S.kint = 0;
+  S.real_orb = H.complex_orbitals ? 0 : 1;
   S.npts = H.spline_npts;
   S.spacing = H.spline_spacing;
   S.inv_spacing = 1.0 / H.spline_spacing;
@@ -207,7 +221,7 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
   S.gweight = c->d_gweight.as<double>();
   S.ion_sin = c->d_ion_sin.as<double>();
   S.ion_cos = c->d_ion_cos.as<double>();
-  if (H.periodic)
+  if (H.periodic && c->mmax != kComplexFamily)
     for (int a = 0; a < H.natoms; a++) {
       int nf = 0;
       for (auto& sh : H.shells)
@@ -299,10 +313,14 @@ static void build_tables(qwg_ctx* c) {
   upload(c->d_shell_cut, sc, st);
   // MO coefficients padded to the orbital stride, both spins
   const int mm = mo_stride_for(c->mmax, std::max(H.nmo[0], H.nmo[1]));
-  std::vector<double> moc((size_t)2 * H.nbasis * mm, 0.0);
+  std::vector<double> moc((size_t)2 * H.nbasis * mm, 0.0), moc_im(moc.size(), 0.0);
   for (int s = 0; s < 2; s++)
     for (int f = 0; f < H.nbasis; f++)
-      for (int i = 0; i < H.nmo[s]; i++) moc[((size_t)s * H.nbasis + f) * mm + i] = H.moc[s][(size_t)f * H.nmo[s] + i];
+      for (int i = 0; i < H.nmo[s]; i++) {
+        moc[((size_t)s * H.nbasis + f) * mm + i] = H.moc[s][(size_t)f * H.nmo[s] + i];
+        moc_im[((size_t)s * H.nbasis + f) * mm + i] = H.moc_im[s][(size_t)f * H.nmo[s] + i];
+      }
+  if (c->mmax != kComplexFamily) moc_im.clear();
   // determinant expansion: weights, (up, down) spin-determinant of each
   // determinant, union columns of every distinct spin-determinant
   upload(c->d_det_c, H.detwt, st);
@@ -316,13 +334,27 @@ static void build_tables(qwg_ctx* c) {
   if (c->precision == QWG_FP64) {
     upload(c->d_spline, il, st);
     upload(c->d_moc, moc, st);
+    upload(c->d_moc_im, moc_im, st);
   } else {
     std::vector<float> sf(il.begin(), il.end());
     std::vector<float> mf(moc.begin(), moc.end());
+    std::vector<float> mfi(moc_im.begin(), moc_im.end());
     upload(c->d_spline, sf, st);
     upload(c->d_moc, mf, st);
+    upload(c->d_moc_im, mfi, st);
   }
   upload(c->d_image_pos, H.image_pos, st);
+  // k-point factor of every image center: e^{i pi k.n} (complex orbitals) or
+  // cos(pi k.n) (real orbitals), n the image's lattice translation
+  // (eval_kpoint_fac, MO_matrix.h:333-342)
+  std::vector<double> kfac(H.image_pos.size() / 3 * 2, 0.0);
+  for (size_t m = 0; m < kfac.size() / 2; m++) {
+    const double dot = H.kpt[0] * H.image_shift[3 * m] + H.kpt[1] * H.image_shift[3 * m + 1] +
+                       H.kpt[2] * H.image_shift[3 * m + 2];
+    kfac[2 * m] = std::cos(dot * M_PI);
+    kfac[2 * m + 1] = H.complex_orbitals ? std::sin(dot * M_PI) : 0.0;
+  }
+  upload(c->d_image_kfac, kfac, st);
   upload(c->d_gvec, H.gvec, st);
   upload(c->d_gweight, H.gweight, st);
   upload(c->d_ion_sin, H.ion_sin, st);
@@ -340,9 +372,12 @@ static int align16(int x) { return (x + 15) / 16 * 16; }
 static void make_layout(qwg_ctx* c) {
   const HostSystem& H = c->H;
   const int N = H.nelec, A = H.natoms;
-  const bool hbm = c->mmax == 0;
+  const bool hbm = hbm_family(c->mmax);
   const int mm = mo_stride_for(c->mmax, std::max(H.nmo[0], H.nmo[1]));
-  const int rs = c->precision == QWG_FP64 ? 8 : 4;
+  // complex orbitals: planar complex inverse, MO rows, basis rows and
+  // projected coefficients (twice the real sizes)
+  const int cf = c->mmax == kComplexFamily ? 2 : 1;
+  const int rs = (c->precision == QWG_FP64 ? 8 : 4) * cf;
   WLayout& L = c->L;
   L.mstride = mm;
   int o = 0;
@@ -366,7 +401,7 @@ static void make_layout(qwg_ctx* c) {
   L.bas = o; o = align16(o + rs * H.nbasis * 5);
   L.newcol = o; o = align16(o + rs * mm * 5);
   L.dG = o; o = align16(o + 8 * 4 * N);
-  L.lu = o; o = align16(o + 8 * (mm * 2 * mm + mm));
+  L.lu = o; o = align16(o + 8 * cf * (mm * 2 * mm + mm));
   if (H.detwt.size() > 1) {
     L.mdv = o; o = align16(o + 8 * mm * mm);
     L.mdr = o; o = align16(o + 8 * QWG_MAXUD * 5);
@@ -435,9 +470,10 @@ static size_t footprint_bytes(const qwg_ctx* c, int max_walkers) {
   size_t total4 = 0;
   for (size_t o = 0; o < H.obj_first.size(); o++) total4 += (size_t)H.spline_npts * H.obj_count[o];
   const size_t ms = mo_stride_for(c->mmax, std::max(H.nmo[0], H.nmo[1]));
-  size_t b = total4 * 4 * (8 + rs) + 2 * (size_t)H.nbasis * ms * rs + H.shells.size() * 32 +
-             H.image_pos.size() * 8 + H.gvec.size() * 8 + 3 * H.gweight.size() * 8;
-  b += W * (2 * 3 * N * 8 + 2 * (size_t)c->L.state_bytes + (c->mmax == 0 ? (size_t)c->L.scratch_bytes : 0) + 20);
+  const size_t cf = c->mmax == kComplexFamily ? 2 : 1;
+  size_t b = total4 * 4 * (8 + rs) + 2 * (size_t)H.nbasis * ms * rs * cf + H.shells.size() * 32 +
+             H.image_pos.size() * 8 * 5 / 3 + H.gvec.size() * 8 + 3 * H.gweight.size() * 8;
+  b += W * (2 * 3 * N * 8 + 2 * (size_t)c->L.state_bytes + (hbm_family(c->mmax) ? (size_t)c->L.scratch_bytes : 0) + 20);
   b += W * 8 * (9 + 5 + 4 * N);  // evaluation outputs (qwg_eval / qwg_dmc_init)
   b += sizeof(BlockAcc) * 1024 + DYN_COUNT * 8 + (size_t)kHistCap * 8 + kStatsLen * 8;
   if (max_walkers > kBranchSmemMax) b += branch_bytes(max_walkers);
@@ -474,6 +510,7 @@ static void launch_walkers(qwg_ctx* c, const StepParams& P, const EvalIO& io, in
       case 8: launch_walkers_t<double, 8>(c, c->sys_d, P, io, mode, nwalk); break;
       case 16: launch_walkers_t<double, 16>(c, c->sys_d, P, io, mode, nwalk); break;
       case 32: launch_walkers_t<double, 32>(c, c->sys_d, P, io, mode, nwalk); break;
+      case kComplexFamily: launch_walkers_t<double, -1>(c, c->sys_d, P, io, mode, nwalk); break;
       default: launch_walkers_t<double, 0>(c, c->sys_d, P, io, mode, nwalk); break;
     }
   } else {
@@ -481,6 +518,7 @@ static void launch_walkers(qwg_ctx* c, const StepParams& P, const EvalIO& io, in
       case 8: launch_walkers_t<float, 8>(c, c->sys_f, P, io, mode, nwalk); break;
       case 16: launch_walkers_t<float, 16>(c, c->sys_f, P, io, mode, nwalk); break;
       case 32: launch_walkers_t<float, 32>(c, c->sys_f, P, io, mode, nwalk); break;
+      case kComplexFamily: launch_walkers_t<float, -1>(c, c->sys_f, P, io, mode, nwalk); break;
       default: launch_walkers_t<float, 0>(c, c->sys_f, P, io, mode, nwalk); break;
     }
   }
@@ -719,6 +757,7 @@ int qwg_inspect_deck(const char* deck_path, qwg_info* info, char* err, int errle
       info->nelec = H.nelec; info->nup = H.nup; info->ndown = H.ndn; info->natoms = H.natoms;
       info->nbasis = H.nbasis; info->nshell = (int)H.shells.size(); info->nmo_up = H.nmo[0];
       info->nmo_down = H.nmo[1]; info->has_pseudo = H.has_pp; info->ion_ion = H.ion_ion;
+      info->complex_orbitals = needs_complex(H) ? 1 : 0;
     }
     return QWG_OK;
   } catch (const std::exception& e) {
@@ -737,6 +776,7 @@ int qwg_footprint(const char* deck_path, int precision, int max_walkers, unsigne
     c->mmax = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
     if (c->mmax < 0) return QWG_ERR_INPUT;
     if (c->H.detwt.size() > 1) c->mmax = 0;  // expansions run on the HBM-resident kernels
+    if (needs_complex(c->H)) c->mmax = kComplexFamily;
     make_layout(c.get());
     *bytes = footprint_bytes(c.get(), max_walkers);
     return QWG_OK;
@@ -778,6 +818,7 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
       if (c->H.periodic) throw InputError("determinant expansions are supported for molecules only");
       mm = 0;  // expansions run on the HBM-resident kernels
     }
+    if (needs_complex(c->H)) mm = kComplexFamily;  // complex orbitals / twisted boundary conditions
     c->mmax = mm;
     if (const char* sched = getenv("QWG_DMC_SCHEDULE")) c->split = strcmp(sched, "fused") != 0;
     if (stream) {
@@ -793,7 +834,7 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
     c->d_R2.alloc((size_t)max_walkers * 3 * N * 8);
     c->d_state.alloc((size_t)max_walkers * c->L.state_bytes);
     c->d_state2.alloc((size_t)max_walkers * c->L.state_bytes);
-    if (c->mmax == 0) c->d_scratch.alloc((size_t)max_walkers * c->L.scratch_bytes);
+    if (hbm_family(c->mmax)) c->d_scratch.alloc((size_t)max_walkers * c->L.scratch_bytes);
     c->d_acc.alloc(sizeof(BlockAcc) * 1024);
     c->d_dyn.alloc(DYN_COUNT * 8);
     CK(cudaMemsetAsync(c->d_dyn.p, 0, DYN_COUNT * 8, c->stream));
@@ -839,6 +880,7 @@ int qwg_get_info(const qwg_ctx* c, qwg_info* info) {
   info->has_pseudo = H.has_pp; info->max_walkers = c->max_walkers; info->precision = c->precision;
   info->walkers_per_cta = c->wpc; info->ion_ion = H.ion_ion;
   info->device_bytes = footprint_bytes(c, c->max_walkers);
+  info->complex_orbitals = c->mmax == kComplexFamily ? 1 : 0;
   return QWG_OK;
 }
 
@@ -1226,7 +1268,7 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
   static_assert(sizeof(BlockAcc) <= 256, "accumulator block exceeds its scratch slot");
   // HBM-resident walkers (more than 32 orbitals per spin) also need their
   // scratch region in the fixed buffer, after the walker states
-  const size_t per = (size_t)c->L.state_bytes + (c->mmax == 0 ? (size_t)c->L.scratch_bytes : 0);
+  const size_t per = (size_t)c->L.state_bytes + (hbm_family(c->mmax) ? (size_t)c->L.scratch_bytes : 0);
   const size_t need = acc_bytes + (size_t)nw * per;
   if (need > QWG_NOALLOC_SCRATCH_BYTES) {
     const size_t maxw = (QWG_NOALLOC_SCRATCH_BYTES - acc_bytes) / per;
@@ -1253,7 +1295,7 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
     P.max_weight = 1.0;
     P.R = d_R;
     P.state = base + acc_bytes;
-    P.scratch = c->mmax == 0 ? base + acc_bytes + (size_t)nw * c->L.state_bytes : nullptr;
+    P.scratch = hbm_family(c->mmax) ? base + acc_bytes + (size_t)nw * c->L.state_bytes : nullptr;
     P.acc = acc;
     P.etrial = c->d_dyn.as<double>();
     EvalIO io{};
@@ -1466,7 +1508,7 @@ int qwg_autotune(qwg_ctx* c, int* walkers_per_cta) {
     io.logpsi = base; io.sign = base + W; io.kinetic = base + 2 * W; io.potential = base + 3 * W;
     io.nonlocal = base + 4 * W; io.grad = base + 5 * W; io.lap = io.grad + n_g;
     // shared memory per walker (none for HBM-resident walkers)
-    const size_t per = c->mmax == 0 ? 0 : (size_t)c->L.bytes;
+    const size_t per = hbm_family(c->mmax) ? 0 : (size_t)c->L.bytes;
     int best = c->wpc;
     float best_ms = 1e30f;
     for (int cand : {1, 2, 4}) {

@@ -37,7 +37,9 @@ struct PPItem {
 
 // MMAX > 0: at most MMAX orbitals per spin, state + scratch in shared
 // memory.  MMAX == 0: any count up to 256 per spin, arrays strided by
-// L.mstride and worked on in place in HBM.
+// L.mstride and worked on in place in HBM.  MMAX == -1 (QWG_MM_CPX): the
+// HBM-resident layout with complex orbitals (Slat_wf<dcomplex>): inverse,
+// MO rows, basis rows and projected coefficients are planar complex arrays.
 // PER: 0 molecule, 1 periodic cell, 2 either (decided at run time); the
 // local-energy kernels are compiled per case, the others check at run time.
 template <typename Real, int MMAX, bool TB, int PER>
@@ -48,6 +50,8 @@ struct Walker {
   unsigned char* sbase;  // scratch
   const Real* moc_s;     // [2][nbasis][mstride] MO coefficients (global, read through L1)
   int lane;
+  static constexpr bool CPX = MMAX < 0;
+  double cr_re = 0.0, cr_im = 0.0;  // complex determinant ratio of the last proposal (CPX)
 
   __device__ __forceinline__ int MS() const {
     if constexpr (MMAX > 0) return MMAX;
@@ -56,11 +60,12 @@ struct Walker {
   __device__ double* R() const { return (double*)(base + L.R); }
   __device__ Real* inv(int s) const {
     if constexpr (MMAX > 0) return (Real*)(base + L.inv) + (size_t)s * MS() * MS();
+    else if constexpr (CPX) return (Real*)(base + L.inv) + (size_t)s * 2 * MS() * MS();  // + MS()^2: imaginary
     else return (Real*)(base + L.inv) + (size_t)s * L.nud * MS() * MS();
   }
   // ---- determinant expansions (HBM-resident kernels, S.ndet > 1)
   __device__ bool multi() const {
-    if constexpr (MMAX > 0) return false;
+    if constexpr (MMAX != 0) return false;
     else return S.ndet > 1;
   }
   __device__ Real* inv_u(int s, int u) const { return (Real*)(base + L.inv) + ((size_t)s * L.nud + u) * MS() * MS(); }
@@ -120,6 +125,47 @@ struct Walker {
   __device__ int spin(int e) const { return e < S.nup ? 0 : 1; }
   __device__ int eloc(int e) const { return e < S.nup ? e : e - S.nup; }
   __device__ const Real* mocs(int s) const { return moc_s + (size_t)s * S.nbasis * MS(); }
+  __device__ const Real* mocs_im(int s) const { return S.moc_im + (size_t)s * S.nbasis * MS(); }
+  // imaginary planes of the complex arrays (CPX)
+  __device__ size_t mov_im_off() const { return (size_t)S.nelec * MS() * 4; }
+  __device__ int newcol_im_off() const { return 5 * MS(); }
+  __device__ int wproj_im_off() const { return L.wchunk * S.nbasis; }
+
+  // Complex determinants (CPX): the recompute of both spins (Slat_wf<dcomplex>::
+  // calcLap, Slat_wf.h:948-1016).
+  __device__ void recompute_cpx() {
+    double* Rp = R();
+    Real* nc = newcol();
+    double* aug = lu();
+    WScal* w = sc();
+    const int ms = MS();
+    double phase = 0.0;
+    for (int s = 0; s < 2; s++) {
+      const int M = S.m[s];
+      const int e0 = s == 0 ? 0 : S.nup;
+      double* ar = aug;
+      double* ai = aug + (size_t)2 * M * M;
+      for (int el = 0; el < M; el++) {
+        const int e = e0 + el;
+        mo_lap_warp_cpx<Real>(S, mocs(s), mocs_im(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], M, ms, bas(), nc, lane);
+        for (int i = lane; i < M; i += 32) {
+          ar[el * 2 * M + i] = double(nc[i * 5]);
+          ai[el * 2 * M + i] = double(nc[newcol_im_off() + i * 5]);
+          Real* mv = mov() + ((size_t)e * ms + i) * 4;
+          Real* mw = mv + mov_im_off();
+          for (int q = 0; q < 4; q++) { mv[q] = nc[i * 5 + 1 + q]; mw[q] = nc[newcol_im_off() + i * 5 + 1 + q]; }
+        }
+        __syncwarp();
+      }
+      double ld = 0.0, ph = 0.0;
+      if (M > 0) gj_inverse_warp_cpx(aug, M, inv(s), inv(s) + (size_t)ms * ms, ms, ld, ph, lane);
+      phase += ph;
+      if (lane == 0) { w->logdet[s] = ld; w->sign[s] = 1.0; }
+      __syncwarp();
+    }
+    if (lane == 0) w->phase = phase;
+    __syncwarp();
+  }
 
   // ---- full recompute: Slat_wf::calcLap (Slat_wf.h:948-1016) + the Jastrow
   // recomputation of every electron (Jastrow2_wf.cpp:988-1157).
@@ -128,6 +174,7 @@ struct Walker {
     Real* nc = newcol();
     double* aug = lu();
     WScal* w = sc();
+    if constexpr (CPX) recompute_cpx();
     for (int s = 0; s < 2 && multi(); s++) {
       // every orbital of the spin's union at every electron, then one
       // inversion per distinct spin-determinant (Slat_wf::calcLap for all
@@ -160,7 +207,7 @@ struct Walker {
       if (lane == 0) { w->logdet[s] = udl()[((size_t)s * L.nud) * 2]; w->sign[s] = udl()[((size_t)s * L.nud) * 2 + 1]; }
     }
     if (multi()) md_weights();
-    for (int s = 0; s < 2 && !multi(); s++) {
+    for (int s = 0; s < 2 && !multi() && !CPX; s++) {
       const int M = S.m[s];
       const int e0 = s == 0 ? 0 : S.nup;
       for (int el = 0; el < M; el++) {
@@ -225,6 +272,20 @@ struct Walker {
     const int s = spin(e), el = eloc(e), M = S.m[s];
     const Real* iv = inv(s) + (size_t)el * MS();
     const Real* mv = mov() + (size_t)e * MS() * 4;
+    if constexpr (CPX) {
+      // real parts of grad D / D and lap D / D: the drift, and with the
+      // Jastrow terms the kinetic energy -1/2 Re(lap psi / psi)
+      // (System::calcKineticSeparated, System.cpp:105-140)
+      const Real* ivi = iv + (size_t)MS() * MS();
+      const Real* mvi = mv + mov_im_off();
+      double b[4] = {0, 0, 0, 0};
+      for (int i = 0; i < M; i++) {
+        const double cr = iv[i], ci = ivi[i];
+        for (int q = 0; q < 4; q++) b[q] += cr * double(mv[4 * i + q]) - ci * double(mvi[4 * i + q]);
+      }
+      g[0] = b[0]; g[1] = b[1]; g[2] = b[2]; l = b[3];
+      return;
+    }
     double a0 = 0, a1 = 0, a2 = 0, a3 = 0;  // FP64 accumulation of the short dots
     for (int i = 0; i < M; i++) {
       double c = iv[i];
@@ -269,6 +330,29 @@ struct Walker {
         r3 += T[u] * rr[u * 5 + 3]; r4 += T[u] * rr[u * 5 + 4];
       }
       r0 /= W; r1 /= W; r2 /= W; r3 /= W; r4 /= W;
+    } else if constexpr (CPX) {
+      // complex ratio R = sum_i invT[el][i] phi_i(p); |R| returned, R kept
+      // for accept; drift and Laplacian from the real parts of the ratios
+      mo_lap_warp_cpx<Real>(S, mocs(s), mocs_im(s), px, py, pz, M, MS(), bas(), nc, lane);
+      const Real* iv = inv(s) + (size_t)el * MS();
+      const Real* ivi = iv + (size_t)MS() * MS();
+      const Real* nci = nc + newcol_im_off();
+      double a[5] = {0, 0, 0, 0, 0}, b[5] = {0, 0, 0, 0, 0};
+      for (int i = 0; i < M; i++) {
+        const double cr = iv[i], ci = ivi[i];
+        for (int q = 0; q < 5; q++) {
+          const double xr = nc[i * 5 + q], xi = nci[i * 5 + q];
+          a[q] += cr * xr - ci * xi;
+          b[q] += cr * xi + ci * xr;
+        }
+      }
+      cr_re = a[0]; cr_im = b[0];
+      const double m2 = a[0] * a[0] + b[0] * b[0];
+      r0 = sqrt(m2);
+      // Re(x / R) = (Re x Re R + Im x Im R) / |R|^2, scaled by |R| for the
+      // division below
+      r1 = (a[1] * a[0] + b[1] * b[0]) / r0; r2 = (a[2] * a[0] + b[2] * b[0]) / r0;
+      r3 = (a[3] * a[0] + b[3] * b[0]) / r0; r4 = (a[4] * a[0] + b[4] * b[0]) / r0;
     } else {
       mo_lap_warp<Real, PER>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
       const Real* iv = inv(s) + (size_t)el * MS();
@@ -412,7 +496,41 @@ struct Walker {
         mv[0] = nc[j * 5 + 1]; mv[1] = nc[j * 5 + 2]; mv[2] = nc[j * 5 + 3]; mv[3] = nc[j * 5 + 4];
       }
     }
-    for (int k = lane; k < M && !multi(); k += 32) {
+    if constexpr (CPX) {
+      // complex Sherman-Morrison update with R = cr_re + i cr_im
+      Real* ivi = iv + (size_t)ms * ms;
+      const Real* nci = nc + newcol_im_off();
+      Real* wki = rowe + ms;
+      Real* rowi = wki + ms;
+      for (int k = lane; k < M; k += 32) {
+        Real ar = 0, ai = 0;
+        for (int i = 0; i < M; i++) {
+          const Real xr = nc[i * 5], xi = nci[i * 5], vr = iv[(size_t)k * ms + i], vi = ivi[(size_t)k * ms + i];
+          ar += xr * vr - xi * vi;
+          ai += xr * vi + xi * vr;
+        }
+        wk[k] = ar; wki[k] = ai;
+        rowe[k] = iv[(size_t)el * ms + k]; rowi[k] = ivi[(size_t)el * ms + k];
+      }
+      __syncwarp();
+      const double m2 = cr_re * cr_re + cr_im * cr_im;
+      const Real qr = Real(cr_re / m2), qi = Real(-cr_im / m2);  // 1 / R
+      for (int idx = lane; idx < M * M; idx += 32) {
+        int k = idx / M, i = idx - k * M;
+        const Real ur = rowe[i] * qr - rowi[i] * qi, ui = rowe[i] * qi + rowi[i] * qr;  // row_el / R
+        if (k == el) { iv[(size_t)k * ms + i] = ur; ivi[(size_t)k * ms + i] = ui; }
+        else {
+          iv[(size_t)k * ms + i] -= ur * wk[k] - ui * wki[k];
+          ivi[(size_t)k * ms + i] -= ur * wki[k] + ui * wk[k];
+        }
+      }
+      for (int i = lane; i < M; i += 32) {
+        Real* mv = mov() + ((size_t)e * ms + i) * 4;
+        Real* mw = mv + mov_im_off();
+        for (int q = 0; q < 4; q++) { mv[q] = nc[i * 5 + 1 + q]; mw[q] = nci[i * 5 + 1 + q]; }
+      }
+    }
+    for (int k = lane; k < M && !multi() && !CPX; k += 32) {
       Real acc = 0;
       for (int i = 0; i < M; i++) acc += nc[i * 5] * iv[(size_t)k * ms + i];
       wk[k] = acc;
@@ -420,12 +538,12 @@ struct Walker {
     }
     __syncwarp();
     const Real invr = Real(1.0 / ratioD);
-    for (int idx = lane; idx < M * M && !multi(); idx += 32) {
+    for (int idx = lane; idx < M * M && !multi() && !CPX; idx += 32) {
       int k = idx / M, i = idx - k * M;
       if (k == el) iv[(size_t)k * ms + i] = rowe[i] * invr;
       else iv[(size_t)k * ms + i] -= rowe[i] * wk[k] * invr;
     }
-    for (int i = lane; i < M && !multi(); i += 32) {
+    for (int i = lane; i < M && !multi() && !CPX; i += 32) {
       Real* mv = mov() + ((size_t)e * ms + i) * 4;
       mv[0] = nc[i * 5 + 1]; mv[1] = nc[i * 5 + 2]; mv[2] = nc[i * 5 + 3]; mv[3] = nc[i * 5 + 4];
     }
@@ -442,7 +560,8 @@ struct Walker {
       Rp[3 * e] = px; Rp[3 * e + 1] = py; Rp[3 * e + 2] = pz;
       WScal* w = sc();
       w->logdet[s] += log(fabs(ratioD));
-      if (ratioD < 0) w->sign[s] = -w->sign[s];
+      if (CPX) w->phase += atan2(cr_im, cr_re);
+      else if (ratioD < 0) w->sign[s] = -w->sign[s];
       w->U += dU;
     }
     __syncwarp();
@@ -637,7 +756,23 @@ struct Walker {
         for (int m = 0; m < M; m++) acc += cf[cu[m]] * iv[m];
         w[((size_t)u * CH + le) * S.nbasis + f] = acc;
       }
-      for (int idx = lane; idx < (e1 - e0) * S.nbasis && !multi(); idx += 32) {
+      for (int idx = lane; idx < (e1 - e0) * S.nbasis && CPX; idx += 32) {
+        // complex w_f = sum_m C[f][m] invT[el][m]
+        const int le = idx / S.nbasis, f = idx - le * S.nbasis;
+        const int e = e0 + le, s = spin(e), el = eloc(e), M = S.m[s];
+        const Real* cf = mocs(s) + (size_t)f * MS();
+        const Real* cfi = mocs_im(s) + (size_t)f * MS();
+        const Real* iv = inv(s) + (size_t)el * MS();
+        const Real* ivi = iv + (size_t)MS() * MS();
+        Real ar = Real(0), ai = Real(0);
+        for (int m = 0; m < M; m++) {
+          ar += cf[m] * iv[m] - cfi[m] * ivi[m];
+          ai += cf[m] * ivi[m] + cfi[m] * iv[m];
+        }
+        w[le * S.nbasis + f] = ar;
+        w[wproj_im_off() + le * S.nbasis + f] = ai;
+      }
+      for (int idx = lane; idx < (e1 - e0) * S.nbasis && !multi() && !CPX; idx += 32) {
         const int le = idx / S.nbasis, f = idx - le * S.nbasis;
         const int e = e0 + le, s = spin(e), el = eloc(e), M = S.m[s];
         const Real* cf = mocs(s) + (size_t)f * MS();
@@ -668,22 +803,36 @@ struct Walker {
         // move relative to the nearest image of the atom, then into the cell
         double nx = Rp[3 * I.e] + qx * I.r - I.dx, ny = Rp[3 * I.e + 1] + qy * I.r - I.dy,
                nz = Rp[3 * I.e + 2] + qz * I.r - I.dz;
-        wrap_pos(S, nx, ny, nz);
         const Real* wr = w + (I.e - e0) * S.nbasis;
         Real rd;
-        if (PER == 1 || (PER == 2 && S.periodic)) {
-          rd = basis_dot_lane_periodic(S, nx, ny, nz, wr);
-        } else if (multi()) {
-          // sum over distinct spin-determinants of T[s][u] R_u / W
-          const int s = spin(I.e);
-          Real ru[QWG_MAXUD];
-          basis_dot_lane_multi(S, nx, ny, nz, wr, CH * S.nbasis, S.nud[s], ru);
-          const double* T = mdt() + QWG_MAXDET + 2 + s * QWG_MAXUD;
-          double acc = 0.0;
-          for (int u = 0; u < S.nud[s]; u++) acc += T[u] * double(ru[u]);
-          rd = Real(acc / mdt()[QWG_MAXDET]);
+        if constexpr (CPX) {
+          // the wrap's k-point phase pi k.n: the overall phase (sign for
+          // integer k) of Periodic_sample::translateElectron enters the point
+          // value (Pseudopotential.cpp:727-745): Re(R e^{-i pi k.n}) for complex
+          // orbitals, R cos(pi k.n) for real orbitals at an integer k-point
+          const double kd = wrap_pos_kphase(S, nx, ny, nz);
+          Real pr, pi;
+          basis_dot_lane_cpx(S, nx, ny, nz, wr, wr + wproj_im_off(), pr, pi);
+          double sn, cs;
+          sincos(kd, &sn, &cs);
+          if (S.real_orb) rd = Real(double(pr) * (S.kint ? cs : 1.0));
+          else rd = Real(double(pr) * cs + double(pi) * sn);
         } else {
-          rd = basis_dot_lane(S, nx, ny, nz, wr);
+          wrap_pos(S, nx, ny, nz);
+          if (PER == 1 || (PER == 2 && S.periodic)) {
+            rd = basis_dot_lane_periodic(S, nx, ny, nz, wr);
+          } else if (multi()) {
+            // sum over distinct spin-determinants of T[s][u] R_u / W
+            const int s = spin(I.e);
+            Real ru[QWG_MAXUD];
+            basis_dot_lane_multi(S, nx, ny, nz, wr, CH * S.nbasis, S.nud[s], ru);
+            const double* T = mdt() + QWG_MAXDET + 2 + s * QWG_MAXUD;
+            double acc = 0.0;
+            for (int u = 0; u < S.nud[s]; u++) acc += T[u] * double(ru[u]);
+            rd = Real(acc / mdt()[QWG_MAXDET]);
+          } else {
+            rd = basis_dot_lane(S, nx, ny, nz, wr);
+          }
         }
         const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);
         double ratio = double(rd * exp(u - Real(Ue()[I.e]))) * S.pp_w[ty][q];
@@ -830,7 +979,8 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
   __syncthreads();
 
   const int wid = blockIdx.x * wpc + warp;
-  constexpr bool HBM = MMAX == 0;  // walker worked on in place in HBM
+  constexpr bool HBM = MMAX <= 0;  // walker worked on in place in HBM
+  constexpr bool CPXK = MMAX < 0;  // complex orbitals
   if (wid < P.nwalk) {
     unsigned char* gstate = P.state + (size_t)wid * L.state_bytes;
     constexpr bool SWEEP_ONLY = mode == KM_SWEEP || mode == KM_TMOVE;  // move-phase shared memory only
@@ -897,7 +1047,8 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
           io.sign[wid] = sgn;
         } else {
           io.logpsi[wid] = w->logdet[0] + w->logdet[1] + w->U;
-          io.sign[wid] = w->sign[0] * w->sign[1];
+          // complex orbitals: arg psi; real orbitals on the complex kernels: the sign
+          io.sign[wid] = !CPXK ? w->sign[0] * w->sign[1] : S.real_orb ? (cos(w->phase) < 0 ? -1.0 : 1.0) : w->phase;
         }
         io.kinetic[wid] = kin;
         io.potential[wid] = pot;
@@ -912,7 +1063,8 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       W.propose(e, mx, my, mz, ratioD, dU, g, l);
       if (lane == 0) {
         io.logpsi[wid] = log(fabs(ratioD)) + dU;
-        io.sign[wid] = ratioD < 0 ? -1.0 : 1.0;
+        // complex orbitals: the phase change; real ones: the sign of the ratio
+        io.sign[wid] = CPXK && !S.real_orb ? atan2(W.cr_im, W.cr_re) : (CPXK ? W.cr_re : ratioD) < 0 ? -1.0 : 1.0;
         io.grad[3 * (size_t)wid] = g[0]; io.grad[3 * (size_t)wid + 1] = g[1]; io.grad[3 * (size_t)wid + 2] = g[2];
         io.lap[wid] = l;
       }
@@ -963,14 +1115,22 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
             double ny = oy + ga[1] * sqt + dv[1];
             double nz = oz + ga[2] * sqt + dv[2];
             double wx = nx, wy = ny, wz = nz;  // the stored position is inside the cell
-            wrap_pos(S, wx, wy, wz);
+            double node = 1.0;  // sign of the continuous ratio across the wrap (complex kernels)
+            if constexpr (CPXK) {
+              const double kd = wrap_pos_kphase(S, wx, wy, wz);
+              if (S.kint) node = cos(kd);  // overall sign of Periodic_sample::translateElectron
+            } else {
+              wrap_pos(S, wx, wy, wz);
+            }
             double ratioD, dU, g1[3], l1;
             W.propose(e, wx, wy, wz, ratioD, dU, g1, l1);
+            if constexpr (CPXK)
+              if (S.real_orb && W.cr_re < 0) node = -node;
             // get_acceptance (Split_sample.cpp:302-373): psi ratio squared
             // times the ratio of drift-diffusion Green's functions
             double ratio = ratioD * exp(dU);
             double acc;
-            if (P.dmc && ratio < 0) acc = 0;  // node restriction
+            if (P.dmc && (ratio < 0 || node < 0)) acc = 0;  // node restriction
             else {
               double bd[3];
               lim_drift(g1, P.tau, bd);

@@ -10,7 +10,9 @@
 namespace qwg {
 
 // Launches k_walkers<Real, MM, mode, has_tb> over nwalk walkers: wpc warps
-// (walkers) per CTA, smem bytes of dynamic shared memory.
+// (walkers) per CTA, smem bytes of dynamic shared memory.  MM: 8/16/32
+// shared-memory walkers, 0 HBM-resident walkers, -1 HBM-resident walkers with
+// complex orbitals.
 template <typename Real, int MM>
 cudaError_t launch_walker_kernels(const DevSys<Real>& S, const WLayout& L, const StepParams& P, const EvalIO& io,
                                   int mode, int nwalk, int wpc, size_t smem, cudaStream_t stream);
@@ -26,6 +28,8 @@ QWG_WALKER_FAMILY(float, 8)
 QWG_WALKER_FAMILY(float, 16)
 QWG_WALKER_FAMILY(float, 32)
 QWG_WALKER_FAMILY(float, 0)
+QWG_WALKER_FAMILY(double, -1)
+QWG_WALKER_FAMILY(float, -1)
 #undef QWG_WALKER_FAMILY
 
 }  // namespace qwg

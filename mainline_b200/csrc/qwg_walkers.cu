@@ -7,7 +7,7 @@
 #include "qwg_launch.cuh"
 
 #if !defined(QWG_REAL) || !defined(QWG_MM)
-#error "qwg_walkers.cu is compiled with -DQWG_REAL=<double|float> -DQWG_MM=<8|16|32|0>"
+#error "qwg_walkers.cu is compiled with -DQWG_REAL=<double|float> -DQWG_MM=<8|16|32|0|-1>"
 #endif
 
 namespace qwg {

@@ -45,7 +45,8 @@ class Info(C.Structure):
     _fields_ = [("nelec", C.c_int), ("nup", C.c_int), ("ndown", C.c_int), ("natoms", C.c_int),
                 ("nbasis", C.c_int), ("nshell", C.c_int), ("nmo_up", C.c_int), ("nmo_down", C.c_int),
                 ("has_pseudo", C.c_int), ("max_walkers", C.c_int), ("precision", C.c_int),
-                ("walkers_per_cta", C.c_int), ("ion_ion", C.c_double), ("device_bytes", C.c_ulonglong)]
+                ("walkers_per_cta", C.c_int), ("ion_ion", C.c_double), ("device_bytes", C.c_ulonglong),
+                ("complex_orbitals", C.c_int)]
 
 
 class EvalOut(C.Structure):

@@ -84,7 +84,9 @@ def _random_orthonormal(rng, nb: int, nmo: int) -> np.ndarray:
 def _write_orb(path: str, coeff: np.ndarray, nfunc_per_center: list[int]) -> None:
     """ORB file: ``mo basis center label`` lines (1-based), COEFFICIENTS, then
     the coefficient list (format read by readorb_noexpand, MO_matrix.h:264-332).
-    ``coeff`` is [totbasis, nmo] with basis functions ordered center by center."""
+    ``coeff`` is [totbasis, nmo] with basis functions ordered center by center;
+    complex coefficients are written as ``(re,im)`` (the stream format of a
+    complex number, read by the CORBITALS path)."""
     nb, nmo = coeff.shape
     lines = []
     vals = []
@@ -100,8 +102,12 @@ def _write_orb(path: str, coeff: np.ndarray, nfunc_per_center: list[int]) -> Non
     with open(path, "w") as fh:
         fh.write("\n".join(lines))
         fh.write("\nCOEFFICIENTS\n")
-        for i in range(0, len(vals), 4):
-            fh.write(" ".join(repr(float(v)) for v in vals[i:i + 4]) + "\n")
+        if np.iscomplexobj(coeff):
+            for i in range(0, len(vals), 4):
+                fh.write(" ".join(f"({float(v.real)!r},{float(v.imag)!r})" for v in vals[i:i + 4]) + "\n")
+        else:
+            for i in range(0, len(vals), 4):
+                fh.write(" ".join(repr(float(v)) for v in vals[i:i + 4]) + "\n")
 
 
 def _jastrow_text(label: str, onebody: np.ndarray, threebody=None, twobody_pp=None) -> str:
@@ -224,7 +230,8 @@ DIAMOND_FRAC = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
 
 
 def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff: float = 16.0,
-                   name: str = "diamond8", method: str | None = None, supercell=(1, 1, 1)) -> Deck:
+                   name: str = "diamond8", method: str | None = None, supercell=(1, 1, 1), kpoint=None,
+                   complex_orbitals: bool = False) -> Deck:
     """Simple-cubic 8-atom diamond-like cell (lattice constant ``a`` bohr) of
     Z_eff=4 pseudo-atoms, 32 electrons (16 up, 16 down).  Per atom 13 periodic
     Gaussians (4 S + 3 P shells, 3 primitives, exponents log-uniform in
@@ -235,7 +242,13 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
     terms, all cut off inside half the cell (3.3 bohr) so the minimum-image
     Jastrow is smooth.  ``supercell`` = (n1, n2, n3) repeats the cell along
     the three axes (16 up + 16 down electrons per repeat), e.g. (2, 2, 2) is
-    the 64-atom, 512-electron cell with a = 13.48 bohr."""
+    the 64-atom, 512-electron cell with a = 13.48 bohr.
+
+    ``kpoint`` = (k1, k2, k3) writes KPOINT (twisted boundary conditions: a
+    translation by lattice vector i multiplies the orbitals by exp(i pi k_i));
+    ``complex_orbitals`` writes CORBITALS with random complex orthonormal
+    coefficients (the imaginary parts are drawn after everything else, so the
+    real parts, geometry and Jastrow equal those of the real deck)."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     ncell = int(np.prod(supercell))
@@ -253,8 +266,17 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
     onebody = rng.normal(0.0, 0.1, size=4)
     threebody = rng.normal(0.0, 0.05, size=8)
     pp = _pseudo_text(rng, label, charge)
+    coeff = np.concatenate([cup, cdn], axis=1)
+    if complex_orbitals:
+        # complex orthonormal columns per spin: QR of (real part + i * fresh normals)
+        im = rng.standard_normal(coeff.shape)
+        parts = []
+        for c0, c1 in ((0, nup), (nup, nup + ndown)):
+            q, r = np.linalg.qr(coeff[:, c0:c1] + 1j * im[:, c0:c1])
+            parts.append(q * (np.diag(r) / np.abs(np.diag(r))).conj()[None, :])
+        coeff = np.concatenate(parts, axis=1)
     orb = os.path.join(outdir, f"{name}.orb")
-    _write_orb(orb, np.concatenate([cup, cdn], axis=1), [nper] * natoms)
+    _write_orb(orb, coeff, [nper] * natoms)
     pos = np.concatenate([(DIAMOND_FRAC + np.array([i, j, k])) * a for i in range(supercell[0])
                           for j in range(supercell[1]) for k in range(supercell[2])])
     edge = [a * n for n in supercell]
@@ -291,12 +313,13 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
         "  ORIGIN { 0 0 0 }",
         f"  CUTOFF_DIVIDER {_fmt(min(edge) / image_cutoff)}",
         "  EWALD_GMAX 8",
-    ] + [f"  ATOM {{ {label} {charge} COOR {_fmt(p[0])} {_fmt(p[1])} {_fmt(p[2])} }}" for p in pos] + [
+    ] + ([f"  KPOINT {{ {_fmt(kpoint[0])} {_fmt(kpoint[1])} {_fmt(kpoint[2])} }}"] if kpoint is not None else []) + [
+        f"  ATOM {{ {label} {charge} COOR {_fmt(p[0])} {_fmt(p[1])} {_fmt(p[2])} }}" for p in pos] + [
         "}",
         pp,
         "TRIALFUNC { SLATER-JASTROW",
         "  WF1 { SLATER",
-        "    ORBITALS { BLAS_MO",
+        "    CORBITALS { BLAS_MO" if complex_orbitals else "    ORBITALS { BLAS_MO",
         f"      NMO {nup + ndown}",
         f"      ORBFILE {os.path.basename(orb)}",
         _basis_text(label, shells, cutoff=16.0),

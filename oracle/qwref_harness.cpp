@@ -22,8 +22,12 @@
 //   nconf x { f64 logpsi; f64 sign; f64 grad[nelec][3]; f64 lap[nelec];
 //             f64 kinetic; f64 potential; f64 nonlocal;
 //             nmove x { f64 dlogpsi; f64 signratio; f64 grad[3]; f64 lap } }
-// where grad/lap are amp(0,1..3) and amp(0,4) of Slat_Jastrow::getLap
-// (wavefunction/Slat_Jastrow.cpp:235-312), kinetic/potential/nonlocal are
+// where grad/lap are amp(0,1..3) and amp(0,4) - |phase(0,1..3)|^2 of
+// Slat_Jastrow::getLap (wavefunction/Slat_Jastrow.cpp:313-357), i.e. the
+// real parts of grad psi/psi and lap psi/psi (the phase terms vanish for real
+// orbitals).  For complex orbitals (CORBITALS) "sign" is the phase of psi
+// (phase(0,0), Wf_return.cpp:129-152) and "signratio" the phase difference
+// of the move.  kinetic/potential/nonlocal are
 // System::calcKinetic, System::calcLoc and the deterministic
 // Pseudopotential::calcNonlocWithTest (system/Pseudopotential.cpp:412-424).
 
@@ -108,13 +112,15 @@ int main(int argc, char** argv) {
     wf->getVal(wfdata, 0, val);
     out.clear();
     out.push_back(val.amp(0, 0));
-    out.push_back(val.sign(0));
+    out.push_back(val.is_complex ? val.phase(0, 0) : double(val.sign(0)));
     vector<double> lapv(nelec);
     for (int e = 0; e < nelec; e++) {
       Wf_return lap(nwf, 5);
       wf->getLap(wfdata, e, lap);
       for (int d = 1; d < 4; d++) out.push_back(lap.amp(0, d));
       lapv[e] = lap.amp(0, 4);
+      if (lap.is_complex)
+        for (int d = 1; d < 4; d++) lapv[e] -= lap.phase(0, d) * lap.phase(0, d);
     }
     out.insert(out.end(), lapv.begin(), lapv.end());
     Array1<doublevar> kin(nwf), nonloc(nwf);
@@ -148,8 +154,12 @@ int main(int argc, char** argv) {
       Wf_return lap(nwf, 5);
       wf->getLap(wfdata, e, lap);
       out.push_back(v1.amp(0, 0) - v0.amp(0, 0));
-      out.push_back(double(v1.sign(0) * v0.sign(0)));
-      for (int d = 1; d < 5; d++) out.push_back(lap.amp(0, d));
+      out.push_back(v1.is_complex ? v1.phase(0, 0) - v0.phase(0, 0) : double(v1.sign(0) * v0.sign(0)));
+      for (int d = 1; d < 4; d++) out.push_back(lap.amp(0, d));
+      double l4 = lap.amp(0, 4);
+      if (lap.is_complex)
+        for (int d = 1; d < 4; d++) l4 -= lap.phase(0, d) * lap.phase(0, d);
+      out.push_back(l4);
     }
     wr(fout, out.data(), out.size());
   }

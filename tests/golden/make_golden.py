@@ -36,13 +36,18 @@ WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseu
                  (0.12, [1, 2, 3, 4, 5, 6, 8], [1, 2, 3, 4, 5, 6, 8]),
                  (0.08, [1, 2, 3, 4, 5, 7, 9], [1, 2, 3, 4, 5, 6, 7]),
                  (0.08, [1, 2, 3, 4, 5, 6, 7], [1, 2, 3, 4, 5, 7, 9]),
-                 (-0.05, [1, 2, 3, 4, 6, 8, 9], [2, 3, 4, 5, 6, 7, 8])]), 17)]
+                 (-0.05, [1, 2, 3, 4, 6, 8, 9], [2, 3, 4, 5, 6, 7, 8])]), 17),
+             # twisted boundary conditions: complex orbitals at a general k-point,
+             # and real orbitals at an integer (antiperiodic) k-point
+             ("diamond8_k", dict(periodic=True, kpoint=(0.5, 0.25, 0.0), complex_orbitals=True), 18),
+             ("diamond8_l", dict(periodic=True, kpoint=(1.0, 1.0, 1.0)), 19)]
 
 
 def make(name, kw, seed):
     if kw.get("periodic"):
         sc = kw.get("supercell", (1, 1, 1))
-        deck = systems.write_periodic(HERE, seed=seed, name=name, supercell=sc)
+        deck = systems.write_periodic(HERE, seed=seed, name=name, supercell=sc, kpoint=kw.get("kpoint"),
+                                      complex_orbitals=kw.get("complex_orbitals", False))
         nconf = 64 if sc == (1, 1, 1) else 16
     elif "nelec" in kw:  # molecules of the batched-uneven workload (odd count; above 32 per spin)
         deck = systems.write_molecule(HERE, name, seed, kw["nelec"])

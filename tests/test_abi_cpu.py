@@ -69,11 +69,12 @@ def test_bad_deck_reports_error(lib, tmp_path):
 
 @pytest.mark.parametrize("edit,msg", [
     (lambda t: t.replace("DETWT { 1.0 }", "DETWT { 0.9 0.1 }"), "every determinant"),
-    (lambda t: t.replace("ORBITALS { BLAS_MO", "CORBITALS { BLAS_MO"), "complex orbitals"),
+    (lambda t: t.replace("ORBITALS { BLAS_MO", "CORBITALS { BLAS_MO").replace("DETWT { 1.0 }", "DETWT { 0.9 0.1 }"),
+     "real orbitals at the Gamma point"),
 ])
 def test_unsupported_wavefunctions_are_rejected(lib, tmp_path, edit, msg):
-    """Malformed determinant expansions and complex orbitals (outside this
-    engine) are rejected with a clear message, not run wrongly."""
+    """Malformed determinant expansions and expansions of complex orbitals
+    (outside this engine) are rejected with a clear message, not run wrongly."""
     import shutil
     src = os.path.join(GOLDEN, "n2_pseudo.qw")
     shutil.copy(os.path.join(GOLDEN, "n2_pseudo.orb"), tmp_path)
@@ -83,3 +84,18 @@ def test_unsupported_wavefunctions_are_rejected(lib, tmp_path, edit, msg):
     p.write_text(edit(text))
     with pytest.raises(engine.QwgError, match=msg):
         engine.inspect_deck(str(p))
+
+
+def test_complex_orbitals_are_recognised(lib, tmp_path):
+    """CORBITALS (complex coefficients, "(re,im)" or plain reals) and a nonzero
+    KPOINT select the complex-orbital kernels."""
+    import shutil
+    src = os.path.join(GOLDEN, "n2_pseudo.qw")
+    shutil.copy(os.path.join(GOLDEN, "n2_pseudo.orb"), tmp_path)
+    p = tmp_path / "c.qw"
+    p.write_text(open(src).read().replace("ORBITALS { BLAS_MO", "CORBITALS { BLAS_MO"))
+    assert engine.inspect_deck(str(p)).complex_orbitals == 1
+    assert engine.inspect_deck(src).complex_orbitals == 0
+    assert engine.inspect_deck(os.path.join(GOLDEN, "diamond8_k.qw")).complex_orbitals == 1
+    assert engine.inspect_deck(os.path.join(GOLDEN, "diamond8_l.qw")).complex_orbitals == 1
+    assert engine.inspect_deck(os.path.join(GOLDEN, "diamond8.qw")).complex_orbitals == 0
