@@ -381,6 +381,12 @@ class System:
             pos.append([float(a[i + 1]), float(a[i + 2]), float(a[i + 3])])
         self.atoms = np.array(pos)
         self.charges = np.array(self.charges)
+        # KPOINT (units of pi per lattice vector; Periodic_system.cpp:106-413)
+        kp = section(sysw, "KPOINT")
+        self.kpt = np.array([float(x) for x in kp[:3]]) if kp else np.zeros(3)
+        # all k components integer: the overall sign of a wrap is tracked
+        # (Periodic_sample.cpp:201-209)
+        self.kint = bool(np.all(self.kpt == np.floor(self.kpt)))
         if self.periodic:
             self._read_cell(sysw)
         tf = section(words, "TRIALFUNC")
@@ -393,7 +399,9 @@ class System:
     # Slater determinant (wavefunction/Slat_wf_data.cpp:34-303, MO_matrix.h:383-462,
     # MO_matrix_blas.h:101-190)
     def _read_slater(self, w, base):
-        orbw = section(w, "ORBITALS")
+        # CORBITALS: complex orbitals, Slat_wf<dcomplex> (Slat_wf_data.cpp:130-147)
+        self.cplx = bool(section(w, "CORBITALS"))
+        orbw = section(w, "CORBITALS") if self.cplx else section(w, "ORBITALS")
         self.mo_kind = orbw[0].upper()
         self.nmo = int(value(orbw, "NMO", conv=int))
         self.basis = [SplineBasis(b) for b in sections(orbw, "BASIS")]
@@ -404,6 +412,14 @@ class System:
             self.center_basis.append([b for b in self.basis if b.label == lab])
         if not self.periodic:
             self.images = [self.atoms[a:a + 1] for a in range(len(self.atoms))]
+            self.image_shifts = [np.zeros((1, 3)) for _ in range(len(self.atoms))]
+        # k-point factor of every image center (eval_kpoint_fac, MO_matrix.h:333-342;
+        # MO_matrix_blas.h:179-188): e^{i pi k.n} for complex orbitals, cos(pi k.n)
+        # for real ones, n the image's lattice translation
+        self.kfac = []
+        for sh in self.image_shifts:
+            dot = np.asarray(sh, dtype=float) @ self.kpt
+            self.kfac.append(np.exp(1j * math.pi * dot) if self.cplx else np.cos(math.pi * dot))
         self.nfunc_center = [sum(b.nfunc for b in bl) for bl in self.center_basis]
         self.totbasis = sum(self.nfunc_center)
         orbfile = value(orbw, "ORBFILE", conv=str)
@@ -417,14 +433,23 @@ class System:
         toks = open(path).read().split()
         k = toks.index("COEFFICIENTS")
         ent = np.array(toks[:k], dtype=np.int64).reshape(-1, 4) - 1
-        coef = np.array(toks[k + 1:], dtype=float)
+        if self.cplx:
+            # "(re,im)" (or a plain real), the stream format of a complex number
+            def cnum(t):
+                if t.startswith("("):
+                    parts = t.strip("()").split(",")
+                    return complex(float(parts[0]), float(parts[1]) if len(parts) > 1 else 0.0)
+                return complex(float(t), 0.0)
+            coef = np.array([cnum(t) for t in toks[k + 1:]])
+        else:
+            coef = np.array(toks[k + 1:], dtype=float)
         maxbasis = max(self.nfunc_center)
         cm = -np.ones((self.nmo, len(self.labels), maxbasis), dtype=np.int64)
         for mo, b, c, lab in ent:
             if mo <= self.nmo:
                 if mo < self.nmo:
                     cm[mo, c, b] = lab
-        moc = np.zeros((self.totbasis, self.nmo))
+        moc = np.zeros((self.totbasis, self.nmo), dtype=complex if self.cplx else float)
         row = 0
         for c, nf in enumerate(self.nfunc_center):
             for f in range(nf):
@@ -516,21 +541,24 @@ class System:
         for c, bl in enumerate(self.center_basis):
             for b in bl:
                 v = 0.0
-                for img in self.images[c]:
+                for img, kf in zip(self.images[c], self.kfac[c]):
                     d = P - img
-                    v = v + b.eval_lap(d)
-                keep = np.abs(v[..., 0]) > 1e-8
+                    v = v + kf * b.eval_lap(d)
+                keep = np.abs(v[..., 0]) > 1e-8          # modulus for complex sums
                 vals.append(np.where(keep[..., None], v, 0.0))
         B = np.concatenate(vals, axis=-2)          # [..., totbasis, 5]
         return np.einsum("...bk,bm->...mk", B, self.moc)
 
     def slater(self, R):
         """log|D|, sign, grad ratios [nc,N,3], lap ratios [nc,N] from the
-        transpose-inverse convention of Slat_wf::calcLap/getDetLap."""
+        transpose-inverse convention of Slat_wf::calcLap/getDetLap.  Complex
+        orbitals: sign is the unit phase factor of D, and the grad / lap ratios
+        are the real parts that enter the drift and -1/2 Re(lap psi / psi)
+        (Wf_return.cpp:129-152, System.cpp:105-140)."""
         nc = R.shape[0]
         mo = self.mo_lap(R)                           # [nc, N, nmo, 5]
         logd = np.zeros(nc)
-        sign = np.ones(nc)
+        sign = np.ones(nc, dtype=mo.dtype)
         g = np.zeros((nc, self.nelec, 3))
         l = np.zeros((nc, self.nelec))
         inv_all = []
@@ -546,7 +574,7 @@ class System:
             sign *= sgn
             Ainv = np.linalg.inv(A)                  # Ainv[i, e]
             # ratio_k(e) = sum_i dphi_i(r_e) Ainv[i, e]
-            r = np.einsum("ceik,cie->cek", M[..., 1:], Ainv)
+            r = np.einsum("ceik,cie->cek", M[..., 1:], Ainv).real
             g[:, e0:e0 + ns] = r[..., :3]
             l[:, e0:e0 + ns] = r[..., 3]
             inv_all.append(Ainv)
@@ -650,7 +678,7 @@ class System:
         U, gU, lU = self.jastrow(R)
         grad = gD + gU
         lap = lD + lU + np.sum(gU * gU, axis=-1) + 2 * np.sum(gD * gU, axis=-1)
-        out = {"logpsi": logd + U, "sign": sign, "grad": grad, "lap": lap,
+        out = {"logpsi": logd + U, "sign": np.angle(sign) if self.cplx else sign, "grad": grad, "lap": lap,
                "kinetic": -0.5 * lap.sum(axis=1),
                "potential": self.ewald(R) if self.periodic else self.coulomb(R)}
         return out
@@ -701,8 +729,9 @@ class System:
                     Rn = R.copy()
                     # move relative to the nearest image of the atom
                     Rn[:, e] = R[:, e] + q[:, iq] * r[:, e:e + 1] - d[:, e]
+                    kd = self._wrap_kphase(Rn[:, e])
                     lp, sg = self.logpsi(Rn)
-                    ratio = np.exp(lp - lp0) * sg * sg0 * p["w"][iq]
+                    ratio = np.exp(lp - lp0) * self._point_sign(sg, sg0, kd) * p["w"][iq]
                     cosq = np.sum(q[:, iq] * d[:, e], axis=-1) / r[:, e]
                     ts = np.zeros(nc)
                     for l in range(nl - 1):
@@ -735,23 +764,57 @@ class System:
                 for iq in range(len(p["w"])):
                     Rn = R.copy()
                     Rn[:, e] = R[:, e] + q[iq] * r[:, e:e + 1] - d[:, e]
+                    kd = self._wrap_kphase(Rn[:, e])
                     Rn = self.wrap(Rn)
                     lp, sg = self.logpsi(Rn)
-                    ratio = np.exp(lp - lp0) * sg * sg0 * p["w"][iq]
+                    ratio = np.exp(lp - lp0) * self._point_sign(sg, sg0, kd) * p["w"][iq]
                     cosq = np.sum(q[iq] * d[0, e]) / r[0, e]
                     ts = sum((2 * l + 1) * vl[l][0, e] * legendre(cosq, l) for l in range(nl - 1))
                     out.append((e, Rn[0, e].copy(), float(ts * ratio[0])))
         return out
 
+    def _wrap_kphase(self, P):
+        """k-point phase pi k.n of putting positions P [nc, 3] into the cell,
+        n the lattice translations applied (+1 per +L_i; Periodic_system::
+        enforcePbc, Periodic_sample::translateElectron, Periodic_sample.cpp:388-420)."""
+        if not self.periodic:
+            return np.zeros(len(P))
+        out = np.zeros(len(P))
+        for c, p in enumerate(np.asarray(P, dtype=float)):
+            n = np.zeros(3)
+            for i in range(3):
+                while True:
+                    if float(np.dot(self.normvec[i], p - self.origin)) < -1e-12:
+                        p = p + self.lat[i]
+                        n[i] += 1
+                    elif float(np.dot(self.normvec[i], p - self.corners[i])) > 1e-12:
+                        p = p - self.lat[i]
+                        n[i] -= 1
+                    else:
+                        break
+            out[c] = math.pi * float(n @ self.kpt)
+        return out
+
+    def _point_sign(self, sg, sg0, kd):
+        """Sign (phase) factor of a quadrature point (Pseudopotential.cpp:727-745):
+        cos(phase' - phase - pi k.n) for complex orbitals; sign' sign cos(pi k.n)
+        for real ones when every k component is an integer (else sign' sign)."""
+        if self.cplx:
+            return np.real(sg / sg0 * np.exp(-1j * kd))
+        return sg * sg0 * (np.cos(kd) if self.kint else 1.0)
+
     def move_ratio(self, R, e, rnew):
-        """ln|psi(R')| - ln|psi(R)|, sign ratio, grad and lap of electron e at R'."""
+        """ln|psi(R')| - ln|psi(R)|, sign ratio (complex orbitals: the phase
+        change), grad and lap of electron e at R'."""
         R = np.asarray(R, dtype=float)
         lp0, s0 = self.logpsi(R)
         Rn = R.copy()
         Rn[np.arange(len(R)), e] = rnew
         ev = self.evaluate(Rn)
+        _, s1 = self.logpsi(Rn)
         idx = np.arange(len(R))
-        return ev["logpsi"] - lp0, ev["sign"] * s0, ev["grad"][idx, e], ev["lap"][idx, e]
+        sr = np.angle(s1 / s0) if self.cplx else s1 * s0
+        return ev["logpsi"] - lp0, sr, ev["grad"][idx, e], ev["lap"][idx, e]
 
 
 def _erfcm(x):
@@ -867,6 +930,7 @@ def _find_centers(self, divider):
             pc[i] = -pc[i]
     corners = org[None, :] + piped
     images = [[] for _ in range(len(self.atoms))]
+    shifts = [[] for _ in range(len(self.atoms))]
     n = 4
     for ii in range(-n, n + 1):
         for jj in range(-n, n + 1):
@@ -877,7 +941,9 @@ def _find_centers(self, divider):
                                  for i in range(3))
                     if inside and np.linalg.norm(pos - cm) < radius:
                         images[at].append(pos)
+                        shifts[at].append((ii, jj, kk))
     self.images = [np.array(im) for im in images]
+    self.image_shifts = [np.array(sh) for sh in shifts]
 
 
 def _min_image(self, dr):
