@@ -222,6 +222,26 @@ def run_extras(stream, dev, seconds=30.0):
     per["config"] = "8 Z_eff=4 atoms, a=6.74 bohr, 32 electrons, 104 basis fns + images, Ewald, e-e-n Jastrow; " \
                     "16384 walkers, tau=0.005, 10-step blocks"
     out["periodic"] = per
+    # twisted boundary conditions: the same cell with complex orbitals at
+    # k = (0.5, 0.25, 0) on the complex-orbital kernels
+    ccell = systems.write_periodic(tmp, seed=13, name="diamond8k_bench", kpoint=(0.5, 0.25, 0.0),
+                                   complex_orbitals=True)
+    cpx = {}
+    for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
+        E = engine.Engine(ccell.path, prec, max_walkers=16384, stream=stream.cuda_stream)
+        E.set_walkers(Rc)
+        E.vmc_block(5, 0.3, seed=SEED + 1)
+        E.dmc_init(timestep=0.005, nstep=10, seed=SEED + 2)
+        E.dmc_block()
+        st = E.dmc_block()
+        cpx[label] = {"walker_steps_per_s": 16384 * 10 / (st["block_ms"] / 1e3), "block_ms": st["block_ms"],
+                      "energy": st["energy"]}
+        E.close()
+    cpx["mixed_vs_fp64"] = cpx["mixed"]["walker_steps_per_s"] / cpx["fp64"]["walker_steps_per_s"]
+    cpx["vs_gamma_real_mixed"] = cpx["mixed"]["walker_steps_per_s"] / per["mixed"]["walker_steps_per_s"]
+    cpx["config"] = "the periodic cell with complex orbitals (CORBITALS) at k=(0.5,0.25,0); 16384 walkers, " \
+                    "tau=0.005, 10-step blocks"
+    out["periodic_complex"] = cpx
     # batched uneven molecules: 16 systems, 8-192 electrons, 512-4096 walkers
     mols = systems.write_batch(os.path.join(tmp, "batch"), nsys=16, seed=SEED % 1000)
     bat = {}

@@ -235,10 +235,22 @@ static int sym_of(const std::string& s) {
   if (ieq(s, "P")) return SYM_P;
   if (ieq(s, "D") || ieq(s, "6D")) return SYM_6D;
   if (ieq(s, "5D")) return SYM_5D;
-  throw InputError("unsupported AOSPLINE shell symmetry " + s + " (supported: S P 5D 6D)");
+  if (ieq(s, "F") || ieq(s, "10F")) return SYM_10F;
+  if (ieq(s, "7F")) return SYM_7F;
+  if (ieq(s, "7F_crystal")) return SYM_7F_CRYSTAL;
+  if (ieq(s, "G") || ieq(s, "15G")) return SYM_15G;
+  if (ieq(s, "9G")) return SYM_9G;
+  throw InputError("unsupported AOSPLINE shell symmetry " + s +
+                   " (supported: S P 5D 6D 7F 10F 7F_crystal 9G 15G)");
 }
-static int sym_nfunc(int s) { return s == SYM_S ? 1 : s == SYM_P ? 3 : s == SYM_6D ? 6 : 5; }
-static int sym_l(int s) { return s == SYM_S ? 0 : s == SYM_P ? 1 : 2; }
+static int sym_nfunc(int s) {
+  static const int nf[9] = {1, 3, 6, 5, 10, 7, 7, 15, 9};
+  return nf[s];
+}
+static int sym_l(int s) {
+  static const int l[9] = {0, 1, 2, 2, 3, 3, 3, 4, 4};
+  return l[s];
+}
 
 struct BasisObj {
   std::string label;
@@ -283,11 +295,12 @@ static BasisObj read_aospline(const std::vector<std::string>& w, HostSystem& S,
       double norm;
       if (ieq(ntype, "GAMESSNORM")) {
         double fac = std::sqrt(2.0 * ex / M_PI), feg = 4.0 * ex, feg2 = feg * feg;
-        const double nl[3] = {std::sqrt(2.0 * feg * fac), std::sqrt(2.0 * feg2 * fac / 3.0),
-                              std::sqrt(2.0 * feg * feg2 * fac / 15.0)};
+        const double nl[5] = {std::sqrt(2.0 * feg * fac), std::sqrt(2.0 * feg2 * fac / 3.0),
+                              std::sqrt(2.0 * feg * feg2 * fac / 15.0), std::sqrt(2.0 * feg2 * feg2 * fac / 105.0),
+                              std::sqrt(2.0 * feg2 * feg2 * feg * fac / 945.0)};
         norm = nl[sym_l(sym)];
       } else if (ieq(ntype, "CRYSTAL")) {
-        const double nl[3] = {1.0, 1.0 / std::sqrt(3.0), 1.0 / std::sqrt(5.0)};
+        const double nl[5] = {1.0, 1.0 / std::sqrt(3.0), 1.0 / std::sqrt(5.0), 1.0 / std::sqrt(7.0), 1.0 / std::sqrt(9.0)};
         norm = nl[sym_l(sym)];
       } else if (ieq(ntype, "NONE")) {
         norm = 1.0;

@@ -25,7 +25,12 @@ bool has_section(const std::vector<std::string>& w, const std::string& name);
 bool find_value(const std::vector<std::string>& w, const std::string& name, std::string& out);
 bool has_keyword(const std::vector<std::string>& w, const std::string& name);
 
-enum ShellSym { SYM_S = 0, SYM_P = 1, SYM_6D = 2, SYM_5D = 3 };
+// Angular sets of Cubic_spline (basis_function/Cubic_spline_build.cpp:26-140,
+// 660-790): F and G shells in Cartesian (10F, 15G), real-harmonic (7F, 9G) and
+// CRYSTAL (7F_crystal) orders.
+enum ShellSym {
+  SYM_S = 0, SYM_P = 1, SYM_6D = 2, SYM_5D = 3, SYM_10F = 4, SYM_7F = 5, SYM_7F_CRYSTAL = 6, SYM_15G = 7, SYM_9G = 8
+};
 enum RadialKind { RAD_CUTOFF_CUSP = 0, RAD_POLYPADE = 1 };
 
 // One radial spline x Cartesian angular set attached to one center.

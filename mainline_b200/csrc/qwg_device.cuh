@@ -460,7 +460,141 @@ __device__ __forceinline__ void shell_lap_store(int sym, double x, double y, dou
   }
 }
 
-__device__ __forceinline__ int sym_nfunc(int sym) { return sym == 0 ? 1 : sym == 1 ? 3 : sym == 2 ? 6 : 5; }
+__device__ __forceinline__ int sym_nfunc(int sym) {
+  return sym == 0 ? 1 : sym == 1 ? 3 : sym == 2 ? 6 : sym == 3 ? 5 : sym == 4 ? 10 : sym <= 6 ? 7 : sym == 7 ? 15 : 9;
+}
+
+// ---- F and G shells (sym >= 4), compiled into the HBM-resident kernels only
+// (decks with such shells run there).  Function q of the shell maps to one
+// angular polynomial A (Cubic_spline_calc.cpp:106-296 values, 600-1080 with
+// derivatives); its gradient and Laplacian enter put_lap.  Index of A:
+// 0-9 Cartesian F (xxx yyy zzz xxy xxz yyx yyz zzx zzy xyz), 10 Fm3, 11 Fm1,
+// 12 F0, 13 Fp1, 14 Fp2, 15 Fp3mod; 16-30 Cartesian G (xxxx yyyy zzzz xxxy
+// xxxz yyyx yyyz zzzx zzzy xxyy xxzz yyzz xxyz yyxz zzxy); 31-39 G0..G8.
+__device__ __forceinline__ int fg_index(int sym, int q) {
+  // 7F: F0 Fm3 Fp3mod Fp2 Fxyz Fm1 Fp1; 7F_crystal: F0 Fp1 Fm1 Fp2 Fxyz Fp3mod Fm3
+  // (Cubic_spline_build.cpp:702-721), packed 3 bits per function, offset 9
+  constexpr int P7F = 3 | 1 << 3 | 6 << 6 | 5 << 9 | 0 << 12 | 2 << 15 | 4 << 18;
+  constexpr int P7FC = 3 | 4 << 3 | 2 << 6 | 5 << 9 | 0 << 12 | 6 << 15 | 1 << 18;
+  switch (sym) {
+    case 4: return q;
+    case 5: return 9 + ((P7F >> (3 * q)) & 7);
+    case 6: return 9 + ((P7FC >> (3 * q)) & 7);
+    case 7: return 16 + q;
+    default: return 31 + q;
+  }
+}
+
+// value of angular polynomial idx (same expressions as the reference's values)
+template <typename T>
+__device__ __forceinline__ T fg_value(int idx, T x, T y, T z) {
+  const T v1 = x * x, v2 = y * y, v3 = z * z;
+  switch (idx) {
+    case 0: return v1 * x;
+    case 1: return v2 * y;
+    case 2: return v3 * z;
+    case 3: return v1 * y;
+    case 4: return v1 * z;
+    case 5: return v2 * x;
+    case 6: return v2 * z;
+    case 7: return x * v3;
+    case 8: return v3 * y;
+    case 9: return x * y * z;
+    case 10: return y * (T(3) * v1 - v2);
+    case 11: return y * (T(4) * v3 - v1 - v2);
+    case 12: return z * (T(2) * v3 - T(3) * (v1 + v2));
+    case 13: return x * (T(4) * v3 - v1 - v2);
+    case 14: return z * (v1 - v2);
+    case 15: return x * (v1 - T(3) * v2);
+    case 16: return v1 * v1;
+    case 17: return v2 * v2;
+    case 18: return v3 * v3;
+    case 19: return v1 * x * y;
+    case 20: return v1 * x * z;
+    case 21: return v2 * y * x;
+    case 22: return v2 * y * z;
+    case 23: return v3 * z * x;
+    case 24: return v3 * z * y;
+    case 25: return v1 * v2;
+    case 26: return v1 * v3;
+    case 27: return v2 * v3;
+    case 28: return v1 * y * z;
+    case 29: return v2 * x * z;
+    case 30: return v3 * x * y;
+    case 31: { const T v5 = v1 + v2 + v3; return T(35) * v3 * v3 - T(30) * v3 * v5 + T(3) * v5 * v5; }
+    case 32: { const T v5 = v1 + v2 + v3; return x * z * (T(7) * v3 - T(3) * v5); }
+    case 33: { const T v5 = v1 + v2 + v3; return y * z * (T(7) * v3 - T(3) * v5); }
+    case 34: { const T v5 = v1 + v2 + v3; return (v1 - v2) * (T(7) * v3 - v5); }
+    case 35: { const T v5 = v1 + v2 + v3; return x * y * (T(7) * v3 - v5); }
+    case 36: return (v1 - T(3) * v2) * x * z;
+    case 37: return (T(3) * v1 - v2) * y * z;
+    case 38: return (v1 - T(3) * v2) * v1 - (T(3) * v1 - v2) * v2;
+    default: return (v1 - v2) * x * y;
+  }
+}
+
+// value, gradient and Laplacian of angular polynomial idx
+__device__ __forceinline__ void fg_lap(int idx, double x, double y, double z, double& A, double& ax, double& ay,
+                                       double& az, double& lA) {
+  const double v1 = x * x, v2 = y * y, v3 = z * z;
+  A = fg_value<double>(idx, x, y, z);
+  lA = 0.0;  // the real-harmonic F and G polynomials are harmonic
+  switch (idx) {
+    case 0: ax = 3 * v1; ay = 0; az = 0; lA = 6 * x; break;
+    case 1: ax = 0; ay = 3 * v2; az = 0; lA = 6 * y; break;
+    case 2: ax = 0; ay = 0; az = 3 * v3; lA = 6 * z; break;
+    case 3: ax = 2 * x * y; ay = v1; az = 0; lA = 2 * y; break;
+    case 4: ax = 2 * x * z; ay = 0; az = v1; lA = 2 * z; break;
+    case 5: ax = v2; ay = 2 * x * y; az = 0; lA = 2 * x; break;
+    case 6: ax = 0; ay = 2 * y * z; az = v2; lA = 2 * z; break;
+    case 7: ax = v3; ay = 0; az = 2 * x * z; lA = 2 * x; break;
+    case 8: ax = 0; ay = v3; az = 2 * y * z; lA = 2 * y; break;
+    case 9: ax = y * z; ay = x * z; az = x * y; break;
+    case 10: ax = 6 * x * y; ay = 3 * (v1 - v2); az = 0; break;
+    case 11: ax = -2 * x * y; ay = 4 * v3 - v1 - 3 * v2; az = 8 * y * z; break;
+    case 12: ax = -6 * x * z; ay = -6 * y * z; az = 6 * v3 - 3 * (v1 + v2); break;
+    case 13: ax = 4 * v3 - 3 * v1 - v2; ay = -2 * x * y; az = 8 * x * z; break;
+    case 14: ax = 2 * x * z; ay = -2 * y * z; az = v1 - v2; break;
+    case 15: ax = 3 * (v1 - v2); ay = -6 * x * y; az = 0; break;
+    case 16: ax = 4 * v1 * x; ay = 0; az = 0; lA = 12 * v1; break;
+    case 17: ax = 0; ay = 4 * v2 * y; az = 0; lA = 12 * v2; break;
+    case 18: ax = 0; ay = 0; az = 4 * v3 * z; lA = 12 * v3; break;
+    case 19: ax = 3 * v1 * y; ay = v1 * x; az = 0; lA = 6 * x * y; break;
+    case 20: ax = 3 * v1 * z; ay = 0; az = v1 * x; lA = 6 * x * z; break;
+    case 21: ax = v2 * y; ay = 3 * v2 * x; az = 0; lA = 6 * x * y; break;
+    case 22: ax = 0; ay = 3 * v2 * z; az = v2 * y; lA = 6 * y * z; break;
+    case 23: ax = v3 * z; ay = 0; az = 3 * v3 * x; lA = 6 * x * z; break;
+    case 24: ax = 0; ay = v3 * z; az = 3 * v3 * y; lA = 6 * y * z; break;
+    case 25: ax = 2 * x * v2; ay = 2 * v1 * y; az = 0; lA = 2 * (v1 + v2); break;
+    case 26: ax = 2 * x * v3; ay = 0; az = 2 * v1 * z; lA = 2 * (v1 + v3); break;
+    case 27: ax = 0; ay = 2 * y * v3; az = 2 * v2 * z; lA = 2 * (v2 + v3); break;
+    case 28: ax = 2 * x * y * z; ay = v1 * z; az = v1 * y; lA = 2 * y * z; break;
+    case 29: ax = v2 * z; ay = 2 * x * y * z; az = x * v2; lA = 2 * x * z; break;
+    case 30: ax = y * v3; ay = x * v3; az = 2 * x * y * z; lA = 2 * x * y; break;
+    case 31:
+      ax = 12 * (v1 + v2 - 4 * v3) * x; ay = 12 * (v1 + v2 - 4 * v3) * y; az = -48 * (v1 + v2 + v3) * z + 80 * v3 * z;
+      break;
+    case 32: ax = (-9 * v1 - 3 * v2 + 4 * v3) * z; ay = -6 * x * y * z; az = (-3 * v1 - 3 * v2 + 12 * v3) * x; break;
+    case 33: ax = -6 * x * y * z; ay = (-3 * v1 - 9 * v2 + 4 * v3) * z; az = (-3 * v1 - 3 * v2 + 12 * v3) * y; break;
+    case 34: ax = 4 * x * (3 * v3 - v1); ay = -4 * y * (3 * v3 - v2); az = 12 * z * (v1 - v2); break;
+    case 35: ax = y * (6 * v3 - 3 * v1 - v2); ay = x * (6 * v3 - v1 - 3 * v2); az = 12 * x * y * z; break;
+    case 36: ax = 3 * (v1 - v2) * z; ay = -6 * x * y * z; az = (v1 - 3 * v2) * x; break;
+    case 37: ax = 6 * x * y * z; ay = 3 * (v1 - v2) * z; az = (3 * v1 - v2) * y; break;
+    case 38: ax = 4 * x * (v1 - 3 * v2); ay = 4 * y * (v2 - 3 * v1); az = 0; break;
+    default: ax = (3 * v1 - v2) * y; ay = (v1 - 3 * v2) * x; az = 0; break;
+  }
+}
+
+template <typename Real, bool ACC>
+__device__ __forceinline__ void shell_lap_store_fg(int sym, double x, double y, double z, double f, double fd,
+                                                   double f2, Real* b) {
+  const int nf = sym_nfunc(sym), l = sym <= 6 ? 3 : 4;
+  for (int q = 0; q < nf; q++) {
+    double A, ax, ay, az, lA;
+    fg_lap(fg_index(sym, q), x, y, z, A, ax, ay, az, lA);
+    put_lap<Real, ACC>(b + 5 * q, A, ax, ay, az, lA, l, x, y, z, f, fd, f2);
+  }
+}
 
 // MO value, gradient and Laplacian of one position, warp-cooperative.
 // Lanes split the shells (radial spline and angular factors in FP64: the
@@ -469,7 +603,7 @@ __device__ __forceinline__ int sym_nfunc(int sym) { return sym == 0 ? 1 : sym ==
 // contraction with the MO coefficients moc_s [nbasis][mstride].
 // PER: 0 molecule, 1 periodic cell (compiled for that case only), 2 decided
 // at run time from S.periodic.
-template <typename Real, int PER>
+template <typename Real, int PER, bool HL = false>
 __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz, int M,
                             Real* bas, Real* out, int lane) {
   for (int s = lane; s < S.nshell; s += 32) {
@@ -490,7 +624,8 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
         double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
         double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
         double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
-        shell_lap_store<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
+        if (HL && si.y >= 4) shell_lap_store_fg<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
+        else shell_lap_store<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
       } else {
         for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
       }
@@ -514,7 +649,8 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
         double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
         double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
         double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
-        shell_lap_store<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
+        if (HL && si.y >= 4) shell_lap_store_fg<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
+        else shell_lap_store<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
       }
       for (int k = 0; k < nf; k++)
         if (!(fabs(double(b[5 * k])) > 1e-8))
@@ -572,7 +708,7 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
 // coefficients w_f = sum_m C[f][m] (A^-1)[m][e] of that electron,
 //   psi_D(p)/psi_D = sum_m phi_m(p) (A^-1)[m][e] = sum_f b_f(p) w_f,
 // an nbasis-term dot product instead of the nbasis x M MO contraction.
-template <typename Real>
+template <typename Real, bool HL = false>
 __device__ __forceinline__ Real basis_dot_lane(const DevSys<Real>& S, double px, double py, double pz,
                                                const Real* w) {
   Real acc = Real(0);
@@ -611,6 +747,12 @@ __device__ __forceinline__ Real basis_dot_lane(const DevSys<Real>& S, double px,
             add(fb + 3, x * y * f); add(fb + 4, x * z * f); add(fb + 5, y * z * f);
             break;
           default:
+            if constexpr (HL) {
+              if (sym >= 4) {
+                for (int q = 0; q < sym_nfunc(sym); q++) add(fb + q, fg_value<Real>(fg_index(sym, q), x, y, z) * f);
+                break;
+              }
+            }
             add(fb, (Real(2) * z * z - x * x - y * y) * f); add(fb + 1, x * z * f); add(fb + 2, y * z * f);
             add(fb + 3, (x * x - y * y) * f); add(fb + 4, x * y * f);
             break;
@@ -657,9 +799,12 @@ __device__ __forceinline__ void basis_dot_lane_multi(const DevSys<Real>& S, doub
           add(fb, x * x * f); add(fb + 1, y * y * f); add(fb + 2, z * z * f);
           add(fb + 3, x * y * f); add(fb + 4, x * z * f); add(fb + 5, y * z * f);
           break;
-        default:
+        case 3:
           add(fb, (Real(2) * z * z - x * x - y * y) * f); add(fb + 1, x * z * f); add(fb + 2, y * z * f);
           add(fb + 3, (x * x - y * y) * f); add(fb + 4, x * y * f);
+          break;
+        default:
+          for (int q = 0; q < sym_nfunc(sym); q++) add(fb + q, fg_value<Real>(fg_index(sym, q), x, y, z) * f);
           break;
       }
     }
@@ -669,7 +814,7 @@ __device__ __forceinline__ void basis_dot_lane_multi(const DevSys<Real>& S, doub
 // Periodic version of basis_dot_lane: each atom's functions are summed over
 // its image centers before the |value| rule and the dot with w.
 constexpr int QWG_MAXF_ATOM = 16;  // basis functions per atom on the periodic path
-template <typename Real>
+template <typename Real, bool HL = false>
 __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, double px, double py, double pz,
                                                         const Real* w) {
   Real acc = Real(0);
@@ -707,6 +852,13 @@ __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, d
             fs[fo + 3] += x * y * f; fs[fo + 4] += x * z * f; fs[fo + 5] += y * z * f;
             break;
           default:
+            if constexpr (HL) {
+              if (sym >= 4) {
+                for (int q = 0; q < sym_nfunc(sym) && fo + q < QWG_MAXF_ATOM; q++)
+                  fs[fo + q] += fg_value<Real>(fg_index(sym, q), x, y, z) * f;
+                break;
+              }
+            }
             fs[fo] += (Real(2) * z * z - x * x - y * y) * f; fs[fo + 1] += x * z * f; fs[fo + 2] += y * z * f;
             fs[fo + 3] += (x * x - y * y) * f; fs[fo + 4] += x * y * f;
             break;
@@ -765,8 +917,13 @@ __device__ void mo_lap_warp_cpx(const DevSys<Real>& S, const Real* moc_re, const
       double f, fd, f2;
       shell_radial64(S, so, si.w, r, f, fd, f2);
       const double kc = S.image_kfac[2 * m], ks = S.image_kfac[2 * m + 1];
-      shell_lap_store<Real, true>(si.y, dx, dy, dz, f * kc, fd * kc, f2 * kc, br);
-      if (ks != 0.0) shell_lap_store<Real, true>(si.y, dx, dy, dz, f * ks, fd * ks, f2 * ks, bi);
+      if (si.y >= 4) {
+        shell_lap_store_fg<Real, true>(si.y, dx, dy, dz, f * kc, fd * kc, f2 * kc, br);
+        if (ks != 0.0) shell_lap_store_fg<Real, true>(si.y, dx, dy, dz, f * ks, fd * ks, f2 * ks, bi);
+      } else {
+        shell_lap_store<Real, true>(si.y, dx, dy, dz, f * kc, fd * kc, f2 * kc, br);
+        if (ks != 0.0) shell_lap_store<Real, true>(si.y, dx, dy, dz, f * ks, fd * ks, f2 * ks, bi);
+      }
     }
     for (int k = 0; k < nf; k++) {
       const double vr = double(br[5 * k]), vi = double(bi[5 * k]);
@@ -809,6 +966,34 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
     for (int k = 0; k < cs.y; k++) {
       const int pk = S.shell_pack[cs.x + k];
       const int sym = pk & 0xf, fb = (pk >> 4) & 0xffff, kk = (pk >> 20) & 0xff;
+      if (sym >= 4) {
+        // F and G shells: one function at a time over the images
+        for (int q = 0; q < sym_nfunc(sym); q++) {
+          const int idx = fg_index(sym, q);
+          Real gr = Real(0), gi = Real(0);
+          for (int m = im.x; m < im.x + im.y; m++) {
+            const double* cp = S.image_pos + 3 * m;
+            const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
+            const Real rd2 = x * x + y * y + z * z;
+            if (!(rd2 < cut2)) continue;
+            const Real rd = sqrt(rd2);
+            if (!(rd < cut)) continue;
+            const int i = int(rd * Real(S.inv_spacing));
+            const Real h = rd - Real(i) * Real(S.spacing);
+            const Real* cf = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4 + 4 * kk;
+            const Real f = __ldg(cf) + h * (__ldg(cf + 1) + h * (__ldg(cf + 2) + h * __ldg(cf + 3)));
+            const Real a = fg_value<Real>(idx, x, y, z) * f;
+            gr += Real(S.image_kfac[2 * m]) * a;
+            gi += Real(S.image_kfac[2 * m + 1]) * a;
+          }
+          if (sqrt(gr * gr + gi * gi) > Real(1e-8)) {
+            const Real wr = w_re[fb + q], wi = w_im[fb + q];
+            acr += gr * wr - gi * wi;
+            aci += gr * wi + gi * wr;
+          }
+        }
+        continue;
+      }
       Real fr[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
       Real fi[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
       for (int m = im.x; m < im.x + im.y; m++) {

@@ -63,6 +63,12 @@ static bool hbm_family(int mmax) { return mmax <= 0; }
 static bool needs_complex(const HostSystem& H) {
   return H.complex_orbitals || H.kpt[0] != 0.0 || H.kpt[1] != 0.0 || H.kpt[2] != 0.0;
 }
+// F and G shells are evaluated by the HBM-resident kernels only
+static bool has_high_l(const HostSystem& H) {
+  for (const Shell& s : H.shells)
+    if (s.sym >= SYM_10F) return true;
+  return false;
+}
 static int mmax_for(int m) {
   if (m <= 8) return 8;
   if (m <= 16) return 16;
@@ -776,6 +782,7 @@ int qwg_footprint(const char* deck_path, int precision, int max_walkers, unsigne
     c->mmax = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
     if (c->mmax < 0) return QWG_ERR_INPUT;
     if (c->H.detwt.size() > 1) c->mmax = 0;  // expansions run on the HBM-resident kernels
+    if (has_high_l(c->H) && c->mmax > 0) c->mmax = 0;
     if (needs_complex(c->H)) c->mmax = kComplexFamily;
     make_layout(c.get());
     *bytes = footprint_bytes(c.get(), max_walkers);
@@ -818,6 +825,7 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
       if (c->H.periodic) throw InputError("determinant expansions are supported for molecules only");
       mm = 0;  // expansions run on the HBM-resident kernels
     }
+    if (has_high_l(c->H) && mm > 0) mm = 0;         // F / G shells: HBM-resident kernels
     if (needs_complex(c->H)) mm = kComplexFamily;  // complex orbitals / twisted boundary conditions
     c->mmax = mm;
     if (const char* sched = getenv("QWG_DMC_SCHEDULE")) c->split = strcmp(sched, "fused") != 0;

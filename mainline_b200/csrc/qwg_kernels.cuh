@@ -51,6 +51,8 @@ struct Walker {
   const Real* moc_s;     // [2][nbasis][mstride] MO coefficients (global, read through L1)
   int lane;
   static constexpr bool CPX = MMAX < 0;
+  // F and G basis shells: compiled into the HBM-resident kernels only
+  static constexpr bool HL = MMAX <= 0;
   double cr_re = 0.0, cr_im = 0.0;  // complex determinant ratio of the last proposal (CPX)
 
   __device__ __forceinline__ int MS() const {
@@ -184,7 +186,7 @@ struct Walker {
       double* vals = mdv();
       for (int el = 0; el < M; el++) {
         const int e = e0 + el;
-        mo_lap_warp<Real, PER>(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], NU, bas(), nc, lane);
+        mo_lap_warp<Real, PER, HL>(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], NU, bas(), nc, lane);
         for (int j = lane; j < NU; j += 32) {
           vals[(size_t)el * ms + j] = double(nc[j * 5]);
           Real* mv = mov() + ((size_t)e * ms + j) * 4;
@@ -212,7 +214,7 @@ struct Walker {
       const int e0 = s == 0 ? 0 : S.nup;
       for (int el = 0; el < M; el++) {
         const int e = e0 + el;
-        mo_lap_warp<Real, PER>(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], M, bas(), nc, lane);
+        mo_lap_warp<Real, PER, HL>(S, mocs(s), Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2], M, bas(), nc, lane);
         for (int i = lane; i < M; i += 32) {
           aug[el * 2 * M + i] = double(nc[i * 5]);
           Real* mv = mov() + ((size_t)e * MS() + i) * 4;
@@ -309,7 +311,7 @@ struct Walker {
     if (multi()) {
       // ratios of every distinct spin-determinant (kept in mdr for accept),
       // combined with the expansion weights
-      mo_lap_warp<Real, PER>(S, mocs(s), px, py, pz, S.nmo_u[s], bas(), nc, lane);
+      mo_lap_warp<Real, PER, HL>(S, mocs(s), px, py, pz, S.nmo_u[s], bas(), nc, lane);
       double* rr = mdr();
       for (int u = lane; u < S.nud[s]; u += 32) {
         const Real* iv = inv_u(s, u) + (size_t)el * MS();
@@ -354,7 +356,7 @@ struct Walker {
       r1 = (a[1] * a[0] + b[1] * b[0]) / r0; r2 = (a[2] * a[0] + b[2] * b[0]) / r0;
       r3 = (a[3] * a[0] + b[3] * b[0]) / r0; r4 = (a[4] * a[0] + b[4] * b[0]) / r0;
     } else {
-      mo_lap_warp<Real, PER>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
+      mo_lap_warp<Real, PER, HL>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
       const Real* iv = inv(s) + (size_t)el * MS();
       for (int i = 0; i < M; i++) {
         double c = iv[i];
@@ -820,7 +822,7 @@ struct Walker {
         } else {
           wrap_pos(S, nx, ny, nz);
           if (PER == 1 || (PER == 2 && S.periodic)) {
-            rd = basis_dot_lane_periodic(S, nx, ny, nz, wr);
+            rd = basis_dot_lane_periodic<Real, HL>(S, nx, ny, nz, wr);
           } else if (multi()) {
             // sum over distinct spin-determinants of T[s][u] R_u / W
             const int s = spin(I.e);
@@ -831,7 +833,7 @@ struct Walker {
             for (int u = 0; u < S.nud[s]; u++) acc += T[u] * double(ru[u]);
             rd = Real(acc / mdt()[QWG_MAXDET]);
           } else {
-            rd = basis_dot_lane(S, nx, ny, nz, wr);
+            rd = basis_dot_lane<Real, HL>(S, nx, ny, nz, wr);
           }
         }
         const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);

@@ -27,7 +27,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-SHELL_NFUNC = {"S": 1, "P": 3, "5D": 5, "6D": 6, "7F": 7, "10F": 10}
+SHELL_NFUNC = {"S": 1, "P": 3, "5D": 5, "6D": 6, "7F": 7, "10F": 10, "7F_crystal": 7, "9G": 9, "15G": 15}
 
 
 @dataclass
@@ -54,16 +54,18 @@ def _fmt(x: float) -> str:
 
 def _basis_shells(rng, nshell: dict, nprim=3, lo=0.1, hi=1e4):
     shells = []
-    for sym in ("S", "P", "6D"):
-        for _ in range(nshell.get(sym, 0)):
+    for sym in nshell:
+        for _ in range(nshell[sym]):
             ex = np.exp(rng.uniform(np.log(lo), np.log(hi), size=nprim))
             co = rng.uniform(0.1, 1.0, size=nprim)
             shells.append((sym, ex, co))
     return shells
 
 
-def _basis_text(label: str, shells, cutoff=None) -> str:
+def _basis_text(label: str, shells, cutoff=None, normtype=None) -> str:
     lines = [f"BASIS {{ {label}", "AOSPLINE"]
+    if normtype is not None:
+        lines.append(f"NORMTYPE {normtype}")
     if cutoff is not None:
         lines.append(f"CUTOFF {_fmt(cutoff)}")
     lines.append("GAMESS {")
@@ -161,13 +163,15 @@ def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
 
 
 def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | None = None,
-             name: str | None = None, expansion=None) -> Deck:
+             name: str | None = None, expansion=None, high_l: bool = False) -> Deck:
     """Two-atom molecule of the all-electron (``pseudo=False``) or Z_eff=5
     pseudopotential (``pseudo=True``) workload.  ``method`` is an optional
     METHOD section body written into the deck (e.g. ``"VMC NBLOCK 50 ..."``).
     ``expansion``: optional determinant expansion [(weight, up orbitals,
     down orbitals)], orbitals numbered from 1 within each spin (7 occupied
-    plus virtual orbitals up to the largest index used)."""
+    plus virtual orbitals up to the largest index used).  ``high_l``: a
+    basis with F and G shells in every angular order (6 S, 3 P, 5D, 7F, 10F,
+    7F_crystal, 9G, 15G per atom, CRYSTAL normalisation)."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     label = "N"
@@ -176,7 +180,11 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
     # all-electron cores need the tight exponents; pseudopotential atoms use the
     # valence range (with [0.1, 1e4] the random-MO trial function sends the
     # reference's own DMC to E_T < -3e4 Ha within 10 blocks)
-    shells = _basis_shells(rng, {"S": 10, "P": 6, "6D": 2}, hi=10.0 if pseudo else 1e4)
+    if high_l:
+        shells = _basis_shells(rng, {"S": 6, "P": 3, "5D": 1, "7F": 1, "10F": 1, "7F_crystal": 1, "9G": 1, "15G": 1},
+                               hi=10.0 if pseudo else 1e4)
+    else:
+        shells = _basis_shells(rng, {"S": 10, "P": 6, "6D": 2}, hi=10.0 if pseudo else 1e4)
     nper = sum(SHELL_NFUNC[s] for s, _, _ in shells)
     nb = 2 * nper
     nspin_mo = nup if not expansion else max(max(max(u), max(d)) for _, u, d in expansion)
@@ -206,7 +214,7 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
         "    ORBITALS { BLAS_MO",
         f"      NMO {2 * nspin_mo}",
         f"      ORBFILE {os.path.basename(orb)}",
-        _basis_text(label, shells),
+        _basis_text(label, shells, normtype="CRYSTAL" if high_l else None),
         "      CENTERS { USEATOMS }",
         "    }",
         f"    DETWT {{ {detwt} }}",
@@ -231,7 +239,7 @@ DIAMOND_FRAC = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
 
 def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff: float = 16.0,
                    name: str = "diamond8", method: str | None = None, supercell=(1, 1, 1), kpoint=None,
-                   complex_orbitals: bool = False) -> Deck:
+                   complex_orbitals: bool = False, high_l: bool = False) -> Deck:
     """Simple-cubic 8-atom diamond-like cell (lattice constant ``a`` bohr) of
     Z_eff=4 pseudo-atoms, 32 electrons (16 up, 16 down).  Per atom 13 periodic
     Gaussians (4 S + 3 P shells, 3 primitives, exponents log-uniform in
@@ -248,13 +256,15 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
     translation by lattice vector i multiplies the orbitals by exp(i pi k_i));
     ``complex_orbitals`` writes CORBITALS with random complex orthonormal
     coefficients (the imaginary parts are drawn after everything else, so the
-    real parts, geometry and Jastrow equal those of the real deck)."""
+    real parts, geometry and Jastrow equal those of the real deck).
+    ``high_l``: per atom one S, P, 5D and 7F_crystal shell (16 functions,
+    CRYSTAL normalisation) instead of 4 S + 3 P."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     ncell = int(np.prod(supercell))
     label, charge, nup, ndown = "X", 4, 16 * ncell, 16 * ncell
     shells = []
-    for sym, n in (("S", 4), ("P", 3)):
+    for sym, n in ((("S", 1), ("P", 1), ("5D", 1), ("7F_crystal", 1)) if high_l else (("S", 4), ("P", 3))):
         for _ in range(n):
             ex = np.exp(rng.uniform(np.log(0.1), np.log(5.0), size=3))
             shells.append((sym, ex, rng.uniform(0.1, 1.0, size=3)))
@@ -322,7 +332,7 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
         "    CORBITALS { BLAS_MO" if complex_orbitals else "    ORBITALS { BLAS_MO",
         f"      NMO {nup + ndown}",
         f"      ORBFILE {os.path.basename(orb)}",
-        _basis_text(label, shells, cutoff=16.0),
+        _basis_text(label, shells, cutoff=16.0, normtype="CRYSTAL" if high_l else None),
         "      CENTERS { USEGLOBAL }",
         "    }",
         "    DETWT { 1.0 }",

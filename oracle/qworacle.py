@@ -114,8 +114,10 @@ def haskey(words, name):
 # cubic spline radial functions (basis_function/Cubic_spline_build.cpp:396-660,
 # Spline_fitter.cpp:153-293)
 
-LVAL = {"S": 0, "P": 1, "5D": 2, "6D": 2, "D": 2, "7F": 3, "10F": 3, "F": 3}
-NFUNC = {"S": 1, "P": 3, "5D": 5, "6D": 6, "D": 6, "10F": 10, "F": 10}
+LVAL = {"S": 0, "P": 1, "5D": 2, "6D": 2, "D": 2, "7F": 3, "10F": 3, "F": 3, "7F_CRYSTAL": 3,
+        "9G": 4, "15G": 4, "G": 4}
+NFUNC = {"S": 1, "P": 3, "5D": 5, "6D": 6, "D": 6, "10F": 10, "F": 10, "7F": 7, "7F_CRYSTAL": 7,
+         "9G": 9, "15G": 15, "G": 15}
 
 
 def spline_fit(x, y, yp1, ypn):
@@ -187,6 +189,7 @@ class SplineBasis:
         p = 0
         while p < len(g):
             sym = g[p].upper()
+            sym = {"D": "6D", "F": "10F", "G": "15G"}.get(sym, sym)
             ng = int(g[p + 1])
             ex, co = [], []
             for i in range(ng):
@@ -205,9 +208,17 @@ class SplineBasis:
                 feg = 4.0 * e
                 feg2 = feg * feg
                 L = LVAL[sym]
-                norm = [math.sqrt(2.0 * feg * fac), math.sqrt(2.0 * feg2 * fac / 3.0),
-                        math.sqrt(2.0 * feg * feg2 * fac / 15.0),
-                        math.sqrt(2.0 * feg2 * feg2 * fac / 105.0)][L]
+                nt = self.norm_type.upper()
+                if nt == "GAMESSNORM":
+                    norm = [math.sqrt(2.0 * feg * fac), math.sqrt(2.0 * feg2 * fac / 3.0),
+                            math.sqrt(2.0 * feg * feg2 * fac / 15.0),
+                            math.sqrt(2.0 * feg2 * feg2 * fac / 105.0),
+                            math.sqrt(2.0 * feg2 * feg2 * feg * fac / 945.0)][L]
+                elif nt == "CRYSTAL":
+                    norm = 1.0 / math.sqrt(2 * L + 1)
+                else:
+                    assert nt == "NONE", nt
+                    norm = 1.0
                 y += norm * cc * np.exp(-e * x * x)
             if self.renorm:
                 pw = LVAL[sym] + 1
@@ -283,6 +294,53 @@ def _angular(sym, x, y, z):
     if sym == "5D":
         return [(2 * z * z - x * x - y * y, -2 * x, -2 * y, 4 * z, zr, 2), (x * z, z, zr, x, zr, 2),
                 (y * z, zr, z, y, zr, 2), (x * x - y * y, 2 * x, -2 * y, zr, zr, 2), (x * y, y, x, zr, zr, 2)]
+    # F and G shells: polynomials of Cubic_spline_calc.cpp:106-296 in the orders of
+    # Cubic_spline_build.cpp:702-776 (gradients and Laplacians by differentiation)
+    x2, y2, z2 = x * x, y * y, z * z
+    F = {
+        "xxx": (x2 * x, 3 * x2, zr, zr, 6 * x), "yyy": (y2 * y, zr, 3 * y2, zr, 6 * y),
+        "zzz": (z2 * z, zr, zr, 3 * z2, 6 * z), "xxy": (x2 * y, 2 * x * y, x2, zr, 2 * y),
+        "xxz": (x2 * z, 2 * x * z, zr, x2, 2 * z), "yyx": (y2 * x, y2, 2 * x * y, zr, 2 * x),
+        "yyz": (y2 * z, zr, 2 * y * z, y2, 2 * z), "zzx": (z2 * x, z2, zr, 2 * x * z, 2 * x),
+        "zzy": (z2 * y, zr, z2, 2 * y * z, 2 * y), "xyz": (x * y * z, y * z, x * z, x * y, zr),
+        "m3": (y * (3 * x2 - y2), 6 * x * y, 3 * (x2 - y2), zr, zr),
+        "m1": (y * (4 * z2 - x2 - y2), -2 * x * y, 4 * z2 - x2 - 3 * y2, 8 * y * z, zr),
+        "0": (z * (2 * z2 - 3 * (x2 + y2)), -6 * x * z, -6 * y * z, 6 * z2 - 3 * (x2 + y2), zr),
+        "p1": (x * (4 * z2 - x2 - y2), 4 * z2 - 3 * x2 - y2, -2 * x * y, 8 * x * z, zr),
+        "p2": (z * (x2 - y2), 2 * x * z, -2 * y * z, x2 - y2, zr),
+        "p3mod": (x * (x2 - 3 * y2), 3 * (x2 - y2), -6 * x * y, zr, zr),
+    }
+    order = {"10F": ["xxx", "yyy", "zzz", "xxy", "xxz", "yyx", "yyz", "zzx", "zzy", "xyz"],
+             "7F": ["0", "m3", "p3mod", "p2", "xyz", "m1", "p1"],
+             "7F_CRYSTAL": ["0", "p1", "m1", "p2", "xyz", "p3mod", "m3"]}
+    if sym in order:
+        return [F[k] + (3,) for k in order[sym]]
+    if sym == "15G":
+        return [(x2 * x2, 4 * x2 * x, zr, zr, 12 * x2, 4), (y2 * y2, zr, 4 * y2 * y, zr, 12 * y2, 4),
+                (z2 * z2, zr, zr, 4 * z2 * z, 12 * z2, 4), (x2 * x * y, 3 * x2 * y, x2 * x, zr, 6 * x * y, 4),
+                (x2 * x * z, 3 * x2 * z, zr, x2 * x, 6 * x * z, 4), (y2 * y * x, y2 * y, 3 * y2 * x, zr, 6 * x * y, 4),
+                (y2 * y * z, zr, 3 * y2 * z, y2 * y, 6 * y * z, 4), (z2 * z * x, z2 * z, zr, 3 * z2 * x, 6 * x * z, 4),
+                (z2 * z * y, zr, z2 * z, 3 * z2 * y, 6 * y * z, 4),
+                (x2 * y2, 2 * x * y2, 2 * x2 * y, zr, 2 * (x2 + y2), 4),
+                (x2 * z2, 2 * x * z2, zr, 2 * x2 * z, 2 * (x2 + z2), 4),
+                (y2 * z2, zr, 2 * y * z2, 2 * y2 * z, 2 * (y2 + z2), 4),
+                (x2 * y * z, 2 * x * y * z, x2 * z, x2 * y, 2 * y * z, 4),
+                (y2 * x * z, y2 * z, 2 * x * y * z, x * y2, 2 * x * z, 4),
+                (z2 * x * y, y * z2, x * z2, 2 * x * y * z, 2 * x * y, 4)]
+    if sym == "9G":
+        r2 = x2 + y2 + z2
+        return [(35 * z2 * z2 - 30 * z2 * r2 + 3 * r2 * r2, 12 * (x2 + y2 - 4 * z2) * x, 12 * (x2 + y2 - 4 * z2) * y,
+                 -48 * r2 * z + 80 * z2 * z, zr, 4),
+                (x * z * (7 * z2 - 3 * r2), (-9 * x2 - 3 * y2 + 4 * z2) * z, -6 * x * y * z,
+                 (-3 * x2 - 3 * y2 + 12 * z2) * x, zr, 4),
+                (y * z * (7 * z2 - 3 * r2), -6 * x * y * z, (-3 * x2 - 9 * y2 + 4 * z2) * z,
+                 (-3 * x2 - 3 * y2 + 12 * z2) * y, zr, 4),
+                ((x2 - y2) * (7 * z2 - r2), 4 * x * (3 * z2 - x2), -4 * y * (3 * z2 - y2), 12 * z * (x2 - y2), zr, 4),
+                (x * y * (7 * z2 - r2), y * (6 * z2 - 3 * x2 - y2), x * (6 * z2 - x2 - 3 * y2), 12 * x * y * z, zr, 4),
+                ((x2 - 3 * y2) * x * z, 3 * (x2 - y2) * z, -6 * x * y * z, (x2 - 3 * y2) * x, zr, 4),
+                ((3 * x2 - y2) * y * z, 6 * x * y * z, 3 * (x2 - y2) * z, (3 * x2 - y2) * y, zr, 4),
+                ((x2 - 3 * y2) * x2 - (3 * x2 - y2) * y2, 4 * x * (x2 - 3 * y2), 4 * y * (y2 - 3 * x2), zr, zr, 4),
+                ((x2 - y2) * x * y, (3 * x2 - y2) * y, (x2 - 3 * y2) * x, zr, zr, 4)]
     raise NotImplementedError(sym)
 
 

@@ -40,21 +40,25 @@ WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseu
              # twisted boundary conditions: complex orbitals at a general k-point,
              # and real orbitals at an integer (antiperiodic) k-point
              ("diamond8_k", dict(periodic=True, kpoint=(0.5, 0.25, 0.0), complex_orbitals=True), 18),
-             ("diamond8_l", dict(periodic=True, kpoint=(1.0, 1.0, 1.0)), 19)]
+             ("diamond8_l", dict(periodic=True, kpoint=(1.0, 1.0, 1.0)), 19),
+             # F and G shells: every angular order (molecule) and 7F_crystal in a cell
+             ("n2_fg", dict(pseudo=True, high_l=True), 20),
+             ("diamond8_f", dict(periodic=True, high_l=True), 21)]
 
 
 def make(name, kw, seed):
     if kw.get("periodic"):
         sc = kw.get("supercell", (1, 1, 1))
         deck = systems.write_periodic(HERE, seed=seed, name=name, supercell=sc, kpoint=kw.get("kpoint"),
-                                      complex_orbitals=kw.get("complex_orbitals", False))
+                                      complex_orbitals=kw.get("complex_orbitals", False),
+                                      high_l=kw.get("high_l", False))
         nconf = 64 if sc == (1, 1, 1) else 16
     elif "nelec" in kw:  # molecules of the batched-uneven workload (odd count; above 32 per spin)
         deck = systems.write_molecule(HERE, name, seed, kw["nelec"])
         nconf = 64 if kw["nelec"] < 64 else 32
     else:
         deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
-        nconf = NCONF if "expansion" not in kw else 64
+        nconf = NCONF if "expansion" not in kw and "high_l" not in kw else 64
     R = systems.random_configs(deck, nconf, seed=seed + 1000)
     NCONF_ = nconf
     rng = np.random.default_rng(seed + 2000)
