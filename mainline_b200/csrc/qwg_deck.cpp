@@ -729,12 +729,16 @@ HostSystem build_system(const std::string& deck_path) {
 
   // ---- TRIALFUNC
   auto tf = get_section(words, "TRIALFUNC");
-  if (tf.empty() || !ieq(tf[0], "SLATER-JASTROW"))
-    throw InputError("TRIALFUNC must be SLATER-JASTROW");
-  auto wf1 = get_section(tf, "WF1");
-  auto wf2 = get_section(tf, "WF2");
-  if (wf1.empty() || !ieq(wf1[0], "SLATER")) throw InputError("WF1 must be SLATER");
-  if (wf2.empty() || !ieq(wf2[0], "JASTROW2")) throw InputError("WF2 must be JASTROW2");
+  std::vector<std::string> wf1, wf2;
+  if (!tf.empty() && ieq(tf[0], "SLATER")) {
+    wf1 = tf;  // a Slater wave function alone (Slat_wf_data, Wavefunction_data.cpp:32-59): U = 0
+  } else {
+    if (tf.empty() || !ieq(tf[0], "SLATER-JASTROW")) throw InputError("TRIALFUNC must be SLATER-JASTROW or SLATER");
+    wf1 = get_section(tf, "WF1");
+    wf2 = get_section(tf, "WF2");
+    if (wf1.empty() || !ieq(wf1[0], "SLATER")) throw InputError("WF1 must be SLATER");
+    if (wf2.empty() || !ieq(wf2[0], "JASTROW2")) throw InputError("WF2 must be JASTROW2");
+  }
 
   // Slater: one or more determinants (DETWT weights, STATES per determinant)
   auto detwt = get_section(wf1, "DETWT");
@@ -755,6 +759,38 @@ HostSystem build_system(const std::string& deck_path) {
   std::vector<BasisObj> bases;
   for (auto& b : all_sections(orbw, "BASIS")) bases.push_back(read_aospline(b, S, tables));
   if (bases.empty()) throw InputError("Didn't find a BASIS section");
+  {
+    // A label may have several BASIS sections: the reference appends every
+    // one to the label's centers (Center_set::assignBasis, Center_set.cpp:
+    // 140-165).  They become one object (one spline row per interval) with the
+    // splines in section order; the sections must share one cutoff.
+    std::vector<BasisObj> merged;
+    std::vector<std::vector<int>> ids;
+    for (auto& B : bases) {
+      size_t m = 0;
+      while (m < merged.size() && merged[m].label != B.label) m++;
+      if (m == merged.size()) {
+        merged.push_back(B);
+        ids.push_back(B.spline_ids);
+        continue;
+      }
+      if (merged[m].threshold != B.threshold)
+        throw InputError("several BASIS sections for " + B.label + " with different cutoffs are not supported");
+      merged[m].syms.insert(merged[m].syms.end(), B.syms.begin(), B.syms.end());
+      merged[m].nfunc += B.nfunc;
+      ids[m].insert(ids[m].end(), B.spline_ids.begin(), B.spline_ids.end());
+    }
+    std::vector<std::vector<double>> reordered;
+    for (size_t m = 0; m < merged.size(); m++) {
+      merged[m].spline_ids.clear();
+      for (int id : ids[m]) {
+        merged[m].spline_ids.push_back((int)reordered.size());
+        reordered.push_back(std::move(tables[id]));
+      }
+    }
+    tables = std::move(reordered);
+    bases = std::move(merged);
+  }
   size_t cpos = 0;
   std::vector<std::string> cent;
   if (find_section(orbw, "CENTERS", cpos, cent) && !has_keyword(cent, "USEATOMS") && !has_keyword(cent, "USEGLOBAL"))
@@ -842,6 +878,40 @@ HostSystem build_system(const std::string& deck_path) {
     }
   }
   for (int k = 0; k < ndet; k++) S.detwt[k] = to_d(detwt[k]);
+  {
+    // Shells none of whose functions carries an orbital coefficient (e.g. a
+    // BASIS section given twice with an ORB file for one copy) add exactly
+    // zero to every orbital: they are left out of the evaluation.
+    std::vector<Shell> kept;
+    std::vector<int> rows;  // old basis row of every kept function
+    for (const Shell& sh : S.shells) {
+      bool used = false;
+      for (int f = sh.first; f < sh.first + sh.nfunc && !used; f++)
+        for (int s = 0; s < 2 && !used; s++)
+          for (int j = 0; j < S.nmo[s] && !used; j++)
+            used = S.moc[s][(size_t)f * S.nmo[s] + j] != 0.0 || S.moc_im[s][(size_t)f * S.nmo[s] + j] != 0.0;
+      if (!used) continue;
+      Shell k = sh;
+      k.first = (int)rows.size();
+      for (int f = sh.first; f < sh.first + sh.nfunc; f++) rows.push_back(f);
+      kept.push_back(k);
+    }
+    if (kept.size() < S.shells.size() && !kept.empty()) {
+      for (int s = 0; s < 2; s++) {
+        const int nm = S.nmo[s];
+        std::vector<double> re(rows.size() * std::max(nm, 1), 0.0), im(re.size(), 0.0);
+        for (size_t r = 0; r < rows.size(); r++)
+          for (int j = 0; j < nm; j++) {
+            re[r * nm + j] = S.moc[s][(size_t)rows[r] * nm + j];
+            im[r * nm + j] = S.moc_im[s][(size_t)rows[r] * nm + j];
+          }
+        S.moc[s] = std::move(re);
+        S.moc_im[s] = std::move(im);
+      }
+      S.shells = std::move(kept);
+      S.nbasis = (int)rows.size();
+    }
+  }
 
   // ---- Jastrow groups
   S.ei_first.assign(S.natoms, 0);

@@ -782,7 +782,7 @@ int qwg_footprint(const char* deck_path, int precision, int max_walkers, unsigne
     c->mmax = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
     if (c->mmax < 0) return QWG_ERR_INPUT;
     if (c->H.detwt.size() > 1) c->mmax = 0;  // expansions run on the HBM-resident kernels
-    if (has_high_l(c->H) && c->mmax > 0) c->mmax = 0;
+    if ((has_high_l(c->H) || c->H.periodic || c->mmax > 8) && c->mmax > 0) c->mmax = 0;
     if (needs_complex(c->H)) c->mmax = kComplexFamily;
     make_layout(c.get());
     *bytes = footprint_bytes(c.get(), max_walkers);
@@ -826,6 +826,18 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
       mm = 0;  // expansions run on the HBM-resident kernels
     }
     if (has_high_l(c->H) && mm > 0) mm = 0;         // F / G shells: HBM-resident kernels
+    // The shared-memory kernels win only for the smallest molecules (up to 8
+    // orbitals per spin); above that, and for periodic cells at every size, the
+    // HBM-resident kernels keep more walkers resident per SM and run faster
+    // (DMC on B200: 8-atom cell 1.4x mixed / 1.6x FP64, 24-electron molecule
+    // 1.3x / 1.1x, 43-electron molecule 1.3x / 2.0x; 14-electron molecule
+    // 0.64x, so it stays on the shared-memory kernels)
+    if ((c->H.periodic || mm > 8) && mm > 0) mm = 0;
+    if (const char* fam = getenv("QWG_KERNEL_FAMILY")) {  // tuning override: "hbm" or "smem"
+      if (strcmp(fam, "hbm") == 0 && mm > 0) mm = 0;
+      if (strcmp(fam, "smem") == 0 && mm == 0 && !has_high_l(c->H) && c->H.detwt.size() == 1)
+        mm = std::max(mmax_for(std::max(c->H.nmo[0], c->H.nmo[1])), 0);
+    }
     if (needs_complex(c->H)) mm = kComplexFamily;  // complex orbitals / twisted boundary conditions
     c->mmax = mm;
     if (const char* sched = getenv("QWG_DMC_SCHEDULE")) c->split = strcmp(sched, "fused") != 0;

@@ -163,7 +163,8 @@ def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
 
 
 def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | None = None,
-             name: str | None = None, expansion=None, high_l: bool = False) -> Deck:
+             name: str | None = None, expansion=None, high_l: bool = False, jastrow: bool = True,
+             dup_basis: bool = False) -> Deck:
     """Two-atom molecule of the all-electron (``pseudo=False``) or Z_eff=5
     pseudopotential (``pseudo=True``) workload.  ``method`` is an optional
     METHOD section body written into the deck (e.g. ``"VMC NBLOCK 50 ..."``).
@@ -171,7 +172,10 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
     down orbitals)], orbitals numbered from 1 within each spin (7 occupied
     plus virtual orbitals up to the largest index used).  ``high_l``: a
     basis with F and G shells in every angular order (6 S, 3 P, 5D, 7F, 10F,
-    7F_crystal, 9G, 15G per atom, CRYSTAL normalisation)."""
+    7F_crystal, 9G, 15G per atom, CRYSTAL normalisation).  ``jastrow=False``
+    writes a Slater wave function alone (TRIALFUNC { SLATER ... });
+    ``dup_basis`` writes the BASIS section twice (the reference appends both to
+    the atoms: the copies' functions carry no orbital coefficients)."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     label = "N"
@@ -209,20 +213,21 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
         f"  ATOM {{ {label} {charge} COOR 0.0 0.0 1.0375 }}",
         "}",
         pp,
-        "TRIALFUNC { SLATER-JASTROW",
-        "  WF1 { SLATER",
+        "TRIALFUNC { SLATER-JASTROW" if jastrow else "TRIALFUNC { SLATER",
+        "  WF1 { SLATER" if jastrow else "",
         "    ORBITALS { BLAS_MO",
         f"      NMO {2 * nspin_mo}",
         f"      ORBFILE {os.path.basename(orb)}",
         _basis_text(label, shells, normtype="CRYSTAL" if high_l else None),
+        _basis_text(label, shells, normtype="CRYSTAL" if high_l else None) if dup_basis else "",
         "      CENTERS { USEATOMS }",
         "    }",
         f"    DETWT {{ {detwt} }}",
         f"    STATES {{ {states} }}",
-        "  }",
-        "  WF2 {",
-        _jastrow_text(label, onebody),
-        "  }",
+        "  }" if jastrow else "",
+        "  WF2 {" if jastrow else "",
+        _jastrow_text(label, onebody) if jastrow else "",
+        "  }" if jastrow else "",
         "}",
         f"METHOD {{ {method} }}" if method else "",
     ]) + "\n"

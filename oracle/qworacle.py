@@ -448,8 +448,11 @@ class System:
         if self.periodic:
             self._read_cell(sysw)
         tf = section(words, "TRIALFUNC")
-        wf1 = section(tf, "WF1")
-        wf2 = section(tf, "WF2")
+        if tf[0].upper() == "SLATER":        # Slater wave function alone: U = 0
+            wf1, wf2 = tf, ["JASTROW2"]
+        else:
+            wf1 = section(tf, "WF1")
+            wf2 = section(tf, "WF2")
         self._read_slater(wf1, os.path.dirname(os.path.abspath(deck_path)))
         self._read_jastrow(wf2)
         self._read_pseudo(sections(words, "PSEUDO"))

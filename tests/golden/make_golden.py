@@ -43,7 +43,9 @@ WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseu
              ("diamond8_l", dict(periodic=True, kpoint=(1.0, 1.0, 1.0)), 19),
              # F and G shells: every angular order (molecule) and 7F_crystal in a cell
              ("n2_fg", dict(pseudo=True, high_l=True), 20),
-             ("diamond8_f", dict(periodic=True, high_l=True), 21)]
+             ("diamond8_f", dict(periodic=True, high_l=True), 21),
+             # a Slater wave function alone, its BASIS section given twice
+             ("n2_slater", dict(pseudo=True, jastrow=False, dup_basis=True), 22)]
 
 
 def make(name, kw, seed):
@@ -58,7 +60,7 @@ def make(name, kw, seed):
         nconf = 64 if kw["nelec"] < 64 else 32
     else:
         deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
-        nconf = NCONF if "expansion" not in kw and "high_l" not in kw else 64
+        nconf = NCONF if not ({"expansion", "high_l", "jastrow"} & set(kw)) else 64
     R = systems.random_configs(deck, nconf, seed=seed + 1000)
     NCONF_ = nconf
     rng = np.random.default_rng(seed + 2000)

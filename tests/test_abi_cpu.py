@@ -62,8 +62,8 @@ def test_spline_tables_match_oracle(lib):
 
 def test_bad_deck_reports_error(lib, tmp_path):
     p = tmp_path / "bad.qw"
-    p.write_text("SYSTEM { MOLECULE NSPIN { 1 0 } ATOM { H 1 COOR 0 0 0 } }\nTRIALFUNC { SLATER }\n")
-    with pytest.raises(engine.QwgError, match="SLATER-JASTROW"):
+    p.write_text("SYSTEM { MOLECULE NSPIN { 1 0 } ATOM { H 1 COOR 0 0 0 } }\nTRIALFUNC { JASTROW2 }\n")
+    with pytest.raises(engine.QwgError, match="SLATER-JASTROW or SLATER"):
         engine.inspect_deck(str(p))
 
 

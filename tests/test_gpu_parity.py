@@ -15,7 +15,8 @@ from mainline_b200 import engine, systems
 
 pytestmark = pytest.mark.gpu
 
-NAMES = ["n2_allelectron", "n2_pseudo", "diamond8", "mol43", "mol72", "cell32", "n2_multidet", "n2_fg", "diamond8_f"]
+NAMES = ["n2_allelectron", "n2_pseudo", "diamond8", "mol43", "mol72", "cell32", "n2_multidet", "n2_fg", "diamond8_f",
+         "n2_slater"]
 FP64_TOL = 1e-10
 
 
@@ -299,3 +300,23 @@ def test_multideterminant_moves_track_state(tmp_path):
     E2 = engine.Engine(bare, engine.FP64, max_walkers=nw)
     E2.set_walkers(E.get_walkers())
     assert _rel(e_moves, E2.eval().energy) < 1e-8
+
+
+@pytest.mark.parametrize("name", ["diamond8", "mol43"])
+def test_shared_memory_kernels_when_forced(name, monkeypatch):
+    """Periodic cells and molecules above 8 orbitals per spin run the
+    HBM-resident kernels by default; QWG_KERNEL_FAMILY=smem puts them back on
+    the shared-memory kernels (16 and 32 orbitals per spin), which must agree
+    with the reference as well."""
+    monkeypatch.setenv("QWG_KERNEL_FAMILY", "smem")
+    g = dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+    E = engine.Engine(os.path.join(GOLDEN, name + ".qw"), engine.FP64, max_walkers=len(g["R"]))
+    E.set_walkers(g["R"])
+    ev = E.eval(g["rot"])
+    assert np.array_equal(ev.sign, g["sign"])
+    assert _rel(ev.logpsi, g["logpsi"]) < FP64_TOL
+    assert _rel(ev.grad, g["grad"]) < FP64_TOL
+    assert _rel(ev.kinetic, g["kinetic"]) < 1e-9
+    assert _rel(ev.nonlocal_, g["nonlocal"]) < FP64_TOL
+    s = E.vmc_block(2, 0.1, seed=3)
+    assert s["nonfinite"] == 0

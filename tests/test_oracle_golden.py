@@ -9,7 +9,7 @@ from conftest import GOLDEN
 import qworacle
 
 NAMES = ["n2_allelectron", "n2_pseudo", "diamond8", "mol43", "mol72", "cell32", "diamond8_k", "diamond8_l", "n2_fg",
-         "diamond8_f"]
+         "diamond8_f", "n2_slater"]
 
 
 def _rel(a, b):
