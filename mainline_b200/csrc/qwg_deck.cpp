@@ -257,6 +257,7 @@ struct BasisObj {
   std::vector<int> syms;
   std::vector<int> spline_ids;  // into HostSystem::spline table
   double threshold = 0;
+  std::vector<double> cuts;     // per spline (Spline_fitter::findCutoff)
   int nfunc = 0;
 };
 
@@ -337,7 +338,10 @@ static BasisObj read_aospline(const std::vector<std::string>& w, HostSystem& S,
   }
   double thr0 = x[n - 1];
   double thr = 0;
-  for (auto& c : coefs) thr = std::max(thr, spline_cutoff(c.data(), n, spacing, thr0));
+  for (auto& c : coefs) {
+    B.cuts.push_back(spline_cutoff(c.data(), n, spacing, thr0));
+    thr = std::max(thr, B.cuts.back());
+  }
   B.threshold = thr;
   for (auto& c : coefs) {
     if (thr0 < thr) {  // pad with zeros out to the common threshold
@@ -750,8 +754,12 @@ HostSystem build_system(const std::string& deck_path) {
   if (S.complex_orbitals && has_section(wf1, "ORBITALS")) throw InputError("both ORBITALS and CORBITALS given");
   auto orbw = get_section(wf1, S.complex_orbitals ? "CORBITALS" : "ORBITALS");
   if (orbw.empty()) throw InputError("Need ORBITALS or CORBITALS section in SLATER wave function");
-  if (!orbw.empty() && (ieq(orbw[0], "CUTOFF_MO") || ieq(orbw[0], "EINSPLINE_MO") || ieq(orbw[0], "BASFUNC_MO")))
-    throw InputError("ORBITALS type " + orbw[0] + " not supported (the dense BLAS_MO evaluator is used)");
+  if (!orbw.empty() && (ieq(orbw[0], "EINSPLINE_MO") || ieq(orbw[0], "BASFUNC_MO")))
+    throw InputError("ORBITALS type " + orbw[0] + " not supported (BLAS_MO and CUTOFF_MO are)");
+  // CUTOFF_MO (MO_matrix_cutoff, MO_matrix.cpp:33-49): per-function spline
+  // cutoffs, no |value| <= 1e-8 skip of basis values, coefficients with
+  // |c| <= 1e-12 dropped and MAGNIFY applied (MO_matrix_cutoff.h:141-247, 413-569)
+  S.cutoff_mo = !orbw.empty() && ieq(orbw[0], "CUTOFF_MO");
   std::string tmp;
   if (!find_value(orbw, "NMO", tmp)) throw InputError("Need NMO in molecular orbital section");
   int nmo = to_i(tmp);
@@ -777,6 +785,7 @@ HostSystem build_system(const std::string& deck_path) {
       if (merged[m].threshold != B.threshold)
         throw InputError("several BASIS sections for " + B.label + " with different cutoffs are not supported");
       merged[m].syms.insert(merged[m].syms.end(), B.syms.begin(), B.syms.end());
+      merged[m].cuts.insert(merged[m].cuts.end(), B.cuts.begin(), B.cuts.end());
       merged[m].nfunc += B.nfunc;
       ids[m].insert(ids[m].end(), B.spline_ids.begin(), B.spline_ids.end());
     }
@@ -813,6 +822,7 @@ HostSystem build_system(const std::string& deck_path) {
         sh.first = first;
         sh.nfunc = sym_nfunc(B.syms[k]);
         sh.cutoff = B.threshold;
+        sh.fcut = B.cuts[k];
         sh.obj = (int)bi;
         sh.k = (int)k;
         first += sh.nfunc;
@@ -834,6 +844,19 @@ HostSystem build_system(const std::string& deck_path) {
   if (orbfile[0] != '/' && !file_exists(orbfile)) orbfile = base + "/" + orbfile;
   std::vector<double> moc_all, moc_all_im;
   read_orb(orbfile, nmo, nfunc_center, moc_all, S.complex_orbitals ? &moc_all_im : nullptr);
+  if (S.cutoff_mo) {
+    const double mag = value_d(orbw, "MAGNIFY", 1.0);
+    for (size_t i = 0; i < moc_all.size(); i++) {
+      const double im = moc_all_im.empty() ? 0.0 : moc_all_im[i];
+      if (!(std::sqrt(moc_all[i] * moc_all[i] + im * im) > 1e-12)) {
+        moc_all[i] = 0.0;
+        if (!moc_all_im.empty()) moc_all_im[i] = 0.0;
+      } else {
+        moc_all[i] *= mag;
+        if (!moc_all_im.empty()) moc_all_im[i] *= mag;
+      }
+    }
+  }
   const bool kpt_nonzero = S.kpt[0] != 0.0 || S.kpt[1] != 0.0 || S.kpt[2] != 0.0;
   if ((S.complex_orbitals || kpt_nonzero) && detwt.size() > 1)
     throw InputError("determinant expansions need real orbitals at the Gamma point");

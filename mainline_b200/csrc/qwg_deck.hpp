@@ -41,6 +41,7 @@ struct Shell {
   int first;       // first basis function (global index)
   int nfunc;
   double cutoff;   // basis-object threshold: r >= cutoff gives zero
+  double fcut;     // the spline's own cutoff (CUTOFF_MO evaluates a function only inside it)
   int obj;         // basis object (BASIS section) the spline belongs to
   int k;           // spline index inside its basis object
 };
@@ -92,6 +93,7 @@ struct HostSystem {
   // same layout; real orbitals with a nonzero k-point also run on the complex
   // kernels (moc_im zero, real k-point factors)
   bool complex_orbitals = false;
+  bool cutoff_mo = false;            // CUTOFF_MO evaluator (else BLAS_MO)
   std::vector<double> moc_im[2];
   double kpt[3] = {0, 0, 0};         // KPOINT (units of pi / lattice vector)
   // determinant expansion sum_k detwt[k] D_up(det_ud[k][0]) D_down(det_ud[k][1])

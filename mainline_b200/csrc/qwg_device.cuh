@@ -133,6 +133,8 @@ struct DevSys {
   int kint;                      // every k component an integer: the overall sign
                                  // cos(pi k.n) of a wrap enters node checks and PP signs
   int real_orb;                  // orbitals real (ORBITALS at a nonzero k-point)
+  int cutoff_mo;                 // CUTOFF_MO evaluator (HBM-resident kernels): shell_cut holds
+                                 // each spline's own cutoff, no |value| <= 1e-8 skip
   int ng;                        // Ewald G-vectors
   const double* gvec;            // [ng][3]
   const double* gweight;         // [ng]
@@ -624,8 +626,19 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
         double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
         double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
         double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
-        if (HL && si.y >= 4) shell_lap_store_fg<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
-        else shell_lap_store<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
+        if (HL && (si.y >= 4 || S.cutoff_mo)) {
+          // accumulate into zeros: no |value| skip for CUTOFF_MO
+          if (S.cutoff_mo)
+            for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
+          if (si.y >= 4) {
+            if (S.cutoff_mo) shell_lap_store_fg<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
+            else shell_lap_store_fg<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
+          } else {
+            shell_lap_store<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
+          }
+        } else {
+          shell_lap_store<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
+        }
       } else {
         for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
       }
@@ -652,9 +665,10 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
         if (HL && si.y >= 4) shell_lap_store_fg<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
         else shell_lap_store<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
       }
-      for (int k = 0; k < nf; k++)
-        if (!(fabs(double(b[5 * k])) > 1e-8))
-          for (int c = 0; c < 5; c++) b[5 * k + c] = Real(0);
+      if (!(HL && S.cutoff_mo))
+        for (int k = 0; k < nf; k++)
+          if (!(fabs(double(b[5 * k])) > 1e-8))
+            for (int c = 0; c < 5; c++) b[5 * k + c] = Real(0);
     }
   }
   __syncwarp();
@@ -712,7 +726,8 @@ template <typename Real, bool HL = false>
 __device__ __forceinline__ Real basis_dot_lane(const DevSys<Real>& S, double px, double py, double pz,
                                                const Real* w) {
   Real acc = Real(0);
-  auto add = [&](int f, Real v) { acc += (fabs(v) > Real(1e-8) ? v : Real(0)) * w[f]; };
+  const bool cmo = HL && S.cutoff_mo;  // CUTOFF_MO: no |value| skip, per-function cutoffs
+  auto add = [&](int f, Real v) { acc += (cmo || fabs(v) > Real(1e-8) ? v : Real(0)) * w[f]; };
   constexpr int B = sizeof(Real) == 4 ? 6 : 4;  // spline rows loaded per batch
   for (int c = 0; c < S.natoms; c++) {
     const int4 cs = S.center_seg[c];  // first shell, shells, object base, splines per row
@@ -736,6 +751,8 @@ __device__ __forceinline__ Real basis_dot_lane(const DevSys<Real>& S, double px,
 #pragma unroll
       for (int j = 0; j < B; j++) {
         if (k0 + j >= cs.y) break;
+        if constexpr (HL)
+          if (cmo && !(rd < Real(S.shell_cut[cs.x + k0 + j]))) continue;
         const int pk = S.shell_pack[cs.x + k0 + j];
         const int sym = pk & 0xf, fb = (pk >> 4) & 0xffff;
         const Real f = cf[j][0] + h * (cf[j][1] + h * (cf[j][2] + h * cf[j][3]));
@@ -771,8 +788,9 @@ __device__ __forceinline__ void basis_dot_lane_multi(const DevSys<Real>& S, doub
                                                      const Real* w, int wstride, int nu, Real* acc) {
 #pragma unroll
   for (int u = 0; u < QWG_MAXUD; u++) acc[u] = Real(0);
+  const bool cmo = S.cutoff_mo;  // HBM-resident kernels only
   auto add = [&](int f, Real v) {
-    const Real vv = fabs(v) > Real(1e-8) ? v : Real(0);
+    const Real vv = cmo || fabs(v) > Real(1e-8) ? v : Real(0);
 #pragma unroll
     for (int u = 0; u < QWG_MAXUD; u++)
       if (u < nu) acc[u] += vv * w[(size_t)u * wstride + f];
@@ -788,6 +806,7 @@ __device__ __forceinline__ void basis_dot_lane_multi(const DevSys<Real>& S, doub
     const Real h = rd - Real(i) * Real(S.spacing);
     const Real* row = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4;
     for (int k0 = 0; k0 < cs.y; k0++) {
+      if (cmo && !(rd < Real(S.shell_cut[cs.x + k0]))) continue;
       const int pk = S.shell_pack[cs.x + k0];
       const int sym = pk & 0xf, fb = (pk >> 4) & 0xffff, kk = (pk >> 20) & 0xff;
       const Real* cf = row + 4 * kk;
@@ -840,6 +859,8 @@ __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, d
       const Real h = rd - Real(i) * Real(S.spacing);
       const Real* row = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4;
       for (int k = 0; k < cs.y; k++) {
+        if constexpr (HL)
+          if (S.cutoff_mo && !(rd < Real(S.shell_cut[cs.x + k]))) continue;
         const int pk = S.shell_pack[cs.x + k];
         const int sym = pk & 0xf, fo = ((pk >> 4) & 0xffff) - fb0, kk = (pk >> 20) & 0xff;
         const Real* cf = row + 4 * kk;
@@ -865,7 +886,8 @@ __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, d
         }
       }
     }
-    for (int q = 0; q < nfa; q++) acc += (fabs(fs[q]) > Real(1e-8) ? fs[q] : Real(0)) * w[fb0 + q];
+    const bool cmo = HL && S.cutoff_mo;
+    for (int q = 0; q < nfa; q++) acc += (cmo || fabs(fs[q]) > Real(1e-8) ? fs[q] : Real(0)) * w[fb0 + q];
   }
   return acc;
 }
@@ -925,7 +947,7 @@ __device__ void mo_lap_warp_cpx(const DevSys<Real>& S, const Real* moc_re, const
         if (ks != 0.0) shell_lap_store<Real, true>(si.y, dx, dy, dz, f * ks, fd * ks, f2 * ks, bi);
       }
     }
-    for (int k = 0; k < nf; k++) {
+    for (int k = 0; k < nf && !S.cutoff_mo; k++) {
       const double vr = double(br[5 * k]), vi = double(bi[5 * k]);
       if (!(sqrt(vr * vr + vi * vi) > 1e-8))
         for (int c = 0; c < 5; c++) br[5 * k + c] = bi[5 * k + c] = Real(0);
@@ -962,10 +984,13 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
     if (cs.y == 0) continue;
     const int2 im = S.atom_images[c];
     const Real cut = Real(S.center_cut[c]);
-    const Real cut2 = cut * cut * Real(1.000001);
     for (int k = 0; k < cs.y; k++) {
       const int pk = S.shell_pack[cs.x + k];
       const int sym = pk & 0xf, fb = (pk >> 4) & 0xffff, kk = (pk >> 20) & 0xff;
+      // CUTOFF_MO: the shell's own cutoff and no |value| skip
+      const Real scut = S.cutoff_mo ? Real(S.shell_cut[cs.x + k]) : cut;
+      const Real scut2 = scut * scut * Real(1.000001);
+      const Real tiny = S.cutoff_mo ? Real(-1) : Real(1e-8);
       if (sym >= 4) {
         // F and G shells: one function at a time over the images
         for (int q = 0; q < sym_nfunc(sym); q++) {
@@ -975,9 +1000,9 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
             const double* cp = S.image_pos + 3 * m;
             const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
             const Real rd2 = x * x + y * y + z * z;
-            if (!(rd2 < cut2)) continue;
+            if (!(rd2 < scut2)) continue;
             const Real rd = sqrt(rd2);
-            if (!(rd < cut)) continue;
+            if (!(rd < scut)) continue;
             const int i = int(rd * Real(S.inv_spacing));
             const Real h = rd - Real(i) * Real(S.spacing);
             const Real* cf = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4 + 4 * kk;
@@ -986,7 +1011,7 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
             gr += Real(S.image_kfac[2 * m]) * a;
             gi += Real(S.image_kfac[2 * m + 1]) * a;
           }
-          if (sqrt(gr * gr + gi * gi) > Real(1e-8)) {
+          if (sqrt(gr * gr + gi * gi) > tiny) {
             const Real wr = w_re[fb + q], wi = w_im[fb + q];
             acr += gr * wr - gi * wi;
             aci += gr * wi + gi * wr;
@@ -1000,9 +1025,9 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
         const double* cp = S.image_pos + 3 * m;
         const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
         const Real rd2 = x * x + y * y + z * z;
-        if (!(rd2 < cut2)) continue;
+        if (!(rd2 < scut2)) continue;
         const Real rd = sqrt(rd2);
-        if (!(rd < cut)) continue;
+        if (!(rd < scut)) continue;
         const int i = int(rd * Real(S.inv_spacing));
         const Real h = rd - Real(i) * Real(S.spacing);
         const Real* cf = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4 + 4 * kk;
@@ -1029,7 +1054,7 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
       const int n = sym_nfunc(sym);
 #pragma unroll
       for (int q = 0; q < 6; q++)
-        if (q < n && sqrt(fr[q] * fr[q] + fi[q] * fi[q]) > Real(1e-8)) {
+        if (q < n && sqrt(fr[q] * fr[q] + fi[q] * fi[q]) > tiny) {
           const Real wr = w_re[fb + q], wi = w_im[fb + q];
           acr += fr[q] * wr - fi[q] * wi;
           aci += fr[q] * wi + fi[q] * wr;

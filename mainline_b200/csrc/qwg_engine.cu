@@ -63,8 +63,9 @@ static bool hbm_family(int mmax) { return mmax <= 0; }
 static bool needs_complex(const HostSystem& H) {
   return H.complex_orbitals || H.kpt[0] != 0.0 || H.kpt[1] != 0.0 || H.kpt[2] != 0.0;
 }
-// F and G shells are evaluated by the HBM-resident kernels only
+// F and G shells and the CUTOFF_MO evaluator run on the HBM-resident kernels only
 static bool has_high_l(const HostSystem& H) {
+  if (H.cutoff_mo) return true;
   for (const Shell& s : H.shells)
     if (s.sym >= SYM_10F) return true;
   return false;
@@ -168,6 +169,7 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
   for (int d = 0; d < 3; d++)
     if (H.kpt[d] != std::floor(H.kpt[d])) S.kint = 0;
   S.real_orb = H.complex_orbitals ? 0 : 1;
+  S.cutoff_mo = H.cutoff_mo ? 1 : 0;
   S.npts = H.spline_npts;
   S.spacing = H.spline_spacing;
   S.inv_spacing = 1.0 / H.spline_spacing;
@@ -311,7 +313,7 @@ static void build_tables(qwg_ctx* c) {
     const Shell& s = H.shells[k];
     si.push_back(make_int4(s.center, s.sym, s.first, s.k));
     so.push_back(make_int2(obj_base[s.obj], H.obj_count[s.obj]));
-    sc.push_back(s.cutoff);
+    sc.push_back(H.cutoff_mo ? s.fcut : s.cutoff);  // CUTOFF_MO: each function inside its own cutoff
   }
   (void)A;
   upload(c->d_shell_i, si, st);

@@ -164,7 +164,7 @@ def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
 
 def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | None = None,
              name: str | None = None, expansion=None, high_l: bool = False, jastrow: bool = True,
-             dup_basis: bool = False) -> Deck:
+             dup_basis: bool = False, mo_kind: str = "BLAS_MO") -> Deck:
     """Two-atom molecule of the all-electron (``pseudo=False``) or Z_eff=5
     pseudopotential (``pseudo=True``) workload.  ``method`` is an optional
     METHOD section body written into the deck (e.g. ``"VMC NBLOCK 50 ..."``).
@@ -215,7 +215,7 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
         pp,
         "TRIALFUNC { SLATER-JASTROW" if jastrow else "TRIALFUNC { SLATER",
         "  WF1 { SLATER" if jastrow else "",
-        "    ORBITALS { BLAS_MO",
+        f"    ORBITALS {{ {mo_kind}",
         f"      NMO {2 * nspin_mo}",
         f"      ORBFILE {os.path.basename(orb)}",
         _basis_text(label, shells, normtype="CRYSTAL" if high_l else None),
@@ -244,7 +244,7 @@ DIAMOND_FRAC = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
 
 def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff: float = 16.0,
                    name: str = "diamond8", method: str | None = None, supercell=(1, 1, 1), kpoint=None,
-                   complex_orbitals: bool = False, high_l: bool = False) -> Deck:
+                   complex_orbitals: bool = False, high_l: bool = False, mo_kind: str = "BLAS_MO") -> Deck:
     """Simple-cubic 8-atom diamond-like cell (lattice constant ``a`` bohr) of
     Z_eff=4 pseudo-atoms, 32 electrons (16 up, 16 down).  Per atom 13 periodic
     Gaussians (4 S + 3 P shells, 3 primitives, exponents log-uniform in
@@ -334,7 +334,7 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
         pp,
         "TRIALFUNC { SLATER-JASTROW",
         "  WF1 { SLATER",
-        "    CORBITALS { BLAS_MO" if complex_orbitals else "    ORBITALS { BLAS_MO",
+        f"    {'CORBITALS' if complex_orbitals else 'ORBITALS'} {{ {mo_kind}",
         f"      NMO {nup + ndown}",
         f"      ORBFILE {os.path.basename(orb)}",
         _basis_text(label, shells, cutoff=16.0, normtype="CRYSTAL" if high_l else None),

@@ -236,6 +236,7 @@ class SplineBasis:
             self.syms.append(sym)
         thr0 = x[n - 1]
         cuts = [spline_findcutoff(c, spacing, thr0) for c in coeffs]
+        self.cuts = cuts                  # per spline (CUTOFF_MO evaluates inside each)
         self.threshold = max(cuts)
         # pad each table out to the common threshold (Spline_fitter::pad)
         self.coeffs = []
@@ -246,9 +247,11 @@ class SplineBasis:
             self.coeffs.append(c)
         self.nfunc = sum(NFUNC[s] for s in self.syms)
 
-    def eval_lap(self, d):
+    def eval_lap(self, d, per_function=False):
         """Values [..., nfunc, 5] = (f, df/dx, df/dy, df/dz, lap) at
-        displacement d [..., 3] from the center (Cubic_spline_calc.cpp:353-)."""
+        displacement d [..., 3] from the center (Cubic_spline_calc.cpp:353-).
+        per_function: zero each function outside its own spline's cutoff (the
+        CUTOFF_MO evaluator, MO_matrix_cutoff.h:480-569)."""
         d = np.asarray(d, dtype=float)
         r2 = np.sum(d * d, axis=-1)
         r = np.sqrt(r2)
@@ -259,7 +262,7 @@ class SplineBasis:
         inv = 1.0 / self.spacing
         k = 0
         with np.errstate(divide="ignore", invalid="ignore"):
-            for sym, c in zip(self.syms, self.coeffs):
+            for sym, c, cut in zip(self.syms, self.coeffs, self.cuts):
                 i = (rr * inv).astype(np.int64)
                 h = rr - i * self.spacing
                 c0, c1, c2, c3 = c[i, 0], c[i, 1], c[i, 2], c[i, 3]
@@ -274,6 +277,8 @@ class SplineBasis:
                     out[..., k, 2] = h1 * y + ay * f
                     out[..., k, 3] = h1 * z + az * f
                     out[..., k, 4] = ang * f2 + (2 * L + 2) * h1 + lapA * f
+                    if per_function:
+                        out[..., k, :] = np.where((r < cut)[..., None], out[..., k, :], 0.0)
                     k += 1
         out[~inside] = 0.0
         return out
@@ -464,6 +469,8 @@ class System:
         self.cplx = bool(section(w, "CORBITALS"))
         orbw = section(w, "CORBITALS") if self.cplx else section(w, "ORBITALS")
         self.mo_kind = orbw[0].upper()
+        self.cutoff_mo = self.mo_kind == "CUTOFF_MO"
+        self.magnify = value(orbw, "MAGNIFY", 1.0)
         self.nmo = int(value(orbw, "NMO", conv=int))
         self.basis = [SplineBasis(b) for b in sections(orbw, "BASIS")]
         # centers = atoms (USEATOMS / USEGLOBAL for molecules); a periodic cell
@@ -487,6 +494,9 @@ class System:
         if not os.path.isabs(orbfile) and not os.path.exists(orbfile):
             orbfile = os.path.join(base, orbfile)
         self.moc = self._read_orb(orbfile)
+        if self.cutoff_mo:
+            # MO_matrix_cutoff::init (MO_matrix_cutoff.h:198-235): |c| <= 1e-12 dropped, MAGNIFY applied
+            self.moc = np.where(np.abs(self.moc) > 1e-12, self.moc * self.magnify, 0.0)
         states = [int(s) - 1 for s in section(w, "STATES")]
         self.occ = [states[:self.nup], states[self.nup:]]
 
@@ -604,8 +614,10 @@ class System:
                 v = 0.0
                 for img, kf in zip(self.images[c], self.kfac[c]):
                     d = P - img
-                    v = v + kf * b.eval_lap(d)
+                    v = v + kf * b.eval_lap(d, per_function=self.cutoff_mo)
                 keep = np.abs(v[..., 0]) > 1e-8          # modulus for complex sums
+                if self.cutoff_mo:                       # no skip of small values
+                    keep = np.ones_like(keep)
                 vals.append(np.where(keep[..., None], v, 0.0))
         B = np.concatenate(vals, axis=-2)          # [..., totbasis, 5]
         return np.einsum("...bk,bm->...mk", B, self.moc)

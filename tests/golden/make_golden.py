@@ -45,7 +45,11 @@ WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseu
              ("n2_fg", dict(pseudo=True, high_l=True), 20),
              ("diamond8_f", dict(periodic=True, high_l=True), 21),
              # a Slater wave function alone, its BASIS section given twice
-             ("n2_slater", dict(pseudo=True, jastrow=False, dup_basis=True), 22)]
+             ("n2_slater", dict(pseudo=True, jastrow=False, dup_basis=True), 22),
+             # the CUTOFF_MO evaluator: a molecule and a complex k-point cell
+             ("n2_cutoff", dict(pseudo=True, mo_kind="CUTOFF_MO"), 23),
+             ("diamond8_kc", dict(periodic=True, kpoint=(0.5, 0.25, 0.0), complex_orbitals=True,
+                                  mo_kind="CUTOFF_MO"), 24)]
 
 
 def make(name, kw, seed):
@@ -53,14 +57,14 @@ def make(name, kw, seed):
         sc = kw.get("supercell", (1, 1, 1))
         deck = systems.write_periodic(HERE, seed=seed, name=name, supercell=sc, kpoint=kw.get("kpoint"),
                                       complex_orbitals=kw.get("complex_orbitals", False),
-                                      high_l=kw.get("high_l", False))
+                                      high_l=kw.get("high_l", False), mo_kind=kw.get("mo_kind", "BLAS_MO"))
         nconf = 64 if sc == (1, 1, 1) else 16
     elif "nelec" in kw:  # molecules of the batched-uneven workload (odd count; above 32 per spin)
         deck = systems.write_molecule(HERE, name, seed, kw["nelec"])
         nconf = 64 if kw["nelec"] < 64 else 32
     else:
         deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
-        nconf = NCONF if not ({"expansion", "high_l", "jastrow"} & set(kw)) else 64
+        nconf = NCONF if not ({"expansion", "high_l", "jastrow", "mo_kind"} & set(kw)) else 64
     R = systems.random_configs(deck, nconf, seed=seed + 1000)
     NCONF_ = nconf
     rng = np.random.default_rng(seed + 2000)

@@ -20,7 +20,7 @@ from mainline_b200 import engine, systems
 
 pytestmark = pytest.mark.gpu
 
-NAMES = ["diamond8_k", "diamond8_l"]
+NAMES = ["diamond8_k", "diamond8_l", "diamond8_kc"]
 FP64_TOL = 1e-10
 
 
@@ -40,7 +40,7 @@ def golden(request):
 
 
 def _check_sign(name, got, ref):
-    if name == "diamond8_k":
+    if name in ("diamond8_k", "diamond8_kc"):
         assert _phase_err(got, ref) < 1e-9
     else:
         assert np.array_equal(got, ref)
