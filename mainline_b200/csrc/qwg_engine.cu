@@ -51,9 +51,10 @@ static void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
   if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
 }
 
-// Kernel family for a system with m orbitals per spin: 8/16/32 select the
-// shared-memory walker kernels; 0 selects the HBM-resident kernels (up to
-// kMaxOrbHBM orbitals per spin); -1 is beyond this build.
+// Kernel families: 8/16/32 the shared-memory walker kernels; 0 the
+// HBM-resident kernels (up to kMaxOrbHBM orbitals per spin); kComplexFamily
+// their complex-orbital variant.  mmax_for gives the size class of m orbitals
+// per spin, -1 beyond this build (checked before a family is chosen).
 constexpr int kMaxOrbHBM = 256;
 static int mo_stride_for(int mmax, int nmo_max) { return mmax > 0 ? mmax : (nmo_max + 3) / 4 * 4; }
 // -1: the HBM-resident kernels with complex orbitals (CORBITALS, or real
@@ -76,6 +77,26 @@ static int mmax_for(int m) {
   if (m <= 32) return 32;
   if (m <= kMaxOrbHBM) return 0;
   return -1;
+}
+// Kernel family of a system (within the 256-orbital limit).  The shared-memory
+// kernels win only for the smallest molecules (up to 8 orbitals per spin);
+// above that, and for periodic cells at every size, the HBM-resident kernels
+// keep more walkers resident per SM and run faster (DMC on B200: 8-atom cell
+// 1.4x mixed / 1.6x FP64, 24-electron molecule 1.3x / 1.1x, 43-electron
+// molecule 1.3x / 2.0x; the 14-electron molecule runs 0.64x on them, so it
+// stays on the shared-memory kernels).  Expansions, F/G shells and CUTOFF_MO
+// need the HBM-resident kernels, complex orbitals their complex variant.
+// QWG_KERNEL_FAMILY=hbm|smem overrides the size rule for tuning.
+static int kernel_family(const HostSystem& H) {
+  if (needs_complex(H)) return kComplexFamily;
+  const int smem = mmax_for(std::max(H.nmo[0], H.nmo[1]));
+  if (H.detwt.size() > 1 || has_high_l(H)) return 0;
+  int mm = (H.periodic || smem > 8) ? 0 : smem;
+  if (const char* fam = getenv("QWG_KERNEL_FAMILY")) {
+    if (strcmp(fam, "hbm") == 0) mm = 0;
+    if (strcmp(fam, "smem") == 0) mm = smem;
+  }
+  return mm;
 }
 
 }  // namespace
@@ -781,11 +802,8 @@ int qwg_footprint(const char* deck_path, int precision, int max_walkers, unsigne
     std::unique_ptr<qwg_ctx> c(new qwg_ctx());
     c->precision = precision;
     c->H = build_system(deck_path);
-    c->mmax = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
-    if (c->mmax < 0) return QWG_ERR_INPUT;
-    if (c->H.detwt.size() > 1) c->mmax = 0;  // expansions run on the HBM-resident kernels
-    if ((has_high_l(c->H) || c->H.periodic || c->mmax > 8) && c->mmax > 0) c->mmax = 0;
-    if (needs_complex(c->H)) c->mmax = kComplexFamily;
+    if (mmax_for(std::max(c->H.nmo[0], c->H.nmo[1])) < 0) return QWG_ERR_INPUT;
+    c->mmax = kernel_family(c->H);
     make_layout(c.get());
     *bytes = footprint_bytes(c.get(), max_walkers);
     return QWG_OK;
@@ -821,27 +839,11 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
   c->max_walkers = max_walkers;
   int rc = guarded(c.get(), [&]() -> int {
     c->H = build_system(deck_path);
-    int mm = mmax_for(std::max(c->H.nmo[0], c->H.nmo[1]));
-    if (mm < 0) throw InputError("more than 256 electrons (or expansion orbitals) of one spin: beyond this engine build");
-    if (c->H.detwt.size() > 1) {
-      if (c->H.periodic) throw InputError("determinant expansions are supported for molecules only");
-      mm = 0;  // expansions run on the HBM-resident kernels
-    }
-    if (has_high_l(c->H) && mm > 0) mm = 0;         // F / G shells: HBM-resident kernels
-    // The shared-memory kernels win only for the smallest molecules (up to 8
-    // orbitals per spin); above that, and for periodic cells at every size, the
-    // HBM-resident kernels keep more walkers resident per SM and run faster
-    // (DMC on B200: 8-atom cell 1.4x mixed / 1.6x FP64, 24-electron molecule
-    // 1.3x / 1.1x, 43-electron molecule 1.3x / 2.0x; 14-electron molecule
-    // 0.64x, so it stays on the shared-memory kernels)
-    if ((c->H.periodic || mm > 8) && mm > 0) mm = 0;
-    if (const char* fam = getenv("QWG_KERNEL_FAMILY")) {  // tuning override: "hbm" or "smem"
-      if (strcmp(fam, "hbm") == 0 && mm > 0) mm = 0;
-      if (strcmp(fam, "smem") == 0 && mm == 0 && !has_high_l(c->H) && c->H.detwt.size() == 1)
-        mm = std::max(mmax_for(std::max(c->H.nmo[0], c->H.nmo[1])), 0);
-    }
-    if (needs_complex(c->H)) mm = kComplexFamily;  // complex orbitals / twisted boundary conditions
-    c->mmax = mm;
+    if (mmax_for(std::max(c->H.nmo[0], c->H.nmo[1])) < 0)
+      throw InputError("more than 256 electrons (or expansion orbitals) of one spin: beyond this engine build");
+    if (c->H.detwt.size() > 1 && c->H.periodic)
+      throw InputError("determinant expansions are supported for molecules only");
+    c->mmax = kernel_family(c->H);
     if (const char* sched = getenv("QWG_DMC_SCHEDULE")) c->split = strcmp(sched, "fused") != 0;
     if (stream) {
       c->stream = (cudaStream_t)stream;
