@@ -161,6 +161,14 @@ int qwg_eval(qwg_ctx* ctx, const double* rot, qwg_eval_out* out);
 int qwg_ratio(qwg_ctx* ctx, const int* e, const double* Rnew, double* dlogpsi, double* sign,
               double* grad, double* lap);
 
+/* VMC move dynamics, the DYNAMICS { SPLIT DEPTH d DIVIDER x } section of a
+ * VMC method (method/Vmc_method.cpp:75-82, Split_sampler::split_driver,
+ * method/Split_sample.cpp:380-478).  depth 2 (the default, with divider 2):
+ * a rejected move is retried from the same point with timestep tau/divider
+ * and the delayed-rejection acceptance (Split_sample.cpp:302-373); depth 1:
+ * one attempt.  DMC always uses depth 1, as the reference does. */
+int qwg_set_vmc_dynamics(qwg_ctx* ctx, int depth, double divider);
+
 /* VMC block on the resident walkers: nstep sweeps (each = one drift-diffusion
  * Metropolis move per electron + one local energy).  stochastic PP unless
  * deterministic_pp. */

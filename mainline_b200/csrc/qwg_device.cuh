@@ -293,6 +293,11 @@ struct StepParams {
   // per walker (TMOVES), 2 one per electron (TMOVESSC)
   int tmoves;
   int tm_cap;           // quadrature terms per walker the candidate buffer holds
+  // VMC dynamics (Split_sampler DEPTH / DIVIDER, the reference's VMC default
+  // 2 / 2): a rejected move is retried from the same point with timestep
+  // tau / divider (delayed rejection); the fused step kernel only
+  int vmc_depth;
+  double vmc_divider;
   double* tm_cand;      // [W][tm_cap] the current electron chunk's point terms
   double* tm_moves;     // [W][N][4] selected targets (x, y, z, 1) or flag 0
 };

@@ -112,6 +112,8 @@ struct qwg_ctx {
   int wpc_sweep = 4;        // walkers per CTA of the move-phase kernel (KM_SWEEP)
   size_t smem_sweep = 0;
   bool split = true;        // DMC steps as sweep + local-energy launches (else one fused launch per chunk)
+  int vmc_depth = 2;        // VMC Split_sampler DEPTH / DIVIDER (Vmc_method.cpp:75-82 defaults)
+  double vmc_divider = 2.0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   long long launches = 0;
@@ -562,6 +564,8 @@ static StepParams base_params(qwg_ctx* c) {
   P.acc = c->d_acc.as<BlockAcc>();
   P.etrial = c->d_dyn.as<double>();
   P.refresh = 1;
+  P.vmc_depth = c->vmc_depth;
+  P.vmc_divider = c->vmc_divider;
   return P;
 }
 
@@ -609,7 +613,9 @@ static void set_tmoves(qwg_ctx* c, StepParams& P) {
 // P.nsteps steps of every walker: one fused launch, or (split schedule) a
 // move launch and a local-energy launch per step.
 static void launch_steps(qwg_ctx* c, StepParams P, const EvalIO& io, int nwalk) {
-  if (!c->split) {
+  // VMC with delayed rejection runs on the fused step kernel, which alone
+  // carries the second-stage move (the DMC move kernel keeps depth 1)
+  if (!c->split || (!P.dmc && P.vmc_depth > 1)) {
     launch_walkers(c, P, io, KM_STEPS, nwalk);
     return;
   }
@@ -1055,6 +1061,14 @@ int qwg_ratio(qwg_ctx* c, const int* e, const double* Rnew, double* dlogpsi, dou
   });
 }
 
+int qwg_set_vmc_dynamics(qwg_ctx* c, int depth, double divider) {
+  if (!c || depth < 1 || depth > 2 || !(divider > 0))
+    return fail(c, QWG_ERR_ARG, "qwg_set_vmc_dynamics: depth must be 1 or 2 and divider positive");
+  c->vmc_depth = depth;
+  c->vmc_divider = divider;
+  return QWG_OK;
+}
+
 int qwg_vmc_block(qwg_ctx* c, int nstep, double timestep, uint64_t seed, int deterministic_pp,
                   qwg_block_stats* stats) {
   if (!c || nstep <= 0 || !(timestep > 0)) return fail(c, QWG_ERR_ARG, "qwg_vmc_block: bad arguments");
@@ -1312,6 +1326,8 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
     P.nsteps = nstep;
     P.refresh = 1;
     P.dmc = 0;
+    P.vmc_depth = c->vmc_depth;
+    P.vmc_divider = c->vmc_divider;
     P.deterministic_pp = deterministic_pp;
     P.tau = timestep;
     P.seed = seed;

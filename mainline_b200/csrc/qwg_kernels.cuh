@@ -1147,6 +1147,53 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
             if (acc + rb.u[0] > 1.0) {
               W.accept(e, wx, wy, wz, ratioD, dU);
               nacc += 1;
+            } else if constexpr (mode == KM_STEPS) {
+              if (!P.dmc && P.vmc_depth > 1) {
+                // delayed rejection, second stage (Split_sampler::split_driver
+                // depth 2, Split_sample.cpp:380-478): a new move from the same
+                // point with timestep tau2 = tau / divider, accepted with
+                // get_acceptance(0, 2) (Split_sample.cpp:302-373)
+                const double tau2 = P.tau / P.vmc_divider;
+                double dv2[3];
+                lim_drift(g0, tau2, dv2);
+                const Rand4 rc = rand4(P.seed, wid, step, e, 4u);
+                const Rand4 rd = rand4(P.seed, wid, step, e, 5u);
+                double gb[4];
+                box_muller(rc.u[0], rc.u[1], gb[0], gb[1]);
+                box_muller(rc.u[2], rc.u[3], gb[2], gb[3]);
+                const double sq2 = sqrt(tau2);
+                const double x2[3] = {ox + gb[0] * sq2 + dv2[0], oy + gb[1] * sq2 + dv2[1], oz + gb[2] * sq2 + dv2[2]};
+                double vx = x2[0], vy = x2[1], vz = x2[2];
+                if constexpr (CPXK) wrap_pos_kphase(S, vx, vy, vz);
+                else wrap_pos(S, vx, vy, vz);
+                double r2D, dU2, g2[3], l2;
+                W.propose(e, vx, vy, vz, r2D, dU2, g2, l2);
+                const double ratio2 = r2D * exp(dU2);  // psi(x2) / psi(x0)
+                const double x1[3] = {nx, ny, nz}, x0[3] = {ox, oy, oz};
+                // ln T(a -> b; t) = -|b - a - limdrift(drift_a, t)|^2 / (2 t)
+                auto lnT = [&](const double* a, const double* ga, const double* b, double t) {
+                  double d[3];
+                  lim_drift(ga, t, d);
+                  double q = 0;
+                  for (int k = 0; k < 3; k++) q += (b[k] - a[k] - d[k]) * (b[k] - a[k] - d[k]);
+                  return -q / (2.0 * t);
+                };
+                // a(2 -> 1): the reverse first stage from x2
+                const double r21 = ratio / ratio2;
+                const double a21 = fmin(1.0, r21 * r21 * exp(lnT(x1, g1, x2, P.tau) - lnT(x2, g2, x1, P.tau)));
+                const double num = 1.0 - a21, den = 1.0 - acc;
+                double acc2;
+                if (fabs(den) < 1e-10) acc2 = fabs(num) < 1e-10 ? 0.0 : 1.0;
+                else {
+                  const double pt = lnT(x2, g2, x1, P.tau) - lnT(x0, g0, x1, P.tau) + lnT(x2, g2, x0, tau2) -
+                                    lnT(x0, g0, x2, tau2);
+                  acc2 = fmin(1.0, ratio2 * ratio2 * exp(pt) * num / den);
+                }
+                if (acc2 + rd.u[0] > 1.0) {
+                  W.accept(e, vx, vy, vz, r2D, dU2);
+                  nacc += 1;
+                }
+              }
             }
           }
         }

@@ -27,7 +27,7 @@ EXPORTS = [
     "qwg_version", "qwg_last_error", "qwg_create", "qwg_destroy", "qwg_get_info", "qwg_inspect_deck",
     "qwg_inspect_spline", "qwg_set_walkers", "qwg_get_walkers", "qwg_set_walkers_device",
     "qwg_get_walker_scalars", "qwg_eval",
-    "qwg_ratio", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
+    "qwg_ratio", "qwg_set_vmc_dynamics", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
     "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready", "qwg_time_kernels",
     "qwg_log_header", "qwg_log_block", "qwg_write_configs", "qwg_count_configs", "qwg_read_configs",
@@ -117,6 +117,7 @@ def load_library(path: str = LIB_PATH):
         "qwg_get_walker_scalars": (C.c_int, [C.c_void_p, dp, dp, C.c_int]),
         "qwg_eval": (C.c_int, [C.c_void_p, dp, P(EvalOut)]),
         "qwg_ratio": (C.c_int, [C.c_void_p, P(C.c_int), dp, dp, dp, dp, dp]),
+        "qwg_set_vmc_dynamics": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
         "qwg_vmc_block": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_int, P(BlockStats)]),
         "qwg_dmc_init": (C.c_int, [C.c_void_p, P(DmcParams)]),
         "qwg_dmc_block": (C.c_int, [C.c_void_p, P(BlockStats)]),
@@ -274,6 +275,10 @@ class Engine:
         self._check(self.lib.qwg_ratio(self.h, e.ctypes.data_as(C.POINTER(C.c_int)), _ptr(rnew), _ptr(dl),
                                        _ptr(sg), _ptr(g), _ptr(lp)), "qwg_ratio")
         return dl, sg, g, lp
+
+    def set_vmc_dynamics(self, depth: int = 2, divider: float = 2.0) -> None:
+        """Split_sampler DEPTH / DIVIDER of the VMC moves (default 2 / 2, as the reference's VMC)."""
+        self._check(self.lib.qwg_set_vmc_dynamics(self.h, depth, divider), "qwg_set_vmc_dynamics")
 
     def vmc_block(self, nstep: int, timestep: float, seed: int = 1, deterministic_pp: bool = False) -> dict:
         st = BlockStats()

@@ -228,6 +228,10 @@ def test_dmc_large_population_branches_in_global_memory():
     nw = 16384
     E = engine.Engine(deck, engine.MIXED, max_walkers=nw)
     E.set_walkers(systems.random_configs(d, nw, seed=6))
+    # the population this test was calibrated on: 5 single-attempt VMC steps
+    # (the random-orbital trial function's E_L spread makes early DMC weights
+    # depend on how the population was equilibrated)
+    E.set_vmc_dynamics(1, 2.0)
     E.vmc_block(5, 0.3, seed=7)
     E.dmc_init(timestep=0.01, nstep=10, seed=8)
     for _ in range(2):
@@ -320,3 +324,27 @@ def test_shared_memory_kernels_when_forced(name, monkeypatch):
     assert _rel(ev.nonlocal_, g["nonlocal"]) < FP64_TOL
     s = E.vmc_block(2, 0.1, seed=3)
     assert s["nonfinite"] == 0
+
+
+def test_vmc_delayed_rejection_samples_the_same_distribution():
+    """VMC with the reference's default dynamics (SPLIT DEPTH 2 DIVIDER 2:
+    a rejected move is retried with half the timestep) and with one attempt
+    per move sample the same |psi|^2: equal energies within the statistical
+    error, a higher acceptance with the second stage."""
+    deck = os.path.join(GOLDEN, "n2_pseudo.qw")
+    d = systems.read_deck(deck)
+    out = {}
+    for depth in (1, 2):
+        E = engine.Engine(deck, engine.FP64, max_walkers=4096)
+        E.set_walkers(systems.random_configs(d, 4096, seed=61))
+        E.set_vmc_dynamics(depth, 2.0)
+        for b in range(5):
+            E.vmc_block(10, 0.5, seed=70 + b, deterministic_pp=True)
+        st = [E.vmc_block(10, 0.5, seed=80 + b, deterministic_pp=True) for b in range(20)]
+        e = np.array([s["energy"] for s in st])
+        out[depth] = (e.mean(), e.std(ddof=1) / np.sqrt(len(e)), np.mean([s["acceptance"] for s in st]))
+        E.close()
+    (e1, s1, a1), (e2, s2, a2) = out[1], out[2]
+    print(f"VMC depth 1: E {e1:.4f} +- {s1:.4f} acc {a1:.3f}; depth 2: E {e2:.4f} +- {s2:.4f} acc {a2:.3f}")
+    assert abs(e1 - e2) < 5 * np.hypot(s1, s2)
+    assert a2 > a1
