@@ -17,7 +17,8 @@
  * walkers, trial energy and counter-based random stream.
  *
  * Threading: one host thread drives a server.  Admission (context creation,
- * VMC equilibration, qwg_dmc_init) runs synchronously inside progress.
+ * VMC equilibration with single-attempt moves, qwg_dmc_init) runs
+ * synchronously inside progress.
  */
 #ifndef QWG_SERVER_H
 #define QWG_SERVER_H

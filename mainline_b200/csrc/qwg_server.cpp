@@ -58,6 +58,9 @@ int admit(qwg_server* s, Job& j) {
     return code;
   };
   if ((rc = qwg_set_walkers(j.ctx, j.R.data(), d.nwalkers)) != QWG_OK) return bail(rc);
+  // admission runs inside progress(): equilibrate with single-attempt moves
+  // (the split step kernels), which keeps the other jobs' blocks flowing
+  if ((rc = qwg_set_vmc_dynamics(j.ctx, 1, 2.0)) != QWG_OK) return bail(rc);
   for (int b = 0; b < d.vmc_blocks; b++) {
     qwg_block_stats st;
     rc = qwg_vmc_block(j.ctx, d.vmc_steps, d.vmc_timestep, d.vmc_seed + (uint64_t)b, d.dmc.deterministic_pp, &st);
