@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <fstream>
@@ -440,8 +441,21 @@ static std::vector<Radial> read_radial(const std::vector<std::string>& w) {
       r.b = 0;
       out.push_back(r);
     }
+  } else if (ieq(w[1], "PADE")) {
+    // Pade_function (basis_function/Pade_function.cpp:21-45, 128-184):
+    // (a_i r / (1 + a_i r))^2 with a_i = ALPHA0 / 2^i, no cutoff
+    const double a0 = value_d(w, "ALPHA0", 0, true);
+    const int nf = (int)value_d(w, "NFUNC", 0, true);
+    for (int i = 0; i < nf; i++) {
+      Radial r;
+      r.kind = RAD_PADE;
+      r.rcut = 1e99;
+      r.a = a0 / std::pow(2.0, i);
+      r.b = 0;
+      out.push_back(r);
+    }
   } else {
-    throw InputError("Jastrow basis type " + w[1] + " not supported (CUTOFF_CUSP, POLYPADE)");
+    throw InputError("Jastrow basis type " + w[1] + " not supported (CUTOFF_CUSP, POLYPADE, PADE)");
   }
   return out;
 }
@@ -474,8 +488,59 @@ static void gesqua(int& aip, std::vector<double>& q, std::vector<double>& wq) {
       q[3 * (i + 7) + 2] = -c;
     }
     wq.assign(12, 1.0 / 12.0);
+  } else if (aip < 32) {
+    // 18: the octahedron's 6 vertices (weight 1/30) and 12 edge midpoints
+    // (1/15); 26: those (40/840, 32/840) plus the cube's 8 vertices (27/840)
+    // (Abramowitz & Stegun 25.4.62-63; gesqua.cpp:121-273 point order)
+    aip = aip < 26 ? 18 : 26;
+    const double pa[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    for (auto& r : pa) q.insert(q.end(), r, r + 3);
+    const double h = 1.0 / std::sqrt(2.0);
+    const int pair[3][2] = {{0, 1}, {0, 2}, {2, 1}};  // (x,y), (x,z), (z,y): first axis varies fastest
+    for (auto& ax : pair)
+      for (int sb = 0; sb < 2; sb++)
+        for (int sa = 0; sa < 2; sa++) {
+          double r[3] = {0, 0, 0};
+          r[ax[0]] = sa ? -h : h;
+          r[ax[1]] = sb ? -h : h;
+          q.insert(q.end(), r, r + 3);
+        }
+    if (aip == 26) {
+      const double b = 1.0 / std::sqrt(3.0);
+      for (int sx = 0; sx < 2; sx++)
+        for (int sz = 0; sz < 2; sz++)
+          for (int sy = 0; sy < 2; sy++) {
+            const double r[3] = {sx ? -b : b, sy ? -b : b, sz ? -b : b};
+            q.insert(q.end(), r, r + 3);
+          }
+      for (int i = 0; i < 26; i++) wq.push_back(i < 6 ? 40.0 / 840.0 : i < 18 ? 32.0 / 840.0 : 27.0 / 840.0);
+    } else {
+      for (int i = 0; i < 18; i++) wq.push_back(i < 6 ? 1.0 / 30.0 : 1.0 / 15.0);
+    }
+  } else if (aip == 32) {
+    // the icosahedron's 12 vertices (weight 5/168) and the dodecahedron's 20
+    // (27/840), as polar angles around z (gesqua.cpp:274-320 point order)
+    q.assign(96, 0.0);
+    q[2] = 1.0; q[5] = -1.0;
+    const double t5 = std::sqrt(15.0 + 6.0 * std::sqrt(5.0));
+    const double th1 = std::acos((2.0 + std::sqrt(5.0)) / t5), th2 = std::acos(1.0 / t5);
+    auto put = [&](int idx, double th, double ph) {
+      q[3 * idx] = std::sin(th) * std::cos(ph);
+      q[3 * idx + 1] = std::sin(th) * std::sin(ph);
+      q[3 * idx + 2] = std::cos(th);
+    };
+    for (int i = 0; i < 5; i++) {
+      const double ev = 2 * i * M_PI / 5, od = (2 * i + 1) * M_PI / 5;
+      put(i + 2, std::atan(2.0), ev);
+      put(i + 7, M_PI - std::atan(2.0), od);
+      put(i + 12, th1, od);
+      put(i + 17, th2, od);
+      put(i + 22, M_PI - th1, ev);
+      put(i + 27, M_PI - th2, ev);
+    }
+    for (int i = 0; i < 32; i++) wq.push_back(i < 12 ? 5.0 / 168.0 : 27.0 / 840.0);
   } else {
-    throw InputError("AIP >= 18 quadratures are not supported (use 4, 6 or 12)");
+    throw InputError("Bad number of AIP's: " + std::to_string(aip) + " (4, 6, 12, 18, 26 or 32)");
   }
 }
 
@@ -944,6 +1009,7 @@ HostSystem build_system(const std::string& deck_path) {
   std::vector<std::vector<ThreeBodyTerm>> tb_at(S.natoms);
   static const int klm_default[12][3] = {{1, 1, 0}, {1, 0, 1}, {1, 1, 1}, {2, 2, 0}, {2, 0, 1}, {2, 0, 2},
                                          {2, 2, 2}, {3, 3, 0}, {3, 0, 2}, {3, 3, 2}, {1, 2, 2}, {2, 3, 2}};
+  bool any3 = false, any3s = false;
   for (auto& g : all_sections(wf2, "GROUP")) {
     int ee0 = (int)S.ee.size();
     for (auto& b : all_sections(g, "EEBASIS")) {
@@ -1002,31 +1068,64 @@ HostSystem build_system(const std::string& deck_path) {
         S.ee_unlike[ee0 + p] += to_d(c[p]);
       }
     }
+    // e-e-n terms: THREEBODY (Jastrow2_three.cpp) or THREEBODY_SPIN
+    // (Jastrow2_three_diffspin.cpp:130-186: LIKE_COEFFICIENTS for pairs of
+    // equal spin, UNLIKE_COEFFICIENTS for opposite spins); SM_TERMS replaces
+    // the default (k, l, m) list
+    std::vector<std::string> tb_sec, tbs_sec;
     pos = 0;
-    if (find_section(g, "THREEBODY", pos, sec)) {
-      if (has_section(sec, "SM_TERMS")) throw InputError("custom SM_TERMS are not supported");
-      double scale = value_d(sec, "SCALE", 1.0);
-      for (auto& c : all_sections(sec, "COEFFICIENTS")) {
-        int np = (int)c.size() - 1;
-        if (np > 12) throw InputError("too many three-body parameters");
+    const bool has3 = find_section(g, "THREEBODY", pos, tb_sec);
+    pos = 0;
+    const bool has3s = find_section(g, "THREEBODY_SPIN", pos, tbs_sec);
+    if (has3 && has3s) throw InputError("Can only have one of THREEBODY_SPIN or THREEBODY");
+    any3 = any3 || has3;
+    any3s = any3s || has3s;
+    if (has3 || has3s) {
+      const std::vector<std::string>& ts = has3 ? tb_sec : tbs_sec;
+      std::vector<std::array<int, 3>> klm;
+      if (has_section(ts, "SM_TERMS")) {
+        auto w = get_section(ts, "SM_TERMS");
+        if (w.size() % 3 != 0) throw InputError("SM_TERMS must contain a multiple of 3 elements");
+        for (size_t q = 0; q < w.size(); q += 3)
+          klm.push_back({std::stoi(w[q]), std::stoi(w[q + 1]), std::stoi(w[q + 2])});
+      } else {
+        for (auto& t : klm_default) klm.push_back({t[0], t[1], t[2]});
+      }
+      const double scale = value_d(ts, "SCALE", 1.0);
+      auto like = all_sections(ts, has3 ? "COEFFICIENTS" : "LIKE_COEFFICIENTS");
+      auto unlike = has3 ? like : all_sections(ts, "UNLIKE_COEFFICIENTS");
+      if (like.size() != unlike.size())
+        throw InputError("Need same amount of LIKE_COEFFICIENTS and UNLIKE_COEFFICIENTS sections in three body");
+      for (size_t sidx = 0; sidx < like.size(); sidx++) {
+        const auto& c = like[sidx];
+        const auto& cu = unlike[sidx];
+        const int np = (int)c.size() - 1;
+        if (cu.size() != c.size() || cu[0] != c[0])
+          throw InputError("three-body spin coefficients: like and unlike sections differ for " + c[0]);
+        if (np > (int)klm.size()) throw InputError("too many three-body parameters on " + c[0]);
+        bool found = false;
         for (int a = 0; a < S.natoms; a++) {
           if (S.labels[a] != c[0]) continue;
+          found = true;
           for (int i = 0; i < np; i++) {
             ThreeBodyTerm t;
-            t.k = ei0[a] + klm_default[i][0];
-            t.l = ei0[a] + klm_default[i][1];
-            t.m = ee0 + klm_default[i][2];
+            t.k = ei0[a] + klm[i][0];
+            t.l = ei0[a] + klm[i][1];
+            t.m = ee0 + klm[i][2];
             t.c = to_d(c[i + 1]) * scale;
-            if (klm_default[i][0] >= (int)ei_at[a].size() - ei0[a] || klm_default[i][1] >= (int)ei_at[a].size() - ei0[a] ||
-                klm_default[i][2] >= nee_g)
+            t.cu = to_d(cu[i + 1]) * scale;
+            if (klm[i][0] < 0 || klm[i][1] < 0 || klm[i][2] < 0 ||
+                klm[i][0] >= (int)ei_at[a].size() - ei0[a] || klm[i][1] >= (int)ei_at[a].size() - ei0[a] ||
+                klm[i][2] >= nee_g)
               throw InputError("Threebody needs more basis functions");
             tb_at[a].push_back(t);
           }
         }
+        if (!found) throw InputError("Couldn't find a matching center for " + c[0]);
       }
     }
-    if (has_section(g, "THREEBODY_SPIN")) throw InputError("THREEBODY_SPIN is not supported");
   }
+  S.tb_stale_ei = any3s && !any3;
   for (int a = 0; a < S.natoms; a++) {
     S.ei_first[a] = (int)S.ei.size();
     S.ei_count[a] = (int)ei_at[a].size();

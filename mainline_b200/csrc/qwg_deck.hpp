@@ -31,7 +31,7 @@ bool has_keyword(const std::vector<std::string>& w, const std::string& name);
 enum ShellSym {
   SYM_S = 0, SYM_P = 1, SYM_6D = 2, SYM_5D = 3, SYM_10F = 4, SYM_7F = 5, SYM_7F_CRYSTAL = 6, SYM_15G = 7, SYM_9G = 8
 };
-enum RadialKind { RAD_CUTOFF_CUSP = 0, RAD_POLYPADE = 1 };
+enum RadialKind { RAD_CUTOFF_CUSP = 0, RAD_POLYPADE = 1, RAD_PADE = 2 };
 
 // One radial spline x Cartesian angular set attached to one center.
 struct Shell {
@@ -55,7 +55,8 @@ struct Radial {
 
 struct ThreeBodyTerm {
   int k, l, m;     // global e-n (per atom) function indices k,l and e-e index m
-  double c;
+  double c;        // coefficient for electron pairs of equal spin
+  double cu;       // coefficient for pairs of opposite spin (= c unless THREEBODY_SPIN)
 };
 
 struct PPAtom {
@@ -111,6 +112,10 @@ struct HostSystem {
   std::vector<double> onebody;       // per ei function (already per atom slice)
   std::vector<int> tb_first, tb_count;     // per atom slice into tb
   std::vector<ThreeBodyTerm> tb;
+  // THREEBODY_SPIN present and no plain THREEBODY group: the reference's
+  // value-only Jastrow update leaves the moved electron's e-n basis values
+  // stale for the e-e-n terms (see DevSys::tb_stale_ei)
+  bool tb_stale_ei = false;
   // periodic cell (SYSTEM { PERIODIC }); molecules keep periodic == false and
   // one "image" per atom (the atom itself)
   bool periodic = false;

@@ -32,13 +32,13 @@ namespace qwg {
 // tables
 
 struct DRadial {
-  int kind;         // 0 CUTOFF_CUSP, 1 POLYPADE
+  int kind;         // 0 CUTOFF_CUSP, 1 POLYPADE, 2 PADE
   double rcut, inv_rcut;
-  double a, b, c;   // CUTOFF_CUSP: cusp, gamma, 1/(3+gamma) ; POLYPADE: beta
+  double a, b, c;   // CUTOFF_CUSP: cusp, gamma, 1/(3+gamma) ; POLYPADE: beta ; PADE: alpha
 };
 struct DTB {
   int k, l, m;      // e-n functions k, l of the atom's type, e-e function m
-  double c;
+  double c, cu;     // coefficient for equal-spin / opposite-spin pairs
 };
 
 // Capacities of the tables carried in the kernel parameter bank.
@@ -48,7 +48,7 @@ constexpr int QWG_MAXEE = 8;       // e-e radial functions
 constexpr int QWG_MAXEI = 8;       // e-n radial functions per type
 constexpr int QWG_MAXTB = 12;      // e-e-n terms per type
 constexpr int QWG_MAXPPT = 16;     // pseudopotential Gaussian terms per type
-constexpr int QWG_MAXQ = 12;       // quadrature points
+constexpr int QWG_MAXQ = 32;       // quadrature points
 constexpr int QWG_MAXSHELL = 1024; // basis shells
 constexpr int QWG_MAXDET = 64;     // determinants of an expansion
 constexpr int QWG_MAXUD = 16;      // distinct determinants of one spin
@@ -105,6 +105,12 @@ struct DevSys {
                                  // three-body) vanishes for electrons at least that far apart
   DTB tb[QWG_MAXT][QWG_MAXTB];
   int has_tb;
+  // value-only ratios (pseudopotential quadrature): the e-e-n terms take the
+  // moved electron's e-n basis at its current position.  The reference's
+  // Jastrow2_wf::updateVal (Jastrow2_wf.cpp:877-882, 931-936) refreshes the
+  // saved e-n basis only when a group has a plain THREEBODY term, so with
+  // THREEBODY_SPIN alone its quadrature ratios see the stale values.
+  int tb_stale_ei;
   // pseudopotential per type (nchan 0: none)
   int has_pp;
   int pp_nchan[QWG_MAXT], pp_aip[QWG_MAXT];
@@ -386,6 +392,12 @@ __device__ __forceinline__ void radial_lap(const DRadial& q, T r, T& f, T& fd, T
     T dadr = ppd * pade2 * ir;
     fd = cusp * dadr;
     lap = cusp * ((ppdd * pade2 - T(2) * gamma * ppd * ppd * pade2 * pade) * ircut + T(2) * dadr);
+  } else if (q.kind == 2) {  // PADE (alpha a): f = (a r / (1 + a r))^2
+    const T pade = T(1) / (T(1) + T(q.a) * r);
+    const T app = T(q.a) * T(q.a) * pade * pade;
+    f = app * r * r;
+    fd = T(2) * app * pade;
+    lap = T(3) * fd * pade;
   } else {            // POLYPADE (beta a)
     const T beta = T(q.a);
     T zpp = zz2 * (T(6) - T(8) * zz + T(3) * zz2);
@@ -405,6 +417,10 @@ __device__ __forceinline__ T radial_val(const DRadial& q, T r) {
   if (q.kind == 0) {
     T pp = zz - zz2 + zz * zz2 * T(1.0 / 3.0);
     return T(q.a) * T(q.rcut) * (pp / (T(1) + T(q.b) * pp) - T(q.c));
+  }
+  if (q.kind == 2) {
+    const T ap = T(q.a) / (T(1) + T(q.a) * r);
+    return ap * ap * r * r;
   }
   T zpp = zz2 * (T(6) - T(8) * zz + T(3) * zz2);
   return (T(1) - zpp) / (T(1) + T(q.a) * zpp);
@@ -1141,15 +1157,17 @@ __device__ __forceinline__ void near_atoms(const DevSys<Real>& S, const double p
 }
 
 // e-e-n terms of the pair (i, j) at one atom of type t (Jastrow2_three.cpp:
-// 138-404): sum_terms c (a_k(i) a_l(j) + a_l(i) a_k(j)) b_m(r_ij), with
-// gradients/laps for both electrons.
+// 138-404; THREEBODY_SPIN, Jastrow2_three_diffspin.cpp:233-330, picks the
+// coefficient by the pair's spins): sum_terms c (a_k(i) a_l(j) + a_l(i) a_k(j))
+// b_m(r_ij), with gradients/laps for both electrons.
 template <typename Real>
-__device__ __forceinline__ void tb_atom(const DevSys<Real>& S, int t, const double di[3], double ri, const double dj[3],
-                                        double rj, const double dij[3], double rij, double& u, double gi[3],
-                                        double& li, double gj[3], double& lj, bool need_derivs) {
+__device__ __forceinline__ void tb_atom(const DevSys<Real>& S, int t, bool same, const double di[3], double ri,
+                                        const double dj[3], double rj, const double dij[3], double rij, double& u,
+                                        double gi[3], double& li, double gj[3], double& lj, bool need_derivs) {
   const int nt = S.tb_n[t];
   for (int n = 0; n < nt; n++) {
-    const DTB& q = S.tb[t][n];
+    const DTB& q0 = S.tb[t][n];
+    struct { int k, l, m; double c; } q{q0.k, q0.l, q0.m, same ? q0.c : q0.cu};
     double aki, akdi, akli, akj, akdj, aklj, ali, aldi, alli, alj, aldj, allj, b, bd, bl;
     radial_lap(S.ei[t][q.k], ri, aki, akdi, akli);
     radial_lap(S.ei[t][q.k], rj, akj, akdj, aklj);
@@ -1178,13 +1196,18 @@ __device__ __forceinline__ void tb_atom(const DevSys<Real>& S, int t, const doub
 }
 
 // Three-body (e-e-n) contribution of the pair (i, j) summed over the atoms
-// (ns: the atoms in range of electron i, from near_atoms at pi).
+// (ns: the atoms in range of electron i, from near_atoms at pi; same: the
+// two electrons have equal spin).
+// pie: the position whose e-n basis values electron i uses (pi except for
+// the stale-basis value path, DevSys::tb_stale_ei); ns was built at pie.
 template <typename Real>
-__device__ void jas_threebody_pair(const DevSys<Real>& S, const NearSet& ns, const double pi[3], const double pj[3],
-                                   double& u, double gi[3], double& li, double gj[3], double& lj, bool need_derivs) {
+__device__ void jas_threebody_pair(const DevSys<Real>& S, const NearSet& ns, bool same, const double pi[3],
+                                   const double pj[3], double& u, double gi[3], double& li, double gj[3], double& lj,
+                                   bool need_derivs, const double* pie = nullptr) {
   u = 0; li = lj = 0;
   for (int d = 0; d < 3; d++) gi[d] = gj[d] = 0;
   if (ns.n == 0) return;
+  if (!pie) pie = pi;
   double dij[3] = {pi[0] - pj[0], pi[1] - pj[1], pi[2] - pj[2]};
   min_image(S, dij[0], dij[1], dij[2]);
   const double rij = sqrt(dij[0] * dij[0] + dij[1] * dij[1] + dij[2] * dij[2]);
@@ -1196,7 +1219,7 @@ __device__ void jas_threebody_pair(const DevSys<Real>& S, const NearSet& ns, con
     const double* ap = S.atom_pos[a];
     double di[3], ri;
     if (ns.n < 0) {
-      di[0] = pi[0] - ap[0]; di[1] = pi[1] - ap[1]; di[2] = pi[2] - ap[2];
+      di[0] = pie[0] - ap[0]; di[1] = pie[1] - ap[1]; di[2] = pie[2] - ap[2];
       min_image(S, di[0], di[1], di[2]);
       ri = sqrt(di[0] * di[0] + di[1] * di[1] + di[2] * di[2]);
     } else {
@@ -1207,7 +1230,7 @@ __device__ void jas_threebody_pair(const DevSys<Real>& S, const NearSet& ns, con
     min_image(S, dj[0], dj[1], dj[2]);
     const double rj = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
     if (!(rj < S.tb_rc[t]) || !(ri < S.tb_rc[t])) continue;  // every term vanishes
-    tb_atom(S, t, di, ri, dj, rj, dij, rij, u, gi, li, gj, lj, need_derivs);
+    tb_atom(S, t, same, di, ri, dj, rj, dij, rij, u, gi, li, gj, lj, need_derivs);
   }
 }
 
@@ -1237,7 +1260,7 @@ __device__ void jas_electron(const DevSys<Real>& S, const double* R, int i, doub
     g[0] += pfd * dx; g[1] += pfd * dy; g[2] += pfd * dz;
     if constexpr (TB) {  // e-e-n terms compiled in only when the deck has them
       double tu, tgi[3], tli, tgj[3], tlj;
-      jas_threebody_pair(S, ns, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, need_derivs);
+      jas_threebody_pair(S, ns, si == (j < S.nup), pi, R + 3 * j, tu, tgi, tli, tgj, tlj, need_derivs);
       u += tu; lap += tli;
       for (int d = 0; d < 3; d++) g[d] += tgi[d];
     }
@@ -1264,8 +1287,9 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
   }
   const bool si = i < S.nup;
   const double pi[3] = {px, py, pz};
+  const double* pie = S.tb_stale_ei ? R + 3 * i : pi;  // e-n position of the e-e-n terms
   NearSet ns;
-  if constexpr (TB) near_atoms(S, pi, ns);
+  if constexpr (TB) near_atoms(S, pie, ns);
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
     double ex = px - R[3 * j], ey = py - R[3 * j + 1], ez = pz - R[3 * j + 2];
@@ -1281,7 +1305,7 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
     }
     if constexpr (TB) {
       double tu, tgi[3], tli, tgj[3], tlj;
-      jas_threebody_pair(S, ns, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false);
+      jas_threebody_pair(S, ns, same, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false, pie);
       u += T(tu);
     }
   }

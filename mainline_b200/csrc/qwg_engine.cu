@@ -134,6 +134,7 @@ struct qwg_ctx {
   size_t io_bytes = 0;
   // dynamics
   uint64_t step_counter = 0;
+  uint64_t noalloc_step_counter = 0;  // steps of qwg_vmc_block_noalloc (its own random streams)
   uint64_t last_refresh = 0;
   uint64_t branch_counter = 0;
   qwg_dmc_params dmc{};
@@ -270,6 +271,7 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     S.ee_unlike[k] = H.ee_unlike[k];
   }
   S.has_tb = H.tb.empty() ? 0 : 1;
+  S.tb_stale_ei = H.tb_stale_ei ? 1 : 0;
   S.has_pp = H.has_pp ? 1 : 0;
   std::vector<int> type_done(types.size(), 0);
   for (int a = 0; a < H.natoms; a++) {
@@ -287,7 +289,7 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     S.tb_rc[t] = 0.0;
     for (int n = 0; n < H.tb_count[a]; n++) {
       const ThreeBodyTerm& q = H.tb[H.tb_first[a] + n];
-      S.tb[t][n] = DTB{q.k - H.ei_first[a], q.l - H.ei_first[a], q.m, q.c};
+      S.tb[t][n] = DTB{q.k - H.ei_first[a], q.l - H.ei_first[a], q.m, q.c, q.cu};
       S.tb_rc[t] = std::max({S.tb_rc[t], S.ei[t][S.tb[t][n].k].rcut, S.ei[t][S.tb[t][n].l].rcut});
     }
     const PPAtom& P = H.pp[a];

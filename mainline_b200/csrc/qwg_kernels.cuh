@@ -404,8 +404,8 @@ struct Walker {
       if constexpr (has3) {
         double pn[3] = {px, py, pz}, po[3] = {ox, oy, oz};
         double tu, tgi[3], tli, tgj[3], tlj, su, sgi[3], sli, sgj[3], slj;
-        jas_threebody_pair(S, nsn, pn, pj, tu, tgi, tli, tgj, tlj, true);
-        jas_threebody_pair(S, nso, po, pj, su, sgi, sli, sgj, slj, true);
+        jas_threebody_pair(S, nsn, same, pn, pj, tu, tgi, tli, tgj, tlj, true);
+        jas_threebody_pair(S, nso, same, po, pj, su, sgi, sli, sgj, slj, true);
         du += tu - su;
         ge[0] += tgi[0]; ge[1] += tgi[1]; ge[2] += tgi[2];
         le += tli;

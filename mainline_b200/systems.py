@@ -143,6 +143,41 @@ def _jastrow_text(label: str, onebody: np.ndarray, threebody=None, twobody_pp=No
     ] + g2)
 
 
+def _jastrow_pade_spin_text(rng, label: str) -> str:
+    """Jastrow with the PADE radial basis (e-e and e-n), TWOBODY_SPIN and an
+    e-e-n THREEBODY_SPIN term on a custom SM_TERMS list, beside the usual
+    cusp group."""
+    ob = rng.normal(0.0, 0.1, size=3)
+    tl, tu = rng.normal(0.0, 0.05, size=4), rng.normal(0.0, 0.05, size=4)
+    return "\n".join([
+        "JASTROW2",
+        "GROUP {",
+        "  EEBASIS { EE CUTOFF_CUSP GAMMA 24.0 CUSP 1.0 CUTOFF 7.5 }",
+        "  EEBASIS { EE CUTOFF_CUSP GAMMA 24.0 CUSP 1.0 CUTOFF 7.5 }",
+        "  TWOBODY_SPIN { FREEZE",
+        "    LIKE_COEFFICIENTS { 0.25 0.0 }",
+        "    UNLIKE_COEFFICIENTS { 0.0 0.5 }",
+        "  }",
+        "}",
+        "GROUP {",
+        "  EEBASIS { EE PADE NFUNC 2 ALPHA0 1.3 }",
+        f"  EIBASIS {{ {label} PADE NFUNC 3 ALPHA0 2.0 }}",
+        "  ONEBODY {",
+        f"    COEFFICIENTS {{ {label} " + " ".join(_fmt(c) for c in ob) + " }",
+        "  }",
+        "  TWOBODY_SPIN {",
+        f"    LIKE_COEFFICIENTS {{ {_fmt(rng.normal(0, 0.1))} {_fmt(rng.normal(0, 0.1))} }}",
+        f"    UNLIKE_COEFFICIENTS {{ {_fmt(rng.normal(0, 0.1))} {_fmt(rng.normal(0, 0.1))} }}",
+        "  }",
+        "  THREEBODY_SPIN {",
+        "    SM_TERMS { 1 1 0  1 0 1  2 1 1  0 2 0 }",
+        f"    LIKE_COEFFICIENTS {{ {label} " + " ".join(_fmt(c) for c in tl) + " }",
+        f"    UNLIKE_COEFFICIENTS {{ {label} " + " ".join(_fmt(c) for c in tu) + " }",
+        "  }",
+        "}",
+    ])
+
+
 def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
     """RGAUSSIAN OLDQMC block: channels l=0, l=1 and the local channel (the
     reference treats the LAST listed channel as local, Pseudopotential.cpp:790).
@@ -164,7 +199,8 @@ def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
 
 def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | None = None,
              name: str | None = None, expansion=None, high_l: bool = False, jastrow: bool = True,
-             dup_basis: bool = False, mo_kind: str = "BLAS_MO") -> Deck:
+             dup_basis: bool = False, mo_kind: str = "BLAS_MO", aip: int = 12,
+             jastrow_variant: str | None = None) -> Deck:
     """Two-atom molecule of the all-electron (``pseudo=False``) or Z_eff=5
     pseudopotential (``pseudo=True``) workload.  ``method`` is an optional
     METHOD section body written into the deck (e.g. ``"VMC NBLOCK 50 ..."``).
@@ -195,7 +231,8 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
     cup = _random_orthonormal(rng, nb, nspin_mo)
     cdn = _random_orthonormal(rng, nb, nspin_mo)
     onebody = rng.normal(0.0, 0.1, size=4)
-    pp = _pseudo_text(rng, label, charge) if pseudo else ""
+    pp = _pseudo_text(rng, label, charge, aip=aip) if pseudo else ""
+    jtext = _jastrow_pade_spin_text(rng, label) if jastrow_variant == "pade_spin" else _jastrow_text(label, onebody)
     name = name or ("n2_pseudo" if pseudo else "n2_allelectron")
     orb = os.path.join(outdir, f"{name}.orb")
     _write_orb(orb, np.concatenate([cup, cdn], axis=1), [nper, nper])
@@ -226,7 +263,7 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
         f"    STATES {{ {states} }}",
         "  }" if jastrow else "",
         "  WF2 {" if jastrow else "",
-        _jastrow_text(label, onebody) if jastrow else "",
+        jtext if jastrow else "",
         "  }" if jastrow else "",
         "}",
         f"METHOD {{ {method} }}" if method else "",

@@ -371,6 +371,14 @@ def cutoff_cusp(r, cusp, gamma, rcut):
     return (np.where(inside, f, 0.0), np.where(inside, cusp * dadr, 0.0), np.where(inside, cusp * lap, 0.0))
 
 
+def pade(r, alpha):
+    """Pade_function::calcLap (Pade_function.cpp:128-184): f = (a r/(1+a r))^2,
+    f'/r = 2 a^2/(1+a r)^3, lap = 6 a^2/(1+a r)^4."""
+    p = 1.0 / (1.0 + alpha * r)
+    app = alpha * alpha * p * p
+    return app * r * r, 2.0 * app * p, 6.0 * app * p * p
+
+
 def poly_pade(r, beta, rcut):
     """Poly_pade_function::calcLap (Poly_pade_function.cpp:183-237) for one
     beta: returns (f, f'/r, lap)."""
@@ -409,6 +417,12 @@ class RadialSet:
             self.n = int(value(words, "NFUNC", conv=int))
             b1 = math.log(b0 + 1.00001)
             self.beta = [b0] + [math.exp(b1 + 1.6 * i) - 1 for i in range(1, self.n)]
+        elif t == "PADE":
+            # Pade_function::read (Pade_function.cpp:21-45): alpha_i = ALPHA0 / 2^i, no cutoff
+            a0 = value(words, "ALPHA0")
+            self.n = int(value(words, "NFUNC", conv=int))
+            self.alpha = [a0 / 2.0 ** i for i in range(self.n)]
+            self.rcut = 1e99
         else:
             raise NotImplementedError(t)
 
@@ -416,6 +430,8 @@ class RadialSet:
         """[..., n, 3] = (f, f'/r, lap)."""
         if self.kind == "CUTOFF_CUSP":
             return np.stack(cutoff_cusp(r, self.cusp, self.gamma, self.rcut), axis=-1)[..., None, :]
+        if self.kind == "PADE":
+            return np.stack([np.stack(pade(r, a), axis=-1) for a in self.alpha], axis=-2)
         return np.stack([np.stack(poly_pade(r, b, self.rcut), axis=-1) for b in self.beta], axis=-2)
 
 
@@ -532,6 +548,7 @@ class System:
     def _read_jastrow(self, w):
         assert w[0].upper() == "JASTROW2", w[0]
         self.groups = []
+        self._has3 = self._has3s = False
         for g in sections(w, "GROUP"):
             grp = {"ee": [RadialSet(b) for b in sections(g, "EEBASIS")],
                    "ei": [RadialSet(b) for b in sections(g, "EIBASIS")]}
@@ -545,10 +562,24 @@ class System:
             tb = section(g, "TWOBODY")
             if tb is not None:
                 grp["twobody"] = [float(x) for x in section(tb, "COEFFICIENTS")]
+            # THREEBODY, or THREEBODY_SPIN with like/unlike coefficients
+            # (Jastrow2_three_diffspin.cpp:130-186); SM_TERMS replaces the default list
             th = section(g, "THREEBODY")
-            if th is not None:
-                grp["threebody"] = {c[0]: [float(x) for x in c[1:]] for c in sections(th, "COEFFICIENTS")}
+            ths = section(g, "THREEBODY_SPIN")
+            self._has3 = getattr(self, "_has3", False) or th is not None
+            self._has3s = getattr(self, "_has3s", False) or ths is not None
+            if th is not None or ths is not None:
+                t = th if th is not None else ths
+                sc = float(value(t, "SCALE", 1.0))
+                like = sections(t, "COEFFICIENTS" if th is not None else "LIKE_COEFFICIENTS")
+                unlike = like if th is not None else sections(t, "UNLIKE_COEFFICIENTS")
+                grp["threebody"] = {c[0]: ([sc * float(x) for x in c[1:]], [sc * float(x) for x in u[1:]])
+                                    for c, u in zip(like, unlike)}
+                sm = section(t, "SM_TERMS")
+                if sm is not None:
+                    grp["klm"] = [(int(sm[i]), int(sm[i + 1]), int(sm[i + 2])) for i in range(0, len(sm), 3)]
             self.groups.append(grp)
+        self.tb_stale_ei = self._has3s and not self._has3
 
     # Pseudopotential (system/Pseudopotential.cpp:874-1033, Rgaussian_function.cpp)
     def _read_pseudo(self, pstexts):
@@ -653,8 +684,11 @@ class System:
             inv_all.append(Ainv)
         return logd, sign, g, l, inv_all, mo
 
-    def jastrow(self, R):
-        """U, per-electron grad U [nc,N,3], lap U [nc,N] (Jastrow2_wf.cpp:988-1221)."""
+    def jastrow(self, R, ei_stale=None):
+        """U, per-electron grad U [nc,N,3], lap U [nc,N] (Jastrow2_wf.cpp:988-1221).
+        ei_stale = (e, Re): the e-e-n terms take electron e's e-n basis values at
+        Re [nc,3] instead of at R[:, e] (the value-only update of the reference
+        with THREEBODY_SPIN; see nonlocal_pp)."""
         nc, N, _ = R.shape
         U = np.zeros(nc)
         G = np.zeros((nc, N, 3))
@@ -670,6 +704,20 @@ class System:
                     fs = [b.eval(r) for b in grp["ei"] if b.label == lab]
                     F = np.concatenate(fs, axis=-2) if fs else np.zeros((nc, N, 0, 3))
                     ei[a] = (F, d)
+                ei3 = ei
+                if ei_stale is not None and "threebody" in grp:
+                    e, Re = ei_stale
+                    ei3 = {}
+                    for a, lab in enumerate(self.labels):
+                        F, d = ei[a]
+                        F, d = F.copy(), d.copy()
+                        de = self.min_image(Re - self.atoms[a])    # [nc,3]
+                        re = np.sqrt(np.sum(de * de, axis=-1))
+                        fs = [b.eval(re) for b in grp["ei"] if b.label == lab]
+                        if fs:
+                            F[:, e] = np.concatenate(fs, axis=-2)
+                        d[:, e] = de
+                        ei3[a] = (F, d)
             if "onebody" in grp:
                 for a, lab in enumerate(self.labels):
                     cf = np.array(grp["onebody"][lab])
@@ -704,18 +752,20 @@ class System:
                     np.add.at(L, (slice(None), iu), lp)
                     np.add.at(L, (slice(None), ju), lp)
                 if "threebody" in grp:
-                    self._threebody(grp, R, ei, E, d, iu, ju, U, G, L)
+                    self._threebody(grp, R, ei3, E, d, iu, ju, spin[iu] == spin[ju], U, G, L)
         return U, G, L
 
-    def _threebody(self, grp, R, ei, E, dij, iu, ju, U, G, L):
+    def _threebody(self, grp, R, ei, E, dij, iu, ju, same, U, G, L):
         """e-e-n term sum_at sum_{i<j} sum_p c_p (a_k(i)a_l(j)+a_l(i)a_k(j)) b_m(ij)
-        (Jastrow2_three.cpp:138-404, default klm table :30-46)."""
-        klm = [(1, 1, 0), (1, 0, 1), (1, 1, 1), (2, 2, 0), (2, 0, 1), (2, 0, 2), (2, 2, 2), (3, 3, 0),
-               (3, 0, 2), (3, 3, 2), (1, 2, 2), (2, 3, 2)]
+        (Jastrow2_three.cpp:138-404, default klm table :30-46); c_p is the like
+        or unlike coefficient by the pair's spins (THREEBODY_SPIN)."""
+        klm = grp.get("klm") or [(1, 1, 0), (1, 0, 1), (1, 1, 1), (2, 2, 0), (2, 0, 1), (2, 0, 2), (2, 2, 2),
+                                 (3, 3, 0), (3, 0, 2), (3, 3, 2), (1, 2, 2), (2, 3, 2)]
         for a, lab in enumerate(self.labels):
-            cfs = grp["threebody"][lab]
+            cl, cu = grp["threebody"][lab]
             F, dia = ei[a]                         # F [nc,N,k,3], dia [nc,N,3]
-            for p, c in enumerate(cfs):
+            for p in range(len(cl)):
+                c = np.where(same, cl[p], cu[p])   # [P]
                 k, l, m = klm[p]
                 ak = F[..., k, :]                  # [nc,N,3] (f, f'/r, lap)
                 al = F[..., l, :]
@@ -724,7 +774,7 @@ class System:
                 aki, akj = ak[:, iu, 0], ak[:, ju, 0]
                 ali, alj = al[:, iu, 0], al[:, ju, 0]
                 s = aki * alj + ali * akj          # [nc,P]
-                U += c * np.sum(s * b[..., 0], axis=1)
+                U += np.sum(c * s * b[..., 0], axis=1)
                 # gradients of a at i and j (vectors)
                 gki = ak[:, iu, 1:2] * dia[:, iu]
                 gkj = ak[:, ju, 1:2] * dia[:, ju]
@@ -733,8 +783,8 @@ class System:
                 gs_i = gki * alj[..., None] + gli * akj[..., None]     # d s / d r_i
                 gs_j = aki[..., None] * glj + ali[..., None] * gkj     # d s / d r_j
                 gb = b[..., 1:2] * dij                                  # d b / d r_i (= -d b/ d r_j)
-                gi = c * (gs_i * b[..., 0:1] + s[..., None] * gb)
-                gj = c * (gs_j * b[..., 0:1] - s[..., None] * gb)
+                gi = c[:, None] * (gs_i * b[..., 0:1] + s[..., None] * gb)
+                gj = c[:, None] * (gs_j * b[..., 0:1] - s[..., None] * gb)
                 lsi = ak[:, iu, 2] * alj + al[:, iu, 2] * akj
                 lsj = aki * al[:, ju, 2] + ali * ak[:, ju, 2]
                 li = c * (lsi * b[..., 0] + s * b[..., 2] + 2 * np.sum(gs_i * gb, axis=-1))
@@ -756,10 +806,10 @@ class System:
                "potential": self.ewald(R) if self.periodic else self.coulomb(R)}
         return out
 
-    def logpsi(self, R):
+    def logpsi(self, R, ei_stale=None):
         R = self.wrap(np.asarray(R, dtype=float))
         logd, sign, *_ = self.slater(R)
-        U, _, _ = self.jastrow(R)
+        U, _, _ = self.jastrow(R, ei_stale)
         return logd + U, sign
 
     def coulomb(self, R):
@@ -803,7 +853,12 @@ class System:
                     # move relative to the nearest image of the atom
                     Rn[:, e] = R[:, e] + q[:, iq] * r[:, e:e + 1] - d[:, e]
                     kd = self._wrap_kphase(Rn[:, e])
-                    lp, sg = self.logpsi(Rn)
+                    # with THREEBODY_SPIN and no plain THREEBODY group, the
+                    # reference's value-only Jastrow update (Jastrow2_wf::updateVal,
+                    # Jastrow2_wf.cpp:877-882, 931-936) does not refresh the moved
+                    # electron's saved e-n basis, so its e-e-n terms see electron
+                    # e's e-n values at its current position
+                    lp, sg = self.logpsi(Rn, (e, R[:, e]) if self.tb_stale_ei else None)
                     ratio = np.exp(lp - lp0) * self._point_sign(sg, sg0, kd) * p["w"][iq]
                     cosq = np.sum(q[:, iq] * d[:, e], axis=-1) / r[:, e]
                     ts = np.zeros(nc)
@@ -1093,7 +1148,7 @@ def legendre(x, l):
 
 
 def gesqua(aip):
-    """Quadrature points/weights (system/gesqua.cpp:32-120) for AIP 4, 6, 12."""
+    """Quadrature points/weights (system/gesqua.cpp:32-320) for AIP 4, 6, 12, 18, 26, 32."""
     if aip < 6:
         q = 1.0 / math.sqrt(3.0)
         pts = np.array([[q, q, q], [q, -q, -q], [-q, q, -q], [-q, -q, q]])
@@ -1101,12 +1156,39 @@ def gesqua(aip):
     if aip < 12:
         pts = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], dtype=float)
         return pts, np.full(6, 1.0 / 6.0)
-    fi0 = math.pi / 5.0
-    c, s = 1.0 / math.sqrt(5.0), 2.0 / math.sqrt(5.0)
-    pts = np.zeros((12, 3))
+    if aip < 18:
+        fi0 = math.pi / 5.0
+        c, s = 1.0 / math.sqrt(5.0), 2.0 / math.sqrt(5.0)
+        pts = np.zeros((12, 3))
+        pts[0, 2], pts[1, 2] = 1.0, -1.0
+        for i in range(5):
+            rk2 = 2 * i
+            pts[i + 2] = [s * math.cos(rk2 * fi0), s * math.sin(rk2 * fi0), c]
+            pts[i + 7] = [s * math.cos((rk2 + 1) * fi0), s * math.sin((rk2 + 1) * fi0), -c]
+        return pts, np.full(12, 1.0 / 12.0)
+    if aip < 32:
+        # gesqua.cpp:121-273: octahedron vertices, edge midpoints, (26) cube vertices
+        h, b = 1.0 / math.sqrt(2.0), 1.0 / math.sqrt(3.0)
+        pts = [[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+               [h, h, 0], [-h, h, 0], [h, -h, 0], [-h, -h, 0],
+               [h, 0, h], [-h, 0, h], [h, 0, -h], [-h, 0, -h],
+               [0, h, h], [0, h, -h], [0, -h, h], [0, -h, -h]]
+        if aip < 26:
+            return np.array(pts, float), np.array([1.0 / 30.0] * 6 + [1.0 / 15.0] * 12)
+        pts += [[sx * b, sy * b, sz * b] for sx in (1, -1) for sz in (1, -1) for sy in (1, -1)]
+        return np.array(pts, float), np.array([40.0 / 840.0] * 6 + [32.0 / 840.0] * 12 + [27.0 / 840.0] * 8)
+    assert aip == 32, aip
+    # gesqua.cpp:274-320: icosahedron + dodecahedron vertices
+    t5 = math.sqrt(15.0 + 6.0 * math.sqrt(5.0))
+    th1, th2 = math.acos((2.0 + math.sqrt(5.0)) / t5), math.acos(1.0 / t5)
+    pts = np.zeros((32, 3))
     pts[0, 2], pts[1, 2] = 1.0, -1.0
+
+    def sph(th, ph):
+        return [math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)]
     for i in range(5):
-        rk2 = 2 * i
-        pts[i + 2] = [s * math.cos(rk2 * fi0), s * math.sin(rk2 * fi0), c]
-        pts[i + 7] = [s * math.cos((rk2 + 1) * fi0), s * math.sin((rk2 + 1) * fi0), -c]
-    return pts, np.full(12, 1.0 / 12.0)
+        ev, od = 2 * i * math.pi / 5, (2 * i + 1) * math.pi / 5
+        pts[i + 2], pts[i + 7] = sph(math.atan(2.0), ev), sph(math.pi - math.atan(2.0), od)
+        pts[i + 12], pts[i + 17] = sph(th1, od), sph(th2, od)
+        pts[i + 22], pts[i + 27] = sph(math.pi - th1, ev), sph(math.pi - th2, ev)
+    return pts, np.array([5.0 / 168.0] * 12 + [27.0 / 840.0] * 20)

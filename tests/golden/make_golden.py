@@ -49,7 +49,12 @@ WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseu
              # the CUTOFF_MO evaluator: a molecule and a complex k-point cell
              ("n2_cutoff", dict(pseudo=True, mo_kind="CUTOFF_MO"), 23),
              ("diamond8_kc", dict(periodic=True, kpoint=(0.5, 0.25, 0.0), complex_orbitals=True,
-                                  mo_kind="CUTOFF_MO"), 24)]
+                                  mo_kind="CUTOFF_MO"), 24),
+             # PADE Jastrow basis, THREEBODY_SPIN on SM_TERMS, 18-point quadrature
+             ("n2_jas", dict(pseudo=True, jastrow_variant="pade_spin", aip=18), 25),
+             # the 26- and 32-point quadratures
+             ("n2_aip26", dict(pseudo=True, aip=26), 26),
+             ("n2_aip32", dict(pseudo=True, aip=32), 27)]
 
 
 def make(name, kw, seed):
@@ -64,7 +69,7 @@ def make(name, kw, seed):
         nconf = 64 if kw["nelec"] < 64 else 32
     else:
         deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
-        nconf = NCONF if not ({"expansion", "high_l", "jastrow", "mo_kind"} & set(kw)) else 64
+        nconf = NCONF if not ({"expansion", "high_l", "jastrow", "mo_kind", "aip"} & set(kw)) else 64
     R = systems.random_configs(deck, nconf, seed=seed + 1000)
     NCONF_ = nconf
     rng = np.random.default_rng(seed + 2000)
