@@ -205,15 +205,22 @@ int qwg_dmc_block_ready(qwg_ctx* ctx);
  * and the block accumulators live in one file-scope device array of
  * QWG_NOALLOC_SCRATCH_BYTES (16 MiB) that every GPU loading the library holds
  * until the process exits.  nw * (per-walker state bytes) + 256 must fit in
- * it, else QWG_ERR_ARG (qwg_last_error names the largest nw that fits).
+ * it; systems with more than 32 orbitals per spin keep their per-walker
+ * scratch there too, so for them nw * (state + scratch bytes) + 256 must fit.
+ * Otherwise QWG_ERR_ARG (qwg_last_error names the largest nw that fits).
  * Buffers are the caller's device memory, ordered on the context's stream:
  *   d_R       [nw][nelec][3] walker positions, read and overwritten
  *   d_energy  [nw] local energy of each walker after the last step (or NULL)
  *   d_sums    [10] block sums: sum w, sum wE, sum wT, sum wV, sum wV_NL,
  *             sum wE^2, accepted moves, attempted moves, non-finite, points
  * The first call on a device looks up that device's address of the array
- * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  All calls share the one array and it keeps the
+ * (cudaGetSymbolAddress, with that device current) and keeps it for the rest
+ * of the process; make that first call before any stream capture.  A
+ * cudaDeviceReset by the host invalidates the kept address: do not call this
+ * entry point again on a device after resetting it.  These calls count their
+ * own steps for the random streams (a separate counter from qwg_vmc_block and
+ * the DMC calls), so they do not shift the streams or the refresh schedule of
+ * the context's regular walkers.  All calls share the one array and it keeps the
  * last call's contents: the accumulators are cleared on every call, and calls
  * whose work overlaps on the GPU (other streams, other contexts) race on it. */
 #define QWG_NOALLOC_SCRATCH_BYTES (16u << 20)

@@ -298,7 +298,7 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     S.pp_cutoff[t] = P.cutoff;
     if (P.nchan > 5) throw InputError("pseudopotential channels beyond l=3 are not supported");
     if ((int)P.term_n.size() > QWG_MAXPPT) throw InputError("more than 16 pseudopotential terms on one atom");
-    if (P.aip > QWG_MAXQ) throw InputError("quadratures above 12 points are not supported");
+    if (P.aip > QWG_MAXQ) throw InputError("quadratures above 32 points are not supported");
     for (int l = 0; l <= P.nchan && P.nchan; l++) S.pp_term_first[t][l] = P.term_first[l];
     for (size_t n = 0; n < P.term_n.size(); n++) {
       S.pp_term[t][n][0] = P.term_n[n];
@@ -1333,7 +1333,7 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
     P.deterministic_pp = deterministic_pp;
     P.tau = timestep;
     P.seed = seed;
-    P.step0 = c->step_counter;
+    P.step0 = c->noalloc_step_counter;
     P.max_weight = 1.0;
     P.R = d_R;
     P.state = base + acc_bytes;
@@ -1344,7 +1344,7 @@ int qwg_vmc_block_noalloc(qwg_ctx* c, double* d_R, int nw, int nstep, double tim
     io.energy = d_energy;
     launch_steps(c, P, io, nw);
     CK(cudaMemcpyAsync(d_sums, acc, 10 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    c->step_counter += nstep;
+    c->noalloc_step_counter += nstep;
     return QWG_OK;
   });
 }
