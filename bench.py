@@ -36,6 +36,40 @@ FEEDBACK_INTERVAL = 5
 SEED = 20261203
 
 
+FP32_SPEC_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+ATOMS = np.array([[0.0, 0.0, -1.0375], [0.0, 0.0, 1.0375]])
+
+
+def _tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        if "bf16_tflops" in d:
+            return d["bf16_tflops"], "measured (cuBLAS bf16 burst)"
+    return 1590.0, "fallback"
+
+
+def move_flops_per_walker(N, M, nb, natoms, k_ee, k_en):
+    """Algorithmic flops of one sweep of N single-electron moves: MO value,
+    gradient and Laplacian (N*5*nb*M*2), ratio and gradient/Laplacian dots
+    (N*5*M*2), Sherman-Morrison updates (N*4*M^2) and the Jastrow of the moved
+    electron (N*((N-1)*k_ee + A*k_en)*12*5)."""
+    return N * 5 * nb * M * 2 + N * 5 * M * 2 + N * 4 * M * M + N * ((N - 1) * k_ee + natoms * k_en) * 60
+
+
+def pp_flops_per_walker(npairs, N, M, nb, natoms, k_ee, k_en, nq=12):
+    """Algorithmic flops of the nonlocal pseudopotential quadrature: per
+    (electron, atom) pair inside the cutoff, nq ratio evaluations (MO values,
+    determinant ratio, Jastrow value)."""
+    return npairs * nq * (nb * M * 2 + 2 * M + 12 * (N * k_ee + natoms * k_en))
+
+
+def pp_pairs(R, atoms, cut):
+    """Mean number of (electron, atom) pairs inside the pseudopotential cutoff."""
+    d = np.linalg.norm(R[:, :, None, :] - atoms[None, None], axis=-1)
+    return float(np.mean(np.sum(d < cut, axis=(1, 2))))
+
+
 def _peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -170,30 +204,87 @@ def run_engine(args, rank, world):
             energies.append(s2["energy"])
         results[label] = {"ms": ms, "steps": steps, "stats": st, "launches": launches, "clocks": cs.summary(),
                           "lat": lat, "energies": energies, "kernel_ms": st["block_ms"], "sweep_ms": sweep_ms,
-                          "eloc_ms": eloc_ms}
+                          "eloc_ms": eloc_ms, "R": E.get_walkers()}
         E.close()
-    # end-to-end through the C-ABI with host buffers: upload walkers, run the
-    # block, download walkers + statistics, every step amortised
-    E = engine.Engine(deck.path, engine.MIXED, max_walkers=NWALK, stream=stream.cuda_stream)
+    # end-to-end through the C-ABI with host buffers: upload walkers from
+    # pinned host memory, run the block, download walkers + statistics
+    e2e = {}
+    for label, prec in arms:
+        e2e[label] = _e2e_block(engine, deck, R0, prec, results[label]["steps"], stream, dev)
+    corr = correlated_mixed_vs_fp64(engine, deck, R0, stream) if args.precision == "both" else None
+    return results, e2e, corr, deck
+
+
+def _e2e_block(engine, deck, R0, prec, steps, stream, dev):
+    import torch
+    E = engine.Engine(deck.path, prec, max_walkers=NWALK, stream=stream.cuda_stream)
     E.set_walkers(R0)
     E.vmc_block(20, 0.3, seed=SEED)
-    steps = results["mixed"]["steps"]
     E.dmc_init(timestep=TAU, nstep=steps, seed=SEED + 5)
     E.dmc_block()
     Rh = E.get_walkers()
     Rpinned = torch.from_numpy(Rh).pin_memory().numpy()
     torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     E.set_walkers(Rpinned)
     E.dmc_init(timestep=TAU, nstep=steps, seed=SEED + 6)
-    st = E.dmc_block()
-    Rout = E.get_walkers()
+    E.dmc_block()
+    E.get_walkers()
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = e0.elapsed_time(e1)
+    ms = e0.elapsed_time(e1)
     E.close()
-    return results, e2e_ms, steps, deck
+    return ms
+
+
+def correlated_mixed_vs_fp64(engine, deck, R0, stream, nblock=10, nstep=20):
+    """Mixed minus FP64 DMC energy with common random numbers: both contexts
+    start from the same equilibrated walkers with the same seed, so their
+    walks coincide until a decision (an acceptance or a branch pairing)
+    falls inside the precision difference.  Reports the per-block energy
+    difference (mean and standard error over blocks) and the bias of the
+    mixed local-energy estimator on the mixed run's final walkers (the same
+    configurations and quadrature rotation evaluated in both precisions)."""
+    F = engine.Engine(deck.path, engine.FP64, max_walkers=NWALK, stream=stream.cuda_stream)
+    F.set_walkers(R0)
+    for b in range(3):
+        F.vmc_block(20, 0.3, seed=SEED + 31 * b)
+    Req = F.get_walkers()
+    energies = {}
+    Rfinal = None
+    for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
+        E = F if label == "fp64" else engine.Engine(deck.path, prec, max_walkers=NWALK, stream=stream.cuda_stream)
+        E.set_walkers(Req)
+        E.dmc_init(timestep=TAU, nstep=nstep, seed=SEED + 77)
+        energies[label] = np.array([E.dmc_block()["energy"] for _ in range(nblock)])
+        if label == "mixed":
+            Rfinal = E.get_walkers()
+            E.close()
+    d = (energies["mixed"] - energies["fp64"]) * 1e3
+    rng = np.random.default_rng(5)
+    rot = np.stack([_rotation(rng) for _ in range(NWALK)])
+    M = engine.Engine(deck.path, engine.MIXED, max_walkers=NWALK, stream=stream.cuda_stream)
+    M.set_walkers(Rfinal)
+    em = M.eval(rot).energy
+    M.close()
+    F.set_walkers(Rfinal)
+    ef = F.eval(rot).energy
+    F.close()
+    de = (em - ef) * 1e3
+    return {"block_difference_mHa": {"mean": float(np.mean(d)), "sem": float(np.std(d, ddof=1) / np.sqrt(len(d))),
+                                     "per_block": [round(float(x), 4) for x in d]},
+            "estimator_bias_mHa": {"mean": float(np.mean(de)), "sem": float(np.std(de, ddof=1) / np.sqrt(len(de))),
+                                   "median_abs": float(np.median(np.abs(de)))},
+            "blocks": nblock, "steps_per_block": nstep, "walkers": NWALK}
+
+
+def _rotation(rng):
+    q = rng.standard_normal(4)
+    a, b, c, d = q / np.linalg.norm(q)
+    return np.array([[a * a + b * b - c * c - d * d, 2 * (b * c - a * d), 2 * (b * d + a * c)],
+                     [2 * (b * c + a * d), a * a - b * b + c * c - d * d, 2 * (c * d - a * b)],
+                     [2 * (b * d - a * c), 2 * (c * d + a * b), a * a - b * b - c * c + d * d]])
 
 
 def run_extras(stream, dev, seconds=30.0):
@@ -284,11 +375,32 @@ def run_extras(stream, dev, seconds=30.0):
     return out
 
 
-def cpu_reference(deck_path, seconds_target=20.0, cores=None):
+def pp_cutoff(deck_text):
+    """Radius beyond which every nonlocal channel of the deck's RGAUSSIAN
+    OLDQMC pseudopotential is below 1e-5 (the scan of Pseudopotential::read:
+    from 20 bohr down in 0.05 steps)."""
+    body = re.search(r"OLDQMC\s*\{([^}]*)\}", deck_text).group(1).split()
+    nl = int(body[1])
+    nper = [int(x) for x in body[2:2 + nl]]
+    terms, it = [], 2 + nl
+    for n in nper:
+        terms.append([(int(float(body[it + 3 * j])) - 2, float(body[it + 3 * j + 1]), float(body[it + 3 * j + 2]))
+                      for j in range(n)])
+        it += 3 * n
+    r = 20.0
+    while r > 0:
+        if any(abs(sum(c * r ** k * np.exp(-a * r * r) for k, a, c in ch)) > 1e-5 for ch in terms[:-1]):
+            return r
+        r -= 0.05
+    return 0.0
+
+
+def cpu_reference(deck_path, repeats=3, short_blocks=1, long_blocks=9, cores=None):
     """Reference qwalk (oracle/_ref/qwalk-Linux, shipped -O3 -ffast-math flags)
     on the host cores: one process per core, DMC on the same deck.  Per-block
-    cost from the difference of a 1-block and a 3-block run (removes start-up
-    and the reference's own VMC warm-up)."""
+    cost from the difference of a short and a long run (removes start-up and
+    the reference's own configuration generation); the pair is repeated and
+    the median rate reported with the spread."""
     qw = os.path.join(ROOT, "oracle", "_ref", "qwalk-Linux")
     if not os.path.exists(qw):
         return None
@@ -297,12 +409,12 @@ def cpu_reference(deck_path, seconds_target=20.0, cores=None):
     base = open(deck_path).read()
     d = os.path.dirname(deck_path)
 
-    def run(nblock):
+    def run(nblock, rep):
         procs = []
         t0 = time.perf_counter()
         for p in range(cores):
-            path = os.path.join(d, f"cpu_{nblock}_{p}.qw")
-            txt = re.sub(r"RANDOMSEED\s*\{[^}]*\}", f"RANDOMSEED {{ {101 + p} {203 + p} }}", base)
+            path = os.path.join(d, f"cpu_{rep}_{nblock}_{p}.qw")
+            txt = re.sub(r"RANDOMSEED\s*\{[^}]*\}", f"RANDOMSEED {{ {101 + p + 1000 * rep} {203 + p} }}", base)
             txt += (f"\nMETHOD {{ DMC NCONFIG {nconf} NBLOCK {nblock} NSTEP {nstep} TIMESTEP {TAU} }}\n")
             open(path, "w").write(txt)
             procs.append(subprocess.Popen([qw, os.path.basename(path)], cwd=d, stdout=subprocess.DEVNULL,
@@ -311,13 +423,18 @@ def cpu_reference(deck_path, seconds_target=20.0, cores=None):
             p.wait()
         return time.perf_counter() - t0
 
-    t1 = run(1)
-    t3 = run(3)
-    per_block = max((t3 - t1) / 2.0, 1e-6)
-    ws = cores * nconf * nstep / per_block
-    return {"value": ws, "unit": "walker-steps/s", "cores": cores, "kind": "reference",
-            "sample": f"{cores} qwalk processes x {nconf} walkers x {nstep} DMC steps/block; "
-                      f"per-block time from 3-block minus 1-block wall ({t3:.1f}s - {t1:.1f}s)"}
+    rates, walls = [], []
+    for rep in range(repeats):
+        ts, tl = run(short_blocks, rep), run(long_blocks, rep)
+        per_block = max((tl - ts) / (long_blocks - short_blocks), 1e-6)
+        rates.append(cores * nconf * nstep / per_block)
+        walls.append((round(ts, 1), round(tl, 1)))
+    return {"value": float(np.median(rates)), "unit": "walker-steps/s", "cores": cores, "kind": "reference",
+            "repeats": [float(r) for r in rates],
+            "spread": float((max(rates) - min(rates)) / np.median(rates)),
+            "sample": f"{cores} qwalk processes x {nconf} walkers x {nstep} DMC steps/block; per-block time from "
+                      f"{long_blocks}-block minus {short_blocks}-block wall, {repeats} repeats (walls s: {walls}); "
+                      "median reported"}
 
 
 def main():
@@ -360,7 +477,7 @@ def main():
         from datetime import timedelta
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    results, e2e_ms, steps, deck = run_engine(args, rank, world)
+    results, e2e, corr, deck = run_engine(args, rank, world)
     if args.precision != "both":  # profiling run: no report line
         if world > 1:
             import torch.distributed as dist
@@ -368,8 +485,9 @@ def main():
         return
     mx = results["mixed"]
     fp = results["fp64"]
+    steps = mx["steps"]
     # max over ranks of the device times (every rank takes part)
-    ms, ms64, e2e_ms = max_over_ranks([mx["ms"], fp["ms"], e2e_ms], "cuda")
+    ms, ms64, e2e_ms, e2e64_ms = max_over_ranks([mx["ms"], fp["ms"], e2e["mixed"], e2e["fp64"]], "cuda")
     ws = aggregate_rate(NWALK * steps, world, ms)
     ws64 = aggregate_rate(NWALK * fp["steps"], world, ms64)
     if rank != 0:
@@ -387,26 +505,40 @@ def main():
     dom = max(kern, key=lambda k: kern[k][0])
     kern_ms_per_launch, bytes_launch = kern[dom]
     achieved = bytes_launch / (kern_ms_per_launch / 1e3) / 1e9
+    flops = move_flops_per_walker(N, M, nb, natoms=2, k_ee=1, k_en=4)
+    pcut = pp_cutoff(open(deck.path).read())
+    npairs = pp_pairs(results["mixed"]["R"], ATOMS, pcut)
+    pp_flops = pp_flops_per_walker(npairs, N, M, nb, natoms=2, k_ee=1, k_en=4)
+    tflops_peak, tsrc = _tensor_peak()
     lat = np.array(mx["lat"])
+    e2e_h2d = NWALK * N * 3 * 8 / steps
+    e2e_d2h = (NWALK * N * 3 * 8 + 96) / steps
     line = {
-        "metric": "DMC walker-steps/s (mixed precision engine; FP64 beside it)",
+        "metric": "DMC walker-steps/s",
         "value": ws, "unit": "walker-steps/s", "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32/f64 mixed (FP64 refresh, energies, weights)", "data": "synthetic (seeded QWalk deck)",
+        "precision": "mixed (the FP64 arm is the fp64 object)",
         "config": {"workload": "n2_pseudo DMC: 2 Z_eff=5 atoms, 14 electrons, 80 basis fns, 12-pt quadrature",
                    "walkers_per_gpu": NWALK, "tau": TAU, "feedback_interval": FEEDBACK_INTERVAL,
+                   "basis_exponents": "log-uniform in [0.1, 10] (valence range); the configuration text's "
+                                      "[0.1, 1e4] is the all-electron range, with which the reference's own DMC "
+                                      "diverges on the random-orbital trial function",
                    "parallelism": f"replicas x{world}", "l2": "walker state resident (working set < L2); "
                    "256 MiB buffer written before the timed block"},
         "fp64": {"value": ws64, "unit": "walker-steps/s", "ms_per_step": ms64 / fp["steps"],
+                 "e2e": {"value": aggregate_rate(NWALK * steps, world, e2e64_ms), "unit": "walker-steps/s",
+                         "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h},
                  "block_energy_mean": float(np.mean(fp["energies"])),
                  "block_energy_sem": float(np.std(fp["energies"]) / np.sqrt(len(fp["energies"])))},
         "mixed_vs_fp64": ws / ws64,
         "mixed_block_energy": {"mean": float(np.mean(mx["energies"])),
                                "sem": float(np.std(mx["energies"]) / np.sqrt(len(mx["energies"])))},
+        "mixed_minus_fp64_mHa": corr,
         "block_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                              "steps_per_block": 20, "walkers": NWALK},
         "e2e": {"value": aggregate_rate(NWALK * steps, world, e2e_ms), "unit": "walker-steps/s",
-                "h2d_bytes_per_step": NWALK * N * 3 * 8 / steps, "d2h_bytes_per_step": (NWALK * N * 3 * 8 + 96) / steps},
+                "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": src, "traffic": _traffic_per_launch(dom),
                      "kernel": {"sweep": "k_walkers<float,8,KM_SWEEP>", "eloc": "k_walkers<float,8,KM_ELOC>"}[dom],
@@ -414,9 +546,24 @@ def main():
                      "algorithmic_bytes_per_launch": bytes_launch,
                      "note": "per launch every walker's resident state is read (and, for the move kernel, "
                              "written) once; the state fits L2, so the kernel is latency/issue-bound, not HBM-bound"},
+        "roofline_compute": {
+            "sweep": {"algorithmic_flops_per_launch": NWALK * flops,
+                      "achieved_tflops": NWALK * flops / (mx["sweep_ms"] / 1e3) / 1e12},
+            "eloc": {"algorithmic_flops_per_launch": NWALK * pp_flops, "pp_pairs_per_walker": npairs,
+                     "pp_cutoff_bohr": pcut, "achieved_tflops": NWALK * pp_flops / (mx["eloc_ms"] / 1e3) / 1e12},
+            "tensor_peak_tflops": tflops_peak, "tensor_peak_source": tsrc,
+            "fp32_cuda_core_peak_tflops": FP32_SPEC_TFLOPS,
+            "fp32_peak_source": "spec arithmetic (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz), not measured",
+            "note": "flops from the per-walker-step formulas of the path (MO products, ratios, Sherman-Morrison, "
+                    "Jastrow; pseudopotential quadrature with the measured pair count); the kernels issue their "
+                    "work on CUDA cores and are issue-bound (ncu issue slots ~48% / 34% busy)"},
         "gpu_launches": mx["launches"],
         "clocks": mx["clocks"],
     }
+    for k in ("sweep", "eloc"):
+        a = line["roofline_compute"][k]["achieved_tflops"]
+        line["roofline_compute"][k]["frac_of_tensor_peak"] = a / tflops_peak
+        line["roofline_compute"][k]["frac_of_fp32_peak"] = a / FP32_SPEC_TFLOPS
     if not args.no_extras and world == 1:
         import torch
         dev = torch.device("cuda", 0)
