@@ -238,45 +238,59 @@ def _e2e_block(engine, deck, R0, prec, steps, stream, dev):
     return ms
 
 
-def correlated_mixed_vs_fp64(engine, deck, R0, stream, nblock=10, nstep=20):
-    """Mixed minus FP64 DMC energy with common random numbers: both contexts
-    start from the same equilibrated walkers with the same seed, so their
-    walks coincide until a decision (an acceptance or a branch pairing)
-    falls inside the precision difference.  Reports the per-block energy
-    difference (mean and standard error over blocks) and the bias of the
-    mixed local-energy estimator on the mixed run's final walkers (the same
-    configurations and quadrature rotation evaluated in both precisions)."""
-    F = engine.Engine(deck.path, engine.FP64, max_walkers=NWALK, stream=stream.cuda_stream)
-    F.set_walkers(R0)
-    for b in range(3):
-        F.vmc_block(20, 0.3, seed=SEED + 31 * b)
-    Req = F.get_walkers()
+def correlated_mixed_vs_fp64(engine, deck, R0, stream, nblock=40, nstep=40):
+    """Mixed minus FP64 DMC energy at equal statistics.
+
+    (1) Common random numbers on the low-variance H4 pseudo-atom chain
+    (tests/golden/h4pp.qw, RHF orbitals, tau=0.05): both contexts start from
+    the same walkers with the same seed, so their walks coincide except where
+    a decision falls inside the precision difference; the per-block energy
+    difference (mean and standard error over blocks) is the precision bias.
+    (2) On the headline molecule, whose random-orbital walks part within a
+    block, the bias of the mixed local-energy estimator: the same
+    configurations (the mixed run's walkers) and quadrature rotation
+    evaluated in both precisions."""
+    from mainline_b200 import systems
+    h4 = os.path.join(ROOT, "tests", "golden", "h4pp.qw")
+    Rh = systems.random_configs(systems.read_deck(h4), NWALK, seed=SEED % 1000)
     energies = {}
-    Rfinal = None
     for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
-        E = F if label == "fp64" else engine.Engine(deck.path, prec, max_walkers=NWALK, stream=stream.cuda_stream)
-        E.set_walkers(Req)
-        E.dmc_init(timestep=TAU, nstep=nstep, seed=SEED + 77)
+        E = engine.Engine(h4, prec, max_walkers=NWALK, stream=stream.cuda_stream)
+        E.set_walkers(Rh)
+        for b in range(5):
+            E.vmc_block(20, 0.5, seed=SEED + b)
+        E.dmc_init(timestep=0.05, nstep=nstep, seed=SEED + 77)
+        for _ in range(5):
+            E.dmc_block()
         energies[label] = np.array([E.dmc_block()["energy"] for _ in range(nblock)])
-        if label == "mixed":
-            Rfinal = E.get_walkers()
-            E.close()
+        E.close()
     d = (energies["mixed"] - energies["fp64"]) * 1e3
+    # estimator bias on the headline workload
+    M = engine.Engine(deck.path, engine.MIXED, max_walkers=NWALK, stream=stream.cuda_stream)
+    M.set_walkers(R0)
+    for b in range(3):
+        M.vmc_block(20, 0.3, seed=SEED + 31 * b)
+    M.dmc_init(timestep=TAU, nstep=20, seed=SEED + 78)
+    M.dmc_block()
+    Rfinal = M.get_walkers()
     rng = np.random.default_rng(5)
     rot = np.stack([_rotation(rng) for _ in range(NWALK)])
-    M = engine.Engine(deck.path, engine.MIXED, max_walkers=NWALK, stream=stream.cuda_stream)
     M.set_walkers(Rfinal)
     em = M.eval(rot).energy
     M.close()
+    F = engine.Engine(deck.path, engine.FP64, max_walkers=NWALK, stream=stream.cuda_stream)
     F.set_walkers(Rfinal)
     ef = F.eval(rot).energy
     F.close()
     de = (em - ef) * 1e3
-    return {"block_difference_mHa": {"mean": float(np.mean(d)), "sem": float(np.std(d, ddof=1) / np.sqrt(len(d))),
-                                     "per_block": [round(float(x), 4) for x in d]},
-            "estimator_bias_mHa": {"mean": float(np.mean(de)), "sem": float(np.std(de, ddof=1) / np.sqrt(len(de))),
-                                   "median_abs": float(np.median(np.abs(de)))},
-            "blocks": nblock, "steps_per_block": nstep, "walkers": NWALK}
+    return {"common_random_numbers": {
+                "workload": "h4pp: 4 H pseudo-atoms, 4 electrons, RHF orbitals, DMC tau=0.05",
+                "mean": float(np.mean(d)), "sem": float(np.std(d, ddof=1) / np.sqrt(len(d))),
+                "blocks": nblock, "steps_per_block": nstep, "walkers": NWALK,
+                "fp64_energy": float(np.mean(energies["fp64"])), "mixed_energy": float(np.mean(energies["mixed"]))},
+            "estimator_bias_headline": {"mean": float(np.mean(de)),
+                                        "sem": float(np.std(de, ddof=1) / np.sqrt(len(de))),
+                                        "median_abs": float(np.median(np.abs(de))), "walkers": NWALK}}
 
 
 def _rotation(rng):

@@ -77,3 +77,26 @@ def test_dmc_energy_matches_reference(precision):
     assert all(0.9 < s["acceptance"] <= 1.0 for s in st)
     mean, err = reblock(en)
     _check("DMC tau=0.05 " + ("fp64" if precision == engine.FP64 else "mixed"), mean, err, r)
+
+
+def test_dmc_mixed_within_0p1_mHa_of_fp64():
+    """Mixed minus FP64 DMC energy with common random numbers: both start
+    from the same walkers with the same seed, so the walks coincide except
+    where a decision falls inside the precision difference, and the
+    per-block difference measures the precision bias directly."""
+    r = REF["dmc_tau0.05"]
+    R0 = _walkers(13)
+    en = {}
+    for prec in (engine.FP64, engine.MIXED):
+        E = engine.Engine(DECK, prec, max_walkers=NW)
+        E.set_walkers(R0)
+        for b in range(5):
+            E.vmc_block(20, 0.5, seed=300 + b)
+        E.dmc_init(timestep=r["timestep"], nstep=r["steps_per_block"], seed=91)
+        en[prec] = np.array([E.dmc_block()["energy"] for _ in range(60)])
+        E.close()
+    d = (en[engine.MIXED] - en[engine.FP64]) * 1e3
+    mean, sem = float(np.mean(d)), float(np.std(d, ddof=1) / np.sqrt(len(d)))
+    print(f"MIXED_MINUS_FP64 DMC tau=0.05: {mean:+.5f} +- {sem:.5f} mHa over {len(d)} blocks")
+    assert sem < 0.05
+    assert abs(mean) < 0.1
