@@ -227,6 +227,17 @@ int qwg_dmc_block_ready(qwg_ctx* ctx);
 int qwg_vmc_block_noalloc(qwg_ctx* ctx, double* d_R, int nw, int nstep, double timestep, uint64_t seed,
                           int deterministic_pp, double* d_energy, double* d_sums);
 
+/* MO value, gradient and Laplacian of every orbital of one spin at npos
+ * positions: out[p][j][0..4] = (phi_j, d/dx, d/dy, d/dz, lap) at pos[p][0..2]
+ * (host arrays; periodic systems wrap the positions into the cell).
+ * Templated_MO_matrix::updateLap (orbitals/MO_matrix.h:101-118) for a batch of
+ * positions, the product of MO_matrix_blas::updateLap
+ * (orbitals/MO_matrix_blas.h:411-491).  QWG_FP64 contexts contract on CUDA
+ * cores in FP64; QWG_MIXED contexts contract all positions in one
+ * tensor-core GEMM (tcgen05, split TF32 with FP32 accumulation, TMA-staged
+ * tiles).  Real orbitals only (QWG_ERR_ARG for complex ones). */
+int qwg_mo_eval(qwg_ctx* ctx, const double* pos, int npos, int spin, double* out);
+
 /* Batched uneven systems: one CUDA graph holding one DMC block of every
  * context (each on its own stream, forked and joined inside the graph), so a
  * single graph launch advances all systems concurrently.  Every context must

@@ -619,20 +619,18 @@ __device__ __forceinline__ void shell_lap_store_fg(int sym, double x, double y, 
   }
 }
 
-// MO value, gradient and Laplacian of one position, warp-cooperative.
-// Lanes split the shells (radial spline and angular factors in FP64: the
-// Laplacian of the tight shells cancels strongly), basis rows go to bas
-// [nbasis][5] as Real, then lanes split the (MO, component) outputs of the
-// contraction with the MO coefficients moc_s [nbasis][mstride].
+// Basis value, gradient and Laplacian of every basis function at one
+// position, warp-cooperative: lanes split the shells (radial spline and
+// angular factors in FP64: the Laplacian of the tight shells cancels
+// strongly); the rows go to bas [nbasis][5] in the output type O.
 // PER: 0 molecule, 1 periodic cell (compiled for that case only), 2 decided
 // at run time from S.periodic.
-template <typename Real, int PER, bool HL = false>
-__device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz, int M,
-                            Real* bas, Real* out, int lane) {
+template <typename O, int PER, bool HL, typename Real>
+__device__ void basis_lap_warp(const DevSys<Real>& S, double px, double py, double pz, O* bas, int lane) {
   for (int s = lane; s < S.nshell; s += 32) {
     int4 si = S.shell_i[s];
     int2 so = S.shell_obj[s];
-    Real* b = bas + si.z * 5;
+    O* b = bas + si.z * 5;
     const int nf = sym_nfunc(si.y);
     const double cut = S.shell_cut[s];
     if (PER == 0 || (PER == 2 && !S.periodic)) {
@@ -650,23 +648,23 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
         if (HL && (si.y >= 4 || S.cutoff_mo)) {
           // accumulate into zeros: no |value| skip for CUTOFF_MO
           if (S.cutoff_mo)
-            for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
+            for (int k = 0; k < 5 * nf; k++) b[k] = O(0);
           if (si.y >= 4) {
-            if (S.cutoff_mo) shell_lap_store_fg<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
-            else shell_lap_store_fg<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
+            if (S.cutoff_mo) shell_lap_store_fg<O, true>(si.y, dx, dy, dz, f, fd, f2, b);
+            else shell_lap_store_fg<O, false>(si.y, dx, dy, dz, f, fd, f2, b);
           } else {
-            shell_lap_store<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
+            shell_lap_store<O, true>(si.y, dx, dy, dz, f, fd, f2, b);
           }
         } else {
-          shell_lap_store<Real, false>(si.y, dx, dy, dz, f, fd, f2, b);
+          shell_lap_store<O, false>(si.y, dx, dy, dz, f, fd, f2, b);
         }
       } else {
-        for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
+        for (int k = 0; k < 5 * nf; k++) b[k] = O(0);
       }
     } else {
       // periodic: sum the shell over the atom's image centers, then apply the
       // |value| <= 1e-8 rule to the sums (MO_matrix_blas.h:444-474)
-      for (int k = 0; k < 5 * nf; k++) b[k] = Real(0);
+      for (int k = 0; k < 5 * nf; k++) b[k] = O(0);
       const int2 im = S.atom_images[si.x];
       const double cut2 = cut * cut * (1.0 + 1e-12);  // beyond it r < cut is certainly false
       for (int m = im.x; m < im.x + im.y; m++) {
@@ -683,15 +681,26 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
         double f = ca.x + h * (ca.y + h * (cb.x + h * cb.y));
         double fd = (ca.y + h * (2.0 * cb.x + h * (3.0 * cb.y))) / r;
         double f2 = 2.0 * cb.x + 6.0 * h * cb.y;
-        if (HL && si.y >= 4) shell_lap_store_fg<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
-        else shell_lap_store<Real, true>(si.y, dx, dy, dz, f, fd, f2, b);
+        if (HL && si.y >= 4) shell_lap_store_fg<O, true>(si.y, dx, dy, dz, f, fd, f2, b);
+        else shell_lap_store<O, true>(si.y, dx, dy, dz, f, fd, f2, b);
       }
       if (!(HL && S.cutoff_mo))
         for (int k = 0; k < nf; k++)
           if (!(fabs(double(b[5 * k])) > 1e-8))
-            for (int c = 0; c < 5; c++) b[5 * k + c] = Real(0);
+            for (int c = 0; c < 5; c++) b[5 * k + c] = O(0);
     }
   }
+  __syncwarp();
+}
+
+// MO value, gradient and Laplacian of one position, warp-cooperative: the
+// basis rows (basis_lap_warp) in bas [nbasis][5] as Real, then lanes split
+// the (MO, component) outputs of the contraction with the MO coefficients
+// moc_s [nbasis][mstride].
+template <typename Real, int PER, bool HL = false>
+__device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px, double py, double pz, int M,
+                            Real* bas, Real* out, int lane) {
+  basis_lap_warp<Real, PER, HL>(S, px, py, pz, bas, lane);
   __syncwarp();
   if (M > 32) {
     // many orbitals: lanes over MOs (coalesced coefficient rows), the basis

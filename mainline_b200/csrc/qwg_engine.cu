@@ -15,6 +15,7 @@
 #include "../../include/qwg.h"
 #include "qwg_deck.hpp"
 #include "qwg_launch.cuh"
+#include "qwg_mo.cuh"
 
 using namespace qwg;
 
@@ -148,6 +149,15 @@ struct qwg_ctx {
   double eref = 0, branch_start = 0, branch_stop = 0;
   std::vector<double> block_energies, block_weights;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // tensor-core MO contraction (mixed precision, real orbitals): the MO
+  // coefficients of each spin transposed to [bn][kpad] and split into TF32
+  // high and low parts, with their TMA tensor maps
+  bool tc_ready = false;
+  int tc_kpad = 0, tc_bn[2] = {0, 0};
+  DevBuf d_tc_b;                 // [spin][hi, lo][256][kpad] FP32
+  CUtensorMap tc_map_b[2][2];
+  DevBuf d_tc_err;               // expired-wait code of the GEMM kernel
+  DevBuf d_mo_scratch;           // qwg_mo_eval work buffers
 };
 
 namespace {
@@ -569,6 +579,100 @@ static StepParams base_params(qwg_ctx* c) {
   P.vmc_depth = c->vmc_depth;
   P.vmc_divider = c->vmc_divider;
   return P;
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core MO contraction: tensor maps and the split-TF32 coefficients.
+
+typedef CUresult (*TensorMapEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                         const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                         CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                         CUtensorMapFloatOOBfill);
+
+static TensorMapEncodeTiled tensor_map_encoder() {
+  static TensorMapEncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (TensorMapEncodeTiled)p;
+  });
+  return fn;
+}
+
+// Tensor map of a row-major FP32 array [outer][inner] read in boxes of 32 x
+// box_outer elements with the 128-byte swizzle (inner must be a multiple of
+// 32 and the base 16-byte aligned; rows past outer read as zeros).
+static void tc_map(CUtensorMap* m, const float* base, uint64_t inner, uint64_t outer, uint32_t box_outer) {
+  TensorMapEncodeTiled enc = tensor_map_encoder();
+  if (!enc) throw CudaError("cuTensorMapEncodeTiled is not available from the driver");
+  if (inner % TC_BK != 0 || ((uintptr_t)base & 15) != 0) throw CudaError("tensor map: bad inner extent or alignment");
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {inner * sizeof(float)};
+  cuuint32_t box[2] = {(cuuint32_t)TC_BK, box_outer};
+  cuuint32_t es[2] = {1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)base, dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+
+// FP32 rounded to TF32 (10 explicit mantissa bits), to nearest, ties away.
+static float tf32_round(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) {
+    u += 0x1000u;
+    u &= 0xffffe000u;
+  }
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
+
+static void tc_setup(qwg_ctx* c) {
+  if (c->tc_ready) return;
+  const HostSystem& H = c->H;
+  const int kpad = (H.nbasis + TC_BK - 1) / TC_BK * TC_BK;
+  c->tc_kpad = kpad;
+  std::vector<float> b((size_t)2 * 2 * 256 * kpad, 0.f);
+  for (int s = 0; s < 2; s++) {
+    if (H.nmo[s] > 256) throw InputError("the tensor-core MO contraction takes at most 256 orbitals per spin");
+    c->tc_bn[s] = std::max(16, (H.nmo[s] + 15) / 16 * 16);
+    for (int j = 0; j < H.nmo[s]; j++)
+      for (int f = 0; f < H.nbasis; f++) {
+        const double v = H.moc[s][(size_t)f * H.nmo[s] + j];
+        const float hi = tf32_round((float)v);
+        b[(((size_t)s * 2 + 0) * 256 + j) * kpad + f] = hi;
+        b[(((size_t)s * 2 + 1) * 256 + j) * kpad + f] = tf32_round((float)(v - (double)hi));
+      }
+  }
+  upload(c->d_tc_b, b, c->stream);
+  for (int s = 0; s < 2; s++)
+    for (int h = 0; h < 2; h++)
+      tc_map(&c->tc_map_b[s][h], c->d_tc_b.as<float>() + ((size_t)s * 2 + h) * 256 * kpad, kpad, c->tc_bn[s],
+             (uint32_t)c->tc_bn[s]);
+  c->d_tc_err.alloc(16);
+  c->tc_ready = true;
+}
+
+// D[r][j] (row stride ldd) = sum_k (a_hi + a_lo)[r][k] (b_hi + b_lo)[j][k]
+// for the orbitals j of one spin, rows r < rows; split-TF32 tensor cores.
+static void tc_gemm(qwg_ctx* c, const float* a_hi, const float* a_lo, int rows, int spin, float* D, int ldd) {
+  const int bn = c->tc_bn[spin];
+  const int stages = bn <= 64 ? 4 : bn <= 128 ? 3 : 2;
+  const size_t smem = tc_smem_bytes(bn, stages);
+  CUtensorMap ma, ml;
+  tc_map(&ma, a_hi, c->tc_kpad, rows, TC_BM);
+  tc_map(&ml, a_lo, c->tc_kpad, rows, TC_BM);
+  TcGemmArgs g{rows, c->tc_kpad / TC_BK, c->H.nmo[spin], bn, ldd, stages, D, c->d_tc_err.as<int>()};
+  CK(cudaFuncSetAttribute(k_mo_gemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_mo_gemm_tf32x3<<<(rows + TC_BM - 1) / TC_BM, TC_THREADS, smem, c->stream>>>(ma, ml, c->tc_map_b[spin][0],
+                                                                               c->tc_map_b[spin][1], g);
+  CK(cudaGetLastError());
+  c->launches++;
 }
 
 static int fail(qwg_ctx* c, int code, const std::string& m) {
@@ -1027,6 +1131,68 @@ int qwg_eval(qwg_ctx* c, const double* rot, qwg_eval_out* out) {
     dl(out->nonlocal, d_nl, W); dl(out->grad, d_g, n_g); dl(out->lap, d_l, n_l);
     CK(cudaStreamSynchronize(c->stream));
     c->state_valid = false;  // eval leaves scratch state unsaved
+    return QWG_OK;
+  });
+}
+
+int qwg_mo_eval(qwg_ctx* c, const double* pos, int npos, int spin, double* out) {
+  if (!c || !pos || !out || npos <= 0 || spin < 0 || spin > 1) return QWG_ERR_ARG;
+  if (c->mmax == kComplexFamily) return fail(c, QWG_ERR_ARG, "qwg_mo_eval: complex orbitals are not supported");
+  if ((size_t)npos * 5 > (size_t)INT32_MAX / 2) return fail(c, QWG_ERR_ARG, "qwg_mo_eval: too many positions");
+  const int nmo = c->H.nmo[spin];
+  if (nmo == 0) return QWG_OK;
+  return guarded(c, [&]() -> int {
+    const int nb = c->H.nbasis;
+    const size_t n_out = (size_t)npos * nmo * 5;
+    std::vector<double> host_out;
+    if (c->precision == QWG_FP64) {
+      const int ms = c->sys_d.mstride;
+      const size_t bytes = 8 * ((size_t)npos * 3 + (size_t)npos * nb * 5 + (size_t)npos * ms * 5 + n_out);
+      if (c->d_mo_scratch.n < bytes) c->d_mo_scratch.alloc(bytes);
+      double* d_pos = c->d_mo_scratch.as<double>();
+      double* bas = d_pos + (size_t)npos * 3;
+      double* osc = bas + (size_t)npos * nb * 5;
+      double* dout = osc + (size_t)npos * ms * 5;
+      CK(cudaMemcpyAsync(d_pos, pos, 8 * (size_t)npos * 3, cudaMemcpyHostToDevice, c->stream));
+      k_mo_rows_cuda<double><<<(npos + 3) / 4, 128, 0, c->stream>>>(
+          c->sys_d, c->sys_d.moc + (size_t)spin * nb * ms, d_pos, npos, nmo, bas, osc, dout);
+      CK(cudaGetLastError());
+      c->launches++;
+      CK(cudaMemcpyAsync(out, dout, 8 * n_out, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      return QWG_OK;
+    }
+    tc_setup(c);
+    const int kpad = c->tc_kpad, bn = c->tc_bn[spin];
+    const size_t rows = (size_t)npos * 5;
+    // doubles: positions, basis rows; floats (256-byte aligned): a_hi, a_lo, D
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t o_bas = al(8 * (size_t)npos * 3), o_ahi = o_bas + al(8 * (size_t)npos * nb * 5);
+    const size_t o_alo = o_ahi + al(4 * rows * kpad), o_d = o_alo + al(4 * rows * kpad);
+    const size_t bytes = o_d + al(4 * rows * bn);
+    if (c->d_mo_scratch.n < bytes) c->d_mo_scratch.alloc(bytes);
+    unsigned char* base = c->d_mo_scratch.as<unsigned char>();
+    double* d_pos = (double*)base;
+    float* a_hi = (float*)(base + o_ahi);
+    float* a_lo = (float*)(base + o_alo);
+    float* D = (float*)(base + o_d);
+    CK(cudaMemcpyAsync(d_pos, pos, 8 * (size_t)npos * 3, cudaMemcpyHostToDevice, c->stream));
+    k_basis_rows_tf32<float><<<(npos + 3) / 4, 128, 0, c->stream>>>(c->sys_f, d_pos, npos, kpad,
+                                                                    (double*)(base + o_bas), a_hi, a_lo);
+    CK(cudaGetLastError());
+    c->launches++;
+    CK(cudaMemsetAsync(c->d_tc_err.p, 0, sizeof(int), c->stream));
+    tc_gemm(c, a_hi, a_lo, (int)rows, spin, D, bn);
+    std::vector<float> hD(rows * bn);
+    int err = 0;
+    CK(cudaMemcpyAsync(hD.data(), D, 4 * rows * bn, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&err, c->d_tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (err) return fail(c, QWG_ERR_CUDA, "qwg_mo_eval: a tensor-core pipeline wait expired (code " +
+                                              std::to_string(err) + ")");
+    for (int p = 0; p < npos; p++)
+      for (int j = 0; j < nmo; j++)
+        for (int q = 0; q < 5; q++) out[((size_t)p * nmo + j) * 5 + q] = hD[((size_t)p * 5 + q) * bn + j];
     return QWG_OK;
   });
 }

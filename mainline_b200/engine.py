@@ -117,6 +117,7 @@ def load_library(path: str = LIB_PATH):
         "qwg_get_walker_scalars": (C.c_int, [C.c_void_p, dp, dp, C.c_int]),
         "qwg_eval": (C.c_int, [C.c_void_p, dp, P(EvalOut)]),
         "qwg_ratio": (C.c_int, [C.c_void_p, P(C.c_int), dp, dp, dp, dp, dp]),
+        "qwg_mo_eval": (C.c_int, [C.c_void_p, dp, C.c_int, C.c_int, dp]),
         "qwg_set_vmc_dynamics": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
         "qwg_vmc_block": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_int, P(BlockStats)]),
         "qwg_dmc_init": (C.c_int, [C.c_void_p, P(DmcParams)]),
@@ -265,6 +266,16 @@ class Engine:
             rp = _ptr(rot)
         self._check(self.lib.qwg_eval(self.h, rp, C.byref(out)), "qwg_eval")
         return EvalResult(o["logpsi"], o["sign"], o["grad"], o["lap"], o["kinetic"], o["potential"], o["nonlocal"])
+
+    def mo_eval(self, pos: np.ndarray, spin: int) -> np.ndarray:
+        """MO value, gradient and Laplacian of every orbital of one spin at
+        positions pos [n, 3]: [n, nmo, 5] (tensor-core GEMM in mixed
+        precision, FP64 CUDA cores otherwise)."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        nmo = self.info.nmo_up if spin == 0 else self.info.nmo_down
+        out = np.zeros((pos.shape[0], nmo, 5))
+        self._check(self.lib.qwg_mo_eval(self.h, _ptr(pos), pos.shape[0], spin, _ptr(out)), "qwg_mo_eval")
+        return out
 
     def ratio(self, e: np.ndarray, rnew: np.ndarray):
         W = self.nwalk
