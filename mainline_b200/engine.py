@@ -26,7 +26,7 @@ MIXED = 1
 EXPORTS = [
     "qwg_version", "qwg_last_error", "qwg_create", "qwg_destroy", "qwg_get_info", "qwg_inspect_deck",
     "qwg_inspect_spline", "qwg_set_walkers", "qwg_get_walkers", "qwg_set_walkers_device",
-    "qwg_get_walker_scalars", "qwg_eval",
+    "qwg_get_walker_scalars", "qwg_eval", "qwg_mo_eval",
     "qwg_ratio", "qwg_set_vmc_dynamics", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
     "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready", "qwg_time_kernels",
