@@ -347,6 +347,36 @@ def run_extras(stream, dev, seconds=30.0):
     cpx["config"] = "the periodic cell with complex orbitals (CORBITALS) at k=(0.5,0.25,0); 16384 walkers, " \
                     "tau=0.005, 10-step blocks"
     out["periodic_complex"] = cpx
+    # 72-electron molecule (HBM-resident kernels): mixed precision with the
+    # tensor-core move schedule, with the CUDA-core contraction, and FP64
+    m72 = os.path.join(ROOT, "tests", "golden", "mol72.qw")
+    Rm = systems.random_configs(systems.read_deck(m72), 4096, seed=SEED % 1000)
+    hm = {}
+    for label, prec, tc in (("mixed", engine.MIXED, "1"), ("mixed_cuda_core_mo", engine.MIXED, "0"),
+                            ("fp64", engine.FP64, "0")):
+        old_tc = os.environ.get("QWG_TC_MOVES")
+        os.environ["QWG_TC_MOVES"] = tc
+        try:
+            E = engine.Engine(m72, prec, max_walkers=4096, stream=stream.cuda_stream)
+        finally:
+            if old_tc is None:
+                os.environ.pop("QWG_TC_MOVES", None)
+            else:
+                os.environ["QWG_TC_MOVES"] = old_tc
+        E.set_walkers(Rm)
+        E.vmc_block(2, 0.1, seed=SEED + 3)
+        E.dmc_init(timestep=0.01, nstep=5, seed=SEED + 4)
+        E.dmc_block()
+        st = E.dmc_block()
+        hm[label] = {"walker_steps_per_s": 4096 * 5 / (st["block_ms"] / 1e3), "block_ms": st["block_ms"],
+                     "energy": st["energy"]}
+        E.close()
+    hm["mixed_vs_fp64"] = hm["mixed"]["walker_steps_per_s"] / hm["fp64"]["walker_steps_per_s"]
+    hm["tensor_core_schedule_gain"] = hm["mixed"]["walker_steps_per_s"] / hm["mixed_cuda_core_mo"]["walker_steps_per_s"]
+    hm["config"] = ("mol72: 10 atoms, 72 electrons (36 per spin), 180 basis functions, HBM-resident kernels; 4096 "
+                    "walkers, DMC tau=0.01, 5-step blocks; mixed = per-electron tensor-core MO contraction "
+                    "(tcgen05 split TF32)")
+    out["hbm_molecule"] = hm
     # batched uneven molecules: 16 systems, 8-192 electrons, 512-4096 walkers
     mols = systems.write_batch(os.path.join(tmp, "batch"), nsys=16, seed=SEED % 1000)
     bat = {}
@@ -462,7 +492,19 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="only the headline workload")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="arms of the headline workload (profiling runs use one)")
+    ap.add_argument("--probe", choices=["tc-sweep"], default=None,
+                    help="profiling driver only, no report line: tc-sweep = one mixed-precision sweep of the "
+                         "72-electron molecule (4096 walkers) on the tensor-core move schedule")
     args = ap.parse_args()
+    if args.probe == "tc-sweep":
+        from mainline_b200 import engine, systems
+        deck = os.path.join(ROOT, "tests", "golden", "mol72.qw")
+        E = engine.Engine(deck, engine.MIXED, max_walkers=NWALK)
+        E.set_walkers(systems.random_configs(systems.read_deck(deck), NWALK, seed=1))
+        E.set_vmc_dynamics(1, 2.0)
+        print("tc-sweep acceptance", E.vmc_block(1, 0.1, seed=2)["acceptance"])
+        E.close()
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
 

@@ -306,6 +306,17 @@ struct StepParams {
   double vmc_divider;
   double* tm_cand;      // [W][tm_cap] the current electron chunk's point terms
   double* tm_moves;     // [W][N][4] selected targets (x, y, z, 1) or flag 0
+  // Tensor-core move schedule (KM_SWEEP, HBM-resident FP32 kernels): one
+  // electron tc_e per launch.  Phase 1 proposes the move and writes the five
+  // basis rows of the proposed position as split-TF32 pairs into the GEMM's
+  // A operand (rows walker * 5 + component, kpad columns); the tensor-core
+  // GEMM contracts them with the MO coefficients into tc_D (row stride
+  // tc_ldd); phase 2 recomputes the same proposal and decides it with the
+  // MO column read from tc_D.  tc_phase 0: the whole sweep in one launch.
+  int tc_phase, tc_e, tc_kpad, tc_ldd;
+  float* tc_ahi;
+  float* tc_alo;
+  const float* tc_D;
 };
 
 // ---------------------------------------------------------------------------

@@ -158,6 +158,12 @@ struct qwg_ctx {
   CUtensorMap tc_map_b[2][2];
   DevBuf d_tc_err;               // expired-wait code of the GEMM kernel
   DevBuf d_mo_scratch;           // qwg_mo_eval work buffers
+  // tensor-core move schedule (mixed precision, HBM-resident real single
+  // determinant): per electron move, the basis rows of every walker's
+  // proposal (A operand, hi and lo planes) and the GEMM's MO columns
+  bool tc_moves = false;
+  int tc_ldd = 0;
+  DevBuf d_tc_a, d_tc_d;
 };
 
 namespace {
@@ -507,6 +513,25 @@ static size_t branch_smem(int W) { return W <= kBranchSmemMax ? branch_bytes(W) 
 
 // Device bytes a context holds for max_walkers walkers (the allocations of
 // qwg_create plus the evaluation buffers qwg_dmc_init sizes).
+constexpr int kTcMinWalkers = 1024;
+
+// The tensor-core move schedule serves the mixed-precision HBM-resident
+// kernels with real orbitals and one determinant (QWG_TC_MOVES=0 turns it
+// off, e.g. to time the CUDA-core contraction beside it).
+static bool tc_moves_eligible(const qwg_ctx* c) {
+  const char* env = std::getenv("QWG_TC_MOVES");
+  if (env && env[0] == '0') return false;
+  return c->precision == QWG_MIXED && c->mmax == 0 && c->H.detwt.size() <= 1 && c->H.nmo[0] <= 256 &&
+         c->H.nmo[1] <= 256;
+}
+
+static size_t tc_moves_bytes(const qwg_ctx* c, size_t W) {
+  const size_t kpad = ((size_t)c->H.nbasis + 31) / 32 * 32;
+  size_t ldd = 16;
+  for (int s = 0; s < 2; s++) ldd = std::max(ldd, ((size_t)c->H.nmo[s] + 15) / 16 * 16);
+  return W * 5 * (kpad * 8 + ldd * 4) + 2 * 2 * 256 * kpad * 4 + 16;
+}
+
 static size_t footprint_bytes(const qwg_ctx* c, int max_walkers) {
   const HostSystem& H = c->H;
   const size_t rs = c->precision == QWG_FP64 ? 8 : 4, N = H.nelec, W = max_walkers;
@@ -518,6 +543,7 @@ static size_t footprint_bytes(const qwg_ctx* c, int max_walkers) {
              H.image_pos.size() * 8 * 5 / 3 + H.gvec.size() * 8 + 3 * H.gweight.size() * 8;
   b += W * (2 * 3 * N * 8 + 2 * (size_t)c->L.state_bytes + (hbm_family(c->mmax) ? (size_t)c->L.scratch_bytes : 0) + 20);
   b += W * 8 * (9 + 5 + 4 * N);  // evaluation outputs (qwg_eval / qwg_dmc_init)
+  if (tc_moves_eligible(c)) b += tc_moves_bytes(c, W);
   b += sizeof(BlockAcc) * 1024 + DYN_COUNT * 8 + (size_t)kHistCap * 8 + kStatsLen * 8;
   if (max_walkers > kBranchSmemMax) b += branch_bytes(max_walkers);
   return b;
@@ -578,6 +604,13 @@ static StepParams base_params(qwg_ctx* c) {
   P.refresh = 1;
   P.vmc_depth = c->vmc_depth;
   P.vmc_divider = c->vmc_divider;
+  if (c->tc_moves) {
+    P.tc_kpad = c->tc_kpad;
+    P.tc_ldd = c->tc_ldd;
+    P.tc_ahi = c->d_tc_a.as<float>();
+    P.tc_alo = P.tc_ahi + (size_t)c->max_walkers * 5 * c->tc_kpad;
+    P.tc_D = c->d_tc_d.as<float>();
+  }
   return P;
 }
 
@@ -680,6 +713,17 @@ static int fail(qwg_ctx* c, int code, const std::string& m) {
   return code;
 }
 
+// After a synchronised block: a tensor-core pipeline wait that expired
+// (bounded waits in the GEMM kernel) becomes a CUDA-class error.
+static int tc_check(qwg_ctx* c) {
+  if (!c->tc_moves) return QWG_OK;
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, c->d_tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (!err) return QWG_OK;
+  return fail(c, QWG_ERR_CUDA, "tensor-core MO contraction: a pipeline wait expired (code " + std::to_string(err) + ")");
+}
+
 template <class F>
 static int guarded(qwg_ctx* c, F&& f) {
   try {
@@ -725,9 +769,26 @@ static void launch_steps(qwg_ctx* c, StepParams P, const EvalIO& io, int nwalk) 
     launch_walkers(c, P, io, KM_STEPS, nwalk);
     return;
   }
+  // the per-electron GEMM fills the GPU only with enough walkers (5 rows
+  // each, 128-row tiles): below kTcMinWalkers the one-launch sweep is faster
+  const bool tc = P.tc_ahi && P.tc_D && nwalk <= c->max_walkers && nwalk >= kTcMinWalkers;
   for (int st = 0; st < P.nsteps; st++) {
     P.st = st;
-    launch_walkers(c, P, io, KM_SWEEP, nwalk);
+    if (tc) {
+      // per electron: proposals + basis rows, one tensor-core GEMM over all
+      // walkers' rows, decisions + Sherman-Morrison updates
+      for (int e = 0; e < c->H.nelec; e++) {
+        P.tc_e = e;
+        P.tc_phase = 1;
+        launch_walkers(c, P, io, KM_SWEEP, nwalk);
+        tc_gemm(c, P.tc_ahi, P.tc_alo, nwalk * 5, e < c->H.nup ? 0 : 1, (float*)P.tc_D, P.tc_ldd);
+        P.tc_phase = 2;
+        launch_walkers(c, P, io, KM_SWEEP, nwalk);
+      }
+      P.tc_phase = 0;
+    } else {
+      launch_walkers(c, P, io, KM_SWEEP, nwalk);
+    }
     launch_walkers(c, P, io, P.tmoves ? KM_ELOC_TM : KM_ELOC, nwalk);
     if (P.tmoves) launch_walkers(c, P, io, KM_TMOVE, nwalk);
   }
@@ -971,6 +1032,14 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
     c->d_state.alloc((size_t)max_walkers * c->L.state_bytes);
     c->d_state2.alloc((size_t)max_walkers * c->L.state_bytes);
     if (hbm_family(c->mmax)) c->d_scratch.alloc((size_t)max_walkers * c->L.scratch_bytes);
+    if (tc_moves_eligible(c.get())) {
+      tc_setup(c.get());
+      c->tc_ldd = std::max(c->tc_bn[0], c->tc_bn[1]);
+      c->d_tc_a.alloc((size_t)max_walkers * 5 * c->tc_kpad * 2 * sizeof(float));
+      c->d_tc_d.alloc((size_t)max_walkers * 5 * c->tc_ldd * sizeof(float));
+      CK(cudaMemsetAsync(c->d_tc_err.p, 0, sizeof(int), c->stream));
+      c->tc_moves = true;
+    }
     c->d_acc.alloc(sizeof(BlockAcc) * 1024);
     c->d_dyn.alloc(DYN_COUNT * 8);
     CK(cudaMemsetAsync(c->d_dyn.p, 0, DYN_COUNT * 8, c->stream));
@@ -1251,6 +1320,7 @@ int qwg_vmc_block(qwg_ctx* c, int nstep, double timestep, uint64_t seed, int det
     std::vector<BlockAcc> h(1);
     CK(cudaMemcpyAsync(h.data(), acc, sizeof(BlockAcc), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (int rc = tc_check(c)) return rc;
     if (stats) {
       memset(stats, 0, sizeof(*stats));
       acc_to_stats(h, stats);
@@ -1402,6 +1472,7 @@ int qwg_dmc_block_wait(qwg_ctx* c, qwg_block_stats* stats) {
     CK(cudaEventSynchronize(c->ev1));
     c->block_pending = false;
     c->step_counter += c->dmc.nstep;
+    if (int rc = tc_check(c)) return rc;
     if (stats) {
       stats_from_sums(c->h_stats, stats);
       float ms = 0;

@@ -3,6 +3,7 @@
 // model.  Reference semantics cited per routine (QWalk/mainline src/).
 #pragma once
 #include "qwg_device.cuh"
+#include "qwg_tc.cuh"
 
 namespace qwg {
 
@@ -50,6 +51,10 @@ struct Walker {
   unsigned char* sbase;  // scratch
   const Real* moc_s;     // [2][nbasis][mstride] MO coefficients (global, read through L1)
   int lane;
+  // MO column of the proposal from the tensor-core GEMM (tc_phase 2):
+  // tcD[(row0 + q) * tc_ldd + i] = component q of orbital i
+  const float* tcD = nullptr;
+  int tc_ldd = 0;
   static constexpr bool CPX = MMAX < 0;
   // F and G basis shells: compiled into the HBM-resident kernels only
   static constexpr bool HL = MMAX <= 0;
@@ -356,7 +361,18 @@ struct Walker {
       r1 = (a[1] * a[0] + b[1] * b[0]) / r0; r2 = (a[2] * a[0] + b[2] * b[0]) / r0;
       r3 = (a[3] * a[0] + b[3] * b[0]) / r0; r4 = (a[4] * a[0] + b[4] * b[0]) / r0;
     } else {
-      mo_lap_warp<Real, PER, HL>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
+      bool from_gemm = false;
+      if constexpr (MMAX == 0 && sizeof(Real) == 4) {
+        if (tcD) {
+          for (int idx = lane; idx < 5 * M; idx += 32) {
+            const int i = idx / 5, q = idx - 5 * i;
+            nc[idx] = Real(tcD[(size_t)q * tc_ldd + i]);
+          }
+          __syncwarp();
+          from_gemm = true;
+        }
+      }
+      if (!from_gemm) mo_lap_warp<Real, PER, HL>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
       const Real* iv = inv(s) + (size_t)el * MS();
       for (int i = 0; i < M; i++) {
         double c = iv[i];
@@ -989,6 +1005,12 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
     unsigned char* wb = HBM ? gstate : smem + moc_bytes + (size_t)warp * (SWEEP_ONLY ? L.sweep_bytes : L.bytes);
     unsigned char* sb = HBM ? P.scratch + (size_t)wid * L.scratch_bytes : wb + L.state_bytes;
     Walker<Real, MMAX, TB, PER> W{S, L, wb, sb, moc_s, lane};
+    // tensor-core move schedule: this launch moves electron P.tc_e only
+    const int tc_phase = (mode == KM_SWEEP && MMAX == 0 && sizeof(Real) == 4) ? P.tc_phase : 0;
+    if (tc_phase == 2) {
+      W.tcD = P.tc_D + (size_t)wid * 5 * P.tc_ldd;
+      W.tc_ldd = P.tc_ldd;
+    }
     const int N = S.nelec;
     double* Rp = W.R();
     const uint64_t step0 = P.dyn_step ? (uint64_t)P.etrial[DYN_STEP] : P.step0;
@@ -999,6 +1021,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
     }
     constexpr bool ELOCM = mode == KM_ELOC || mode == KM_ELOC_TM;  // local-energy phase
     if (ELOCM || mode == KM_TMOVE || (mode == KM_SWEEP && P.st > 0)) refresh = 0;  // a chunk's first sweep only
+    if (tc_phase == 2 || (tc_phase == 1 && P.tc_e > 0)) refresh = 0;  // the sweep's first launch only
     constexpr bool STEPS = mode == KM_STEPS || mode == KM_SWEEP || ELOCM || mode == KM_TMOVE;
     if (!STEPS || refresh) {
       for (int i = lane; i < 3 * N; i += 32) Rp[i] = P.R[(size_t)wid * 3 * N + i];
@@ -1101,7 +1124,8 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       for (int st = st0; st < st1; st++) {
         const uint64_t step = step0 + st;
         if constexpr (!ELOCM) {
-          for (int e = 0; e < N; e++) {
+          const int e_lo = tc_phase ? P.tc_e : 0, e_hi = tc_phase ? P.tc_e + 1 : N;
+          for (int e = e_lo; e < e_hi; e++) {
             // Split_sampler::split_driver depth 1 (Split_sample.cpp:380-478)
             double g0[3], l0;
             W.electron_grad(e, g0, l0);
@@ -1123,6 +1147,23 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
               if (S.kint) node = cos(kd);  // overall sign of Periodic_sample::translateElectron
             } else {
               wrap_pos(S, wx, wy, wz);
+            }
+            if (tc_phase == 1) {
+              // basis rows of the proposed position -> split-TF32 A rows of
+              // this walker (rows wid * 5 + component)
+              Real* b = W.bas();
+              basis_lap_warp<Real, PER, (MMAX <= 0)>(S, wx, wy, wz, b, lane);
+              float* ah = P.tc_ahi + (size_t)wid * 5 * P.tc_kpad;
+              float* al = P.tc_alo + (size_t)wid * 5 * P.tc_kpad;
+              for (int idx = lane; idx < 5 * P.tc_kpad; idx += 32) {
+                const int c = idx / P.tc_kpad, f = idx - c * P.tc_kpad;
+                const float v = f < S.nbasis ? float(b[(size_t)f * 5 + c]) : 0.0f;
+                float hi, lo;
+                tc_split_tf32(v, hi, lo);
+                ah[idx] = hi;
+                al[idx] = lo;
+              }
+              continue;
             }
             double ratioD, dU, g1[3], l1;
             W.propose(e, wx, wy, wz, ratioD, dU, g1, l1);

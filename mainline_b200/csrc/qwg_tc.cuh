@@ -14,9 +14,10 @@
 // columns.  Thread 0 issues the TMA loads of the K chunks (32 FP32 = one
 // 128-byte swizzle row) into a ring of shared-memory stages and the MMAs
 // (tcgen05.mma.cta_group::1.kind::tf32, M = 128, N = bn); each stage is
-// released by tcgen05.commit to its mbarrier.  The accumulator lives in
-// tensor memory (bn FP32 columns x 128 lanes); the four warps read their 32
-// lanes back with tcgen05.ld.  TMA sources are this GPU's own global memory
+// released by tcgen05.commit to its mbarrier.  The accumulators live in
+// tensor memory (2 bn FP32 columns x 128 lanes: the high products and the
+// cross terms apart); the four warps read their 32 lanes back with
+// tcgen05.ld and add the two.  TMA sources are this GPU's own global memory
 // only and no load uses cluster multicast.
 //
 // Every wait is bounded (iteration and time limit): on expiry the CTA
@@ -115,6 +116,17 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
                : "memory");
 }
 
+// 16 consecutive FP32 columns of this thread's tensor-memory lane (the warp
+// reads its 32 lanes); complete after tcgen05.wait::ld.
+__device__ __forceinline__ void tc_ld16(uint32_t addr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(addr));
+}
+
 // Split of an FP32 value into two TF32 parts (round to nearest, ties away):
 // hi + lo reproduces v to ~2^-22 relative.
 __device__ __forceinline__ void tc_split_tf32(float v, float& hi, float& lo) {
@@ -133,6 +145,7 @@ __host__ __device__ constexpr size_t tc_smem_bytes(int bn, int stages) {
   return 1024 + (size_t)stages * tc_stage_bytes(bn) + 256;
 }
 
+#ifndef QWG_WALKERS_ONLY  // the GEMM kernel lives in the engine translation unit
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_mo_gemm_tf32x3(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
                      const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
@@ -148,8 +161,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   __shared__ int s_fail;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row0 = blockIdx.x * TC_BM;
+  // two accumulators: columns [0, bn) take A_hi B_hi, [bn, 2 bn) the cross
+  // terms A_hi B_lo + A_lo B_hi (added in FP32 in the epilogue, so the small
+  // terms do not lose bits against the large running sum)
   uint32_t ncols = 32;
-  while ((int)ncols < g.bn) ncols <<= 1;
+  while ((int)ncols < 2 * g.bn) ncols <<= 1;
 
   if (threadIdx.x == 0) {
     s_fail = 0;
@@ -195,9 +211,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
       for (int k = 0; k < 4; k++) {  // UMMA K = 8 TF32 = 32 bytes: advance the start address by 2 x 16 B
         const uint64_t o = 2ull * k;
-        tc_mma_tf32(tmem, ahi + o, bhi + o, idesc, (cc > 0 || k > 0) ? 1u : 0u);
-        tc_mma_tf32(tmem, ahi + o, blo + o, idesc, 1u);
-        tc_mma_tf32(tmem, alo + o, bhi + o, idesc, 1u);
+        const uint32_t acc = (cc > 0 || k > 0) ? 1u : 0u;
+        tc_mma_tf32(tmem, ahi + o, bhi + o, idesc, acc);
+        tc_mma_tf32(tmem + (uint32_t)g.bn, ahi + o, blo + o, idesc, acc);
+        tc_mma_tf32(tmem + (uint32_t)g.bn, alo + o, bhi + o, idesc, 1u);
       }
       tc_commit(empty + s);
       // refill the stage of the previous chunk once its MMAs completed (the
@@ -223,20 +240,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int r = row0 + warp * 32 + lane;
     for (int c0 = 0; c0 < g.bn; c0 += 16) {
-      uint32_t v[16];
+      uint32_t v[16], w[16];
       const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-          "%15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(addr));
+      tc_ld16(addr, v);
+      tc_ld16(addr + (uint32_t)g.bn, w);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (r < g.rows) {
         float* d = g.D + (size_t)r * g.ldd;
 #pragma unroll
         for (int j = 0; j < 16; j++)
-          if (c0 + j < g.n) d[c0 + j] = __uint_as_float(v[j]);
+          if (c0 + j < g.n) d[c0 + j] = __uint_as_float(v[j]) + __uint_as_float(w[j]);
       }
     }
   }
@@ -249,5 +262,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
   }
 }
+#endif  // QWG_WALKERS_ONLY
 
 }  // namespace qwg

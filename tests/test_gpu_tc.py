@@ -81,3 +81,61 @@ def test_mo_eval_rejects_bad_arguments():
     with pytest.raises(engine.QwgError):
         E.mo_eval(np.zeros((4, 3)), 2)
     E.close()
+
+
+def _vmc_depth1(deck, R0, tc):
+    old = os.environ.get("QWG_TC_MOVES")
+    os.environ["QWG_TC_MOVES"] = "1" if tc else "0"
+    try:
+        E = engine.Engine(deck, engine.MIXED, max_walkers=len(R0))
+    finally:
+        if old is None:
+            del os.environ["QWG_TC_MOVES"]
+        else:
+            os.environ["QWG_TC_MOVES"] = old
+    E.set_vmc_dynamics(1, 2.0)
+    E.set_walkers(R0)
+    st = E.vmc_block(2, 0.1, seed=7)
+    R = E.get_walkers()
+    E.close()
+    return st, R
+
+
+@pytest.mark.parametrize("name", ["mol72", "cell32"])
+def test_tensor_core_moves_follow_cuda_core_moves(name):
+    """The per-electron tensor-core move schedule (proposal + basis rows,
+    one GEMM over all walkers, decision + Sherman-Morrison update) walks the
+    same paths as the one-launch CUDA-core sweep from the same walkers and
+    random streams: only decisions within the ~1e-6 difference of the MO
+    values can differ, and positions follow to the precision of the drift.""" 
+    deck = os.path.join(GOLDEN, name + ".qw")
+    d = systems.read_deck(deck)
+    R0 = systems.random_configs(d, 1024, seed=11)  # the schedule runs from 1024 walkers
+    st_tc, R_tc = _vmc_depth1(deck, R0, True)
+    st_cc, R_cc = _vmc_depth1(deck, R0, False)
+    # the drift of later moves uses gradients from either contraction, so
+    # positions of the same decisions agree to ~1e-7 bohr, not bit for bit
+    dev = np.max(np.abs(R_tc - R_cc), axis=-1)
+    same = dev < 1e-3  # a different decision moves an electron by ~sqrt(tau) = 0.3 bohr
+    print(f"TC_MOVES {name}: {100 * same.mean():.2f}% of electrons within 1e-3 bohr (median deviation "
+          f"{np.median(dev):.1e}), acceptance "
+          f"{st_tc['acceptance']:.4f} (tensor cores) vs {st_cc['acceptance']:.4f}, energy {st_tc['energy']:.4f} vs "
+          f"{st_cc['energy']:.4f}")
+    assert same.mean() > 0.99
+    assert np.median(dev) < 1e-4
+    assert abs(st_tc["acceptance"] - st_cc["acceptance"]) < 0.005
+    assert np.isfinite(st_tc["energy"])
+
+
+def test_tensor_core_moves_dmc_block():
+    deck = os.path.join(GOLDEN, "cell32.qw")
+    d = systems.read_deck(deck)
+    E = engine.Engine(deck, engine.MIXED, max_walkers=1024)
+    E.set_walkers(systems.random_configs(d, 1024, seed=12))
+    E.vmc_block(2, 0.3, seed=1)
+    E.dmc_init(timestep=0.005, nstep=5, seed=3)
+    for _ in range(2):
+        s = E.dmc_block()
+        assert np.isfinite(s["energy"]) and s["nonfinite"] == 0
+        assert 0.9 < s["acceptance"] <= 1.0
+    E.close()
