@@ -492,10 +492,26 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="only the headline workload")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="arms of the headline workload (profiling runs use one)")
-    ap.add_argument("--probe", choices=["tc-sweep"], default=None,
+    ap.add_argument("--probe", default=None,
                     help="profiling driver only, no report line: tc-sweep = one mixed-precision sweep of the "
-                         "72-electron molecule (4096 walkers) on the tensor-core move schedule")
+                         "72-electron molecule (4096 walkers) on the tensor-core move schedule; "
+                         "branch:<deck>:<walkers> = two mixed-precision DMC blocks of 5 steps of a golden deck "
+                         "(population control share)")
     args = ap.parse_args()
+    if args.probe and args.probe.startswith("branch:"):
+        from mainline_b200 import engine, systems
+        _, name, nw = args.probe.split(":")
+        deck = os.path.join(ROOT, "tests", "golden", name + ".qw")
+        nw = int(nw)
+        E = engine.Engine(deck, engine.MIXED, max_walkers=nw)
+        E.set_walkers(systems.random_configs(systems.read_deck(deck), nw, seed=1))
+        E.vmc_block(2, 0.1, seed=2)
+        E.dmc_init(timestep=0.01, nstep=5, seed=3)
+        for _ in range(2):
+            st = E.dmc_block()
+        print("branch probe", name, nw, "block ms", st["block_ms"])
+        E.close()
+        return
     if args.probe == "tc-sweep":
         from mainline_b200 import engine, systems
         deck = os.path.join(ROOT, "tests", "golden", "mol72.qw")

@@ -156,10 +156,14 @@ bool has_keyword(const std::vector<std::string>& w, const std::string& name) {
   return false;
 }
 
+// Every number of a deck or orbital file: a non-finite value (nan, inf)
+// would reach the device tables and turn every walker non-finite, so it is
+// refused at read time.
 static double to_d(const std::string& s) {
   char* end = nullptr;
   double v = std::strtod(s.c_str(), &end);
   if (end == s.c_str()) throw InputError("expected a number, got '" + s + "'");
+  if (!std::isfinite(v)) throw InputError("non-finite number '" + s + "' in the input");
   return v;
 }
 static int to_i(const std::string& s) {

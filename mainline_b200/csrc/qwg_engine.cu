@@ -1365,18 +1365,24 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
     io.nonlocal = base + 4 * W; io.grad = base + 5 * W; io.lap = io.grad + n_g;
     StepParams P = base_params(c);
     launch_walkers(c, P, io, KM_EVAL, W);
-    std::vector<double> k(W), v(W), nl(W), el(W);
+    std::vector<double> k(W), v(W), nl(W), el(W), lp(W);
     CK(cudaMemcpyAsync(k.data(), io.kinetic, 8 * W, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(v.data(), io.potential, 8 * W, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(nl.data(), io.nonlocal, 8 * W, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(lp.data(), io.logpsi, 8 * W, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     double sum = 0;
     int good = 0;
     for (int w = 0; w < W; w++) {
       el[w] = k[w] + v[w] + nl[w];
+      // a zero determinant (log|D| = -1e201, the exact zero of the inversion)
+      // leaves no usable local energy
+      if (!(lp[w] > -1e200)) el[w] = NAN;
       if (std::isfinite(el[w])) { sum += el[w]; good++; }
     }
-    if (!good) return fail(c, QWG_ERR_NUMERIC, "qwg_dmc_init: no walker has a finite local energy");
+    if (!good)
+      return fail(c, QWG_ERR_NUMERIC,
+                  "qwg_dmc_init: no walker has a finite local energy (non-finite values or a zero determinant)");
     // find_cutoffs (Dmc_method.cpp:262-300)
     double eavg = sum / good, var = 0;
     for (int w = 0; w < W; w++)
