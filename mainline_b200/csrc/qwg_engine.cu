@@ -163,6 +163,9 @@ struct qwg_ctx {
   // proposal (A operand, hi and lo planes) and the GEMM's MO columns
   bool tc_moves = false;
   int tc_ldd = 0;
+  // population control on the device-wide sort at every population size
+  // (QWG_BRANCH_DEVICE_WIDE=1; by default only above kBranchSmemMax walkers)
+  bool branch_device_wide = false;
   DevBuf d_tc_a, d_tc_d;
 };
 
@@ -511,6 +514,27 @@ static size_t branch_bytes(int W) {
 }
 static size_t branch_smem(int W) { return W <= kBranchSmemMax ? branch_bytes(W) : 0; }
 
+// Device-wide population control (populations above kBranchSmemMax): the
+// sort's double buffers, counts, new weights, digit counts and partial sums
+// in the context's branch buffer.
+static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+static size_t branch_big_bytes(int W, BranchBig* G, unsigned char* base) {
+  const int ntiles = (W + RADIX_TILE - 1) / RADIX_TILE, nprep = (W + 255) / 256, npb = (W / 2 + 255) / 256 + 1;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t at = o; o += align256(bytes); return at; };
+  const size_t k0 = take((size_t)W * 8), k1 = take((size_t)W * 8), i0 = take((size_t)W * 4),
+               i1 = take((size_t)W * 4), cn = take((size_t)W * 4), nw = take((size_t)W * 8),
+               hi = take((size_t)256 * ntiles * 4), ps = take((size_t)nprep * 8), np = take((size_t)npb * 4);
+  if (G && base) {
+    G->key[0] = (unsigned long long*)(base + k0); G->key[1] = (unsigned long long*)(base + k1);
+    G->idx[0] = (int*)(base + i0); G->idx[1] = (int*)(base + i1);
+    G->cnt = (int*)(base + cn); G->nw = (double*)(base + nw); G->hist = (int*)(base + hi);
+    G->psum = (double*)(base + ps); G->npair = (int*)(base + np);
+    G->ntiles = ntiles; G->nprep = nprep; G->npairblk = npb;
+  }
+  return o;
+}
+
 // Device bytes a context holds for max_walkers walkers (the allocations of
 // qwg_create plus the evaluation buffers qwg_dmc_init sizes).
 constexpr int kTcMinWalkers = 1024;
@@ -545,7 +569,7 @@ static size_t footprint_bytes(const qwg_ctx* c, int max_walkers) {
   b += W * 8 * (9 + 5 + 4 * N);  // evaluation outputs (qwg_eval / qwg_dmc_init)
   if (tc_moves_eligible(c)) b += tc_moves_bytes(c, W);
   b += sizeof(BlockAcc) * 1024 + DYN_COUNT * 8 + (size_t)kHistCap * 8 + kStatsLen * 8;
-  if (max_walkers > kBranchSmemMax) b += branch_bytes(max_walkers);
+  if (max_walkers > kBranchSmemMax) b += branch_big_bytes(max_walkers, nullptr, nullptr);
   return b;
 }
 
@@ -837,17 +861,30 @@ static void run_branch(qwg_ctx* c, const BlockAcc* acc, int nsteps) {
   B.dyn = c->d_dyn.as<double>();
   B.src_of = c->d_src.as<int>();
   B.new_w = c->d_neww.as<double>();
-  size_t sm = branch_smem(c->nwalk);
-  if (sm == 0) {  // large population: keys and counts in the context's global buffer
-    B.gkey = c->d_branch.as<double>();
-    B.gidx = (int*)(B.gkey + p2);
-    B.gcnt = B.gidx + p2;
-    B.gnw = (double*)(((uintptr_t)(B.gcnt + c->nwalk) + 15) & ~(uintptr_t)15);
+  size_t sm = c->branch_device_wide ? 0 : branch_smem(c->nwalk);
+  if (sm == 0) {
+    // large population: the device-wide sort (8 stable 8-bit passes), the
+    // pairing over all CTAs and a one-CTA gather map
+    BranchBig G{};
+    branch_big_bytes(c->nwalk, &G, c->d_branch.as<unsigned char>());
+    const int W = c->nwalk;
+    k_branch_prep<<<G.nprep, 256, 0, c->stream>>>(B, G);
+    for (int pass = 0; pass < 8; pass++) {
+      const int a = pass & 1;
+      k_radix_hist<<<G.ntiles, 256, 0, c->stream>>>(G.key[a], W, 8 * pass, G.hist, G.ntiles);
+      k_radix_scan<<<1, 1024, 0, c->stream>>>(G.hist, 256 * G.ntiles);
+      k_radix_scatter<<<G.ntiles, 256, 0, c->stream>>>(G.key[a], G.idx[a], G.key[1 - a], G.idx[1 - a], W, 8 * pass,
+                                                        G.hist, G.ntiles);
+    }
+    k_branch_pairs<<<G.npairblk, 256, 0, c->stream>>>(B, G, 0);
+    k_branch_finish<<<1, 1024, 0, c->stream>>>(B, G);
+    CK(cudaGetLastError());
+    c->launches += 2 + 3 * 8 + 1;
   } else {
     ensure_smem_attr(k_branch, sm);
+    k_branch<<<1, 1024, sm, c->stream>>>(B);
+    CK(cudaGetLastError());
   }
-  k_branch<<<1, 1024, sm, c->stream>>>(B);
-  CK(cudaGetLastError());
   const int n3 = 3 * c->H.nelec;
   k_gather<<<c->nwalk, 128, 0, c->stream>>>(c->nwalk, n3, c->L.state_bytes, c->L.scal, c->d_src.as<int>(),
                                             c->d_neww.as<double>(), c->d_R.as<double>(),
@@ -1032,6 +1069,7 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
     c->d_state.alloc((size_t)max_walkers * c->L.state_bytes);
     c->d_state2.alloc((size_t)max_walkers * c->L.state_bytes);
     if (hbm_family(c->mmax)) c->d_scratch.alloc((size_t)max_walkers * c->L.scratch_bytes);
+    if (const char* bw = std::getenv("QWG_BRANCH_DEVICE_WIDE")) c->branch_device_wide = bw[0] == '1';
     if (tc_moves_eligible(c.get())) {
       tc_setup(c.get());
       c->tc_ldd = std::max(c->tc_bn[0], c->tc_bn[1]);
@@ -1432,10 +1470,10 @@ int qwg_dmc_init(qwg_ctx* c, const qwg_dmc_params* p) {
       CK(cudaStreamSynchronize(c->stream));
     }
     if (W > kMaxDmcWalkers) throw InputError("DMC populations above 262144 walkers are beyond this engine build");
-    if (branch_smem(W)) {
+    if (branch_smem(W) && !c->branch_device_wide) {
       ensure_smem_attr(k_branch, branch_smem(W));
-    } else if (c->d_branch.n < branch_bytes(W)) {
-      c->d_branch.alloc(branch_bytes(W));
+    } else if (c->d_branch.n < branch_big_bytes(W, nullptr, nullptr)) {
+      c->d_branch.alloc(branch_big_bytes(W, nullptr, nullptr));
     }
     const long long l0 = c->launches;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));

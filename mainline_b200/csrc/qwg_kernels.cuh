@@ -1435,6 +1435,202 @@ __global__ void __launch_bounds__(1024) k_branch(BranchParams B) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Population control for large populations (more walkers than the one-CTA
+// kernel keeps in shared memory): the same E_T feedback, pairing and copy
+// order as k_branch, with the sort of the weights done device-wide.
+//   k_branch_prep    counts 1, new weights, 64-bit sort keys (the bits of a
+//                    non-negative double order like the value) and walker
+//                    indices; per-CTA weight sums
+//   k_radix_hist / k_radix_scan / k_radix_scatter   one stable LSD pass of
+//                    8 bits over (key, index) pairs: per-tile digit counts,
+//                    their digit-major exclusive scan, and the scatter with
+//                    in-tile ranks in element order (ties stay in index
+//                    order, as the one-CTA sort breaks them); 8 passes
+//   k_branch_pairs   pair k: the k-th heaviest (while >= 1.8) with the k-th
+//                    lightest, the split/kill draw of k_branch
+//   k_branch_finish  (one CTA) E_T feedback from the weight sum, exclusive
+//                    prefix sum of the counts in walker order into the gather
+//                    map, counters
+constexpr int RADIX_TILE = 2048;  // elements per CTA (256 threads x 8)
+
+struct BranchBig {
+  unsigned long long* key[2];  // [W] double buffers of the sort
+  int* idx[2];                 // [W]
+  int* cnt;                    // [W]
+  double* nw;                  // [W]
+  int* hist;                   // [256][ntiles] digit counts, then their offsets
+  double* psum;                // [prep CTAs] weight sums
+  int* npair;                  // [pair CTAs] pairs
+  int ntiles, nprep, npairblk;
+};
+
+__global__ void __launch_bounds__(256) k_branch_prep(BranchParams B, BranchBig G) {
+  __shared__ double red[8];
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  double w = 0.0;
+  if (i < B.nwalk) {
+    w = ((const WScal*)(B.state + (size_t)i * B.state_bytes + B.scal_off))->weight;
+    G.cnt[i] = 1;
+    G.nw[i] = w;
+    G.key[0][i] = (unsigned long long)__double_as_longlong(w);
+    G.idx[0][i] = i;
+  }
+  double v = warp_sum(w);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int k = 0; k < 8; k++) t += red[k];
+    G.psum[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_radix_hist(const unsigned long long* key, int n, int shift, int* hist,
+                                                    int ntiles) {
+  __shared__ int cnt[256];
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * RADIX_TILE;
+  for (int j = 0; j < RADIX_TILE / 256; j++) {
+    const int e = base + j * 256 + threadIdx.x;
+    if (e < n) atomicAdd(&cnt[(int)((key[e] >> shift) & 255ull)], 1);
+  }
+  __syncthreads();
+  hist[threadIdx.x * ntiles + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// exclusive scan of hist[256 * ntiles] in place (digit-major), one CTA
+__global__ void __launch_bounds__(1024) k_radix_scan(int* hist, int total) {
+  __shared__ int part[1024];
+  const int per = (total + 1023) / 1024;
+  const int s0 = threadIdx.x * per, s1 = min(total, s0 + per);
+  int run = 0;
+  for (int i = s0; i < s1; i++) run += hist[i];
+  part[threadIdx.x] = run;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {  // inclusive Hillis-Steele scan of the chunk sums
+    int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int off = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (int i = s0; i < s1; i++) {
+    const int v = hist[i];
+    hist[i] = off;
+    off += v;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_radix_scatter(const unsigned long long* kin, const int* iin,
+                                                       unsigned long long* kout, int* iout, int n, int shift,
+                                                       const int* off, int ntiles) {
+  __shared__ int wcount[8][256];
+  __shared__ int run[256];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  run[t] = 0;
+  const int base = blockIdx.x * RADIX_TILE;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int j = 0; j < RADIX_TILE / 256; j++) {
+    for (int k = t; k < 8 * 256; k += 256) (&wcount[0][0])[k] = 0;
+    __syncthreads();
+    const int e = base + j * 256 + t;
+    const bool valid = e < n;
+    unsigned long long key = 0;
+    int d = 256;  // invalid lanes share a digit no valid lane has
+    if (valid) {
+      key = kin[e];
+      d = (int)((key >> shift) & 255ull);
+    }
+    const unsigned m = __match_any_sync(0xffffffffu, d);
+    const int lrank = __popc(m & lt);
+    if (valid && lrank == 0) wcount[warp][d] = __popc(m);
+    __syncthreads();
+    if (valid) {
+      int before = 0;
+      for (int w = 0; w < warp; w++) before += wcount[w][d];
+      const int pos = off[d * ntiles + blockIdx.x] + run[d] + before + lrank;
+      kout[pos] = key;
+      iout[pos] = iin[e];
+    }
+    __syncthreads();
+    int sd = 0;
+    for (int w = 0; w < 8; w++) sd += wcount[w][t];
+    run[t] += sd;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_branch_pairs(BranchParams B, BranchBig G, int sorted) {
+  __shared__ int red[8];
+  const unsigned long long* key = G.key[sorted];
+  const int* idx = G.idx[sorted];
+  const int W = B.nwalk;
+  const int k = blockIdx.x * 256 + threadIdx.x;
+  int paired = 0;
+  if (k < W / 2) {
+    const int big = W - 1 - k;
+    const double w1 = __longlong_as_double((long long)key[big]);
+    if (big > 1 && w1 >= 1.8 && k < big) {
+      const int wb = idx[big], ws = idx[k];
+      const double w2 = __longlong_as_double((long long)key[k]);
+      const double weight1 = w1 / (w1 + w2);
+      Rand4 r = rand4(B.seed, (uint32_t)k, (uint64_t)B.dyn[DYN_BRANCH], 0u, 5u);
+      const double merged = (w1 + w2) / 2.0;
+      if (weight1 + r.u[0] >= 1.0) { G.cnt[wb] = 2; G.cnt[ws] = 0; G.nw[wb] = merged; }
+      else { G.cnt[wb] = 0; G.cnt[ws] = 2; G.nw[ws] = merged; }
+      paired = 1;
+    }
+  }
+  const int c = __reduce_add_sync(0xffffffffu, paired);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < 8; w++) t += red[w];
+    G.npair[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_branch_finish(BranchParams B, BranchBig G) {
+  __shared__ int chunk_sum[1024];
+  const int t = threadIdx.x, nt = blockDim.x, W = B.nwalk;
+  if (t == 0) {
+    double v = 0;
+    for (int b = 0; b < G.nprep; b++) v += G.psum[b];
+    double acc_ratio = B.acc->attempted > 0 ? B.acc->accepted / B.acc->attempted : 1.0;
+    B.dyn[DYN_TEFF] = B.timestep * acc_ratio;
+    B.dyn[DYN_ETRIAL] = B.dyn[DYN_EREF] - B.feedback * log(v / double(W));
+    B.dyn[DYN_SUMW] = v;
+    int np = 0;
+    for (int b = 0; b < G.npairblk; b++) np += G.npair[b];
+    if (np) B.dyn[DYN_PAIRS] += double(np);
+  }
+  const int per = (W + nt - 1) / nt;
+  const int s0 = t * per, s1 = min(W, s0 + per);
+  int cs = 0;
+  for (int i = s0; i < s1; i++) cs += G.cnt[i];
+  chunk_sum[t] = cs;
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+    for (int i = 0; i < nt; i++) { const int v = chunk_sum[i]; chunk_sum[i] = run; run += v; }
+  }
+  __syncthreads();
+  int off = chunk_sum[t];
+  for (int i = s0; i < s1; i++)
+    for (int c = 0; c < G.cnt[i]; c++) {
+      if (off < W) { B.src_of[off] = i; B.new_w[off] = G.nw[i]; }
+      off++;
+    }
+  __syncthreads();
+  if (t == 0) {
+    B.dyn[DYN_STEP] += double(B.nsteps);
+    B.dyn[DYN_BRANCH] += 1.0;
+  }
+}
+
 // Gather walkers into their new slots (positions + resident state).
 __global__ void k_gather(int nwalk, int n3, int state_bytes, int scal_off, const int* src_of, const double* new_w,
                          const double* R, const unsigned char* state, double* R2, unsigned char* state2) {

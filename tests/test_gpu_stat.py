@@ -79,6 +79,23 @@ def test_dmc_energy_matches_reference(precision):
     _check("DMC tau=0.05 " + ("fp64" if precision == engine.FP64 else "mixed"), mean, err, r)
 
 
+def test_dmc_energy_large_population_matches_reference():
+    """16384 walkers: population control on the device-wide sort."""
+    r = REF["dmc_tau0.05"]
+    d = systems.read_deck(DECK)
+    E = engine.Engine(DECK, engine.FP64, max_walkers=16384)
+    E.set_walkers(systems.random_configs(d, 16384, seed=14))
+    for b in range(10):
+        E.vmc_block(20, 0.5, seed=400 + b)
+    E.dmc_init(timestep=r["timestep"], nstep=r["steps_per_block"], seed=78)
+    for _ in range(r["equilibration_blocks"]):
+        E.dmc_block()
+    en = [E.dmc_block()["energy"] for _ in range(120)]
+    E.close()
+    mean, err = reblock(en)
+    _check("DMC tau=0.05 fp64, 16384 walkers", mean, err, r)
+
+
 def test_dmc_mixed_within_0p1_mHa_of_fp64():
     """Mixed minus FP64 DMC energy with common random numbers: both start
     from the same walkers with the same seed, so the walks coincide until a
