@@ -377,8 +377,8 @@ def run_extras(stream, dev, seconds=30.0):
                     "walkers, DMC tau=0.01, 5-step blocks; mixed = per-electron tensor-core MO contraction "
                     "(tcgen05 split TF32)")
     out["hbm_molecule"] = hm
-    # batched uneven molecules: 16 systems, 8-192 electrons, 512-4096 walkers
-    mols = systems.write_batch(os.path.join(tmp, "batch"), nsys=16, seed=SEED % 1000)
+    # batched uneven molecules: 64 systems, 8-192 electrons, 512-4096 walkers
+    mols = systems.write_batch(os.path.join(tmp, "batch"), nsys=64, seed=SEED % 1000)
     bat = {}
     for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
         engines = []
@@ -400,19 +400,19 @@ def run_extras(stream, dev, seconds=30.0):
         for E in engines:
             E.close()
     bat["mixed_vs_fp64"] = bat["mixed"]["walker_steps_per_s"] / bat["fp64"]["walker_steps_per_s"]
-    bat["config"] = ("16 seeded molecules, 2-32 atoms Z_eff 1-6, electrons log-uniform 8-192 (" +
+    bat["config"] = ("64 seeded molecules, 2-32 atoms Z_eff 1-6, electrons log-uniform 8-192 (" +
                      ",".join(str(d.nelec) for d, _ in mols) + "), 512-4096 walkers, one 5-step DMC block of "
                      "every system per graph launch; host wall time")
     out["batched"] = bat
     # serving: Poisson 2 jobs/s, bounded window
-    jobs = serving.workload(os.path.join(tmp, "serve"), njobs=12, seed=SEED % 997, emin=16, emax=64)
+    jobs = serving.workload(os.path.join(tmp, "serve"), njobs=12, seed=SEED % 997, emin=16, emax=128)
     srv = {}
     for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
         r = serving.run(jobs, prec, budget_bytes=120 << 30, nstep=5, time_limit=seconds)
         r.pop("events")
         srv[label] = r
     srv["mixed_vs_fp64"] = srv["mixed"]["walker_steps_per_s"] / srv["fp64"]["walker_steps_per_s"]
-    srv["config"] = (f"12 jobs, Poisson 2/s, seeded molecules and 8-atom cells of 16-64 electrons, 1024-8192 "
+    srv["config"] = (f"12 jobs, Poisson 2/s, seeded molecules and cells of 16-128 electrons, 1024-8192 "
                      f"walkers, 20-100 blocks of 5 steps, 120 GiB admission budget; first {seconds:.0f} s of the "
                      "stream (jobs still running at the limit are counted up to it)")
     out["serving"] = srv

@@ -7,7 +7,7 @@ in real time, reporting throughput and per-block latency percentiles.
 Workload (the serving configuration): jobs arrive as a Poisson process
 (mean ``rate`` jobs/s); each job is a seeded molecule (Z_eff 1-6 pseudo-atoms)
 or a periodic cell of the 8-atom Z_eff=4 family (supercells of 1, 4 or 8
-cells: 32, 128 or 512 electrons) with electron counts log-uniform in
+cells: 32, 128 or 256 electrons) with electron counts log-uniform in
 [emin, emax], 1024-8192 walkers and 20-100 blocks (log-uniform).
 """
 from __future__ import annotations
@@ -20,7 +20,10 @@ import numpy as np
 
 from . import engine, systems
 
-CELL_SIZES = {32: (1, 1, 1), 128: (2, 2, 1), 512: (2, 2, 2)}
+# electrons of the neutral cell -> supercell repeats of the 8-atom, 32-electron
+# cell; (2, 2, 2) is the 64-atom cell with a = 13.48 bohr and 832 basis
+# functions (64 atoms of Z_eff 4: 128 up, 128 down electrons)
+CELL_SIZES = {32: (1, 1, 1), 128: (2, 2, 1), 256: (2, 2, 2)}
 
 
 @dataclass

@@ -292,7 +292,7 @@ def write_periodic(outdir: str, seed: int = 4321, a: float = 6.74, image_cutoff:
     terms, all cut off inside half the cell (3.3 bohr) so the minimum-image
     Jastrow is smooth.  ``supercell`` = (n1, n2, n3) repeats the cell along
     the three axes (16 up + 16 down electrons per repeat), e.g. (2, 2, 2) is
-    the 64-atom, 512-electron cell with a = 13.48 bohr.
+    the 64-atom, 256-electron cell with a = 13.48 bohr (64 atoms of Z_eff 4).
 
     ``kpoint`` = (k1, k2, k3) writes KPOINT (twisted boundary conditions: a
     translation by lattice vector i multiplies the orbitals by exp(i pi k_i));
