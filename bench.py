@@ -238,7 +238,7 @@ def _e2e_block(engine, deck, R0, prec, steps, stream, dev):
     return ms
 
 
-def correlated_mixed_vs_fp64(engine, deck, R0, stream, nblock=40, nstep=40):
+def correlated_mixed_vs_fp64(engine, deck, R0, stream, npair=8, nblock=10, nstep=20):
     """Mixed minus FP64 DMC energy at equal statistics.
 
     (1) Common random numbers on the low-variance H4 pseudo-atom chain
@@ -252,19 +252,28 @@ def correlated_mixed_vs_fp64(engine, deck, R0, stream, nblock=40, nstep=40):
     evaluated in both precisions."""
     from mainline_b200 import systems
     h4 = os.path.join(ROOT, "tests", "golden", "h4pp.qw")
-    Rh = systems.random_configs(systems.read_deck(h4), NWALK, seed=SEED % 1000)
-    energies = {}
-    for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
-        E = engine.Engine(h4, prec, max_walkers=NWALK, stream=stream.cuda_stream)
-        E.set_walkers(Rh)
-        for b in range(5):
-            E.vmc_block(20, 0.5, seed=SEED + b)
-        E.dmc_init(timestep=0.05, nstep=nstep, seed=SEED + 77)
-        for _ in range(5):
-            E.dmc_block()
-        energies[label] = np.array([E.dmc_block()["energy"] for _ in range(nblock)])
-        E.close()
-    d = (energies["mixed"] - energies["fp64"]) * 1e3
+    F = engine.Engine(h4, engine.FP64, max_walkers=NWALK, stream=stream.cuda_stream)
+    F.set_walkers(systems.random_configs(systems.read_deck(h4), NWALK, seed=SEED % 1000))
+    for b in range(10):
+        F.vmc_block(20, 0.5, seed=SEED + b)
+    Rh = F.get_walkers()
+    F.close()
+    # independent pairs (fresh seeds), each a short walk from the same
+    # equilibrated walkers: pairs whose walks stay together measure the bias
+    # to ~1e-6 mHa; a pair that parts adds its block noise to the spread
+    pair_means, en_f, en_m = [], [], []
+    for k in range(npair):
+        energies = {}
+        for label, prec in (("fp64", engine.FP64), ("mixed", engine.MIXED)):
+            E = engine.Engine(h4, prec, max_walkers=NWALK, stream=stream.cuda_stream)
+            E.set_walkers(Rh)
+            E.dmc_init(timestep=0.05, nstep=nstep, seed=SEED + 77 + 1000 * k)
+            energies[label] = np.array([E.dmc_block()["energy"] for _ in range(nblock)])
+            E.close()
+        pair_means.append(float(np.mean(energies["mixed"] - energies["fp64"]) * 1e3))
+        en_f.append(np.mean(energies["fp64"]))
+        en_m.append(np.mean(energies["mixed"]))
+    d = np.array(pair_means)
     # estimator bias on the headline workload
     M = engine.Engine(deck.path, engine.MIXED, max_walkers=NWALK, stream=stream.cuda_stream)
     M.set_walkers(R0)
@@ -286,8 +295,9 @@ def correlated_mixed_vs_fp64(engine, deck, R0, stream, nblock=40, nstep=40):
     return {"common_random_numbers": {
                 "workload": "h4pp: 4 H pseudo-atoms, 4 electrons, RHF orbitals, DMC tau=0.05",
                 "mean": float(np.mean(d)), "sem": float(np.std(d, ddof=1) / np.sqrt(len(d))),
-                "blocks": nblock, "steps_per_block": nstep, "walkers": NWALK,
-                "fp64_energy": float(np.mean(energies["fp64"])), "mixed_energy": float(np.mean(energies["mixed"]))},
+                "per_pair": [round(x, 6) for x in pair_means], "pairs": npair,
+                "blocks_per_pair": nblock, "steps_per_block": nstep, "walkers": NWALK,
+                "fp64_energy": float(np.mean(en_f)), "mixed_energy": float(np.mean(en_m))},
             "estimator_bias_headline": {"mean": float(np.mean(de)),
                                         "sem": float(np.std(de, ddof=1) / np.sqrt(len(de))),
                                         "median_abs": float(np.median(np.abs(de))), "walkers": NWALK}}
