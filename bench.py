@@ -508,6 +508,30 @@ def main():
                          "branch:<deck>:<walkers> = two mixed-precision DMC blocks of 5 steps of a golden deck "
                          "(population control share)")
     args = ap.parse_args()
+    if args.probe and args.probe.startswith("phases:"):
+        # walker-kernel phase counters of the profiling library (built by
+        # python -m mainline_b200.build --phases): DMC blocks of a golden deck
+        os.environ["QWG_LIBRARY"] = os.path.join(ROOT, "mainline_b200", "libqwg_phases.so")
+        from mainline_b200 import engine, systems
+        _, name, nw = args.probe.split(":")
+        deck = os.path.join(ROOT, "tests", "golden", name + ".qw")
+        nw = int(nw)
+        out = {"deck": name, "walkers": nw}
+        for label, prec in (("mixed", engine.MIXED), ("fp64", engine.FP64)):
+            E = engine.Engine(deck, prec, max_walkers=nw)
+            E.set_walkers(systems.random_configs(systems.read_deck(deck), nw, seed=1))
+            E.vmc_block(2, 0.1, seed=2)
+            E.dmc_init(timestep=0.01, nstep=10, seed=3)
+            E.dmc_block()
+            E.phase_counters(reset=True)
+            st = E.dmc_block()
+            ph = E.phase_counters()
+            ws = nw * 10
+            out[label] = {"block_ms": st["block_ms"],
+                          "cycles_per_walker_step": {k: round(v / ws) for k, v in ph.items()}}
+            E.close()
+        print(json.dumps(out))
+        return
     if args.probe and args.probe.startswith("branch:"):
         from mainline_b200 import engine, systems
         _, name, nw = args.probe.split(":")

@@ -238,6 +238,17 @@ int qwg_vmc_block_noalloc(qwg_ctx* ctx, double* d_R, int nw, int nstep, double t
  * tiles).  Real orbitals only (QWG_ERR_ARG for complex ones). */
 int qwg_mo_eval(qwg_ctx* ctx, const double* pos, int npos, int spin, double* out);
 
+/* Walker-kernel phase counters (no counterpart in the reference: a profiling
+ * aid).  In the profiling build libqwg_phases.so every walker's warp adds the
+ * clock cycles it spends in each phase: out[0] MO rows of proposals, [1] rest
+ * of a proposal (ratio, drift, Jastrow), [2] Sherman-Morrison updates, [3]
+ * kinetic energy, [4] Coulomb/Ewald, [5] quadrature Jastrow values, [6]
+ * quadrature pairs, [7] projected coefficients, [8] quadrature points, [9]
+ * full recomputes, [10] whole step-mode launches; n <= 16 counters are
+ * copied, reset != 0 clears them.  The regular library returns
+ * QWG_ERR_STATE. */
+int qwg_phase_counters(qwg_ctx* ctx, unsigned long long* out, int n, int reset);
+
 /* Batched uneven systems: one CUDA graph holding one DMC block of every
  * context (each on its own stream, forked and joined inside the graph), so a
  * single graph launch advances all systems concurrently.  Every context must

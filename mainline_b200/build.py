@@ -44,7 +44,18 @@ def _stale(out, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, extra_nvflags=None) -> str:
+def build(verbose: bool = False, extra_nvflags=None, phases: bool = False) -> str:
+    """Build libqwg.so; phases=True builds the profiling library
+    libqwg_phases.so (walker-kernel phase counters, -DQWG_PHASES) in its own
+    object folder."""
+    if phases:
+        global BUILD, LIB
+        saved = BUILD, LIB
+        BUILD, LIB = os.path.join(HERE, "_build_phases"), os.path.join(HERE, "libqwg_phases.so")
+        try:
+            return build(verbose, list(extra_nvflags or []) + ["-DQWG_PHASES"], False)
+        finally:
+            BUILD, LIB = saved
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
     headers.append(os.path.join(ROOT, "include", "qwg.h"))
@@ -82,4 +93,4 @@ def build(verbose: bool = False, extra_nvflags=None) -> str:
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    print(build(verbose="-v" in sys.argv, phases="--phases" in sys.argv))

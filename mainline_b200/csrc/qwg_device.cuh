@@ -275,6 +275,32 @@ enum DynSlot {
 };
 
 // Launch parameters shared by the step kernels.
+// Phase counters of the walker kernels, compiled in with -DQWG_PHASES only
+// (the profiling build libqwg_phases.so): each counter sums the clock64()
+// cycles lane 0 of a walker's warp spends in one phase, over every walker.
+enum QwgPhase {
+  PH_MO = 0,          // basis rows + MO contraction of a proposal (or its read from the GEMM)
+  PH_PROPOSE_REST,    // ratio, drift, Jastrow of the moved electron
+  PH_ACCEPT,          // Sherman-Morrison update and state bookkeeping
+  PH_KINETIC,
+  PH_POTENTIAL,       // Coulomb or Ewald
+  PH_PP_JASTROW,      // quadrature: Jastrow values of the electrons at their positions
+  PH_PP_ITEMS,        // quadrature: (electron, atom) pairs inside the cutoff
+  PH_PP_PROJECT,      // quadrature: projected coefficients C A^-1
+  PH_PP_POINTS,       // quadrature: point ratios (basis values, Jastrow)
+  PH_REFRESH,         // full recompute and re-inversion
+  PH_WALKER,          // a walker's whole step-mode launch (moves or local energy)
+  PH_COUNT = 16
+};
+#ifdef QWG_PHASES
+#define QWG_PHASE_BEGIN(t) const long long t = clock64();
+#define QWG_PHASE_END(t, slot, ctr) \
+  if ((ctr) && (threadIdx.x & 31) == 0) atomicAdd(&(ctr)[slot], (unsigned long long)(clock64() - t));
+#else
+#define QWG_PHASE_BEGIN(t)
+#define QWG_PHASE_END(t, slot, ctr)
+#endif
+
 struct StepParams {
   int nwalk;
   int nsteps;
@@ -317,6 +343,7 @@ struct StepParams {
   float* tc_ahi;
   float* tc_alo;
   const float* tc_D;
+  unsigned long long* phases;  // [PH_COUNT] counters (profiling builds), or null
 };
 
 // ---------------------------------------------------------------------------

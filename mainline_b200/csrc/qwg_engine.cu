@@ -166,6 +166,7 @@ struct qwg_ctx {
   // population control on the device-wide sort at every population size
   // (QWG_BRANCH_DEVICE_WIDE=1; by default only above kBranchSmemMax walkers)
   bool branch_device_wide = false;
+  DevBuf d_phases;  // walker-kernel phase counters (profiling builds, -DQWG_PHASES)
   DevBuf d_tc_a, d_tc_d;
 };
 
@@ -628,6 +629,7 @@ static StepParams base_params(qwg_ctx* c) {
   P.refresh = 1;
   P.vmc_depth = c->vmc_depth;
   P.vmc_divider = c->vmc_divider;
+  P.phases = c->d_phases.p ? c->d_phases.as<unsigned long long>() : nullptr;
   if (c->tc_moves) {
     P.tc_kpad = c->tc_kpad;
     P.tc_ldd = c->tc_ldd;
@@ -1070,6 +1072,10 @@ int qwg_create(const char* deck_path, int precision, int max_walkers, void* stre
     c->d_state2.alloc((size_t)max_walkers * c->L.state_bytes);
     if (hbm_family(c->mmax)) c->d_scratch.alloc((size_t)max_walkers * c->L.scratch_bytes);
     if (const char* bw = std::getenv("QWG_BRANCH_DEVICE_WIDE")) c->branch_device_wide = bw[0] == '1';
+#ifdef QWG_PHASES
+    c->d_phases.alloc(PH_COUNT * sizeof(unsigned long long));
+    CK(cudaMemsetAsync(c->d_phases.p, 0, PH_COUNT * sizeof(unsigned long long), c->stream));
+#endif
     if (tc_moves_eligible(c.get())) {
       tc_setup(c.get());
       c->tc_ldd = std::max(c->tc_bn[0], c->tc_bn[1]);
@@ -1238,6 +1244,19 @@ int qwg_eval(qwg_ctx* c, const double* rot, qwg_eval_out* out) {
     dl(out->nonlocal, d_nl, W); dl(out->grad, d_g, n_g); dl(out->lap, d_l, n_l);
     CK(cudaStreamSynchronize(c->stream));
     c->state_valid = false;  // eval leaves scratch state unsaved
+    return QWG_OK;
+  });
+}
+
+int qwg_phase_counters(qwg_ctx* c, unsigned long long* out, int n, int reset) {
+  if (!c || (n > 0 && !out)) return QWG_ERR_ARG;
+  if (!c->d_phases.p) return fail(c, QWG_ERR_STATE, "qwg_phase_counters: this library was built without phase "
+                                                    "counters (build libqwg_phases.so)");
+  return guarded(c, [&]() -> int {
+    CK(cudaStreamSynchronize(c->stream));
+    const int m = std::min(n, (int)PH_COUNT);
+    if (m > 0) CK(cudaMemcpy(out, c->d_phases.p, m * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    if (reset) CK(cudaMemset(c->d_phases.p, 0, PH_COUNT * sizeof(unsigned long long)));
     return QWG_OK;
   });
 }

@@ -55,6 +55,7 @@ struct Walker {
   // tcD[(row0 + q) * tc_ldd + i] = component q of orbital i
   const float* tcD = nullptr;
   int tc_ldd = 0;
+  unsigned long long* ph = nullptr;  // phase counters (profiling builds)
   static constexpr bool CPX = MMAX < 0;
   // F and G basis shells: compiled into the HBM-resident kernels only
   static constexpr bool HL = MMAX <= 0;
@@ -361,6 +362,7 @@ struct Walker {
       r1 = (a[1] * a[0] + b[1] * b[0]) / r0; r2 = (a[2] * a[0] + b[2] * b[0]) / r0;
       r3 = (a[3] * a[0] + b[3] * b[0]) / r0; r4 = (a[4] * a[0] + b[4] * b[0]) / r0;
     } else {
+      QWG_PHASE_BEGIN(t_mo)
       bool from_gemm = false;
       if constexpr (MMAX == 0 && sizeof(Real) == 4) {
         if (tcD) {
@@ -373,6 +375,7 @@ struct Walker {
         }
       }
       if (!from_gemm) mo_lap_warp<Real, PER, HL>(S, mocs(s), px, py, pz, M, bas(), nc, lane);
+      QWG_PHASE_END(t_mo, PH_MO, ph)
       const Real* iv = inv(s) + (size_t)el * MS();
       for (int i = 0; i < M; i++) {
         double c = iv[i];
@@ -380,6 +383,7 @@ struct Walker {
         r3 += c * double(nc[i * 5 + 3]); r4 += c * double(nc[i * 5 + 4]);
       }
     }
+    QWG_PHASE_BEGIN(t_rest)
     ratioD = double(r0);
     double gD[3] = {double(r1) / ratioD, double(r2) / ratioD, double(r3) / ratioD};
     double lD = double(r4) / ratioD;
@@ -463,6 +467,7 @@ struct Walker {
     __syncwarp();
     if (lane == 0) { dG()[4 * e] = gu[0]; dG()[4 * e + 1] = gu[1]; dG()[4 * e + 2] = gu[2]; dG()[4 * e + 3] = lu_; }
     __syncwarp();
+    QWG_PHASE_END(t_rest, PH_PROPOSE_REST, ph)
   }
 
   // ---- accept the proposal of electron e: Sherman-Morrison update of the
@@ -711,9 +716,11 @@ struct Walker {
     double res_total = 1.0, res_x = 0, res_y = 0, res_z = 0;  // one-move-per-walker reservoir
     int res_e = -1;
     // per-electron Jastrow value at the current position
+    QWG_PHASE_BEGIN(t_ue)
     for (int e = lane; e < N; e += 32)
       Ue()[e] = double(jas_electron_val<Real, TB>(S, Rp, e, Rp[3 * e], Rp[3 * e + 1], Rp[3 * e + 2]));
     __syncwarp();
+    QWG_PHASE_END(t_ue, PH_PP_JASTROW, ph)
     double vnl = 0;
     // electrons in chunks of L.wchunk: the (electron, atom) items of the
     // chunk in electron-major order, the chunk's projected coefficients, then
@@ -723,6 +730,7 @@ struct Walker {
     Real* w = wproj();
     for (int e0 = 0; e0 < N; e0 += CH) {
       const int e1 = min(N, e0 + CH);
+      QWG_PHASE_BEGIN(t_items)
       int nitems = 0;
       for (int base0 = e0 * A; base0 < e1 * A; base0 += 32) {
         const int idx = base0 + lane;
@@ -759,7 +767,9 @@ struct Walker {
         nitems += __popc(m);
       }
       __syncwarp();
+      QWG_PHASE_END(t_items, PH_PP_ITEMS, ph)
       if (nitems == 0) continue;
+      QWG_PHASE_BEGIN(t_proj)
       const int nproj = multi() ? L.nud : 1;  // projected-coefficient sets per electron
       for (int idx = lane; idx < (e1 - e0) * S.nbasis * nproj && multi(); idx += 32) {
         // one set per distinct spin-determinant u: w_f = sum_i C[f][col_u(i)] (A_u^-1)[i][e]
@@ -806,6 +816,8 @@ struct Walker {
         w[le * S.nbasis + f] = acc;
       }
       __syncwarp();
+      QWG_PHASE_END(t_proj, PH_PP_PROJECT, ph)
+      QWG_PHASE_BEGIN(t_pts)
       int total = 0;
       for (int k = 0; k < nitems; k++) total += S.pp_aip[S.atom_type[it[k].a]];
       int k = 0, qoff = 0;  // running item cursor for this lane's points
@@ -867,6 +879,7 @@ struct Walker {
         if (tmoves) cand[p] = ts * ratio;
       }
       __syncwarp();
+      QWG_PHASE_END(t_pts, PH_PP_POINTS, ph)
       if (tmoves) {
         // target of point p of this chunk (the same arithmetic as above)
         auto point_pos = [&](int p, double& x, double& y, double& z) {
@@ -1006,6 +1019,8 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
     unsigned char* sb = HBM ? P.scratch + (size_t)wid * L.scratch_bytes : wb + L.state_bytes;
     Walker<Real, MMAX, TB, PER> W{S, L, wb, sb, moc_s, lane};
     // tensor-core move schedule: this launch moves electron P.tc_e only
+    W.ph = P.phases;
+    QWG_PHASE_BEGIN(t_walker)
     const int tc_phase = (mode == KM_SWEEP && MMAX == 0 && sizeof(Real) == 4) ? P.tc_phase : 0;
     if (tc_phase == 2) {
       W.tcD = P.tc_D + (size_t)wid * 5 * P.tc_ldd;
@@ -1031,7 +1046,9 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
       double keep_e = 0, keep_w = 1;
       if (STEPS) { keep_e = ((WScal*)(gstate + L.scal))->eold; keep_w = ((WScal*)(gstate + L.scal))->weight; }
       __syncwarp();
+      QWG_PHASE_BEGIN(t_ref)
       W.recompute();
+      QWG_PHASE_END(t_ref, PH_REFRESH, P.phases)
       if (lane == 0 && STEPS) { W.sc()->eold = keep_e; W.sc()->weight = keep_w; }
       __syncwarp();
     } else if constexpr (!HBM) {
@@ -1186,7 +1203,9 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
             }
             natt += 1;
             if (acc + rb.u[0] > 1.0) {
+              QWG_PHASE_BEGIN(t_acc)
               W.accept(e, wx, wy, wz, ratioD, dU);
+              QWG_PHASE_END(t_acc, PH_ACCEPT, P.phases)
               nacc += 1;
             } else if constexpr (mode == KM_STEPS) {
               if (!P.dmc && P.vmc_depth > 1) {
@@ -1243,8 +1262,12 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
           Rand4 rr = rand4(P.seed, wid, step, 0xffffu, 3u);
           double rm[9];
           random_rotation(rr, rm);
+          QWG_PHASE_BEGIN(t_kin)
           double kin = W.kinetic();
+          QWG_PHASE_END(t_kin, PH_KINETIC, P.phases)
+          QWG_PHASE_BEGIN(t_pot)
           double pot = W.coulomb();
+          QWG_PHASE_END(t_pot, PH_POTENTIAL, P.phases)
           double nl = 0.0;
           if (S.has_pp) {
             if constexpr (mode == KM_ELOC_TM)
@@ -1280,6 +1303,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
           npts += 1;
         }
       }
+      QWG_PHASE_END(t_walker, PH_WALKER, P.phases)
       if (lane == 0) {
         if (!ELOCM) { atomicAdd(&cta_acc[6], nacc); atomicAdd(&cta_acc[7], natt); }
         if (mode != KM_SWEEP) {

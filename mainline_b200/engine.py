@@ -26,7 +26,7 @@ MIXED = 1
 EXPORTS = [
     "qwg_version", "qwg_last_error", "qwg_create", "qwg_destroy", "qwg_get_info", "qwg_inspect_deck",
     "qwg_inspect_spline", "qwg_set_walkers", "qwg_get_walkers", "qwg_set_walkers_device",
-    "qwg_get_walker_scalars", "qwg_eval", "qwg_mo_eval",
+    "qwg_get_walker_scalars", "qwg_eval", "qwg_mo_eval", "qwg_phase_counters",
     "qwg_ratio", "qwg_set_vmc_dynamics", "qwg_vmc_block", "qwg_dmc_init", "qwg_dmc_block", "qwg_dmc_block_async", "qwg_dmc_block_wait",
     "qwg_vmc_block_noalloc", "qwg_batch_create", "qwg_batch_block", "qwg_batch_destroy", "qwg_autotune",
     "qwg_launch_count", "qwg_reset_launch_count", "qwg_footprint", "qwg_dmc_block_ready", "qwg_time_kernels",
@@ -118,6 +118,7 @@ def load_library(path: str = LIB_PATH):
         "qwg_eval": (C.c_int, [C.c_void_p, dp, P(EvalOut)]),
         "qwg_ratio": (C.c_int, [C.c_void_p, P(C.c_int), dp, dp, dp, dp, dp]),
         "qwg_mo_eval": (C.c_int, [C.c_void_p, dp, C.c_int, C.c_int, dp]),
+        "qwg_phase_counters": (C.c_int, [C.c_void_p, P(C.c_ulonglong), C.c_int, C.c_int]),
         "qwg_set_vmc_dynamics": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
         "qwg_vmc_block": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_int, P(BlockStats)]),
         "qwg_dmc_init": (C.c_int, [C.c_void_p, P(DmcParams)]),
@@ -276,6 +277,15 @@ class Engine:
         out = np.zeros((pos.shape[0], nmo, 5))
         self._check(self.lib.qwg_mo_eval(self.h, _ptr(pos), pos.shape[0], spin, _ptr(out)), "qwg_mo_eval")
         return out
+
+    PHASES = ["mo_rows", "propose_rest", "accept", "kinetic", "potential", "pp_jastrow", "pp_items", "pp_project",
+              "pp_points", "refresh", "walker_launch"]
+
+    def phase_counters(self, reset: bool = False) -> dict:
+        """Clock cycles per walker-kernel phase (profiling build only)."""
+        buf = (C.c_ulonglong * 16)()
+        self._check(self.lib.qwg_phase_counters(self.h, buf, 16, int(reset)), "qwg_phase_counters")
+        return {name: int(buf[i]) for i, name in enumerate(self.PHASES)}
 
     def ratio(self, e: np.ndarray, rnew: np.ndarray):
         W = self.nwalk

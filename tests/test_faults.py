@@ -1,5 +1,6 @@
 """Faulty inputs, injected on the host: non-finite numbers in the tables,
-truncated or missing orbital files, and a singular orbital set.  The deck
+truncated or missing orbital files, and a singular orbital set (an orbital
+that is zero everywhere).  The deck
 reader (qwg_inspect_deck, no GPU) refuses the first kinds with
 QWG_ERR_INPUT and a message; a wave function whose determinant vanishes
 everywhere reaches the device, evaluates to log|psi| = -1e201 (an exact zero
@@ -69,15 +70,16 @@ def test_missing_orbital_file(tmp_path):
 
 
 def _singular_deck(tmp_path):
-    """Spin-up orbital 2 made a copy of orbital 1 (its ORB records point at
-    orbital 1's coefficient labels)."""
+    """Spin-up orbital 2 made identically zero: its ORB records point at one
+    extra coefficient label whose value is 0, so every Slater matrix has a
+    zero column (an exactly singular orbital set)."""
     deck, orb = _copy(tmp_path)
     txt = orb.read_text()
     head, tail = txt.split("COEFFICIENTS\n", 1)
     recs = [ln.split() for ln in head.splitlines() if ln.strip()]
-    lab1 = {(r[1], r[2]): r[3] for r in recs if r[0] == "1"}
-    out = [" ".join([r[0], r[1], r[2], lab1[(r[1], r[2])] if r[0] == "2" else r[3]]) for r in recs]
-    orb.write_text("\n".join(out) + "\nCOEFFICIENTS\n" + tail)
+    zero = max(int(r[3]) for r in recs) + 1
+    out = [" ".join([r[0], r[1], r[2], str(zero) if r[0] == "2" else r[3]]) for r in recs]
+    orb.write_text("\n".join(out) + "\nCOEFFICIENTS\n" + tail.rstrip("\n") + "\n0.0\n")
     return deck
 
 
