@@ -548,9 +548,10 @@ static void gesqua(int& aip, std::vector<double>& q, std::vector<double>& wq) {
   }
 }
 
-static double pp_radial(const PPAtom& P, int l, double r) {
+static double pp_radial(const PPAtom& P, int spin, int l, double r) {
+  const std::vector<int>& tf = spin == 0 ? P.term_first : P.term_first_dn;
   double v = 0;
-  for (int t = P.term_first[l]; t < P.term_first[l + 1]; t++) {
+  for (int t = tf[l]; t < tf[l + 1]; t++) {
     double ex = std::min(P.term_a[t] * r * r, 60.0);
     v += P.term_c[t] * std::pow(r, P.term_n[t]) * std::exp(-ex);
   }
@@ -1149,37 +1150,57 @@ HostSystem build_system(const std::string& deck_path) {
   // ---- PSEUDO
   S.pp.assign(S.natoms, PPAtom());
   for (auto& t : all_sections(words, "PSEUDO")) {
-    if (has_keyword(t, "SPIN_DEP")) throw InputError("SPIN_DEP pseudopotentials are not supported");
-    if (has_keyword(t, "ADD_ZEFF")) throw InputError("ADD_ZEFF is not supported");
     PPAtom P;
     P.aip = (int)value_d(t, "AIP", 6);
-    auto bw = get_section(t, "BASIS");
-    if (bw.size() < 2 || !ieq(bw[1], "RGAUSSIAN")) throw InputError("PSEUDO BASIS must be RGAUSSIAN");
-    auto oq = get_section(bw, "OLDQMC");
-    if (oq.size() < 2) throw InputError("badly formed OLDQMC section");
-    size_t it = 1;
-    P.nchan = to_i(oq[it++]);
-    std::vector<int> nper(P.nchan);
-    for (int l = 0; l < P.nchan; l++) nper[l] = to_i(oq[it++]);
-    P.term_first.push_back(0);
-    for (int l = 0; l < P.nchan; l++) {
-      for (int j = 0; j < nper[l]; j++) {
-        if (it + 2 >= oq.size()) throw InputError("truncated OLDQMC section");
-        P.term_n.push_back(to_d(oq[it]) - 2.0);
-        P.term_a.push_back(to_d(oq[it + 1]));
-        P.term_c.push_back(to_d(oq[it + 2]));
-        it += 3;
+    // RGAUSSIAN OLDQMC channels appended to P's term list; returns the
+    // per-channel term offsets (Rgaussian_function.cpp:24-107)
+    auto read_rgaussian = [&](const std::vector<std::string>& bw) {
+      if (bw.size() < 2 || !ieq(bw[1], "RGAUSSIAN")) throw InputError("PSEUDO BASIS must be RGAUSSIAN");
+      auto oq = get_section(bw, "OLDQMC");
+      if (oq.size() < 2) throw InputError("badly formed OLDQMC section");
+      size_t it = 1;
+      const int nchan = to_i(oq[it++]);
+      std::vector<int> nper(nchan);
+      for (int l = 0; l < nchan; l++) nper[l] = to_i(oq[it++]);
+      std::vector<int> first{(int)P.term_n.size()};
+      for (int l = 0; l < nchan; l++) {
+        for (int j = 0; j < nper[l]; j++) {
+          if (it + 2 >= oq.size()) throw InputError("truncated OLDQMC section");
+          P.term_n.push_back(to_d(oq[it]) - 2.0);
+          P.term_a.push_back(to_d(oq[it + 1]));
+          P.term_c.push_back(to_d(oq[it + 2]));
+          it += 3;
+        }
+        first.push_back((int)P.term_n.size());
       }
-      P.term_first.push_back((int)P.term_n.size());
+      return first;
+    };
+    // SPIN_DEP: separate radial bases for spin-up and spin-down electrons
+    // (Pseudopotential.cpp:912-933); ADD_ZEFF adds Z_ion / r to the local
+    // channel (:309-316, 937-939)
+    if (has_keyword(t, "SPIN_DEP")) {
+      P.term_first = read_rgaussian(get_section(t, "BASIS_UP"));
+      P.term_first_dn = read_rgaussian(get_section(t, "BASIS_DN"));
+      if (P.term_first.size() != P.term_first_dn.size())
+        throw InputError("SPIN_DEP: BASIS_UP and BASIS_DN have different channel counts");
+    } else {
+      P.term_first = read_rgaussian(get_section(t, "BASIS"));
+      P.term_first_dn = P.term_first;
     }
+    P.nchan = (int)P.term_first.size() - 1;
+    P.add_zeff = has_keyword(t, "ADD_ZEFF");
     gesqua(P.aip, P.quad, P.weight);
     // evaluation radius: scan from 20 bohr down in 0.05 steps for the first
-    // |v_l| > 1e-5 of each nonlocal channel (a channel never above it keeps 20)
+    // |v_l| > 1e-5 of each nonlocal channel for either spin (a channel never
+    // above it keeps 20)
     std::vector<double> cutL(std::max(P.nchan - 1, 0), 20.0);
     std::vector<int> found(cutL.size(), 0);
     for (double r = 20.0; r > 0; r -= 0.05)
       for (int l = 0; l + 1 < P.nchan; l++)
-        if (std::fabs(pp_radial(P, l, r)) > 1e-5 && !found[l]) { cutL[l] = r - 0.05; found[l] = 1; }
+        if ((std::fabs(pp_radial(P, 0, l, r)) > 1e-5 || std::fabs(pp_radial(P, 1, l, r)) > 1e-5) && !found[l]) {
+          cutL[l] = r - 0.05;
+          found[l] = 1;
+        }
     P.cutoff = 0;
     for (double c : cutL) P.cutoff = std::max(P.cutoff, c);
     bool any = false;

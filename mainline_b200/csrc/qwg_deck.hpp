@@ -63,7 +63,9 @@ struct PPAtom {
   int nchan = 0;                 // channels incl. the local one (last)
   int aip = 0;                   // quadrature points
   double cutoff = 0.0;           // nonlocal evaluation radius
-  std::vector<int> term_first;   // [nchan+1]
+  std::vector<int> term_first;   // [nchan+1] terms of each channel for spin-up electrons
+  std::vector<int> term_first_dn;  // [nchan+1] for spin-down electrons (= term_first unless SPIN_DEP)
+  bool add_zeff = false;         // ADD_ZEFF: the local channel also carries +Z_ion / r
   std::vector<double> term_n;    // r power (already n-2)
   std::vector<double> term_a;    // Gaussian exponent
   std::vector<double> term_c;    // coefficient

@@ -47,7 +47,7 @@ constexpr int QWG_MAXT = 8;        // atom types (labels)
 constexpr int QWG_MAXEE = 8;       // e-e radial functions
 constexpr int QWG_MAXEI = 8;       // e-n radial functions per type
 constexpr int QWG_MAXTB = 12;      // e-e-n terms per type
-constexpr int QWG_MAXPPT = 16;     // pseudopotential Gaussian terms per type
+constexpr int QWG_MAXPPT = 24;     // pseudopotential Gaussian terms per type (both spins of SPIN_DEP)
 constexpr int QWG_MAXQ = 32;       // quadrature points
 constexpr int QWG_MAXSHELL = 1024; // basis shells
 constexpr int QWG_MAXDET = 64;     // determinants of an expansion
@@ -115,7 +115,9 @@ struct DevSys {
   int has_pp;
   int pp_nchan[QWG_MAXT], pp_aip[QWG_MAXT];
   double pp_cutoff[QWG_MAXT];
-  int pp_term_first[QWG_MAXT][8];
+  int pp_term_first[QWG_MAXT][8];      // spin-up electrons
+  int pp_term_first_dn[QWG_MAXT][8];   // spin-down electrons (SPIN_DEP; else the same)
+  int pp_addzeff[QWG_MAXT];            // ADD_ZEFF: +Z_ion/r in the local channel
   double pp_term[QWG_MAXT][QWG_MAXPPT][3];  // (n, a, c)
   double pp_quad[QWG_MAXT][QWG_MAXQ][3];
   double pp_w[QWG_MAXT][QWG_MAXQ];

@@ -317,9 +317,13 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     S.pp_aip[t] = P.aip;
     S.pp_cutoff[t] = P.cutoff;
     if (P.nchan > 5) throw InputError("pseudopotential channels beyond l=3 are not supported");
-    if ((int)P.term_n.size() > QWG_MAXPPT) throw InputError("more than 16 pseudopotential terms on one atom");
+    if ((int)P.term_n.size() > QWG_MAXPPT) throw InputError("more than 24 pseudopotential terms on one atom (both spins)");
     if (P.aip > QWG_MAXQ) throw InputError("quadratures above 32 points are not supported");
-    for (int l = 0; l <= P.nchan && P.nchan; l++) S.pp_term_first[t][l] = P.term_first[l];
+    for (int l = 0; l <= P.nchan && P.nchan; l++) {
+      S.pp_term_first[t][l] = P.term_first[l];
+      S.pp_term_first_dn[t][l] = P.term_first_dn[l];
+    }
+    S.pp_addzeff[t] = P.add_zeff ? 1 : 0;
     for (size_t n = 0; n < P.term_n.size(); n++) {
       S.pp_term[t][n][0] = P.term_n[n];
       S.pp_term[t][n][1] = P.term_a[n];

@@ -680,9 +680,12 @@ struct Walker {
     return warp_sum(v) + S.ion_ion;
   }
 
-  __device__ double pp_radial(int t, int l, double r) const {
+  // Radial v_l(r) of channel l for an electron of spin s (SPIN_DEP tables
+  // per spin, Pseudopotential::getRadial, Pseudopotential.cpp:305-336).
+  __device__ double pp_radial(int t, int s, int l, double r) const {
+    const int* tf = s == 0 ? S.pp_term_first[t] : S.pp_term_first_dn[t];
     double v = 0;
-    for (int n = S.pp_term_first[t][l]; n < S.pp_term_first[t][l + 1]; n++) {
+    for (int n = tf[l]; n < tf[l + 1]; n++) {
       const double* q = S.pp_term[t][n];
       double ex = fmin(q[1] * r * r, 60.0);
       const double pw = q[0];
@@ -746,8 +749,9 @@ struct Walker {
             item.dx = Rp[3 * e] - ap[0]; item.dy = Rp[3 * e + 1] - ap[1]; item.dz = Rp[3 * e + 2] - ap[2];
             min_image(S, item.dx, item.dy, item.dz);
             item.r = sqrt(item.dx * item.dx + item.dy * item.dy + item.dz * item.dz);
-            vloc += pp_radial(t, nch - 1, item.r);
-            for (int l = 0; l < 4; l++) item.vl[l] = (l < nch - 1) ? pp_radial(t, l, item.r) : 0.0;
+            const int sp = spin(e);
+            vloc += pp_radial(t, sp, nch - 1, item.r) + (S.pp_addzeff[t] ? S.atom_charge[a] / item.r : 0.0);
+            for (int l = 0; l < 4; l++) item.vl[l] = (l < nch - 1) ? pp_radial(t, sp, l, item.r) : 0.0;
             if (deterministic) {
               take = item.r < S.pp_cutoff[t];
             } else {
@@ -994,6 +998,11 @@ template <>
 struct MinBlocks<KM_ELOC> { static constexpr int value = QWG_MIN_BLOCKS_ELOC; };
 template <>
 struct MinBlocks<KM_ELOC_TM> { static constexpr int value = QWG_MIN_BLOCKS_ELOC; };
+
+// the parameter bank, layout, step parameters and I/O pointers travel as
+// kernel parameters (at most 32764 bytes on sm_70 and later)
+static_assert(sizeof(DevSys<double>) + sizeof(WLayout) + sizeof(StepParams) + sizeof(EvalIO) <= 32764,
+              "walker kernel parameters exceed 32764 bytes");
 
 template <typename Real, int MMAX, int mode, bool TB, int PER>
 __global__ void __launch_bounds__(128, MinBlocks<mode>::value)

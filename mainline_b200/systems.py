@@ -178,6 +178,28 @@ def _jastrow_pade_spin_text(rng, label: str) -> str:
     ])
 
 
+def _oldqmc_lines(rng, zeff: float) -> list:
+    lines = ["  OLDQMC {", "  0.0 3", "  3 3 3"]
+    for _l in range(2):
+        for _ in range(3):
+            lines.append(f"    2 {_fmt(rng.uniform(1.0, 10.0))} {_fmt(rng.uniform(-5.0, 5.0))}")
+    lines.append(f"    1 {_fmt(rng.uniform(1.0, 10.0))} {_fmt(zeff)}")
+    for _ in range(2):
+        lines.append(f"    2 {_fmt(rng.uniform(1.0, 10.0))} {_fmt(rng.uniform(-5.0, 5.0))}")
+    lines.append("  }")
+    return lines
+
+
+def _pseudo_text_spin(rng, label: str, zeff: float, aip: int, add_zeff: bool) -> str:
+    """SPIN_DEP pseudopotential: separate RGAUSSIAN OLDQMC bases for spin-up
+    (BASIS_UP) and spin-down (BASIS_DN) electrons, optionally ADD_ZEFF."""
+    lines = [f"PSEUDO {{ {label}", "  SPIN_DEP"] + (["  ADD_ZEFF"] if add_zeff else []) + [f"  AIP {aip}"]
+    for sec in ("BASIS_UP", "BASIS_DN"):
+        lines += [f"  {sec} {{ {label}", "  RGAUSSIAN"] + _oldqmc_lines(rng, zeff) + ["  }"]
+    lines.append("}")
+    return "\n".join(lines)
+
+
 def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
     """RGAUSSIAN OLDQMC block: channels l=0, l=1 and the local channel (the
     reference treats the LAST listed channel as local, Pseudopotential.cpp:790).
@@ -200,7 +222,7 @@ def _pseudo_text(rng, label: str, zeff: float, aip: int = 12) -> str:
 def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | None = None,
              name: str | None = None, expansion=None, high_l: bool = False, jastrow: bool = True,
              dup_basis: bool = False, mo_kind: str = "BLAS_MO", aip: int = 12,
-             jastrow_variant: str | None = None) -> Deck:
+             jastrow_variant: str | None = None, pp_variant: str | None = None) -> Deck:
     """Two-atom molecule of the all-electron (``pseudo=False``) or Z_eff=5
     pseudopotential (``pseudo=True``) workload.  ``method`` is an optional
     METHOD section body written into the deck (e.g. ``"VMC NBLOCK 50 ..."``).
@@ -211,7 +233,11 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
     7F_crystal, 9G, 15G per atom, CRYSTAL normalisation).  ``jastrow=False``
     writes a Slater wave function alone (TRIALFUNC { SLATER ... });
     ``dup_basis`` writes the BASIS section twice (the reference appends both to
-    the atoms: the copies' functions carry no orbital coefficients)."""
+    the atoms: the copies' functions carry no orbital coefficients).
+    ``aip``: the pseudopotential quadrature (4, 6, 12, 18, 26 or 32 points).
+    ``jastrow_variant="pade_spin"``: the PADE / THREEBODY_SPIN / SM_TERMS
+    Jastrow of _jastrow_pade_spin_text.  ``pp_variant="spin_dep"``: a SPIN_DEP
+    pseudopotential with ADD_ZEFF (_pseudo_text_spin)."""
     os.makedirs(outdir, exist_ok=True)
     rng = np.random.default_rng(seed)
     label = "N"
@@ -232,6 +258,8 @@ def write_n2(outdir: str, seed: int = 1234, pseudo: bool = False, method: str | 
     cdn = _random_orthonormal(rng, nb, nspin_mo)
     onebody = rng.normal(0.0, 0.1, size=4)
     pp = _pseudo_text(rng, label, charge, aip=aip) if pseudo else ""
+    if pseudo and pp_variant == "spin_dep":
+        pp = _pseudo_text_spin(rng, label, charge, aip, add_zeff=True)
     jtext = _jastrow_pade_spin_text(rng, label) if jastrow_variant == "pade_spin" else _jastrow_text(label, onebody)
     name = name or ("n2_pseudo" if pseudo else "n2_allelectron")
     orb = os.path.join(outdir, f"{name}.orb")

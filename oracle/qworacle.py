@@ -582,29 +582,65 @@ class System:
         self.tb_stale_ei = self._has3s and not self._has3
 
     # Pseudopotential (system/Pseudopotential.cpp:874-1033, Rgaussian_function.cpp)
+    @staticmethod
+    def _read_rgaussian(bw):
+        """OLDQMC channels of an RGAUSSIAN basis (Rgaussian_function.cpp:24-107)."""
+        oq = section(bw, "OLDQMC")
+        it = 1  # zeff
+        nl = int(oq[it]); it += 1
+        nper = [int(oq[it + l]) for l in range(nl)]
+        it += nl
+        chans = []
+        for l in range(nl):
+            terms = []
+            for _ in range(nper[l]):
+                terms.append((float(oq[it]) - 2.0, float(oq[it + 1]), float(oq[it + 2])))
+                it += 3
+            chans.append(terms)
+        return chans
+
     def _read_pseudo(self, pstexts):
+        """SPIN_DEP: BASIS_UP / BASIS_DN radial sets per electron spin;
+        ADD_ZEFF: +Z_ion/r in the local channel (Pseudopotential.cpp:305-336,
+        874-1033)."""
         self.pp = {}
         for t in pstexts:
             lab = t[0]
             aip = int(value(t, "AIP", 6, int))
-            bw = section(t, "BASIS")
-            oq = section(bw, "OLDQMC")
-            it = 0
-            it += 1  # zeff
-            nl = int(oq[it]); it += 1
-            nper = [int(oq[it + l]) for l in range(nl)]
-            it += nl
-            chans = []
-            for l in range(nl):
-                terms = []
-                for _ in range(nper[l]):
-                    terms.append((float(oq[it]) - 2.0, float(oq[it + 1]), float(oq[it + 2])))
-                    it += 3
-                chans.append(terms)
-            self.pp[lab] = {"aip": aip, "chans": chans}
+            if haskey(t, "SPIN_DEP"):
+                up = self._read_rgaussian(section(t, "BASIS_UP"))
+                dn = self._read_rgaussian(section(t, "BASIS_DN"))
+            else:
+                up = dn = self._read_rgaussian(section(t, "BASIS"))
+            self.pp[lab] = {"aip": aip, "chans": up, "chans_dn": dn, "add_zeff": haskey(t, "ADD_ZEFF")}
         for lab, p in self.pp.items():
             p["quad"], p["w"] = gesqua(p["aip"])
-            p["cutoff"] = self._pp_cutoff(p["chans"])
+            p["cutoff"] = self._pp_cutoff_pair(p["chans"], p["chans_dn"])
+
+    def _pp_cutoff_pair(self, up, dn):
+        """The cutoff scan over both spins' channels."""
+        nl = len(up)
+        cutL = [20.0] * (nl - 1)
+        found = [False] * (nl - 1)
+        r = 20.0
+        while r > 0:
+            vu, vd = self._vl(up, r), self._vl(dn, r)
+            for l in range(nl - 1):
+                if (abs(float(vu[l])) > 1e-5 or abs(float(vd[l])) > 1e-5) and not found[l]:
+                    cutL[l] = r - 0.05
+                    found[l] = True
+            r -= 0.05
+        return max(cutL) if cutL else 0.0
+
+    def _vl_spin(self, p, r, a):
+        """Channel radials [nl][nc, N] for every electron with its spin's
+        basis; the local channel with ADD_ZEFF's Z_ion / r."""
+        vu, vd = self._vl(p["chans"], r), self._vl(p["chans_dn"], r)
+        up = np.arange(r.shape[-1]) < self.nup
+        vl = [np.where(up, u, d) for u, d in zip(vu, vd)]
+        if p["add_zeff"]:
+            vl[-1] = vl[-1] + self.charges[a] / r
+        return vl
 
     @staticmethod
     def _vl(chans, r):
@@ -840,7 +876,7 @@ class System:
                 continue
             d = self.min_image(R - self.atoms[a])
             r = np.sqrt(np.sum(d * d, axis=-1))
-            vl = self._vl(p["chans"], r)
+            vl = self._vl_spin(p, r, a)
             nl = len(p["chans"])
             tot += np.sum(vl[nl - 1], axis=1)
             q = np.einsum("qk,ckj->cqj", p["quad"], rot)     # rotated points [nc,Q,3]
@@ -883,7 +919,7 @@ class System:
                 continue
             d = self.min_image(R - self.atoms[a])
             r = np.sqrt(np.sum(d * d, axis=-1))
-            vl = self._vl(p["chans"], r)
+            vl = self._vl_spin(p, r, a)
             nl = len(p["chans"])
             q = p["quad"] @ np.asarray(rot, dtype=float)
             for e in range(N):

@@ -54,7 +54,9 @@ WORKLOADS = [("n2_allelectron", dict(pseudo=False), 11), ("n2_pseudo", dict(pseu
              ("n2_jas", dict(pseudo=True, jastrow_variant="pade_spin", aip=18), 25),
              # the 26- and 32-point quadratures
              ("n2_aip26", dict(pseudo=True, aip=26), 26),
-             ("n2_aip32", dict(pseudo=True, aip=32), 27)]
+             ("n2_aip32", dict(pseudo=True, aip=32), 27),
+             # SPIN_DEP radial sets per spin, with ADD_ZEFF
+             ("n2_ppspin", dict(pseudo=True, pp_variant="spin_dep"), 28)]
 
 
 def make(name, kw, seed):
@@ -69,7 +71,7 @@ def make(name, kw, seed):
         nconf = 64 if kw["nelec"] < 64 else 32
     else:
         deck = systems.write_n2(HERE, seed=seed, name=name, **kw)
-        nconf = NCONF if not ({"expansion", "high_l", "jastrow", "mo_kind", "aip"} & set(kw)) else 64
+        nconf = NCONF if not ({"expansion", "high_l", "jastrow", "mo_kind", "aip", "pp_variant"} & set(kw)) else 64
     R = systems.random_configs(deck, nconf, seed=seed + 1000)
     NCONF_ = nconf
     rng = np.random.default_rng(seed + 2000)

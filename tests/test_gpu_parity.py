@@ -16,7 +16,7 @@ from mainline_b200 import engine, systems
 pytestmark = pytest.mark.gpu
 
 NAMES = ["n2_allelectron", "n2_pseudo", "diamond8", "mol43", "mol72", "cell32", "n2_multidet", "n2_fg", "diamond8_f",
-         "n2_slater", "n2_cutoff", "n2_jas", "n2_aip26", "n2_aip32"]
+         "n2_slater", "n2_cutoff", "n2_jas", "n2_aip26", "n2_aip32", "n2_ppspin"]
 FP64_TOL = 1e-10
 
 

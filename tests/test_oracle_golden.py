@@ -9,7 +9,7 @@ from conftest import GOLDEN
 import qworacle
 
 NAMES = ["n2_allelectron", "n2_pseudo", "diamond8", "mol43", "mol72", "cell32", "diamond8_k", "diamond8_l", "n2_fg",
-         "diamond8_f", "n2_slater", "n2_cutoff", "diamond8_kc", "n2_jas", "n2_aip26", "n2_aip32"]
+         "diamond8_f", "n2_slater", "n2_cutoff", "diamond8_kc", "n2_jas", "n2_aip26", "n2_aip32", "n2_ppspin"]
 
 
 def _rel(a, b):
@@ -23,7 +23,7 @@ def case(request):
     # the restatement is slow in numpy for the periodic and the large decks
     keep = {"diamond8": 8, "mol72": 4, "cell32": 2, "diamond8_k": 6, "diamond8_l": 6, "n2_fg": 32,
             "diamond8_f": 6, "n2_cutoff": 32, "diamond8_kc": 4, "n2_jas": 16, "n2_aip26": 8,
-            "n2_aip32": 8}.get(request.param)
+            "n2_aip32": 8, "n2_ppspin": 16}.get(request.param)
     if keep:
         g = {k: v[:keep] for k, v in g.items()}
     return request.param, qworacle.System(os.path.join(GOLDEN, request.param + ".qw")), g
