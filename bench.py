@@ -319,6 +319,23 @@ def run_extras(stream, dev, seconds=30.0):
     from mainline_b200 import engine, serving, systems
     tmp = tempfile.mkdtemp(prefix="qwg_extra_")
     out = {}
+    # cfg 1: the all-electron molecule in FP64 VMC (256 walkers, tau 0.3,
+    # 100-step blocks, Split_sampler depth 2 as the reference's VMC)
+    ae = systems.write_n2(tmp, seed=11, pseudo=False, name="n2_allelectron_bench")
+    E = engine.Engine(ae.path, engine.FP64, max_walkers=256, stream=stream.cuda_stream)
+    E.set_walkers(systems.random_configs(ae, 256, seed=SEED))
+    E.vmc_block(100, 0.3, seed=SEED)
+    vst = [E.vmc_block(100, 0.3, seed=SEED + 1 + b) for b in range(10)]
+    E.close()
+    vms = float(np.sum([v["block_ms"] for v in vst]))
+    out["vmc_allelectron"] = {
+        "fp64": {"walker_steps_per_s": 256 * 100 * len(vst) / (vms / 1e3), "block_ms": vms / len(vst),
+                 "energy": float(np.mean([v["energy"] for v in vst])),
+                 "acceptance": float(np.mean([v["acceptance"] for v in vst]))},
+        "config": "cfg 1: two all-electron Z=7 atoms, 14 electrons, 80 Cartesian Gaussians (exponents 0.1-1e4), "
+                  "FP64 VMC, 256 walkers, tau=0.3, 10 timed blocks of 100 steps; the random-orbital trial function "
+                  "of the tight all-electron basis has local energies of order 1e3 Ha, so the energy is a "
+                  "throughput by-product, not a physical value"}
     # periodic: 8-atom cell, 32 electrons, tau 0.005, 16384 walkers
     cell = systems.write_periodic(tmp, seed=13, name="diamond8_bench")
     Rc = systems.random_configs(cell, 16384, seed=SEED)

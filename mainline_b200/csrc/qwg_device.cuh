@@ -292,6 +292,7 @@ enum QwgPhase {
   PH_PP_POINTS,       // quadrature: point ratios (basis values, Jastrow)
   PH_REFRESH,         // full recompute and re-inversion
   PH_WALKER,          // a walker's whole step-mode launch (moves or local energy)
+  PH_PP_POINT_JAS,    // the Jastrow part of PH_PP_POINTS (lane 0's share of the warp)
   PH_COUNT = 16
 };
 #ifdef QWG_PHASES
@@ -389,12 +390,20 @@ __device__ __forceinline__ Rand4 rand4(uint64_t seed, uint32_t walker, uint64_t 
   return o;
 }
 
+// Two normal deviates from two uniforms (Box-Muller), in FP32 with the fast
+// intrinsics, the angle taken in [-pi, pi) where __sincosf is accurate to
+// ~2^-21 (a half turn of the angle maps the pair to its negative, so the
+// deviates keep their distribution).  They only draw the proposal; the
+// acceptance uses the realised displacement, and the FP32 rounding (~1e-7
+// relative) perturbs the proposal density far below any statistical error,
+// while the FP64 transcendentals leave the move loop.  Both precisions draw
+// the same deviates.
 __device__ __forceinline__ void box_muller(double u1, double u2, double& g1, double& g2) {
-  double rad = sqrt(-2.0 * log(u1));
-  double s, c;
-  sincospi(2.0 * u2, &s, &c);
-  g1 = rad * c;
-  g2 = rad * s;
+  const float rad = sqrtf(-2.0f * __logf(float(u1)));
+  float s, c;
+  __sincosf(6.2831853071795864f * (float(u2) - 0.5f), &s, &c);
+  g1 = double(rad * c);
+  g2 = double(rad * s);
 }
 
 // ---------------------------------------------------------------------------

@@ -868,7 +868,9 @@ struct Walker {
             rd = basis_dot_lane<Real, HL>(S, nx, ny, nz, wr);
           }
         }
+        QWG_PHASE_BEGIN(t_pj)
         const Real u = jas_electron_val<Real, TB>(S, Rp, I.e, nx, ny, nz);
+        QWG_PHASE_END(t_pj, PH_PP_POINT_JAS, ph)
         double ratio = double(rd * exp(u - Real(Ue()[I.e]))) * S.pp_w[ty][q];
         // cos of the angle between the original and the quadrature direction
         const double* ap = S.atom_pos[I.a];

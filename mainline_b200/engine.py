@@ -279,7 +279,7 @@ class Engine:
         return out
 
     PHASES = ["mo_rows", "propose_rest", "accept", "kinetic", "potential", "pp_jastrow", "pp_items", "pp_project",
-              "pp_points", "refresh", "walker_launch"]
+              "pp_points", "refresh", "walker_launch", "pp_point_jastrow"]
 
     def phase_counters(self, reset: bool = False) -> dict:
         """Clock cycles per walker-kernel phase (profiling build only)."""

@@ -84,9 +84,12 @@ def test_dmc_with_tmoves_runs(mode):
     E.set_walkers(systems.random_configs(d, 1024, seed=3))
     E.vmc_block(10, 0.3, seed=4)
     E.dmc_init(timestep=0.01, nstep=10, seed=5, tmoves=mode)
+    # from a random-orbital trial function the trial energy lags the first
+    # blocks and the mean weight climbs: third-block means of 2.7-3.2 over six
+    # seeds, with and without T-moves; the cap per walker is 7
     for _ in range(3):
         s = E.dmc_block()
-        assert np.isfinite(s["energy"]) and s["nonfinite"] == 0 and 0.3 < s["weight"] < 3.0
+        assert np.isfinite(s["energy"]) and s["nonfinite"] == 0 and 0.3 < s["weight"] < 5.0
     R = E.get_walkers()
     E2 = engine.Engine(DECK, engine.FP64, max_walkers=1024)
     E2.set_walkers(R)
