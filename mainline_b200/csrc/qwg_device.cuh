@@ -130,6 +130,14 @@ struct DevSys {
   double alpha, ewald_const;
   int2 atom_images[QWG_MAXA];    // (first, count) into image_pos
   const double* image_pos;       // [nimage][3] basis centers (atoms and their images)
+  // sub-cell candidate lists of the image sums: the cell cut into sub_n[0] x
+  // sub_n[1] x sub_n[2] parallelepipeds; sub_seg[s * natoms + c] = (first,
+  // count) into sub_idx, the image indices of atom c (in image order) within
+  // reach of some point of sub-cell s.  Null for molecules.
+  int sub_n[3];
+  double sub_inv_h[3];           // 1 / (normvec[i] . lat[i])
+  const int2* sub_seg;
+  const int* sub_idx;
   // complex-orbital kernels (CORBITALS, or real orbitals at a nonzero k-point):
   // planar complex tables (imaginary plane of the MO coefficients in moc_im,
   // same layout as moc); image_kfac[m] = k-point factor of image center m,
@@ -193,6 +201,38 @@ __device__ __forceinline__ void wrap_pos(const DevSys<Real>& S, double& x, doubl
       else break;
     }
   }
+}
+
+// Sub-cell of a position inside the cell (the frame of wrap_pos), or -1
+// outside it or without lists (molecules).
+template <typename Real>
+__device__ __forceinline__ int subcell_of(const DevSys<Real>& S, double x, double y, double z) {
+  if (S.sub_seg == nullptr) return -1;
+  int id = 0;
+  for (int i = 0; i < 3; i++) {
+    const double* n = S.normvec[i];
+    const double f = (n[0] * (x - S.origin[0]) + n[1] * (y - S.origin[1]) + n[2] * (z - S.origin[2])) * S.sub_inv_h[i];
+    if (!(f > -1e-9 && f < 1.0 + 1e-9)) return -1;
+    id = id * S.sub_n[i] + min(S.sub_n[i] - 1, max(0, int(f * double(S.sub_n[i]))));
+  }
+  return id;
+}
+
+// The image centers of atom c a position of sub-cell sc can reach: the
+// listed subset (same order) or, for sc < 0, all of the atom's images.
+struct ImgRange {
+  const int* idx;
+  int first, count;
+  __device__ __forceinline__ int operator[](int t) const { return idx ? __ldg(idx + first + t) : first + t; }
+};
+template <typename Real>
+__device__ __forceinline__ ImgRange images_of(const DevSys<Real>& S, int sc, int c) {
+  if (sc >= 0) {
+    const int2 g = __ldg(&S.sub_seg[(size_t)sc * S.natoms + c]);
+    return {S.sub_idx, g.x, g.y};
+  }
+  const int2 im = S.atom_images[c];
+  return {nullptr, im.x, im.y};
 }
 
 // wrap_pos that also returns the lattice translations applied (nshift[i] +1
@@ -676,6 +716,7 @@ __device__ __forceinline__ void shell_lap_store_fg(int sym, double x, double y, 
 // at run time from S.periodic.
 template <typename O, int PER, bool HL, typename Real>
 __device__ void basis_lap_warp(const DevSys<Real>& S, double px, double py, double pz, O* bas, int lane) {
+  const int sc = PER == 0 ? -1 : subcell_of(S, px, py, pz);
   for (int s = lane; s < S.nshell; s += 32) {
     int4 si = S.shell_i[s];
     int2 so = S.shell_obj[s];
@@ -714,10 +755,10 @@ __device__ void basis_lap_warp(const DevSys<Real>& S, double px, double py, doub
       // periodic: sum the shell over the atom's image centers, then apply the
       // |value| <= 1e-8 rule to the sums (MO_matrix_blas.h:444-474)
       for (int k = 0; k < 5 * nf; k++) b[k] = O(0);
-      const int2 im = S.atom_images[si.x];
+      const ImgRange im = images_of(S, sc, si.x);
       const double cut2 = cut * cut * (1.0 + 1e-12);  // beyond it r < cut is certainly false
-      for (int m = im.x; m < im.x + im.y; m++) {
-        const double* cp = S.image_pos + 3 * m;
+      for (int t = 0; t < im.count; t++) {
+        const double* cp = S.image_pos + 3 * im[t];
         double dx = px - cp[0], dy = py - cp[1], dz = pz - cp[2];
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (!(r2 < cut2)) continue;
@@ -916,6 +957,7 @@ template <typename Real, bool HL = false>
 __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, double px, double py, double pz,
                                                         const Real* w) {
   Real acc = Real(0);
+  const int sc = subcell_of(S, px, py, pz);
   for (int c = 0; c < S.natoms; c++) {
     const int4 cs = S.center_seg[c];  // first shell, shells, object base, splines per row
     if (cs.y == 0) continue;
@@ -924,11 +966,11 @@ __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, d
     for (int k = 0; k < cs.y; k++) nfa += sym_nfunc(S.shell_pack[cs.x + k] & 0xf);
     for (int q = 0; q < QWG_MAXF_ATOM; q++) fs[q] = Real(0);
     const int fb0 = (S.shell_pack[cs.x] >> 4) & 0xffff;
-    const int2 im = S.atom_images[c];
+    const ImgRange im = images_of(S, sc, c);
     const Real cut = Real(S.center_cut[c]);
     const Real cut2 = cut * cut * Real(1.000001);  // beyond it rd < cut is certainly false
-    for (int m = im.x; m < im.x + im.y; m++) {
-      const double* cp = S.image_pos + 3 * m;
+    for (int t = 0; t < im.count; t++) {
+      const double* cp = S.image_pos + 3 * im[t];
       const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
       const Real rd2 = x * x + y * y + z * z;
       if (!(rd2 < cut2)) continue;
@@ -998,6 +1040,7 @@ template <typename Real>
 __device__ void mo_lap_warp_cpx(const DevSys<Real>& S, const Real* moc_re, const Real* moc_im, double px, double py,
                                 double pz, int M, int ms, Real* bas, Real* out, int lane) {
   const int nb5 = 5 * S.nbasis;
+  const int sc = subcell_of(S, px, py, pz);
   for (int s = lane; s < S.nshell; s += 32) {
     const int4 si = S.shell_i[s];
     const int2 so = S.shell_obj[s];
@@ -1007,8 +1050,9 @@ __device__ void mo_lap_warp_cpx(const DevSys<Real>& S, const Real* moc_re, const
     for (int k = 0; k < 5 * nf; k++) br[k] = bi[k] = Real(0);
     const double cut = S.shell_cut[s];
     const double cut2 = cut * cut * (1.0 + 1e-12);
-    const int2 im = S.atom_images[si.x];
-    for (int m = im.x; m < im.x + im.y; m++) {
+    const ImgRange im = images_of(S, sc, si.x);
+    for (int t = 0; t < im.count; t++) {
+      const int m = im[t];
       const double* cp = S.image_pos + 3 * m;
       const double dx = px - cp[0], dy = py - cp[1], dz = pz - cp[2];
       const double r2 = dx * dx + dy * dy + dz * dz;
@@ -1058,10 +1102,11 @@ template <typename Real>
 __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double px, double py, double pz,
                                                    const Real* w_re, const Real* w_im, Real& out_re, Real& out_im) {
   Real acr = Real(0), aci = Real(0);
+  const int sc = subcell_of(S, px, py, pz);
   for (int c = 0; c < S.natoms; c++) {
     const int4 cs = S.center_seg[c];  // first shell, shells, object base, splines per row
     if (cs.y == 0) continue;
-    const int2 im = S.atom_images[c];
+    const ImgRange im = images_of(S, sc, c);
     const Real cut = Real(S.center_cut[c]);
     for (int k = 0; k < cs.y; k++) {
       const int pk = S.shell_pack[cs.x + k];
@@ -1075,7 +1120,8 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
         for (int q = 0; q < sym_nfunc(sym); q++) {
           const int idx = fg_index(sym, q);
           Real gr = Real(0), gi = Real(0);
-          for (int m = im.x; m < im.x + im.y; m++) {
+          for (int t = 0; t < im.count; t++) {
+            const int m = im[t];
             const double* cp = S.image_pos + 3 * m;
             const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
             const Real rd2 = x * x + y * y + z * z;
@@ -1100,7 +1146,8 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
       }
       Real fr[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
       Real fi[6] = {Real(0), Real(0), Real(0), Real(0), Real(0), Real(0)};
-      for (int m = im.x; m < im.x + im.y; m++) {
+      for (int t = 0; t < im.count; t++) {
+        const int m = im[t];
         const double* cp = S.image_pos + 3 * m;
         const Real x = Real(px - cp[0]), y = Real(py - cp[1]), z = Real(pz - cp[2]);
         const Real rd2 = x * x + y * y + z * z;

@@ -121,6 +121,9 @@ struct qwg_ctx {
   // tables
   DevBuf d_shell_i, d_shell_obj, d_shell_cut, d_spline, d_spline64, d_moc, d_moc_im, d_image_kfac;
   DevBuf d_image_pos, d_gvec, d_gweight, d_ion_sin, d_ion_cos;
+  DevBuf d_sub_seg, d_sub_idx;  // sub-cell candidate lists of the image sums
+  int sub_n[3] = {0, 0, 0};
+  double sub_inv_h[3] = {0, 0, 0};
   DevBuf d_det_c, d_det_ud, d_ud_cols;  // determinant expansion tables
   DevSys<double> sys_d{};
   DevSys<float> sys_f{};
@@ -268,6 +271,11 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
   S.ewald_const = H.ewald_const;
   for (int a = 0; a < H.natoms; a++) S.atom_images[a] = make_int2(H.image_first[a], H.image_count[a]);
   S.image_pos = c->d_image_pos.as<double>();
+  if (H.periodic) {
+    for (int i = 0; i < 3; i++) { S.sub_n[i] = c->sub_n[i]; S.sub_inv_h[i] = c->sub_inv_h[i]; }
+    S.sub_seg = c->d_sub_seg.as<int2>();
+    S.sub_idx = c->d_sub_idx.as<int>();
+  }
   S.ng = (int)H.gweight.size();
   S.gvec = c->d_gvec.as<double>();
   S.gweight = c->d_gweight.as<double>();
@@ -334,6 +342,74 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
       S.pp_w[t][q] = P.weight[q];
     }
   }
+}
+
+// Sub-cell candidate lists of the periodic image sums (every periodic basis
+// evaluation, both precisions).  The cell is cut into n0 x n1 x n2
+// parallelepipeds about 1 bohr high; for sub-cell s and atom c the list holds
+// the indices of c's image centers, in image order, within cutoff(c) + R +
+// 1e-3 bohr of the sub-cell's center, R its circumradius and cutoff(c) the
+// largest cutoff of c's shells.  A position inside s is within R of that
+// center, so every image within cutoff of it is listed, and a sum over the
+// listed images adds the same terms in the same order as one over all images.
+struct SubcellLists {
+  int n[3] = {0, 0, 0};
+  double inv_h[3] = {0, 0, 0};
+  std::vector<int2> seg;
+  std::vector<int> idx;
+};
+static SubcellLists make_subcell_lists(const HostSystem& H) {
+  SubcellLists L;
+  if (!H.periodic) return L;
+  const int A = H.natoms;
+  const double* a = H.lat;
+  double vol;
+  {
+    const double* u = a + 3; const double* v = a + 6;
+    const double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2], cz = u[0] * v[1] - u[1] * v[0];
+    vol = std::fabs(a[0] * cx + a[1] * cy + a[2] * cz);
+  }
+  for (int i = 0; i < 3; i++) {
+    const double* u = a + 3 * ((i + 1) % 3); const double* v = a + 3 * ((i + 2) % 3);
+    const double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2], cz = u[0] * v[1] - u[1] * v[0];
+    const double h = vol / std::sqrt(cx * cx + cy * cy + cz * cz);
+    L.n[i] = std::max(1, std::min(16, (int)std::ceil(h / 1.0)));
+    const double* nv = H.normvec + 3 * i;
+    L.inv_h[i] = 1.0 / (nv[0] * a[3 * i] + nv[1] * a[3 * i + 1] + nv[2] * a[3 * i + 2]);
+  }
+  double R = 0.0;  // circumradius of a sub-cell: the longest half body diagonal
+  const int sg[4][3] = {{1, 1, 1}, {1, 1, -1}, {1, -1, 1}, {-1, 1, 1}};
+  for (const auto& g : sg) {
+    double v[3];
+    for (int j = 0; j < 3; j++)
+      v[j] = 0.5 * (g[0] * a[j] / L.n[0] + g[1] * a[3 + j] / L.n[1] + g[2] * a[6 + j] / L.n[2]);
+    R = std::max(R, std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+  }
+  std::vector<double> cmax(A, 0.0);
+  for (const Shell& s : H.shells)
+    cmax[s.center] = std::max(cmax[s.center], std::max(s.cutoff, H.cutoff_mo ? s.fcut : 0.0));
+  const int nsub = L.n[0] * L.n[1] * L.n[2];
+  L.seg.resize((size_t)nsub * A);
+  for (int g0 = 0; g0 < L.n[0]; g0++)
+    for (int g1 = 0; g1 < L.n[1]; g1++)
+      for (int g2 = 0; g2 < L.n[2]; g2++) {
+        const int s = (g0 * L.n[1] + g1) * L.n[2] + g2;
+        double ctr[3];
+        for (int j = 0; j < 3; j++)
+          ctr[j] = H.origin[j] + (g0 + 0.5) / L.n[0] * a[j] + (g1 + 0.5) / L.n[1] * a[3 + j] +
+                   (g2 + 0.5) / L.n[2] * a[6 + j];
+        for (int c = 0; c < A; c++) {
+          const int first = (int)L.idx.size();
+          const double reach = cmax[c] + R + 1e-3;
+          for (int m = H.image_first[c]; m < H.image_first[c] + H.image_count[c]; m++) {
+            const double dx = H.image_pos[3 * m] - ctr[0], dy = H.image_pos[3 * m + 1] - ctr[1],
+                         dz = H.image_pos[3 * m + 2] - ctr[2];
+            if (dx * dx + dy * dy + dz * dz < reach * reach) L.idx.push_back(m);
+          }
+          L.seg[(size_t)s * A + c] = make_int2(first, (int)L.idx.size() - first);
+        }
+      }
+  return L;
 }
 
 static void build_tables(qwg_ctx* c) {
@@ -416,6 +492,12 @@ static void build_tables(qwg_ctx* c) {
   upload(c->d_gweight, H.gweight, st);
   upload(c->d_ion_sin, H.ion_sin, st);
   upload(c->d_ion_cos, H.ion_cos, st);
+  if (H.periodic) {
+    const SubcellLists sl = make_subcell_lists(H);
+    upload(c->d_sub_seg, sl.seg, st);
+    upload(c->d_sub_idx, sl.idx, st);
+    for (int i = 0; i < 3; i++) { c->sub_n[i] = sl.n[i]; c->sub_inv_h[i] = sl.inv_h[i]; }
+  }
   fill_sys<double>(c, c->sys_d, obj_base);
   fill_sys<float>(c, c->sys_f, obj_base);
   const void* req[] = {c->sys_d.shell_i, c->sys_d.shell_obj, c->sys_d.shell_cut, c->sys_d.spline,
@@ -570,6 +652,10 @@ static size_t footprint_bytes(const qwg_ctx* c, int max_walkers) {
   const size_t cf = c->mmax == kComplexFamily ? 2 : 1;
   size_t b = total4 * 4 * (8 + rs) + 2 * (size_t)H.nbasis * ms * rs * cf + H.shells.size() * 32 +
              H.image_pos.size() * 8 * 5 / 3 + H.gvec.size() * 8 + 3 * H.gweight.size() * 8;
+  if (H.periodic) {
+    const SubcellLists sl = make_subcell_lists(H);
+    b += sl.seg.size() * sizeof(int2) + sl.idx.size() * sizeof(int);
+  }
   b += W * (2 * 3 * N * 8 + 2 * (size_t)c->L.state_bytes + (hbm_family(c->mmax) ? (size_t)c->L.scratch_bytes : 0) + 20);
   b += W * 8 * (9 + 5 + 4 * N);  // evaluation outputs (qwg_eval / qwg_dmc_init)
   if (tc_moves_eligible(c)) b += tc_moves_bytes(c, W);
