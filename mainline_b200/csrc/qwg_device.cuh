@@ -463,17 +463,26 @@ __device__ __forceinline__ float warp_sum(float v) {
 // ---------------------------------------------------------------------------
 // radial functions
 
+// Quotient of the Jastrow radials: the fast FP32 divide (__fdividef, 2 ulp
+// for the O(1) denominators here) in the working precision of the mixed path,
+// the IEEE divide in FP64.
+template <typename T>
+__device__ __forceinline__ T jdiv(T x, T y) {
+  if constexpr (sizeof(T) == 4) return __fdividef(x, y);
+  else return x / y;
+}
+
 // Jastrow radial function (value, f'/r, 3D Laplacian).  Zero at r >= rcut.
 template <typename T>
 __device__ __forceinline__ void radial_lap(const DRadial& q, T r, T& f, T& fd, T& lap) {
   if (!(r < T(q.rcut))) { f = fd = lap = T(0); return; }
   const T ircut = T(q.inv_rcut);
   const T zz = r * ircut, zz2 = zz * zz;
-  const T ir = T(1) / r;
+  const T ir = jdiv(T(1), r);
   if (q.kind == 0) {  // CUTOFF_CUSP (cusp a, gamma b, 1/(3+gamma) c)
     const T cusp = T(q.a), gamma = T(q.b);
     T pp = zz - zz2 + zz * zz2 * T(1.0 / 3.0);
-    T pade = T(1) / (T(1) + gamma * pp);
+    T pade = jdiv(T(1), T(1) + gamma * pp);
     f = cusp * T(q.rcut) * (pp * pade - T(q.c));
     T pade2 = pade * pade;
     T ppd = T(1) - T(2) * zz + zz2;
@@ -482,7 +491,7 @@ __device__ __forceinline__ void radial_lap(const DRadial& q, T r, T& f, T& fd, T
     fd = cusp * dadr;
     lap = cusp * ((ppdd * pade2 - T(2) * gamma * ppd * ppd * pade2 * pade) * ircut + T(2) * dadr);
   } else if (q.kind == 2) {  // PADE (alpha a): f = (a r / (1 + a r))^2
-    const T pade = T(1) / (T(1) + T(q.a) * r);
+    const T pade = jdiv(T(1), T(1) + T(q.a) * r);
     const T app = T(q.a) * T(q.a) * pade * pade;
     f = app * r * r;
     fd = T(2) * app * pade;
@@ -492,7 +501,7 @@ __device__ __forceinline__ void radial_lap(const DRadial& q, T r, T& f, T& fd, T
     T zpp = zz2 * (T(6) - T(8) * zz + T(3) * zz2);
     T zppd = T(12) * zz * (T(1) - T(2) * zz + zz2);
     T zppdd2 = T(6) - T(24) * zz + T(18) * zz2;
-    T zpade = T(1) / (T(1) + beta * zpp), zpade2 = zpade * zpade;
+    T zpade = jdiv(T(1), T(1) + beta * zpp), zpade2 = zpade * zpade;
     f = (T(1) - zpp) * zpade;
     fd = -zppd * zpade2 * (beta + T(1)) * ir * ircut;
     T crsdd2 = -zpade2 * (zppdd2 - beta * zppd * zppd * zpade) * (beta + T(1)) * ircut * ircut;
@@ -505,14 +514,14 @@ __device__ __forceinline__ T radial_val(const DRadial& q, T r) {
   const T zz = r * T(q.inv_rcut), zz2 = zz * zz;
   if (q.kind == 0) {
     T pp = zz - zz2 + zz * zz2 * T(1.0 / 3.0);
-    return T(q.a) * T(q.rcut) * (pp / (T(1) + T(q.b) * pp) - T(q.c));
+    return T(q.a) * T(q.rcut) * (jdiv(pp, T(1) + T(q.b) * pp) - T(q.c));
   }
   if (q.kind == 2) {
-    const T ap = T(q.a) / (T(1) + T(q.a) * r);
+    const T ap = jdiv(T(q.a), T(1) + T(q.a) * r);
     return ap * ap * r * r;
   }
   T zpp = zz2 * (T(6) - T(8) * zz + T(3) * zz2);
-  return (T(1) - zpp) / (T(1) + T(q.a) * zpp);
+  return jdiv(T(1) - zpp, T(1) + T(q.a) * zpp);
 }
 
 // ---------------------------------------------------------------------------
@@ -1394,7 +1403,17 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
   const double pi[3] = {px, py, pz};
   const double* pie = S.tb_stale_ei ? R + 3 * i : pi;  // e-n position of the e-e-n terms
   NearSet ns;
-  if constexpr (TB) near_atoms(S, pie, ns);
+  // e-e-n: the e-n values of electron i at its atoms in range, once per
+  // point instead of once per pair (a near set that overflowed takes the
+  // general pair routine)
+  T av[TB ? QWG_NEAR : 1][QWG_MAXEI];
+  if constexpr (TB) {
+    near_atoms(S, pie, ns);
+    for (int q = 0; q < ns.n; q++) {
+      const int t = S.atom_type[ns.a[q]];
+      for (int k = 0; k < S.ei_n[t]; k++) av[q][k] = radial_val<T>(S.ei[t][k], T(ns.r[q]));
+    }
+  }
   for (int j = 0; j < S.nelec; j++) {
     if (j == i) continue;
     double ex = px - R[3 * j], ey = py - R[3 * j + 1], ez = pz - R[3 * j + 2];
@@ -1409,9 +1428,29 @@ __device__ T jas_electron_val(const DevSys<Real>& S, const double* R, int i, dou
       if (c != 0.0) u += T(c) * radial_val<T>(S.ee[k], r);
     }
     if constexpr (TB) {
-      double tu, tgi[3], tli, tgj[3], tlj;
-      jas_threebody_pair(S, ns, same, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false, pie);
-      u += T(tu);
+      if (ns.n < 0) {
+        double tu, tgi[3], tli, tgj[3], tlj;
+        jas_threebody_pair(S, ns, same, pi, R + 3 * j, tu, tgi, tli, tgj, tlj, false, pie);
+        u += T(tu);
+      } else {
+        // sum over the atoms of c (a_k(i) a_l(j) + a_l(i) a_k(j)) b_m(r_ij)
+        // (the terms of tb_atom, values only)
+        for (int q = 0; q < ns.n; q++) {
+          const int a = ns.a[q], t = S.atom_type[a];
+          const double* ap = S.atom_pos[a];
+          double jx = R[3 * j] - ap[0], jy = R[3 * j + 1] - ap[1], jz = R[3 * j + 2] - ap[2];
+          min_image(S, jx, jy, jz);
+          const T rj = T(sqrt(jx * jx + jy * jy + jz * jz));
+          if (!(rj < T(S.tb_rc[t]))) continue;  // every term vanishes
+          T aj[QWG_MAXEI];
+          for (int k = 0; k < S.ei_n[t]; k++) aj[k] = radial_val<T>(S.ei[t][k], rj);
+          for (int n = 0; n < S.tb_n[t]; n++) {
+            const DTB& tq = S.tb[t][n];
+            const T c = T(same ? tq.c : tq.cu);
+            u += c * (av[q][tq.k] * aj[tq.l] + av[q][tq.l] * aj[tq.k]) * radial_val<T>(S.ee[tq.m], r);
+          }
+        }
+      }
     }
   }
   return u;
