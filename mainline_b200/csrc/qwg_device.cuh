@@ -1348,6 +1348,74 @@ __device__ void jas_threebody_pair(const DevSys<Real>& S, const NearSet& ns, boo
   }
 }
 
+// e-e-n terms of the pair (e, j) before (old position) and after (new
+// position) a move of e, in one pass over the atoms in range of either
+// position: electron j's radials serve both positions, and each position's
+// radials are taken once per atom and function.  dn / dq: new / old position
+// minus r_j (minimum image), rn / rq their lengths.  Adds U_new - U_old to du,
+// the new position's gradient and Laplacian terms to gi / li, and the change
+// of electron j's to dgj / dlj (the sums of tb_atom over both near sets).
+// Near sets that overflowed are not handled here (callers use
+// jas_threebody_pair for them).
+template <typename Real>
+__device__ void tb_pair_move(const DevSys<Real>& S, const NearSet& nsn, const NearSet& nso, bool same,
+                             const double pj[3], const double dn[3], double rn, const double dq[3], double rq,
+                             double& du, double gi[3], double& li, double dgj[3], double& dlj) {
+  int qn = 0, qo = 0;
+  while (qn < nsn.n || qo < nso.n) {
+    const int an = qn < nsn.n ? nsn.a[qn] : S.natoms, ao = qo < nso.n ? nso.a[qo] : S.natoms;
+    const int a = min(an, ao);
+    const bool hn = an == a, ho = ao == a;
+    const int t = S.atom_type[a];
+    const double* ap = S.atom_pos[a];
+    double dj[3] = {pj[0] - ap[0], pj[1] - ap[1], pj[2] - ap[2]};
+    min_image(S, dj[0], dj[1], dj[2]);
+    const double rj = sqrt(dj[0] * dj[0] + dj[1] * dj[1] + dj[2] * dj[2]);
+    if (rj < S.tb_rc[t]) {
+      const int ne = S.ei_n[t];
+      double fj[QWG_MAXEI], fdj[QWG_MAXEI], flj[QWG_MAXEI];
+      for (int k = 0; k < ne; k++) radial_lap(S.ei[t][k], rj, fj[k], fdj[k], flj[k]);
+      for (int side = 0; side < 2; side++) {
+        if (side == 0 ? !hn : !ho) continue;
+        const NearSet& ns = side == 0 ? nsn : nso;
+        const int q = side == 0 ? qn : qo;
+        const double* di = ns.d[q];
+        const double ri = ns.r[q];
+        const double* dij = side == 0 ? dn : dq;
+        const double rij = side == 0 ? rn : rq;
+        const double sg = side == 0 ? 1.0 : -1.0;
+        double fi[QWG_MAXEI], fdi[QWG_MAXEI], fli[QWG_MAXEI];
+        for (int k = 0; k < ne; k++) radial_lap(S.ei[t][k], ri, fi[k], fdi[k], fli[k]);
+        for (int n = 0; n < S.tb_n[t]; n++) {
+          const DTB& q0 = S.tb[t][n];
+          const int k = q0.k, l = q0.l;
+          const double c = same ? q0.c : q0.cu;
+          double b, bd, bl;
+          radial_lap(S.ee[q0.m], rij, b, bd, bl);
+          const double sv = fi[k] * fj[l] + fi[l] * fj[k];
+          du += sg * c * sv * b;
+          double dsi = 0, dsj = 0, gsi[3], gsj[3], gb[3];
+          for (int d = 0; d < 3; d++) {
+            gsi[d] = fdi[k] * di[d] * fj[l] + fdi[l] * di[d] * fj[k];
+            gsj[d] = fi[k] * fdj[l] * dj[d] + fi[l] * fdj[k] * dj[d];
+            gb[d] = bd * dij[d];
+            dsi += gsi[d] * gb[d];
+            dsj += gsj[d] * gb[d];
+          }
+          if (side == 0) {
+            for (int d = 0; d < 3; d++) gi[d] += c * (gsi[d] * b + sv * gb[d]);
+            li += c * ((fli[k] * fj[l] + fli[l] * fj[k]) * b + sv * bl + 2 * dsi);
+          }
+          for (int d = 0; d < 3; d++) dgj[d] += sg * c * (gsj[d] * b - sv * gb[d]);
+          dlj += sg * c * ((fi[k] * flj[l] + fi[l] * flj[k]) * b + sv * bl - 2 * dsj);
+        }
+      }
+    }
+    if (hn) qn++;
+    if (ho) qo++;
+  }
+}
+
 // Everything of the Jastrow exponent that depends on electron i placed at p
 // (others at R): value U_i (one-body + all pairs with i), gradient, lap.
 template <bool TB, typename Real>

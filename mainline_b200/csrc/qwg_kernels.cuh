@@ -422,15 +422,24 @@ struct Walker {
       // gradient w.r.t. r_j of u(r_e - r_j) = -f'/r (r_e - r_j)
       double g0 = -fn * nx + fo * qx, g1 = -fn * ny + fo * qy, g2 = -fn * nz + fo * qz, l0 = ln - lo;
       if constexpr (has3) {
-        double pn[3] = {px, py, pz}, po[3] = {ox, oy, oz};
-        double tu, tgi[3], tli, tgj[3], tlj, su, sgi[3], sli, sgj[3], slj;
-        jas_threebody_pair(S, nsn, same, pn, pj, tu, tgi, tli, tgj, tlj, true);
-        jas_threebody_pair(S, nso, same, po, pj, su, sgi, sli, sgj, slj, true);
-        du += tu - su;
-        ge[0] += tgi[0]; ge[1] += tgi[1]; ge[2] += tgi[2];
-        le += tli;
-        g0 += tgj[0] - sgj[0]; g1 += tgj[1] - sgj[1]; g2 += tgj[2] - sgj[2];
-        l0 += tlj - slj;
+        if (nsn.n >= 0 && nso.n >= 0) {
+          const double dn[3] = {nx, ny, nz}, dq[3] = {qx, qy, qz};
+          const double rnd = sqrt(nx * nx + ny * ny + nz * nz), rqd = sqrt(qx * qx + qy * qy + qz * qz);
+          double dgj[3] = {0, 0, 0}, dlj = 0;
+          tb_pair_move(S, nsn, nso, same, pj, dn, rnd, dq, rqd, du, ge, le, dgj, dlj);
+          g0 += dgj[0]; g1 += dgj[1]; g2 += dgj[2];
+          l0 += dlj;
+        } else {
+          double pn[3] = {px, py, pz}, po[3] = {ox, oy, oz};
+          double tu, tgi[3], tli, tgj[3], tlj, su, sgi[3], sli, sgj[3], slj;
+          jas_threebody_pair(S, nsn, same, pn, pj, tu, tgi, tli, tgj, tlj, true);
+          jas_threebody_pair(S, nso, same, po, pj, su, sgi, sli, sgj, slj, true);
+          du += tu - su;
+          ge[0] += tgi[0]; ge[1] += tgi[1]; ge[2] += tgi[2];
+          le += tli;
+          g0 += tgj[0] - sgj[0]; g1 += tgj[1] - sgj[1]; g2 += tgj[2] - sgj[2];
+          l0 += tlj - slj;
+        }
       }
       dg[0] = g0; dg[1] = g1; dg[2] = g2; dg[3] = l0;
     }
