@@ -336,6 +336,10 @@ def run_extras(stream, dev, seconds=30.0):
                   "FP64 VMC, 256 walkers, tau=0.3, 10 timed blocks of 100 steps; the random-orbital trial function "
                   "of the tight all-electron basis has local energies of order 1e3 Ha, so the energy is a "
                   "throughput by-product, not a physical value"}
+    # the reference on the host cores, same deck, VMC with its default sampler
+    out["vmc_allelectron"]["cpu_baseline"] = cpu_reference(os.path.abspath(ae.path), repeats=1, short_blocks=1,
+                                                           long_blocks=3, nconf=64, nstep=100, tau=0.3,
+                                                           method="VMC")
     # periodic: 8-atom cell, 32 electrons, tau 0.005, 16384 walkers
     cell = systems.write_periodic(tmp, seed=13, name="diamond8_bench")
     Rc = systems.random_configs(cell, 16384, seed=SEED)
@@ -346,13 +350,16 @@ def run_extras(stream, dev, seconds=30.0):
         E.vmc_block(5, 0.3, seed=SEED + 1)
         E.dmc_init(timestep=0.005, nstep=10, seed=SEED + 2)
         E.dmc_block()
-        st = E.dmc_block()
-        per[label] = {"walker_steps_per_s": 16384 * 10 / (st["block_ms"] / 1e3), "block_ms": st["block_ms"],
-                      "energy": st["energy"]}
+        sts = [E.dmc_block() for _ in range(3)]
+        bms = float(np.median([x["block_ms"] for x in sts]))
+        per[label] = {"walker_steps_per_s": 16384 * 10 / (bms / 1e3), "block_ms": bms,
+                      "energy": float(np.mean([x["energy"] for x in sts]))}
         E.close()
     per["mixed_vs_fp64"] = per["mixed"]["walker_steps_per_s"] / per["fp64"]["walker_steps_per_s"]
     per["config"] = "8 Z_eff=4 atoms, a=6.74 bohr, 32 electrons, 104 basis fns + images, Ewald, e-e-n Jastrow; " \
-                    "16384 walkers, tau=0.005, 10-step blocks"
+                    "16384 walkers, tau=0.005, 10-step blocks, median of 3 after one warm-up block"
+    per["cpu_baseline"] = cpu_reference(os.path.abspath(cell.path), repeats=1, short_blocks=1, long_blocks=3,
+                                        nconf=16, nstep=10, tau=0.005)
     out["periodic"] = per
     # twisted boundary conditions: the same cell with complex orbitals at
     # k = (0.5, 0.25, 0) on the complex-orbital kernels
@@ -466,7 +473,8 @@ def pp_cutoff(deck_text):
     return 0.0
 
 
-def cpu_reference(deck_path, repeats=3, short_blocks=1, long_blocks=9, cores=None):
+def cpu_reference(deck_path, repeats=3, short_blocks=1, long_blocks=9, cores=None, nconf=64, nstep=50, tau=None,
+                  method="DMC"):
     """Reference qwalk (oracle/_ref/qwalk-Linux, shipped -O3 -ffast-math flags)
     on the host cores: one process per core, DMC on the same deck.  Per-block
     cost from the difference of a short and a long run (removes start-up and
@@ -476,34 +484,43 @@ def cpu_reference(deck_path, repeats=3, short_blocks=1, long_blocks=9, cores=Non
     if not os.path.exists(qw):
         return None
     cores = cores or os.cpu_count() or 1
-    nconf, nstep = 64, 50
+    tau = TAU if tau is None else tau
     base = open(deck_path).read()
     d = os.path.dirname(deck_path)
 
+    stem = os.path.splitext(os.path.basename(deck_path))[0]
+
     def run(nblock, rep):
+        # file names per deck: qwalk picks up <input>.config from an earlier run of the same name
         procs = []
         t0 = time.perf_counter()
         for p in range(cores):
-            path = os.path.join(d, f"cpu_{rep}_{nblock}_{p}.qw")
+            path = os.path.join(d, f"cpu_{stem}_{rep}_{nblock}_{p}.qw")
             txt = re.sub(r"RANDOMSEED\s*\{[^}]*\}", f"RANDOMSEED {{ {101 + p + 1000 * rep} {203 + p} }}", base)
-            txt += (f"\nMETHOD {{ DMC NCONFIG {nconf} NBLOCK {nblock} NSTEP {nstep} TIMESTEP {TAU} }}\n")
+            txt += (f"\nMETHOD {{ {method} NCONFIG {nconf} NBLOCK {nblock} NSTEP {nstep} TIMESTEP {tau} }}\n")
             open(path, "w").write(txt)
             procs.append(subprocess.Popen([qw, os.path.basename(path)], cwd=d, stdout=subprocess.DEVNULL,
                                           stderr=subprocess.DEVNULL))
-        for p in procs:
-            p.wait()
+        codes = [p.wait() for p in procs]
+        if any(codes):
+            raise RuntimeError(f"reference qwalk exited with status {max(codes, key=abs)} on {stem}")
         return time.perf_counter() - t0
 
     rates, walls = [], []
     for rep in range(repeats):
-        ts, tl = run(short_blocks, rep), run(long_blocks, rep)
+        try:
+            ts, tl = run(short_blocks, rep), run(long_blocks, rep)
+        except RuntimeError:
+            return None
+        if not tl > ts + 0.05:  # the longer run must take longer: anything else is a failed run
+            return None
         per_block = max((tl - ts) / (long_blocks - short_blocks), 1e-6)
         rates.append(cores * nconf * nstep / per_block)
         walls.append((round(ts, 1), round(tl, 1)))
     return {"value": float(np.median(rates)), "unit": "walker-steps/s", "cores": cores, "kind": "reference",
             "repeats": [float(r) for r in rates],
             "spread": float((max(rates) - min(rates)) / np.median(rates)),
-            "sample": f"{cores} qwalk processes x {nconf} walkers x {nstep} DMC steps/block; per-block time from "
+            "sample": f"{cores} qwalk processes x {nconf} walkers x {nstep} {method} steps/block; per-block time from "
                       f"{long_blocks}-block minus {short_blocks}-block wall, {repeats} repeats (walls s: {walls}); "
                       "median reported"}
 
