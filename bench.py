@@ -476,10 +476,10 @@ def pp_cutoff(deck_text):
 def cpu_reference(deck_path, repeats=3, short_blocks=1, long_blocks=9, cores=None, nconf=64, nstep=50, tau=None,
                   method="DMC"):
     """Reference qwalk (oracle/_ref/qwalk-Linux, shipped -O3 -ffast-math flags)
-    on the host cores: one process per core, DMC on the same deck.  Per-block
-    cost from the difference of a short and a long run (removes start-up and
-    the reference's own configuration generation); the pair is repeated and
-    the median rate reported with the spread."""
+    on the host cores: one process per core, DMC (or VMC) on the same deck.
+    Per-block cost from the difference of a short and a long run (removes
+    start-up and the reference's own configuration generation); the pair is
+    repeated and the fastest rate reported with the spread."""
     qw = os.path.join(ROOT, "oracle", "_ref", "qwalk-Linux")
     if not os.path.exists(qw):
         return None
@@ -517,12 +517,14 @@ def cpu_reference(deck_path, repeats=3, short_blocks=1, long_blocks=9, cores=Non
         per_block = max((tl - ts) / (long_blocks - short_blocks), 1e-6)
         rates.append(cores * nconf * nstep / per_block)
         walls.append((round(ts, 1), round(tl, 1)))
-    return {"value": float(np.median(rates)), "unit": "walker-steps/s", "cores": cores, "kind": "reference",
+    # the host is shared with other jobs: contention only slows a run, so the
+    # fastest repeat is the reference's own speed
+    return {"value": float(np.max(rates)), "unit": "walker-steps/s", "cores": cores, "kind": "reference",
             "repeats": [float(r) for r in rates],
             "spread": float((max(rates) - min(rates)) / np.median(rates)),
             "sample": f"{cores} qwalk processes x {nconf} walkers x {nstep} {method} steps/block; per-block time from "
                       f"{long_blocks}-block minus {short_blocks}-block wall, {repeats} repeats (walls s: {walls}); "
-                      "median reported"}
+                      "the fastest repeat reported"}
 
 
 def main():
