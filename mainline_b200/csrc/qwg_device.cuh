@@ -846,6 +846,19 @@ __device__ void mo_lap_warp(const DevSys<Real>& S, const Real* moc_s, double px,
   __syncwarp();
 }
 
+// Cubic spline value at offset h from the row's 4 coefficients c (16-byte
+// aligned): one 16-byte load in FP32, two in FP64.
+template <typename Real>
+__device__ __forceinline__ Real spline_val(const Real* c, Real h) {
+  if constexpr (sizeof(Real) == 4) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(c));
+    return v.x + h * (v.y + h * (v.z + h * v.w));
+  } else {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(c)), b = __ldg(reinterpret_cast<const double2*>(c) + 1);
+    return a.x + h * (a.y + h * (b.x + h * b.y));
+  }
+}
+
 // Determinant ratio of one electron moved to p, evaluated entirely by the
 // calling lane (pseudopotential quadrature points): with the projected
 // coefficients w_f = sum_m C[f][m] (A^-1)[m][e] of that electron,
@@ -874,8 +887,14 @@ __device__ __forceinline__ Real basis_dot_lane(const DevSys<Real>& S, double px,
       for (int j = 0; j < B; j++)
         if (k0 + j < cs.y) {
           const int k = (S.shell_pack[cs.x + k0 + j] >> 20) & 0xff;
-#pragma unroll
-          for (int q = 0; q < 4; q++) cf[j][q] = __ldg(row + 4 * k + q);
+          if constexpr (sizeof(Real) == 4) {
+            const float4 v = __ldg(reinterpret_cast<const float4*>(row + 4 * k));
+            cf[j][0] = v.x; cf[j][1] = v.y; cf[j][2] = v.z; cf[j][3] = v.w;
+          } else {
+            const double2 a = __ldg(reinterpret_cast<const double2*>(row + 4 * k));
+            const double2 b = __ldg(reinterpret_cast<const double2*>(row + 4 * k) + 1);
+            cf[j][0] = a.x; cf[j][1] = a.y; cf[j][2] = b.x; cf[j][3] = b.y;
+          }
         }
 #pragma unroll
       for (int j = 0; j < B; j++) {
@@ -939,7 +958,7 @@ __device__ __forceinline__ void basis_dot_lane_multi(const DevSys<Real>& S, doub
       const int pk = S.shell_pack[cs.x + k0];
       const int sym = pk & 0xf, fb = (pk >> 4) & 0xffff, kk = (pk >> 20) & 0xff;
       const Real* cf = row + 4 * kk;
-      const Real f = __ldg(cf) + h * (__ldg(cf + 1) + h * (__ldg(cf + 2) + h * __ldg(cf + 3)));
+      const Real f = spline_val(cf, h);
       switch (sym) {
         case 0: add(fb, f); break;
         case 1: add(fb, x * f); add(fb + 1, y * f); add(fb + 2, z * f); break;
@@ -994,7 +1013,7 @@ __device__ __forceinline__ Real basis_dot_lane_periodic(const DevSys<Real>& S, d
         const int pk = S.shell_pack[cs.x + k];
         const int sym = pk & 0xf, fo = ((pk >> 4) & 0xffff) - fb0, kk = (pk >> 20) & 0xff;
         const Real* cf = row + 4 * kk;
-        const Real f = __ldg(cf) + h * (__ldg(cf + 1) + h * (__ldg(cf + 2) + h * __ldg(cf + 3)));
+        const Real f = spline_val(cf, h);
         switch (sym) {
           case 0: fs[fo] += f; break;
           case 1: fs[fo] += x * f; fs[fo + 1] += y * f; fs[fo + 2] += z * f; break;
@@ -1140,7 +1159,7 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
             const int i = int(rd * Real(S.inv_spacing));
             const Real h = rd - Real(i) * Real(S.spacing);
             const Real* cf = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4 + 4 * kk;
-            const Real f = __ldg(cf) + h * (__ldg(cf + 1) + h * (__ldg(cf + 2) + h * __ldg(cf + 3)));
+            const Real f = spline_val(cf, h);
             const Real a = fg_value<Real>(idx, x, y, z) * f;
             gr += Real(S.image_kfac[2 * m]) * a;
             gi += Real(S.image_kfac[2 * m + 1]) * a;
@@ -1166,7 +1185,7 @@ __device__ __forceinline__ void basis_dot_lane_cpx(const DevSys<Real>& S, double
         const int i = int(rd * Real(S.inv_spacing));
         const Real h = rd - Real(i) * Real(S.spacing);
         const Real* cf = S.spline + ((size_t)cs.z + (size_t)i * cs.w) * 4 + 4 * kk;
-        const Real f = __ldg(cf) + h * (__ldg(cf + 1) + h * (__ldg(cf + 2) + h * __ldg(cf + 3)));
+        const Real f = spline_val(cf, h);
         Real a[6];
         int n;
         switch (sym) {
