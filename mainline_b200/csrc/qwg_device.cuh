@@ -149,6 +149,7 @@ struct DevSys {
   int kint;                      // every k component an integer: the overall sign
                                  // cos(pi k.n) of a wrap enters node checks and PP signs
   int real_orb;                  // orbitals real (ORBITALS at a nonzero k-point)
+  int xl;                        // F/G shells or CUTOFF_MO: the FP32 HBM-resident kernels compiled with their code
   int cutoff_mo;                 // CUTOFF_MO evaluator (HBM-resident kernels): shell_cut holds
                                  // each spline's own cutoff, no |value| <= 1e-8 skip
   int ng;                        // Ewald G-vectors

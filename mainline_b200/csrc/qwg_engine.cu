@@ -217,6 +217,7 @@ static void fill_sys(qwg_ctx* c, DevSys<Real>& S, const std::vector<int>& obj_ba
     if (H.kpt[d] != std::floor(H.kpt[d])) S.kint = 0;
   S.real_orb = H.complex_orbitals ? 0 : 1;
   S.cutoff_mo = H.cutoff_mo ? 1 : 0;
+  S.xl = has_high_l(H) ? 1 : 0;
   S.npts = H.spline_npts;
   S.spacing = H.spline_spacing;
   S.inv_spacing = 1.0 / H.spline_spacing;

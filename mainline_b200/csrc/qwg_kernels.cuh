@@ -43,7 +43,10 @@ struct PPItem {
 // MO rows, basis rows and projected coefficients are planar complex arrays.
 // PER: 0 molecule, 1 periodic cell, 2 either (decided at run time); the
 // local-energy kernels are compiled per case, the others check at run time.
-template <typename Real, int MMAX, bool TB, int PER>
+// XL: the F/G-shell and CUTOFF_MO code (HBM-resident kernels; the FP32 ones
+// are also compiled without it for the decks that need none, as that code's
+// register demand costs the move kernel ~5% in spills).
+template <typename Real, int MMAX, bool TB, int PER, bool XL = (MMAX <= 0)>
 struct Walker {
   const DevSys<Real>& S;
   const WLayout& L;
@@ -57,8 +60,8 @@ struct Walker {
   int tc_ldd = 0;
   unsigned long long* ph = nullptr;  // phase counters (profiling builds)
   static constexpr bool CPX = MMAX < 0;
-  // F and G basis shells: compiled into the HBM-resident kernels only
-  static constexpr bool HL = MMAX <= 0;
+  // F and G basis shells and CUTOFF_MO: compiled into the HBM-resident kernels only
+  static constexpr bool HL = MMAX < 0 || (MMAX == 0 && XL);
   double cr_re = 0.0, cr_im = 0.0;  // complex determinant ratio of the last proposal (CPX)
 
   __device__ __forceinline__ int MS() const {
@@ -1015,7 +1018,7 @@ struct MinBlocks<KM_ELOC_TM> { static constexpr int value = QWG_MIN_BLOCKS_ELOC;
 static_assert(sizeof(DevSys<double>) + sizeof(WLayout) + sizeof(StepParams) + sizeof(EvalIO) <= 32764,
               "walker kernel parameters exceed 32764 bytes");
 
-template <typename Real, int MMAX, int mode, bool TB, int PER>
+template <typename Real, int MMAX, int mode, bool TB, int PER, bool XL = (MMAX <= 0)>
 __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
     k_walkers(const __grid_constant__ DevSys<Real> S, const __grid_constant__ WLayout L, StepParams P, EvalIO io) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1037,7 +1040,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
     constexpr bool SWEEP_ONLY = mode == KM_SWEEP || mode == KM_TMOVE;  // move-phase shared memory only
     unsigned char* wb = HBM ? gstate : smem + moc_bytes + (size_t)warp * (SWEEP_ONLY ? L.sweep_bytes : L.bytes);
     unsigned char* sb = HBM ? P.scratch + (size_t)wid * L.scratch_bytes : wb + L.state_bytes;
-    Walker<Real, MMAX, TB, PER> W{S, L, wb, sb, moc_s, lane};
+    Walker<Real, MMAX, TB, PER, XL> W{S, L, wb, sb, moc_s, lane};
     // tensor-core move schedule: this launch moves electron P.tc_e only
     W.ph = P.phases;
     QWG_PHASE_BEGIN(t_walker)
@@ -1189,7 +1192,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
               // basis rows of the proposed position -> split-TF32 A rows of
               // this walker (rows wid * 5 + component)
               Real* b = W.bas();
-              basis_lap_warp<Real, PER, (MMAX <= 0)>(S, wx, wy, wz, b, lane);
+              basis_lap_warp<Real, PER, (MMAX < 0 || (MMAX == 0 && XL))>(S, wx, wy, wz, b, lane);
               float* ah = P.tc_ahi + (size_t)wid * 5 * P.tc_kpad;
               float* al = P.tc_alo + (size_t)wid * 5 * P.tc_kpad;
               for (int idx = lane; idx < 5 * P.tc_kpad; idx += 32) {

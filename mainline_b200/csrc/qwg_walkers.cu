@@ -30,15 +30,24 @@ cudaError_t ensure_smem_attr(K kern, size_t bytes) {
   return cudaSuccess;
 }
 
+// compiled variants: with/without e-e-n terms; the local-energy kernels also
+// per molecule / periodic cell (the others check at run time)
+template <typename Real, int MM, int MODE, bool XL>
+auto pick_kernel(const DevSys<Real>& S) {
+  constexpr bool SPLIT_PER = MODE == KM_ELOC || MODE == KM_ELOC_TM;
+  constexpr int P0 = SPLIT_PER ? 0 : 2, P1 = SPLIT_PER ? 1 : 2;
+  return S.periodic ? (S.has_tb ? k_walkers<Real, MM, MODE, true, P1, XL> : k_walkers<Real, MM, MODE, false, P1, XL>)
+                    : (S.has_tb ? k_walkers<Real, MM, MODE, true, P0, XL> : k_walkers<Real, MM, MODE, false, P0, XL>);
+}
+
 template <typename Real, int MM, int MODE>
 cudaError_t launch_mode(const DevSys<Real>& S, const WLayout& L, const StepParams& P, const EvalIO& io, int nwalk,
                         int wpc, size_t smem, cudaStream_t stream) {
-  // compiled variants: with/without e-e-n terms; the local-energy kernels
-  // also per molecule / periodic cell (the others check at run time)
-  constexpr bool SPLIT_PER = MODE == KM_ELOC || MODE == KM_ELOC_TM;
-  constexpr int P0 = SPLIT_PER ? 0 : 2, P1 = SPLIT_PER ? 1 : 2;
-  auto kern = S.periodic ? (S.has_tb ? k_walkers<Real, MM, MODE, true, P1> : k_walkers<Real, MM, MODE, false, P1>)
-                         : (S.has_tb ? k_walkers<Real, MM, MODE, true, P0> : k_walkers<Real, MM, MODE, false, P0>);
+  // the FP32 HBM-resident kernels without the F/G-shell and CUTOFF_MO code
+  // for the decks that have neither
+  auto kern = pick_kernel<Real, MM, MODE, (MM <= 0)>(S);
+  if constexpr (MM == 0 && sizeof(Real) == 4)
+    if (!S.xl) kern = pick_kernel<Real, MM, MODE, false>(S);
   cudaError_t e = ensure_smem_attr(kern, smem);
   if (e != cudaSuccess) return e;
   if (nwalk <= 0) return cudaSuccess;  // attribute set only (before a stream capture)
