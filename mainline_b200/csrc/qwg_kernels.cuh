@@ -401,7 +401,37 @@ struct Walker {
       near_atoms(S, po, nso);
     }
     double du = 0.0, ge[3] = {0, 0, 0}, le = 0.0;
-    for (int j = lane; j < S.nelec; j += 32) {
+    const bool halves = !has3 && S.nelec <= 16;
+    if (halves) {
+      // at most 16 electrons and no e-e-n terms: lanes 0-15 take the pairs
+      // (e, j) at the proposed position, lanes 16-31 the same pairs at the
+      // current one; each proposed-position lane collects its partner's terms
+      const int j = lane & 15;
+      const bool newp = lane < 16, live = j < S.nelec && j != e;
+      double u1 = 0.0, f1 = 0.0, l1 = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
+      if (live) {
+        const double* pj = Rp + 3 * j;
+        dx = (newp ? px : ox) - pj[0]; dy = (newp ? py : oy) - pj[1]; dz = (newp ? pz : oz) - pj[2];
+        min_image(S, dx, dy, dz);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < S.ee_rc2) jas_pair_t<Real>(S, se == (j < S.nup), sqrt(Real(d2)), u1, f1, l1);
+      }
+      const double qgx = __shfl_xor_sync(0xffffffffu, f1 * dx, 16), qgy = __shfl_xor_sync(0xffffffffu, f1 * dy, 16),
+                   qgz = __shfl_xor_sync(0xffffffffu, f1 * dz, 16), ql = __shfl_xor_sync(0xffffffffu, l1, 16);
+      if (newp) {
+        du += u1;
+        ge[0] += f1 * dx; ge[1] += f1 * dy; ge[2] += f1 * dz;
+        le += l1;
+        if (live) {
+          // gradient w.r.t. r_j of u(r_e - r_j) = -f'/r (r_e - r_j)
+          double* dg = dG() + 4 * j;
+          dg[0] = -f1 * dx + qgx; dg[1] = -f1 * dy + qgy; dg[2] = -f1 * dz + qgz; dg[3] = l1 - ql;
+        }
+      } else {
+        du -= u1;
+      }
+    }
+    for (int j = halves ? S.nelec : lane; j < S.nelec; j += 32) {
       double* dg = dG() + 4 * j;
       if (j == e) continue;
       const double* pj = Rp + 3 * j;
@@ -1165,17 +1195,34 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
         const uint64_t step = step0 + st;
         if constexpr (!ELOCM) {
           const int e_lo = tc_phase ? P.tc_e : 0, e_hi = tc_phase ? P.tc_e + 1 : N;
+          float pga[3] = {0.0f, 0.0f, 0.0f};  // lane k: deviates of electron e + k of the current 32
+          double prb = 0.0;                   // and its acceptance number
           for (int e = e_lo; e < e_hi; e++) {
             // Split_sampler::split_driver depth 1 (Split_sample.cpp:380-478)
+            if (((e - e_lo) & 31) == 0) {
+              // the proposal deviates and acceptance numbers of the next 32
+              // electrons, one electron per lane (the same counter-based
+              // streams as drawing them electron by electron)
+              const int ee = e + lane;
+              if (ee < e_hi) {
+                const Rand4 ra = rand4(P.seed, wid, step, ee, 1u);
+                const Rand4 rb = rand4(P.seed, wid, step, ee, 2u);
+                double g[4];
+                box_muller(ra.u[0], ra.u[1], g[0], g[1]);
+                box_muller(ra.u[2], ra.u[3], g[2], g[3]);
+                pga[0] = float(g[0]); pga[1] = float(g[1]); pga[2] = float(g[2]);  // exact: FP32 deviates
+                prb = rb.u[0];
+              }
+            }
+            const int src = (e - e_lo) & 31;
+            const double ga[3] = {double(__shfl_sync(0xffffffffu, pga[0], src)),
+                                  double(__shfl_sync(0xffffffffu, pga[1], src)),
+                                  double(__shfl_sync(0xffffffffu, pga[2], src))};
+            const double rbu = __shfl_sync(0xffffffffu, prb, src);
             double g0[3], l0;
             W.electron_grad(e, g0, l0);
             double dv[3];
             lim_drift(g0, P.tau, dv);
-            Rand4 ra = rand4(P.seed, wid, step, e, 1u);
-            Rand4 rb = rand4(P.seed, wid, step, e, 2u);
-            double ga[4];
-            box_muller(ra.u[0], ra.u[1], ga[0], ga[1]);
-            box_muller(ra.u[2], ra.u[3], ga[2], ga[3]);
             const double ox = Rp[3 * e], oy = Rp[3 * e + 1], oz = Rp[3 * e + 2];
             double nx = ox + ga[0] * sqt + dv[0];
             double ny = oy + ga[1] * sqt + dv[1];
@@ -1225,7 +1272,7 @@ __global__ void __launch_bounds__(128, MinBlocks<mode>::value)
               acc = fmin(1.0, ratio * ratio * exp((bw - fw) / (2.0 * P.tau)));
             }
             natt += 1;
-            if (acc + rb.u[0] > 1.0) {
+            if (acc + rbu > 1.0) {
               QWG_PHASE_BEGIN(t_acc)
               W.accept(e, wx, wy, wz, ratioD, dU);
               QWG_PHASE_END(t_acc, PH_ACCEPT, P.phases)
