@@ -381,36 +381,58 @@ def run_extras(stream, dev, seconds=30.0):
     cpx["config"] = "the periodic cell with complex orbitals (CORBITALS) at k=(0.5,0.25,0); 16384 walkers, " \
                     "tau=0.005, 10-step blocks"
     out["periodic_complex"] = cpx
-    # 72-electron molecule (HBM-resident kernels): mixed precision with the
-    # tensor-core move schedule, with the CUDA-core contraction, and FP64
-    m72 = os.path.join(ROOT, "tests", "golden", "mol72.qw")
-    Rm = systems.random_configs(systems.read_deck(m72), 4096, seed=SEED % 1000)
-    hm = {}
-    for label, prec, tc in (("mixed", engine.MIXED, "1"), ("mixed_cuda_core_mo", engine.MIXED, "0"),
-                            ("fp64", engine.FP64, "0")):
-        old_tc = os.environ.get("QWG_TC_MOVES")
-        os.environ["QWG_TC_MOVES"] = tc
-        try:
-            E = engine.Engine(m72, prec, max_walkers=4096, stream=stream.cuda_stream)
-        finally:
-            if old_tc is None:
+    # HBM-resident kernels: the 72-electron molecule and the 128-electron cell
+    # in mixed precision with the default move schedule, with the per-electron
+    # tensor-core schedule forced on or off beside it, and in FP64
+    def hbm_rates(deck_path, nw, tau, nstep, variants):
+        R = systems.random_configs(systems.read_deck(deck_path), nw, seed=SEED % 1000)
+        res = {}
+        for label, prec, tc in variants:
+            old_tc = os.environ.get("QWG_TC_MOVES")
+            if tc is None:
                 os.environ.pop("QWG_TC_MOVES", None)
             else:
-                os.environ["QWG_TC_MOVES"] = old_tc
-        E.set_walkers(Rm)
-        E.vmc_block(2, 0.1, seed=SEED + 3)
-        E.dmc_init(timestep=0.01, nstep=5, seed=SEED + 4)
-        E.dmc_block()
-        st = E.dmc_block()
-        hm[label] = {"walker_steps_per_s": 4096 * 5 / (st["block_ms"] / 1e3), "block_ms": st["block_ms"],
-                     "energy": st["energy"]}
-        E.close()
+                os.environ["QWG_TC_MOVES"] = tc
+            try:
+                E = engine.Engine(deck_path, prec, max_walkers=nw, stream=stream.cuda_stream)
+            finally:
+                if old_tc is None:
+                    os.environ.pop("QWG_TC_MOVES", None)
+                else:
+                    os.environ["QWG_TC_MOVES"] = old_tc
+            E.set_walkers(R)
+            E.vmc_block(2, 0.1, seed=SEED + 3)
+            E.dmc_init(timestep=tau, nstep=nstep, seed=SEED + 4)
+            E.dmc_block()
+            st = E.dmc_block()
+            res[label] = {"walker_steps_per_s": nw * nstep / (st["block_ms"] / 1e3), "block_ms": st["block_ms"],
+                          "energy": st["energy"]}
+            E.close()
+        return res
+
+    m72 = os.path.join(ROOT, "tests", "golden", "mol72.qw")
+    hm = hbm_rates(m72, 4096, 0.01, 5, (("mixed", engine.MIXED, None),
+                                        ("mixed_tensor_core_moves", engine.MIXED, "1"),
+                                        ("fp64", engine.FP64, None)))
     hm["mixed_vs_fp64"] = hm["mixed"]["walker_steps_per_s"] / hm["fp64"]["walker_steps_per_s"]
-    hm["tensor_core_schedule_gain"] = hm["mixed"]["walker_steps_per_s"] / hm["mixed_cuda_core_mo"]["walker_steps_per_s"]
+    hm["tensor_core_schedule_gain"] = (hm["mixed_tensor_core_moves"]["walker_steps_per_s"] /
+                                       hm["mixed"]["walker_steps_per_s"])
     hm["config"] = ("mol72: 10 atoms, 72 electrons (36 per spin), 180 basis functions, HBM-resident kernels; 4096 "
-                    "walkers, DMC tau=0.01, 5-step blocks; mixed = per-electron tensor-core MO contraction "
-                    "(tcgen05 split TF32)")
+                    "walkers, DMC tau=0.01, 5-step blocks; mixed = the default move schedule (one-launch CUDA-core "
+                    "sweep below 16384 basis functions x orbitals), mixed_tensor_core_moves = the per-electron "
+                    "tensor-core MO contraction (tcgen05 split TF32) forced on")
     out["hbm_molecule"] = hm
+    c32 = os.path.join(ROOT, "tests", "golden", "cell32.qw")
+    hc = hbm_rates(c32, 2048, 0.005, 5, (("mixed", engine.MIXED, None),
+                                         ("mixed_cuda_core_moves", engine.MIXED, "0"),
+                                         ("fp64", engine.FP64, None)))
+    hc["mixed_vs_fp64"] = hc["mixed"]["walker_steps_per_s"] / hc["fp64"]["walker_steps_per_s"]
+    hc["tensor_core_schedule_gain"] = hc["mixed"]["walker_steps_per_s"] / hc["mixed_cuda_core_moves"]["walker_steps_per_s"]
+    hc["config"] = ("cell32: 32 Z_eff=4 atoms, 13.48x13.48x6.74 bohr, 128 electrons (64 per spin), 416 basis functions "
+                    "+ images, HBM-resident kernels; 2048 walkers, DMC tau=0.005, 5-step blocks; mixed = the default "
+                    "move schedule (per-electron tensor-core MO contraction), mixed_cuda_core_moves = the one-launch "
+                    "CUDA-core sweep forced on")
+    out["hbm_cell"] = hc
     # batched uneven molecules: 64 systems, 8-192 electrons, 512-4096 walkers
     mols = systems.write_batch(os.path.join(tmp, "batch"), nsys=64, seed=SEED % 1000)
     bat = {}

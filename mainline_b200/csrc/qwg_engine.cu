@@ -628,13 +628,22 @@ static size_t branch_big_bytes(int W, BranchBig* G, unsigned char* base) {
 constexpr int kTcMinWalkers = 1024;
 
 // The tensor-core move schedule serves the mixed-precision HBM-resident
-// kernels with real orbitals and one determinant (QWG_TC_MOVES=0 turns it
-// off, e.g. to time the CUDA-core contraction beside it).
+// kernels with real orbitals and one determinant, by default when the
+// contraction of a move (basis functions x orbitals per spin) is at least
+// kTcMinContraction: measured on one B200 (DMC, mixed), the schedule is 1.10x
+// the one-launch CUDA-core sweep on a 128-electron cell (416 x 64), 0.92-0.98x
+// on a 72-electron molecule (180 x 36) and 0.98-1.00x on a 32-electron cell
+// (104 x 16), since it pays three launches per electron.  QWG_TC_MOVES=1
+// forces it on, QWG_TC_MOVES=0 off (to time either beside the other).
+constexpr size_t kTcMinContraction = 16384;
 static bool tc_moves_eligible(const qwg_ctx* c) {
+  if (!(c->precision == QWG_MIXED && c->mmax == 0 && c->H.detwt.size() <= 1 && c->H.nmo[0] <= 256 &&
+        c->H.nmo[1] <= 256))
+    return false;
   const char* env = std::getenv("QWG_TC_MOVES");
   if (env && env[0] == '0') return false;
-  return c->precision == QWG_MIXED && c->mmax == 0 && c->H.detwt.size() <= 1 && c->H.nmo[0] <= 256 &&
-         c->H.nmo[1] <= 256;
+  if (env && env[0] == '1') return true;
+  return (size_t)c->H.nbasis * (size_t)std::max(c->H.nmo[0], c->H.nmo[1]) >= kTcMinContraction;
 }
 
 static size_t tc_moves_bytes(const qwg_ctx* c, size_t W) {
