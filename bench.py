@@ -562,7 +562,7 @@ def main():
                     help="arms of the headline workload (profiling runs use one)")
     ap.add_argument("--probe", default=None,
                     help="profiling driver only, no report line: tc-sweep = one mixed-precision sweep of the "
-                         "72-electron molecule (4096 walkers) on the tensor-core move schedule; "
+                         "72-electron molecule (4096 walkers) on the tensor-core move schedule (forced on); "
                          "branch:<deck>:<walkers> = two mixed-precision DMC blocks of 5 steps of a golden deck "
                          "(population control share)")
     args = ap.parse_args()
@@ -607,6 +607,7 @@ def main():
     if args.probe == "tc-sweep":
         from mainline_b200 import engine, systems
         deck = os.path.join(ROOT, "tests", "golden", "mol72.qw")
+        os.environ["QWG_TC_MOVES"] = "1"  # below the schedule's size rule: forced on
         E = engine.Engine(deck, engine.MIXED, max_walkers=NWALK)
         E.set_walkers(systems.random_configs(systems.read_deck(deck), NWALK, seed=1))
         E.set_vmc_dynamics(1, 2.0)
